@@ -1,0 +1,374 @@
+"""Benchmark of the Fold3dPMM sweep on B200.
+
+Workload (one "step"): a full reference-model solve -- the reference's drift
+medium (F = 1.1, a = (-0.35, 0.4, 0.7)), its implicit-surface source, a 512^3
+grid (h = 10/511), 8 sweeps of the six directional passes, exactly the
+reference driver's loop (Stencil-OpenACC/AN_ISO_1_OpenACC.c:1187-1237).  The
+published single-GPU A100 figure for this workload is 3.037851 s
+(plots/perfect-2-gpu.py:24), i.e. 2.1166 Gcell-updates/s.
+
+Metric: Gcell-updates/s = nominal point updates / time, nominal updates per
+sweep = 2 * [(nx-1)ny nz + (ny-1)nx nz + (nz-1)nx ny].
+
+  value : device-resident throughput -- each step copies the pristine initial
+          field (already in HBM) into the working field and solves; timed
+          with CUDA events on the solve stream.  The 1.09 GB field is larger
+          than L2, so no flush is needed between steps.
+  e2e   : the same solve through the C-ABI host entry point
+          (fold3d_solve_host) from pinned host memory: H2D copy of the field,
+          solve, D2H copy of the result, all inside the timed region.
+
+N > 1 GPUs: a single solve does not shard (every plane depends on the whole
+previous plane), so each rank solves its own replica (weak scaling, no
+collective on the data path); value = all ranks' updates / max-over-ranks
+time.
+
+--impl reference: the reference's own CPU implementation (oracle/_ref:
+AN_ISO_1_OpenACC.c built for the host; its OpenMP transform on all host
+cores), each step a bounded sample of the same workload (the first planes of
+each of the six passes of sweep 1, from the same initial field).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fgcs-openacc-advanced_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+PUBLISHED_S = {512: 3.037851, 1280: 35.163471}  # plots/perfect-2-gpu.py:24 (V2, A100, 8 sweeps)
+REF_F, REF_A = 1.1, (-0.35, 0.4, 0.7)
+BYTES_PER_UPDATE = 16  # read old target + write new target, FP64; medium is constant (m = 0)
+
+
+def nominal_updates(n, sweeps):
+    return sweeps * 6 * (n - 1) * n * n
+
+
+def published_rate(n, sweeps=8):
+    s = PUBLISHED_S.get(n)
+    return None if s is None else nominal_updates(n, sweeps) / s / 1e9
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        rows = []
+        for ln in (self.out or "").splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, flags in rows:
+            for nm, fl in zip(names, flags):
+                if fl.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None):
+    """Time the reference's own sweep functions (oracle/_ref, OpenMP
+    transform on `threads` cores) on the first planes of each of the six
+    passes of sweep 1, starting from T0.  Returns (updates/s, info)."""
+    import numpy as np
+
+    from oracle import RefLib, build
+
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    path = build.ref_lib_path(n, omp=True)
+    kind = "reference"
+    if not os.path.exists(path):
+        raise RuntimeError("reference host build missing: %s" % path)
+    r = RefLib(n, omp=True)
+    T = np.array(T0, copy=True)
+    # calibrate: one plane of x_down
+    t = time.perf_counter()
+    r.plane(T, 0, 1)
+    per_plane = max(time.perf_counter() - t, 1e-4)
+    if planes is None:
+        planes = max(1, min(n - 1, int((seconds or 10.0) / (6 * per_plane))))
+    T = np.array(T0, copy=True)
+    t = time.perf_counter()
+    for d in range(6):
+        first, step = (1, 1) if d in (0, 2, 5) else (n, -1)
+        for p in range(planes):
+            r.plane(T, d, first + step * p)
+    dt = time.perf_counter() - t
+    upd = 6 * planes * n * n
+    info = {"kind": kind, "cores": int(os.environ.get("OMP_NUM_THREADS", host_threads())),
+            "sample": "%d planes of each of the 6 passes of sweep 1 at %d^3 (%d updates), reference "
+                      "AN_ISO_1_OpenACC.c host build, OpenMP transform" % (planes, n, upd),
+            "seconds": dt, "planes": planes}
+    return upd / dt, info
+
+
+def run_reference(args):
+    """--impl reference: rank 0 only."""
+    import numpy as np
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.size
+    from oracle import RefLib, build, ref_spacing
+
+    try:
+        if not os.path.exists(build.ref_lib_path(n, omp=True)):
+            if build.reference_available():
+                build.build_ref(n)
+            else:
+                raise RuntimeError("no host build of the reference at %d^3" % n)
+        threads = host_threads()
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        r = RefLib(n, omp=True)
+        T0 = r.init_implicit()  # the reference's own ImplicitInitialiser
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e).splitlines()[0]}))
+        return
+    rates = []
+    info = None
+    planes = None
+    for it in range(args.warmup + args.steps):
+        rate, info = reference_cpu_sample(T0, n, seconds=args.ref_seconds, planes=planes, threads=threads)
+        planes = info["planes"]
+        if it >= args.warmup:
+            rates.append(rate)
+    value = statistics.mean(rates) / 1e9
+    upd_per_step = 6 * planes * n * n
+    out = {
+        "impl": "reference", "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": upd_per_step / (value * 1e9) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic: reference implicit-surface source",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": info["cores"], "kind": "reference",
+                         "sample": info["sample"]},
+        "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def workload_config(args):
+    return {"workload": "fold-ref %d^3 implicit-surface source, %d sweeps" % (args.size, args.sweeps),
+            "grid": args.size, "sweeps": args.sweeps, "medium": "F=1.1 a=(-0.35,0.4,0.7)",
+            "spacing": "h=10/(n-1)", "engine": args.engine, "skip": bool(args.skip),
+            "l2": "field %.2f GB > 126 MB L2; no flush needed" % ((args.size + 2) ** 3 * 8 / 1e9),
+            "parallelism": "replicas" if args.gpus > 1 else "single"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--sweeps", type=int, default=8)
+    ap.add_argument("--engine", choices=["planes", "wavefront", "auto"], default="auto")
+    ap.add_argument("--skip", type=int, default=0, help="tile skipping (bit-exact); 0 = evaluate every update")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=4.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    import fold3dpmm as f3d
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    n, sweeps = args.size, args.sweeps
+    h = 10.0 / (n - 1.0)
+    engine = {"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT, "auto": f3d.ENGINE_AUTO}[args.engine]
+    opts = f3d.opts(max_sweeps=sweeps, fixed=True, engine=engine, skip=bool(args.skip))
+
+    t0 = time.perf_counter()
+    T0_host = f3d.init_implicit(n, n, n, h)
+    init_s = time.perf_counter() - t0
+    T0_pin = torch.from_numpy(T0_host).pin_memory()
+    out_pin = torch.empty_like(T0_pin).pin_memory()
+    T0_dev = T0_pin.to("cuda", non_blocking=False)
+    T_dev = torch.empty_like(T0_dev)
+    ctx = f3d.Context(local)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def step():
+        T_dev.copy_(T0_dev)
+        return ctx.solve(T_dev, h, None, opts, stream=sp)
+
+    rep = None
+    for _ in range(args.warmup):
+        rep = step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms = 0.0
+    evaluated = 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rep = step()
+            kernel_ms += rep.elapsed_ms
+            evaluated += rep.evaluated_updates
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    upd = nominal_updates(n, sweeps)
+    value = world * upd * args.steps / (ms / 1e3) / 1e9
+    engine_ran = {1: "planes", 2: "wavefront"}.get(rep.engine, str(rep.engine))
+    launches_per_step = sweeps * 6 * (n - 1) if rep.engine == f3d.ENGINE_PLANES else sweeps * 6
+
+    # end to end through the host entry point (pinned in, pinned out)
+    e2e = None
+    if not args.no_e2e:
+        ctx.solve(T0_pin, h, None, opts, stream=sp, out=out_pin)  # warm: allocates the context buffer
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.solve(T0_pin, h, None, opts, stream=sp, out=out_pin)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nb = T0_pin.numel() * 8
+        e2e = {"value": world * upd * args.steps / (ems / 1e3) / 1e9, "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": ems / args.steps}
+        if not np.array_equal(out_pin.numpy().view(np.uint64), T_dev.cpu().numpy().view(np.uint64)):
+            raise RuntimeError("host-path result differs from the device-path result")
+
+    peak, peak_kind = load_peaks()
+    solve_ms = kernel_ms / args.steps
+    alg_bytes = BYTES_PER_UPDATE * upd
+    launches = launches_per_step * args.steps
+    achieved = alg_bytes / (solve_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_kind": peak_kind,
+                "kernel": "plane_kernel" if rep.engine == f3d.ENGINE_PLANES else "wavefront_kernel",
+                "alg_bytes_per_launch": alg_bytes / launches_per_step,
+                "avg_launch_us": solve_ms * 1e3 / launches_per_step,
+                "note": "FP64-ALU bound: ~100 FLOP per 16 B"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            rate, info = reference_cpu_sample(T0_host, n, seconds=args.cpu_seconds, threads=host_threads())
+            cpu = {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": info["cores"], "kind": info["kind"],
+                   "sample": info["sample"]}
+        except Exception as e:
+            cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: %s" % str(e).splitlines()[0]}
+
+    pub = published_rate(n, sweeps) if sweeps == 8 else None
+    out = {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": (value / pub) if pub else None, "dtype": "f64",
+        "data": "synthetic: reference implicit-surface source and drift medium (no dataset)",
+        "config": workload_config(args) | {"engine": engine_ran},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clocks, "solve_ms": solve_ms, "evaluated_updates_per_step": evaluated / args.steps,
+        "init_s": init_s, "host_threads": host_threads(),
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

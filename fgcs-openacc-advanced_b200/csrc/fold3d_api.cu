@@ -1,0 +1,488 @@
+// fold3d_api.cu -- the C-ABI: contexts, whole solves, per-plane steps, the
+// reference-compatible sweep entry points and the OpenACC runtime subset the
+// reference driver calls.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "fold3d_acc.h"
+#include "fold3d_internal.h"
+
+namespace fold3d {
+
+const DirSpec kDirs[6] = {
+    {0, +1, 2, +1, 1, +1},  // x_down  AN_ISO_1_OpenACC.c:180
+    {0, -1, 2, -1, 1, -1},  // x_up    :334
+    {2, +1, 1, +1, 0, +1},  // k_up    :790
+    {2, -1, 1, -1, 0, -1},  // k_down  :944
+    {1, -1, 0, -1, 2, -1},  // y_up    :485
+    {1, +1, 0, +1, 2, +1},  // y_down  :636
+};
+
+static thread_local std::string t_err;
+
+int set_error(int code, const std::string &msg)
+{
+    t_err = msg;
+    return code;
+}
+int cuda_error(cudaError_t e, const char *what)
+{
+    return set_error(FOLD3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+void clear_error() { t_err.clear(); }
+
+static void strides(const fold3d_grid &g, long long st[3])
+{
+    st[0] = 1;
+    st[1] = (long long)g.nx + 2;
+    st[2] = ((long long)g.nx + 2) * ((long long)g.ny + 2);
+}
+
+PlaneGeom make_geom(const fold3d_grid &g, int dir)
+{
+    const DirSpec &d = kDirs[dir];
+    const int n[3] = {g.nx, g.ny, g.nz};
+    long long st[3];
+    strides(g, st);
+    const int u = (d.nrm == 0) ? 1 : 0;
+    const int v = (d.nrm == 2) ? 1 : 2;
+    PlaneGeom p;
+    p.s_nrm = st[d.nrm];
+    p.sn = d.sg * st[d.nrm];
+    p.sx = d.xs * st[d.xa];
+    p.sy = d.ys * st[d.ya];
+    p.su = st[u];
+    p.sv = st[v];
+    p.nu = n[u];
+    p.nv = n[v];
+    p.nplanes = n[d.nrm];
+    return p;
+}
+
+LocalFrameH make_frame(const fold3d_grid &g, const fold3d_medium &m, int dir)
+{
+    const DirSpec &d = kDirs[dir];
+    const double h[3] = {g.dx, g.dy, g.dz};
+    const double a[3] = {m.ax, m.ay, m.az};
+    LocalFrameH L;
+    L.F = m.F;
+    L.ax = d.xs * a[d.xa];
+    L.ay = d.ys * a[d.ya];
+    L.az = d.sg * a[d.nrm];
+    L.hz = h[d.nrm];
+    L.hx = h[d.xa];
+    L.hy = h[d.ya];
+    // The reference driver's diagonals, e.g. DXYP = sqrt(DX*DX + dy*dy)
+    // (AN_ISO_1_OpenACC.c:1158-1160); the sum is commutative in IEEE.
+    L.hxy = std::sqrt(L.hx * L.hx + L.hy * L.hy);
+    L.hxz = std::sqrt(L.hx * L.hx + L.hz * L.hz);
+    L.hyz = std::sqrt(L.hy * L.hy + L.hz * L.hz);
+    return L;
+}
+
+static int check_grid(const fold3d_grid *g)
+{
+    if (!g) return set_error(FOLD3D_ERR_INVALID, "grid is NULL");
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+        return set_error(FOLD3D_ERR_INVALID, "grid sizes must be >= 2");
+    if (!(g->dx > 0 && g->dy > 0 && g->dz > 0) || !std::isfinite(g->dx) ||
+        !std::isfinite(g->dy) || !std::isfinite(g->dz))
+        return set_error(FOLD3D_ERR_INVALID, "grid spacings must be finite and > 0");
+    const double cells = (double)(g->nx + 2) * (g->ny + 2) * (g->nz + 2);
+    if (cells > 4.0e18 / 8) return set_error(FOLD3D_ERR_INVALID, "grid too large");
+    return FOLD3D_OK;
+}
+
+static int check_medium(const fold3d_medium *m)
+{
+    if (!m) return set_error(FOLD3D_ERR_INVALID, "medium is NULL");
+    if (!(m->F > 0) || !std::isfinite(m->F) || !std::isfinite(m->ax) || !std::isfinite(m->ay) ||
+        !std::isfinite(m->az))
+        return set_error(FOLD3D_ERR_INVALID, "medium must be finite with F > 0");
+    return FOLD3D_OK;
+}
+
+static size_t field_cells(const fold3d_grid &g)
+{
+    return (size_t)(g.nx + 2) * (size_t)(g.ny + 2) * (size_t)(g.nz + 2);
+}
+
+static uint64_t nominal_per_sweep(const fold3d_grid &g)
+{
+    const uint64_t nx = g.nx, ny = g.ny, nz = g.nz;
+    return 2 * ((nx - 1) * ny * nz + (ny - 1) * nx * nz + (nz - 1) * nx * ny);
+}
+
+}  // namespace fold3d
+
+using namespace fold3d;
+
+// ------------------------------------------------------------------------
+// Context
+// ------------------------------------------------------------------------
+struct fold3d_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;  // blocking w.r.t. the legacy stream
+    unsigned long long *d_maxd = nullptr;
+    unsigned long long *h_maxd = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // PLANES engine: one sweep captured as a graph, cached per (T, grid, medium)
+    cudaGraphExec_t sweep_exec = nullptr;
+    double *key_T = nullptr;
+    fold3d_grid key_g{};
+    fold3d_medium key_m{};
+    // buffer for fold3d_solve_host
+    double *d_field = nullptr;
+    size_t d_field_cells = 0;
+};
+
+namespace {
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+const char *fold3d_last_error(void) { return t_err.c_str(); }
+
+const char *fold3d_version(void) { return "fold3dpmm-b200 0.1 (sm_100a)"; }
+
+void fold3d_default_opts(fold3d_opts *o)
+{
+    if (!o) return;
+    o->max_sweeps = 1000;
+    o->fixed = 0;
+    o->tol = 0.0;
+    o->engine = FOLD3D_ENGINE_AUTO;
+    o->skip = 1;
+}
+
+int fold3d_create(fold3d_ctx **out, int device)
+{
+    clear_error();
+    if (!out) return set_error(FOLD3D_ERR_INVALID, "ctx out-pointer is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) return set_error(FOLD3D_ERR_INVALID, "no such device");
+    DeviceGuard dg(device);
+    fold3d_ctx *c = new (std::nothrow) fold3d_ctx();
+    if (!c) return set_error(FOLD3D_ERR_NOMEM, "host allocation failed");
+    c->device = device;
+    if ((e = cudaStreamCreate(&c->stream)) != cudaSuccess ||
+        (e = cudaMalloc(&c->d_maxd, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMallocHost(&c->h_maxd, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess) {
+        fold3d_destroy(c);
+        return cuda_error(e, "context setup");
+    }
+    *out = c;
+    return FOLD3D_OK;
+}
+
+void fold3d_destroy(fold3d_ctx *c)
+{
+    if (!c) return;
+    DeviceGuard dg(c->device);
+    if (c->sweep_exec) cudaGraphExecDestroy(c->sweep_exec);
+    if (c->d_field) cudaFree(c->d_field);
+    if (c->d_maxd) cudaFree(c->d_maxd);
+    if (c->h_maxd) cudaFreeHost(c->h_maxd);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"
+
+// One sweep (max-delta reset + the 6 passes) captured into a graph.
+static int build_sweep_graph(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T)
+{
+    if (c->sweep_exec && c->key_T == T && !memcmp(&c->key_g, &g, sizeof g) &&
+        !memcmp(&c->key_m, &m, sizeof m))
+        return FOLD3D_OK;
+    if (c->sweep_exec) {
+        cudaGraphExecDestroy(c->sweep_exec);
+        c->sweep_exec = nullptr;
+    }
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamBeginCapture");
+    cudaError_t le = cudaMemsetAsync(c->d_maxd, 0, sizeof(unsigned long long), c->stream);
+    for (int dir = 0; dir < 6 && le == cudaSuccess; ++dir) {
+        const PlaneGeom pg = make_geom(g, dir);
+        const LocalFrameH L = make_frame(g, m, dir);
+        int src = pass_first(pg, dir);
+        for (int p = 0; p < pass_count(pg) && le == cudaSuccess; ++p, src += kDirs[dir].sg)
+            le = launch_plane(T, pg, L, src, c->d_maxd, c->stream);
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(c->stream, &graph);
+    if (le != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_error(le, "capturing the sweep");
+    }
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&c->sweep_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        c->sweep_exec = nullptr;
+        return cuda_error(e, "cudaGraphInstantiate");
+    }
+    c->key_T = T;
+    c->key_g = g;
+    c->key_m = m;
+    return FOLD3D_OK;
+}
+
+static int solve_planes(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T,
+                        const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
+{
+    int rc = build_sweep_graph(c, g, m, T);
+    if (rc) return rc;
+    cudaError_t e;
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    int sweeps = 0;
+    double delta = 0.0;
+    while (sweeps < o.max_sweeps) {
+        if ((e = cudaGraphLaunch(c->sweep_exec, s)) != cudaSuccess) return cuda_error(e, "cudaGraphLaunch");
+        ++sweeps;
+        if (!o.fixed) {
+            if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+                return cuda_error(e, "cudaMemcpyAsync");
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "sweep");
+            memcpy(&delta, c->h_maxd, 8);
+            if (delta <= o.tol) break;
+        }
+    }
+    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_error(e, "cudaMemcpyAsync");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "solve");
+    memcpy(&delta, c->h_maxd, 8);
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        rep->sweeps = sweeps;
+        rep->max_delta = delta;
+        rep->elapsed_ms = ms;
+        rep->nominal_updates = nominal_per_sweep(g) * (uint64_t)sweeps;
+        rep->evaluated_updates = rep->nominal_updates;
+        rep->engine = FOLD3D_ENGINE_PLANES;
+    }
+    return FOLD3D_OK;
+}
+
+extern "C" {
+
+int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
+                 const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (!T) return set_error(FOLD3D_ERR_INVALID, "field is NULL");
+    if (!o) return set_error(FOLD3D_ERR_INVALID, "opts is NULL");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_medium(m))) return rc;
+    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (o->engine < 0 || o->engine > FOLD3D_ENGINE_WAVEFRONT)
+        return set_error(FOLD3D_ERR_INVALID, "unknown engine");
+    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return solve_planes(c, *g, *m, T, *o, s, rep);
+}
+
+int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,
+                      double *T_out, const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (!T_in || !T_out) return set_error(FOLD3D_ERR_INVALID, "field is NULL");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    DeviceGuard dg(c->device);
+    const size_t cells = field_cells(*g);
+    cudaError_t e;
+    if (c->d_field_cells < cells) {
+        if (c->d_field) cudaFree(c->d_field);
+        c->d_field = nullptr;
+        c->d_field_cells = 0;
+        if (c->sweep_exec && c->key_T) c->key_T = nullptr;  // force a re-capture
+        if ((e = cudaMalloc(&c->d_field, cells * sizeof(double))) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        c->d_field_cells = cells;
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if ((e = cudaMemcpyAsync(c->d_field, T_in, cells * sizeof(double), cudaMemcpyHostToDevice, s)) !=
+        cudaSuccess)
+        return cuda_error(e, "host-to-device copy");
+    rc = fold3d_solve(c, g, m, c->d_field, o, s, rep);
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(T_out, c->d_field, cells * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+        cudaSuccess)
+        return cuda_error(e, "device-to-host copy");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "device-to-host copy");
+    return FOLD3D_OK;
+}
+
+int fold3d_plane(const fold3d_grid *g, const fold3d_medium *m, double *T, int dir, int src, void *stream)
+{
+    clear_error();
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_medium(m))) return rc;
+    if (!T) return set_error(FOLD3D_ERR_INVALID, "field is NULL");
+    if (dir < 0 || dir > 5) return set_error(FOLD3D_ERR_INVALID, "dir must be 0..5");
+    const PlaneGeom pg = make_geom(*g, dir);
+    const int tgt = src + kDirs[dir].sg;
+    if (src < 1 || src > pg.nplanes || tgt < 1 || tgt > pg.nplanes)
+        return set_error(FOLD3D_ERR_INVALID, "plane index out of range");
+    cudaError_t e = launch_plane(T, pg, make_frame(*g, *m, dir), src, nullptr, (cudaStream_t)stream);
+    return e == cudaSuccess ? FOLD3D_OK : cuda_error(e, "plane launch");
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
+// Reference-compatible sweep entry points and OpenACC runtime subset
+// ------------------------------------------------------------------------
+namespace {
+std::mutex g_compat_mu;
+std::map<uintptr_t, size_t> g_acc_allocs;  // base -> bytes, from acc_malloc
+int g_compat_n[3] = {0, 0, 0};
+
+// Grid of a compat call: the size set by fold3d_compat_set_grid, else the
+// cube whose field fills the acc_malloc allocation T points into.
+bool compat_grid(const double *T, fold3d_grid &g)
+{
+    std::lock_guard<std::mutex> lk(g_compat_mu);
+    if (g_compat_n[0] > 0) {
+        g.nx = g_compat_n[0];
+        g.ny = g_compat_n[1];
+        g.nz = g_compat_n[2];
+    } else {
+        auto it = g_acc_allocs.upper_bound((uintptr_t)T);
+        if (it == g_acc_allocs.begin()) return false;
+        --it;
+        if ((uintptr_t)T >= it->first + it->second) return false;
+        const size_t cells = it->second / sizeof(double);
+        long long p = (long long)std::llround(std::cbrt((double)cells));
+        while (p * p * p > (long long)cells) --p;
+        while ((p + 1) * (p + 1) * (p + 1) <= (long long)cells) ++p;
+        if (p * p * p != (long long)cells || p < 4) return false;
+        g.nx = g.ny = g.nz = (int)(p - 2);
+    }
+    g.dx = g.dy = g.dz = 1.0;  // geometry only; spacings come from the call
+    return true;
+}
+
+void compat_plane(int dir, double *T, int src, double dzz, double dxx, double dyy, double dxy, double dxz,
+                  double dyz, double F, double ay, double ax, double az)
+{
+    clear_error();
+    fold3d_grid g;
+    if (!T || !compat_grid(T, g)) {
+        set_error(FOLD3D_ERR_INVALID,
+                  "function_*: grid size unknown (call fold3d_compat_set_grid or allocate with acc_malloc)");
+        return;
+    }
+    const PlaneGeom pg = make_geom(g, dir);
+    const int tgt = src + kDirs[dir].sg;
+    if (src < 1 || src > pg.nplanes || tgt < 1 || tgt > pg.nplanes) {
+        set_error(FOLD3D_ERR_INVALID, "function_*: plane index out of range");
+        return;
+    }
+    // The caller's arguments are already in the direction's local frame
+    // (the reference driver permutes them, AN_ISO_1_OpenACC.c:1198-1235).
+    const LocalFrameH L = {F, ax, ay, az, dzz, dxx, dyy, dxy, dxz, dyz};
+    cudaError_t e = launch_plane(T, pg, L, src, nullptr, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) cuda_error(e, "function_*");
+}
+}  // namespace
+
+extern "C" {
+
+int fold3d_compat_set_grid(int nx, int ny, int nz)
+{
+    clear_error();
+    if ((nx | ny | nz) != 0 && (nx < 2 || ny < 2 || nz < 2))
+        return set_error(FOLD3D_ERR_INVALID, "grid sizes must be >= 2 (or all 0 to unset)");
+    std::lock_guard<std::mutex> lk(g_compat_mu);
+    g_compat_n[0] = nx;
+    g_compat_n[1] = ny;
+    g_compat_n[2] = nz;
+    return FOLD3D_OK;
+}
+
+#define FOLD3D_COMPAT(name, dir)                                                                    \
+    void name(double *T, int p, double dzz, double dxx, double dyy, double dxy, double dxz, double dyz, \
+              double F, double ay, double ax, double az)                                            \
+    {                                                                                               \
+        compat_plane(dir, T, p, dzz, dxx, dyy, dxy, dxz, dyz, F, ay, ax, az);                       \
+    }
+FOLD3D_COMPAT(function_x_down, FOLD3D_X_DOWN)
+FOLD3D_COMPAT(function_x_up, FOLD3D_X_UP)
+FOLD3D_COMPAT(function_k_up, FOLD3D_K_UP)
+FOLD3D_COMPAT(function_k_down, FOLD3D_K_DOWN)
+FOLD3D_COMPAT(function_y_up, FOLD3D_Y_UP)
+FOLD3D_COMPAT(function_y_down, FOLD3D_Y_DOWN)
+#undef FOLD3D_COMPAT
+
+// The OpenACC runtime calls of the reference driver (AN_ISO_1_OpenACC.c:
+// 1184-1186, 1241), over the CUDA runtime.  acc_malloc also records the
+// allocation so the sweep entry points can recover the grid size.
+void *acc_malloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        set_error(FOLD3D_ERR_NOMEM, "acc_malloc: cudaMalloc failed");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_compat_mu);
+    g_acc_allocs[(uintptr_t)p] = bytes;
+    return p;
+}
+
+void acc_free(void *p)
+{
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        g_acc_allocs.erase((uintptr_t)p);
+    }
+    cudaFree(p);
+}
+
+void acc_memcpy_to_device(void *dst, void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) cuda_error(e, "acc_memcpy_to_device");
+}
+
+void acc_memcpy_from_device(void *dst, void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) cuda_error(e, "acc_memcpy_from_device");
+}
+
+}  // extern "C"

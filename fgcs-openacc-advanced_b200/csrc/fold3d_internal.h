@@ -1,0 +1,52 @@
+// fold3d_internal.h -- shared declarations of the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "fold3dpmm.h"
+
+namespace fold3d {
+
+// One row per reference sweep function in the driver's order
+// (AN_ISO_1_OpenACC.c:1195-1236).  nrm: axis normal to the planes; sg = +1
+// when the target plane is src+1; (xa, xs) and (ya, ys): axis and sign of the
+// local x and y neighbours (xt, yt).  The local drift is
+// (xs*a[xa], ys*a[ya], sg*a[nrm]) and the spacings (h[nrm], h[xa], h[ya]).
+struct DirSpec {
+    int nrm, sg, xa, xs, ya, ys;
+};
+extern const DirSpec kDirs[6];
+
+// In-plane geometry of one direction on one grid (all strides in elements).
+struct PlaneGeom {
+    long long sn;       // target = source + sn
+    long long sx, sy;   // signed strides of the local x / y neighbours
+    long long su, sv;   // strides of the two in-plane axes, u the faster one
+    long long s_nrm;    // unsigned stride along the plane normal
+    int nu, nv;         // interior extents along u and v
+    int nplanes;        // extent along the normal
+};
+
+struct LocalFrameH {  // host mirror of fold3d::LocalFrame (same layout)
+    double F, ax, ay, az, hz, hx, hy, hxy, hxz, hyz;
+};
+
+PlaneGeom make_geom(const fold3d_grid &g, int dir);
+LocalFrameH make_frame(const fold3d_grid &g, const fold3d_medium &m, int dir);
+
+// Source plane indices of a pass, in the reference's order.
+inline int pass_first(const PlaneGeom &pg, int dir) { return kDirs[dir].sg > 0 ? 1 : pg.nplanes; }
+inline int pass_count(const PlaneGeom &pg) { return pg.nplanes - 1; }
+
+// Error recording (thread-local message readable by fold3d_last_error).
+int set_error(int code, const std::string &msg);
+int cuda_error(cudaError_t e, const char *what);
+void clear_error();
+
+// Kernel launchers (fold3d_kernels.cu).
+cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, int src,
+                         unsigned long long *maxd, cudaStream_t s);
+
+}  // namespace fold3d

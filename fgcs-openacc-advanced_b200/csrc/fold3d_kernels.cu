@@ -1,0 +1,74 @@
+// fold3d_kernels.cu -- per-plane sweep kernel (the PLANES engine).
+//
+// One thread per target point of a plane, as in the reference's OpenACC
+// regions (AN_ISO_1_OpenACC.c:188-193), but with the block shaped 32 x 8 over
+// the plane's two axes so that, for the y and z directions, each warp reads
+// whole 256-byte rows.  The kernel also folds |T_new - T_old| into a
+// per-sweep maximum (warp shuffle, then shared memory, then one atomicMax per
+// block on the IEEE bit pattern, which orders like the value for
+// non-negative doubles).
+#include "fold3d_internal.h"
+#include "fold3d_solver.cuh"
+
+namespace fold3d {
+
+static_assert(sizeof(LocalFrame) == sizeof(LocalFrameH), "frame layout");
+
+__device__ __forceinline__ void block_max_to(double d, unsigned long long *out)
+{
+    __shared__ double wmax[32];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nthreads = blockDim.x * blockDim.y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((tid & 31) == 0) wmax[tid >> 5] = d;
+    __syncthreads();
+    if (tid < 32) {
+        d = (tid < (nthreads >> 5)) ? wmax[tid] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+        if (tid == 0 && d > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(d));
+    }
+}
+
+__global__ void __launch_bounds__(256) plane_kernel(double *__restrict__ T, long long src_off,
+                                                    PlaneGeom g, LocalFrame L,
+                                                    unsigned long long *__restrict__ maxd)
+{
+    const int u = blockIdx.x * 32 + threadIdx.x + 1;
+    const int v = blockIdx.y * 8 + threadIdx.y + 1;
+    double delta = 0.0;
+    if (u <= g.nu && v <= g.nv) {
+        const long long src = src_off + (long long)u * g.su + (long long)v * g.sv;
+        const long long tgt = src + g.sn;
+        Stencil9 s;
+        // The source plane is not written by this launch: read-only path.
+        s.st = fabs(__ldg(T + src));
+        s.xt = fabs(__ldg(T + src + g.sx));
+        s.yt = fabs(__ldg(T + src + g.sy));
+        s.xnt = fabs(__ldg(T + src - g.sx));
+        s.ynt = fabs(__ldg(T + src - g.sy));
+        s.txm = fabs(__ldg(T + src + g.sx - g.sy));
+        s.txy = fabs(__ldg(T + src + g.sx + g.sy));
+        s.tym = fabs(__ldg(T + src - g.sx + g.sy));
+        s.txnyn = fabs(__ldg(T + src - g.sx - g.sy));
+        const double told = T[tgt];
+        const double tnew = point_update(told, s, L);
+        T[tgt] = tnew;
+        delta = fabs(tnew - told);
+    }
+    if (maxd) block_max_to(delta, maxd);
+}
+
+cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &Lh, int src,
+                         unsigned long long *maxd, cudaStream_t s)
+{
+    LocalFrame L;
+    memcpy(&L, &Lh, sizeof(L));
+    dim3 block(32, 8);
+    dim3 grid((pg.nu + 31) / 32, (pg.nv + 7) / 8);
+    plane_kernel<<<grid, block, 0, s>>>(T, (long long)src * pg.s_nrm, pg, L, maxd);
+    return cudaGetLastError();
+}
+
+}  // namespace fold3d

@@ -1,0 +1,246 @@
+"""ctypes binding of libfold3dpmm.so (the C-ABI declared in include/fold3dpmm.h).
+
+This is the Python host side of the library: it mirrors the C entry points
+one to one and adds nothing to the numerics.  Every solve runs in the CUDA
+kernels of libfold3dpmm.so; if the library has not been built, loading it
+raises instead of falling back to anything else.
+
+Fields are numpy (host) or torch (device) float64 arrays of shape
+(nz+2, ny+2, nx+2) in C order, i.e. flat index i + (nx+2)*(j + (ny+2)*k), the
+reference's layout (Stencil-OpenACC/AN_ISO_1_OpenACC.c:195).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfold3dpmm.so")
+
+OK, ERR_INVALID, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(6)
+MAXT = 10e15 * 1.0
+X_DOWN, X_UP, K_UP, K_DOWN, Y_UP, Y_DOWN = range(6)
+ENGINE_AUTO, ENGINE_PLANES, ENGINE_WAVEFRONT = range(3)
+
+# The reference medium (Stencil-OpenACC/Fold3dPMM.h:49-52).
+REF_F = 1.1
+REF_A = (-0.35, 0.4, 0.7)
+
+# Every exported symbol of include/fold3dpmm.h and include/fold3d_acc.h.
+EXPORTED = (
+    "fold3d_last_error", "fold3d_version", "fold3d_default_opts", "fold3d_create", "fold3d_destroy",
+    "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
+    "fold3d_exact_time", "fold3d_compat_set_grid",
+    "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
+    "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
+    "function_k_down",
+    "acc_malloc", "acc_free", "acc_memcpy_to_device", "acc_memcpy_from_device",
+)
+
+
+class Fold3dError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("fold3d error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double)]
+
+
+class Medium(C.Structure):
+    _fields_ = [("F", C.c_double), ("ax", C.c_double), ("ay", C.c_double), ("az", C.c_double)]
+
+
+class Opts(C.Structure):
+    _fields_ = [("max_sweeps", C.c_int), ("fixed", C.c_int), ("tol", C.c_double),
+                ("engine", C.c_int), ("skip", C.c_int)]
+
+
+class Report(C.Structure):
+    _fields_ = [("sweeps", C.c_int), ("max_delta", C.c_double), ("elapsed_ms", C.c_double),
+                ("nominal_updates", C.c_uint64), ("evaluated_updates", C.c_uint64),
+                ("engine", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libfold3dpmm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libfold3dpmm.so is not built (run __graft_entry__.build() or "
+                           "python fgcs-openacc-advanced_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    P = C.POINTER
+    L.fold3d_last_error.restype = C.c_char_p
+    L.fold3d_version.restype = C.c_char_p
+    L.fold3d_default_opts.argtypes = [P(Opts)]
+    L.fold3d_create.argtypes = [P(vp), i]
+    L.fold3d_destroy.argtypes = [vp]
+    L.fold3d_solve.argtypes = [vp, P(Grid), P(Medium), vp, P(Opts), vp, P(Report)]
+    L.fold3d_solve_host.argtypes = [vp, P(Grid), P(Medium), vp, vp, P(Opts), vp, P(Report)]
+    L.fold3d_plane.argtypes = [P(Grid), P(Medium), vp, i, i, vp]
+    L.fold3d_init_implicit.argtypes = [vp, P(Grid), P(Medium)]
+    L.fold3d_init_point.argtypes = [vp, P(Grid), i, i, i]
+    L.fold3d_exact_time.argtypes = [P(Medium), d, d, d]
+    L.fold3d_exact_time.restype = d
+    L.fold3d_compat_set_grid.argtypes = [i, i, i]
+    L.InitFoldFromPoint.argtypes = [d] * 7
+    L.InitFoldFromPoint.restype = d
+    L.ImpSurfF.argtypes = [d] * 3
+    L.ImpSurfF.restype = d
+    L.ImplicitInitialiser.argtypes = [vp, i, i, i, d, d, d]
+    for n in ("function_x_down", "function_x_up", "function_y_up", "function_y_down",
+              "function_k_up", "function_k_down"):
+        getattr(L, n).argtypes = [vp, i] + [d] * 10
+    L.acc_malloc.argtypes = [C.c_size_t]
+    L.acc_malloc.restype = vp
+    L.acc_free.argtypes = [vp]
+    L.acc_memcpy_to_device.argtypes = [vp, vp, C.c_size_t]
+    L.acc_memcpy_from_device.argtypes = [vp, vp, C.c_size_t]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().fold3d_last_error().decode()
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise Fold3dError(rc, last_error())
+
+
+def version() -> str:
+    return lib().fold3d_version().decode()
+
+
+def grid(nx, ny, nz, h) -> Grid:
+    if not hasattr(h, "__len__"):
+        h = (h, h, h)
+    return Grid(int(nx), int(ny), int(nz), float(h[0]), float(h[1]), float(h[2]))
+
+
+def medium(F=REF_F, a=REF_A) -> Medium:
+    return Medium(float(F), float(a[0]), float(a[1]), float(a[2]))
+
+
+def opts(max_sweeps=1000, fixed=False, tol=0.0, engine=ENGINE_AUTO, skip=True) -> Opts:
+    o = Opts()
+    lib().fold3d_default_opts(C.byref(o))
+    o.max_sweeps, o.fixed, o.tol, o.engine, o.skip = int(max_sweeps), int(bool(fixed)), float(tol), \
+        int(engine), int(bool(skip))
+    return o
+
+
+def grid_of(T) -> tuple:
+    nz, ny, nx = (int(s) - 2 for s in T.shape)
+    return nx, ny, nz
+
+
+def _host_ptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("field must be a C-contiguous float64 array")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _any_host_ptr(a):
+    if isinstance(a, np.ndarray):
+        return _host_ptr(a)
+    import torch
+
+    if a.dtype != torch.float64 or not a.is_contiguous() or a.is_cuda:
+        raise ValueError("host field must be a contiguous float64 CPU tensor")
+    return C.c_void_p(a.data_ptr())
+
+
+def _dev_ptr(t):
+    import torch
+
+    if t.dtype != torch.float64 or not t.is_contiguous() or not t.is_cuda:
+        raise ValueError("device field must be a contiguous float64 CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def init_implicit(nx, ny, nz, h, med: Medium | None = None) -> np.ndarray:
+    """Host field initialised from the reference's implicit surface."""
+    T = np.empty((nz + 2, ny + 2, nx + 2), dtype=np.float64)
+    _check(lib().fold3d_init_implicit(_host_ptr(T), C.byref(grid(nx, ny, nz, h)),
+                                      C.byref(med or medium())))
+    return T
+
+
+def init_point(nx, ny, nz, src) -> np.ndarray:
+    T = np.empty((nz + 2, ny + 2, nx + 2), dtype=np.float64)
+    _check(lib().fold3d_init_point(_host_ptr(T), C.byref(grid(nx, ny, nz, 1.0)), *map(int, src)))
+    return T
+
+
+def exact_time(med: Medium, x, y, z) -> float:
+    return lib().fold3d_exact_time(C.byref(med), float(x), float(y), float(z))
+
+
+class Context:
+    """A fold3d_ctx on one device."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check(lib().fold3d_create(C.byref(self._h), int(device)))
+
+    def close(self):
+        if self._h:
+            lib().fold3d_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def solve(self, T, h, med: Medium | None = None, o: Opts | None = None, stream=None,
+              out=None) -> Report:
+        """Solve in place.  T: float64 CUDA tensor (device path), or a host
+        array -- numpy, or a (pinned) CPU torch tensor -- for the host path,
+        which copies in and out inside the call; `out` then receives the
+        result (default: T itself)."""
+        nx, ny, nz = grid_of(T)
+        g = grid(nx, ny, nz, h)
+        rep = Report()
+        o = o or opts()
+        med = med or medium()
+        s = C.c_void_p(stream) if stream else None
+        if isinstance(T, np.ndarray) or not T.is_cuda:
+            src = _any_host_ptr(T)
+            dst = _any_host_ptr(out) if out is not None else src
+            _check(lib().fold3d_solve_host(self._h, C.byref(g), C.byref(med), src, dst, C.byref(o), s,
+                                           C.byref(rep)))
+        else:
+            _check(lib().fold3d_solve(self._h, C.byref(g), C.byref(med), _dev_ptr(T), C.byref(o), s,
+                                      C.byref(rep)))
+        return rep
+
+
+def plane(T, h, dir_, src, med: Medium | None = None, stream=None):
+    """One plane step on a device field (asynchronous on stream)."""
+    nx, ny, nz = grid_of(T)
+    _check(lib().fold3d_plane(C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()), _dev_ptr(T),
+                              int(dir_), int(src), C.c_void_p(stream) if stream else None))

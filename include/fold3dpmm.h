@@ -1,0 +1,206 @@
+/*
+ * fold3dpmm.h -- C-ABI of the B200 Fold3dPMM library (libfold3dpmm.so).
+ *
+ * Fold3dPMM is the parallel marching method for the anisotropic ("folding")
+ * 3-D eikonal equation of ezhilmathik/FGCS-OpenACC-Advanced: the travel-time
+ * field is swept plane by plane in the six axis directions, every point of a
+ * plane being updated from the already updated previous plane by a local
+ * upwind solver, and the sweeps repeat until the field stops changing.
+ *
+ * Two layers are declared here.
+ *
+ * 1. Reference-compatible entry points, with the names, argument lists and
+ *    semantics of the reference, so that the reference's C host driver
+ *    (Stencil-OpenACC/AN_ISO_1_OpenACC.c:main) runs on this library
+ *    unchanged.  They have no error channel (void, as in the reference);
+ *    failures are recorded and readable with fold3d_last_error().
+ *
+ * 2. The native API (fold3d_*): run-time grid sizes (the three axes may
+ *    differ), run-time medium, whole solves on the GPU with a convergence
+ *    test, status codes, no exits and no traps.
+ *
+ * Array layout (both layers): a field of (nx+2)*(ny+2)*(nz+2) doubles with one
+ * ghost layer per face, element (i,j,k) at T[i + (nx+2)*(j + (ny+2)*k)], interior
+ * indices 1..n.  Axis i has spacing dx and drift ax, j: dy/ay, k: dz/az.  The
+ * sign of T marks the side of the source surface; |T| is the travel time;
+ * FOLD3D_MAXT marks unreached points.  Ghost cells are read, never written.
+ */
+#ifndef FOLD3DPMM_NATIVE_H
+#define FOLD3DPMM_NATIVE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Only the declarations of this header are exported from the shared library
+ * (it is built with -fvisibility=hidden). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define FOLD3D_OK 0
+#define FOLD3D_ERR_INVALID 1     /* bad argument (null pointer, bad size)  */
+#define FOLD3D_ERR_NOMEM 2       /* host or device allocation failed       */
+#define FOLD3D_ERR_CUDA 3        /* a CUDA runtime call failed             */
+#define FOLD3D_ERR_TIMEOUT 4     /* a bounded device-side wait gave up      */
+#define FOLD3D_ERR_UNSUPPORTED 5 /* valid request this build cannot serve  */
+
+/* Unreached time, Fold3dPMM.h:6 (MAXT). */
+#define FOLD3D_MAXT (10e15 * 1.0)
+
+/* Sweep directions, in the order the reference driver runs them each sweep
+ * (AN_ISO_1_OpenACC.c:1195-1236). */
+enum fold3d_dir {
+    FOLD3D_X_DOWN = 0, /* target plane i+1 from i, i = 1..nx-1  (function_x_down) */
+    FOLD3D_X_UP = 1,   /* target plane i-1 from i, i = nx..2    (function_x_up)   */
+    FOLD3D_K_UP = 2,   /* target plane k+1 from k, k = 1..nz-1  (function_k_up)   */
+    FOLD3D_K_DOWN = 3, /* target plane k-1 from k, k = nz..2    (function_k_down) */
+    FOLD3D_Y_UP = 4,   /* target plane j-1 from j, j = ny..2    (function_y_up)   */
+    FOLD3D_Y_DOWN = 5  /* target plane j+1 from j, j = 1..ny-1  (function_y_down) */
+};
+
+/* Execution engines for a whole solve. */
+enum fold3d_engine {
+    FOLD3D_ENGINE_AUTO = 0,
+    FOLD3D_ENGINE_PLANES = 1,    /* one kernel per plane, each sweep a CUDA graph    */
+    FOLD3D_ENGINE_WAVEFRONT = 2  /* one persistent kernel per pass, tile dataflow     */
+};
+
+typedef struct {
+    int nx, ny, nz;       /* interior points per axis (>= 2)          */
+    double dx, dy, dz;    /* grid spacing per axis (> 0)              */
+} fold3d_grid;
+
+/* The reference's medium: isotropic speed F plus a constant drift
+ * a = (ax, ay, az); the unit-time wavefront from a point is the sphere
+ * |x - a| = F (Fold3dPMM.c:9-26).  Requires F*F > |a|^2. */
+typedef struct {
+    double F;
+    double ax, ay, az;
+} fold3d_medium;
+
+typedef struct {
+    int max_sweeps;   /* sweeps to run at most (>= 1)                          */
+    int fixed;        /* non-zero: run exactly max_sweeps, no convergence test   */
+                      /* (the reference driver runs a fixed 8, :1187)            */
+    double tol;       /* else stop after the first sweep with max|dT| <= tol     */
+    int engine;       /* enum fold3d_engine                                      */
+    int skip;         /* non-zero: skip tiles whose inputs did not change since   */
+                      /* their last update in that direction (result unchanged, */
+                      /* bit for bit); wavefront engine only                     */
+} fold3d_opts;
+
+typedef struct {
+    int sweeps;                  /* sweeps run                                 */
+    double max_delta;            /* max |T_after - T_before| of the last sweep */
+    double elapsed_ms;           /* device time of the sweeps (CUDA events)    */
+    uint64_t nominal_updates;    /* point updates the reference would do       */
+    uint64_t evaluated_updates;  /* point updates actually evaluated           */
+    int engine;                  /* engine that ran                            */
+} fold3d_report;
+
+typedef struct fold3d_ctx fold3d_ctx;
+
+/* ------------------------------------------------------------------------ */
+/* Native API                                                                */
+/* ------------------------------------------------------------------------ */
+
+/* Message of the last failure on the calling host thread ("" if none). */
+const char *fold3d_last_error(void);
+
+/* Library version string. */
+const char *fold3d_version(void);
+
+/* Default options: fixed = 0, max_sweeps = 1000, tol = 0.0 (run until the
+ * field stops changing), engine = AUTO, skip = 1. */
+void fold3d_default_opts(fold3d_opts *o);
+
+/* Context: owns device scratch, graphs and events for one device.  One
+ * context per host thread, or externally synchronised. */
+int fold3d_create(fold3d_ctx **ctx, int device);
+void fold3d_destroy(fold3d_ctx *ctx);
+
+/* Solve in place on a device field.  T_dev: device pointer to the
+ * (nx+2)(ny+2)(nz+2) field.  stream: a cudaStream_t (NULL = legacy default
+ * stream).  Returns when the solve has finished on the device.  rep may be
+ * NULL. */
+int fold3d_solve(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_medium *m,
+                 double *T_dev, const fold3d_opts *o, void *stream, fold3d_report *rep);
+
+/* Same, for fields in host memory: copies T_in to the device, solves, copies
+ * the result to T_out (T_out may equal T_in).  Pinned host buffers make the
+ * copies faster.  Device memory is allocated by the context and kept for
+ * reuse. */
+int fold3d_solve_host(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_medium *m,
+                      const double *T_in, double *T_out, const fold3d_opts *o, void *stream,
+                      fold3d_report *rep);
+
+/* One plane step on a device field: update plane src+1 (down) or src-1 (up)
+ * of direction dir from plane src.  Asynchronous on stream. */
+int fold3d_plane(const fold3d_grid *g, const fold3d_medium *m, double *T_dev, int dir,
+                 int src, void *stream);
+
+/* Implicit-surface source initialisation of a host field (the reference's
+ * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).
+ * Uses all host cores. */
+int fold3d_init_implicit(double *T_host, const fold3d_grid *g, const fold3d_medium *m);
+
+/* Point source: T = +MAXT everywhere, T[si,sj,sk] = 0 (host field). */
+int fold3d_init_point(double *T_host, const fold3d_grid *g, int si, int sj, int sk);
+
+/* Exact travel time of the homogeneous medium from the origin to (x,y,z),
+ * FOLD3D_MAXT where undefined (InitFoldFromPoint, Fold3dPMM.c:9-26). */
+double fold3d_exact_time(const fold3d_medium *m, double x, double y, double z);
+
+/* Grid size the reference-compatible sweep functions assume for a device
+ * field (they have no size argument, AN_ISO_1_OpenACC.c:180).  If never set,
+ * the size is taken from the allocation made by this library's acc_malloc. */
+int fold3d_compat_set_grid(int nx, int ny, int nz);
+
+/* ------------------------------------------------------------------------ */
+/* Reference-compatible entry points                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Fold3dPMM.h:58-75 / Fold3dPMM.c:9-126.  Host functions; T is a host field
+ * of a cubic grid whose pitch is nx+2 (the reference's HEIGHT). */
+double InitFoldFromPoint(double F, double ax, double ay, double az, double x, double y,
+                         double z);
+double ImpSurfF(double x, double y, double z);
+/* Fold3dPMM.h:81-85 / Fold3dPMM.c:129-389: medium = the reference constants
+ * F = 1.1, a = (-0.35, 0.4, 0.7). */
+void ImplicitInitialiser(double *T, int nx, int ny, int nz, double dxx, double dyy,
+                         double dzz);
+
+/* AN_ISO_1_OpenACC.c:180, 334, 485, 636, 790, 944.  T is a DEVICE pointer
+ * (the reference's deviceptr(T), :189).  The plane index and the permuted
+ * spacings and drift are those the reference driver passes (:1195-1236):
+ * (dzz, dxx, dyy) = spacing normal to the plane, along the local x and y
+ * neighbours; dxy, dxz, dyz the diagonals; (ax, ay, az) the drift in that
+ * local frame.  Synchronous, like the reference's OpenACC regions. */
+void function_x_down(double *T, int i, double dzz, double dxx, double dyy, double dxy,
+                     double dxz, double dyz, double F, double ay, double ax, double az);
+void function_x_up(double *T, int i, double dzz, double dxx, double dyy, double dxy,
+                   double dxz, double dyz, double F, double ay, double ax, double az);
+void function_y_up(double *T, int j, double dzz, double dxx, double dyy, double dxy,
+                   double dxz, double dyz, double F, double ay, double ax, double az);
+void function_y_down(double *T, int j, double dzz, double dxx, double dyy, double dxy,
+                     double dxz, double dyz, double F, double ay, double ax, double az);
+void function_k_up(double *T, int k, double dzz, double dxx, double dyy, double dxy,
+                   double dxz, double dyz, double F, double ay, double ax, double az);
+void function_k_down(double *T, int k, double dzz, double dxx, double dyy, double dxy,
+                     double dxz, double dyz, double F, double ay, double ax, double az);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FOLD3DPMM_NATIVE_H */

@@ -1,0 +1,189 @@
+"""CPU oracle for the Fold3dPMM plane sweep -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its
+``cpu_baseline`` leg and ``--impl reference``) may import this package, and
+only as the checker or the timed CPU baseline; the product library never
+does.
+
+Two oracles live here:
+
+* :class:`Oracle` wraps ``liboracle.so``, this repository's plain-C
+  restatement of the reference's single-device path (run-time sizes,
+  non-cubic grids, run-time medium).
+* :class:`RefLib` wraps ``_ref/n<N>/libref[_omp].so``, the reference's own
+  ``AN_ISO_1_OpenACC.c`` + ``Fold3dPMM.c`` compiled for the host at a fixed
+  cubic size N, driven plane by plane in the order and with the arguments of
+  the reference's ``main`` (``Stencil-OpenACC/AN_ISO_1_OpenACC.c:1195-1236``).
+
+Arrays are numpy float64 of shape (nz+2, ny+2, nx+2) in C order, so the flat
+index is ``i + (nx+2)*(j + (ny+2)*k)`` as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# Reference medium and source constants (Fold3dPMM.h:6, :49-52).
+MAXT = 10e15 * 1.0
+REF_F = 1.1
+REF_A = (-0.35, 0.4, 0.7)
+
+_dbl = C.c_double
+_int = C.c_int
+_ptr = C.c_void_p
+
+
+def ref_spacing(n: int) -> float:
+    """Grid spacing of the reference driver, h = (10 - 0) / (n - 1.0)
+    (AN_ISO_1_OpenACC.c:1154-1156)."""
+    return (10.0 - 0.0) / (n - 1.0)
+
+
+def empty_field(nx: int, ny: int, nz: int) -> np.ndarray:
+    return np.empty((nz + 2, ny + 2, nx + 2), dtype=np.float64)
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ptr)
+
+
+class Oracle:
+    """ctypes wrapper of liboracle.so (oracle/fold3d_oracle.c)."""
+
+    def __init__(self, path: str | None = None):
+        if path is None:
+            path = os.path.join(HERE, "liboracle.so")
+            if not os.path.exists(path):
+                from . import build
+
+                build.build_oracle()
+        L = C.CDLL(path)
+        L.orc_plane.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int, _int]
+        L.orc_pass.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int]
+        L.orc_solve.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int, _dbl,
+                                C.POINTER(_dbl)]
+        L.orc_solve.restype = _int
+        L.orc_init_implicit.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl]
+        L.orc_init_implicit.restype = _int
+        L.orc_init_point.argtypes = [_ptr, _int, _int, _int, _int, _int, _int]
+        L.orc_fold_from_point.argtypes = [_dbl] * 7
+        L.orc_fold_from_point.restype = _dbl
+        L.orc_surface.argtypes = [_dbl] * 3
+        L.orc_surface.restype = _dbl
+        L.orc_last_overfull.restype = C.c_long
+        self.L = L
+
+    @staticmethod
+    def _dims(T):
+        nz, ny, nx = (s - 2 for s in T.shape)
+        return nx, ny, nz
+
+    def init_implicit(self, nx, ny, nz, h, F=REF_F, a=REF_A) -> np.ndarray:
+        T = empty_field(nx, ny, nz)
+        rc = self.L.orc_init_implicit(_p(T), nx, ny, nz, h[0], h[1], h[2], F, *a)
+        if rc != 0:
+            raise MemoryError("orc_init_implicit failed")
+        return T
+
+    def init_point(self, nx, ny, nz, src) -> np.ndarray:
+        T = empty_field(nx, ny, nz)
+        self.L.orc_init_point(_p(T), nx, ny, nz, *src)
+        return T
+
+    def plane(self, T, h, dir_, src, F=REF_F, a=REF_A):
+        self.L.orc_plane(_p(T), *self._dims(T), h[0], h[1], h[2], F, *a, dir_, src)
+
+    def pass_(self, T, h, dir_, F=REF_F, a=REF_A):
+        self.L.orc_pass(_p(T), *self._dims(T), h[0], h[1], h[2], F, *a, dir_)
+
+    def solve(self, T, h, nsweeps, tol=-1.0, F=REF_F, a=REF_A):
+        """In place.  Returns (sweeps_run, max|dT| of the last sweep)."""
+        d = _dbl(0.0)
+        s = self.L.orc_solve(_p(T), *self._dims(T), h[0], h[1], h[2], F, *a, nsweeps, tol, C.byref(d))
+        if s < 0:
+            raise MemoryError("orc_solve failed")
+        return s, d.value
+
+    def fold_from_point(self, F, ax, ay, az, x, y, z) -> float:
+        return self.L.orc_fold_from_point(F, ax, ay, az, x, y, z)
+
+    def overfull_voxels(self) -> int:
+        return self.L.orc_last_overfull()
+
+
+# The reference driver's sweep order and argument permutations
+# (AN_ISO_1_OpenACC.c:1195-1236).  Each entry: symbol, plane range kind,
+# spacing permutation, drift arguments (ay, ax, az) as passed.
+_REF_CALLS = (
+    ("function_x_down", "up", ("DX", "dz", "dy", "DYZP", "DXZP", "DXYP"), (+1, "y"), (+1, "z"), (+1, "x")),
+    ("function_x_up", "down", ("DX", "dz", "dy", "DYZP", "DXZP", "DXYP"), (-1, "y"), (-1, "z"), (-1, "x")),
+    ("function_k_up", "up", ("dz", "dy", "DX", "DXYP", "DYZP", "DXZP"), (+1, "x"), (+1, "y"), (+1, "z")),
+    ("function_k_down", "down", ("dz", "dy", "DX", "DXYP", "DYZP", "DXZP"), (-1, "x"), (-1, "y"), (-1, "z")),
+    ("function_y_up", "down", ("dy", "DX", "dz", "DXZP", "DXYP", "DYZP"), (-1, "z"), (-1, "x"), (-1, "y")),
+    ("function_y_down", "up", ("dy", "DX", "dz", "DXZP", "DXYP", "DYZP"), (+1, "z"), (+1, "x"), (+1, "y")),
+)
+
+
+class RefLib:
+    """The reference's own code built for the host at size n (oracle/_ref)."""
+
+    def __init__(self, n: int, omp: bool = False):
+        from . import build
+
+        path = build.ref_lib_path(n, omp)
+        if not os.path.exists(path):
+            build.build_ref(n)
+        self.n = n
+        L = C.CDLL(path)
+        L.ImplicitInitialiser.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl]
+        L.InitFoldFromPoint.argtypes = [_dbl] * 7
+        L.InitFoldFromPoint.restype = _dbl
+        L.ImpSurfF.argtypes = [_dbl] * 3
+        L.ImpSurfF.restype = _dbl
+        for name, *_ in _REF_CALLS:
+            getattr(L, name).argtypes = [_ptr, _int] + [_dbl] * 10
+        self.L = L
+        DX = dy = dz = ref_spacing(n)
+        self.sp = {
+            "DX": DX, "dy": dy, "dz": dz,
+            "DXYP": math.sqrt(DX * DX + dy * dy),
+            "DXZP": math.sqrt(DX * DX + dz * dz),
+            "DYZP": math.sqrt(dy * dy + dz * dz),
+        }
+        self.const = {"x": REF_A[0], "y": REF_A[1], "z": REF_A[2]}
+
+    def init_implicit(self) -> np.ndarray:
+        n = self.n
+        T = empty_field(n, n, n)
+        self.L.ImplicitInitialiser(_p(T), n, n, n, self.sp["DX"], self.sp["dy"], self.sp["dz"])
+        return T
+
+    def _args(self, entry):
+        _, _, sp, *drift = entry
+        s = [self.sp[k] for k in sp]
+        d = [sg * self.const[c] for sg, c in drift]
+        return s + [REF_F] + d
+
+    def plane(self, T, dir_, src):
+        entry = _REF_CALLS[dir_]
+        getattr(self.L, entry[0])(_p(T), src, *self._args(entry))
+
+    def pass_(self, T, dir_):
+        n = self.n
+        entry = _REF_CALLS[dir_]
+        fn = getattr(self.L, entry[0])
+        args = self._args(entry)
+        planes = range(1, n) if entry[1] == "up" else range(n, 1, -1)
+        for s in planes:
+            fn(_p(T), s, *args)
+
+    def sweeps(self, T, nsweeps):
+        for _ in range(nsweeps):
+            for d in range(6):
+                self.pass_(T, d)

@@ -1,0 +1,540 @@
+/*
+ * fold3d_oracle.c -- CPU oracle for the Fold3dPMM plane sweep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
+ * calls this file; only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg use it, and only as the checker.
+ *
+ * It is a plain-C restatement of the reference's single-device path
+ * (ezhilmathik/FGCS-OpenACC-Advanced, Stencil-OpenACC/AN_ISO_1_OpenACC.c and
+ * Stencil-OpenACC/Fold3dPMM.c) with three generalisations that do not change
+ * the arithmetic of any cubic reference case:
+ *   - grid sizes are run-time values and the three axes may differ
+ *     (the reference fixes _nx=_ny=_nz and one pitch HEIGHT, Fold3dPMM.h:27-30);
+ *   - the medium (F, ax, ay, az) is a run-time value (the reference hard-codes
+ *     _Fc, _axx, _ayy, _azz, Fold3dPMM.h:49-52, AN_ISO_1_OpenACC.c:50-53);
+ *   - the six copy-pasted sweep functions are one table-driven routine.
+ *
+ * Parity: pinned.  tests/golden/ holds outputs of the reference's own code
+ * (compiled from its sources by oracle/build.py into oracle/_ref/) and the
+ * tests check this file against them bit for bit.
+ *
+ * Every floating-point expression keeps the reference's operand order; the
+ * file must be compiled with -ffp-contract=off (no FMA contraction), as the
+ * reference's host build is.
+ *
+ * Array layout (AN_ISO_1_OpenACC.c:195, Fold3dPMM.c:143): T[i + Px*(j + Py*k)]
+ * with Px = nx+2, Py = ny+2, one ghost layer on every face; interior indices
+ * run 1..n per axis.  Axis 0 = i (spacing dx), 1 = j (dy), 2 = k (dz).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_MAXT (10e15 * 1.0) /* Fold3dPMM.h:6 */
+
+/* The reference overrides fmin with a ternary macro (AN_ISO_1_OpenACC.c:32-34). */
+static inline double omin(double a, double b) { return (a < b) ? a : b; }
+/* sign(a) maps 0 to -1 (AN_ISO_1_OpenACC.c:36-38). */
+static inline double osign(double a) { return (a > 0) ? 1.0 : -1.0; }
+
+/* ------------------------------------------------------------------------ */
+/* Local solvers                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Edge (two-point) candidate from segment s0-s1 of the previous plane.
+ * Follows FoldEdge2Points, AN_ISO_1_OpenACC.c:59-114 (OPTTEST off). */
+static void orc_edge(double *tn, double s0, double s1, double F, double ax,
+                     double ay, double az, double hx, double hz)
+{
+    if (*tn < omin(s1, s0) || (ax > 0.0 && s1 > s0))
+        return;
+    double g = F * F - ay * ay;
+    double d = (s1 - s0) / hx;
+    double c = (1.0 - d * ax);
+    double q = g * (c * c - d * d * (g - az * az));
+    if (0.0 < q) {
+        c = (-az * c + sqrt(q)) / (g - az * az);
+        q = s0 + hz * c;
+        if (q < *tn && q > omin(s0, s1)) {
+            g = sqrt((d * d + c * c) * F * F / g);
+            /* :90 computes a first footpoint that :92 overwrites; dead. */
+            double xe = -hz * (d + ax * g) / (c + az * g);
+            if (0.0 < xe && xe < hx)
+                *tn = q;
+        }
+    }
+    if (*tn > s1) { /* fall-back from s1 alone, :99-113 */
+        c = (-hx * ax + hz * az);
+        g = hx * hx + hz * hz;
+        q = (F * F - ax * ax - ay * ay - az * az) * g + c * c;
+        if (q > 0.0) {
+            c = c + sqrt(q);
+            if (c > 0.0)
+                *tn = omin(*tn, s1 + g / c);
+        }
+    }
+}
+
+/* Triangle (three-point) candidate from s0-s1-s2, then the nested edge on
+ * s1-s2 with a rotated drift.  Follows FoldSurf3Points,
+ * AN_ISO_1_OpenACC.c:119-175 (UNROLLED on, OPTTEST off). */
+static void orc_surf(double *tn, double s0, double s1, double s2, double F,
+                     double ax, double ay, double az, double hx, double hy,
+                     double hz, double hxz)
+{
+    if (*tn < omin(s0, omin(s1, s2)) || (ax > 0.0 && s1 > s0) ||
+        (ay > 0.0 && s2 > s1))
+        return;
+    double dx = (s1 - s0) / hx;
+    double dy = (s2 - s1) / hy;
+    double dd = dx * dx + dy * dy;
+    double g = F * F - az * az;
+    double al = 1.0 - ax * dx - ay * dy;
+    double q = al * al - dd * g;
+    if (q > 0.0) {
+        al = (-az * al + F * sqrt(q)) / g;
+        g = s0 + hz * al;
+        if (g < *tn && g > omin(omin(s0, s1), s2)) {
+            q = sqrt(dd + al * al);
+            dd = -hz / (F * al + az * q);
+            double xe = dd * (F * dx + ax * q);
+            double ye = dd * (F * dy + ay * q);
+            if (0.0 <= omin(xe, ye) && ye * hx <= xe * hy && xe <= hx)
+                *tn = g;
+        }
+    }
+    if (*tn > omin(s1, s2) && (!(ax * hz + az * hx > 0.0 && s1 > s2)))
+        orc_edge(tn, s1, s2, F, ay, (ax * hz + az * hx) / hxz,
+                 (-ax * hx + az * hz) / hxz, hy, hxz);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sweep directions                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* One row per reference sweep function, in the driver's order
+ * (AN_ISO_1_OpenACC.c:1195-1236): x_down, x_up, k_up, k_down, y_up, y_down.
+ *   nrm  : axis normal to the planes; sg: +1 if the target is src+1
+ *   xa,xs: axis and sign of the local "x" neighbour (xt)
+ *   ya,ys: axis and sign of the local "y" neighbour (yt)
+ * The neighbour offsets of every function (e.g. :195-204 for x_down) are
+ * xt=+x, yt=+y, xnt=-x, ynt=-y, txy=+x+y, txm=+x-y, tym=-x+y, txnyn=-x-y in
+ * that local frame, and the local drift is (xs*a[xa], ys*a[ya], sg*a[nrm])
+ * (:206, :359, :816, :971, :511, :663). */
+typedef struct { int nrm, sg, xa, xs, ya, ys; } orc_dir;
+static const orc_dir ORC_DIRS[6] = {
+    {0, +1, 2, +1, 1, +1}, /* function_x_down :180 */
+    {0, -1, 2, -1, 1, -1}, /* function_x_up   :334 */
+    {2, +1, 1, +1, 0, +1}, /* function_k_up   :790 */
+    {2, -1, 1, -1, 0, -1}, /* function_k_down :944 */
+    {1, -1, 0, -1, 2, -1}, /* function_y_up   :485 */
+    {1, +1, 0, +1, 2, +1}, /* function_y_down :636 */
+};
+
+typedef struct {
+    int n[3];
+    int64_t stride[3];
+} orc_grid;
+
+static orc_grid orc_make_grid(int nx, int ny, int nz)
+{
+    orc_grid g;
+    g.n[0] = nx; g.n[1] = ny; g.n[2] = nz;
+    g.stride[0] = 1;
+    g.stride[1] = (int64_t)(nx + 2);
+    g.stride[2] = (int64_t)(nx + 2) * (ny + 2);
+    return g;
+}
+
+/* Update of one target point from the source plane; body of every
+ * function_* (e.g. :195-326).  Returns nothing; writes T[tgt]. */
+static void orc_point(double *T, int64_t tgt, int64_t src, int64_t sx,
+                      int64_t sy, double F, double ax, double ay, double az,
+                      double hz, double hx, double hy, double hxy, double hxz,
+                      double hyz)
+{
+    double tnew = fabs(T[tgt]);
+    double st = fabs(T[src]);
+    double xt = fabs(T[src + sx]);
+    double yt = fabs(T[src + sy]);
+    double xnt = fabs(T[src - sx]);
+    double ynt = fabs(T[src - sy]);
+    double txm = fabs(T[src + sx - sy]);
+    double txy = fabs(T[src + sx + sy]);
+    double tym = fabs(T[src - sx + sy]);
+    double txnyn = fabs(T[src - sx - sy]);
+
+    if (T[tgt] < 0) { /* negative side: drift reversed, :207-212 */
+        ax *= -1;
+        ay *= -1;
+        az *= -1;
+    }
+    if (st < tnew) { /* one-dimensional normal candidate, :214-228 */
+        double q = (F * F - (ax * ax + ay * ay)) * hz * hz;
+        if (q > 0.0) {
+            q = az * hz + sqrt(q);
+            if (q > 0.0)
+                tnew = omin(tnew, st + hz * hz / q);
+        }
+    }
+    /* early exit and the fixed 16-call order, :231-253 */
+    if (!(tnew < st && tnew < omin(xt, yt) && tnew < omin(txy, txm) &&
+          tnew < omin(txnyn, tym))) {
+        orc_surf(&tnew, st, xt, txy, F, ax, ay, az, hx, hy, hz, hxz);
+        orc_surf(&tnew, st, xt, txm, F, ax, -ay, az, hx, hy, hz, hxz);
+        orc_surf(&tnew, st, xnt, txnyn, F, -ax, -ay, az, hx, hy, hz, hxz);
+        orc_surf(&tnew, st, xnt, tym, F, -ax, ay, az, hx, hy, hz, hxz);
+        orc_surf(&tnew, st, ynt, txnyn, F, -ay, -ax, az, hy, hx, hz, hyz);
+        orc_surf(&tnew, st, ynt, txm, F, -ay, ax, az, hy, hx, hz, hyz);
+        orc_surf(&tnew, st, yt, txy, F, ay, ax, az, hy, hx, hz, hyz);
+        orc_surf(&tnew, st, yt, tym, F, ay, -ax, az, hy, hx, hz, hyz);
+
+        orc_edge(&tnew, st, xt, F, ax, ay, az, hx, hz);
+        orc_edge(&tnew, st, txy, F, (ax * hx + ay * hy) / hxy,
+                 (-ax * hy + ay * hx) / hxy, az, hxy, hz);
+        orc_edge(&tnew, st, yt, F, ay, ax, az, hy, hz);
+        orc_edge(&tnew, st, tym, F, -(ax * hx - ay * hy) / hxy,
+                 (ax * hy + ay * hx) / hxy, az, hxy, hz);
+        orc_edge(&tnew, st, xnt, F, -ax, ay, az, hx, hz);
+        orc_edge(&tnew, st, txnyn, F, -(ax * hx + ay * hy) / hxy,
+                 (-ax * hy + ay * hx) / hxy, az, hxy, hz);
+        orc_edge(&tnew, st, ynt, F, -ay, ax, az, hy, hz);
+        orc_edge(&tnew, st, txm, F, (ax * hx - ay * hy) / hxy,
+                 (ax * hy + ay * hx) / hxy, az, hxy, hz);
+    }
+    T[tgt] = (osign(T[tgt]) * 1.0) * tnew; /* :326 */
+}
+
+/* One plane step: update plane (src + sg) from plane src in direction dir.
+ * Equivalent to one call of the matching function_* with the driver's
+ * argument permutation (:1198, :1205, :1212, :1219, :1227, :1234). */
+void orc_plane(double *T, int nx, int ny, int nz, double dx, double dy,
+               double dz, double F, double a0, double a1, double a2, int dir,
+               int src)
+{
+    const orc_grid g = orc_make_grid(nx, ny, nz);
+    const orc_dir d = ORC_DIRS[dir];
+    const double h[3] = {dx, dy, dz};
+    const double a[3] = {a0, a1, a2};
+    const double hz = h[d.nrm], hx = h[d.xa], hy = h[d.ya];
+    const double hxy = sqrt(hx * hx + hy * hy);
+    const double hxz = sqrt(hx * hx + hz * hz);
+    const double hyz = sqrt(hy * hy + hz * hz);
+    const double ax = d.xs * a[d.xa], ay = d.ys * a[d.ya], az = d.sg * a[d.nrm];
+    const int64_t sx = d.xs * g.stride[d.xa], sy = d.ys * g.stride[d.ya];
+    const int64_t sn = g.stride[d.nrm];
+    /* the two in-plane axes, in increasing axis order */
+    int u = (d.nrm == 0) ? 1 : 0;
+    int v = (d.nrm == 2) ? 1 : 2;
+    const int nu = g.n[u], nv = g.n[v];
+    const int64_t su = g.stride[u], sv = g.stride[v];
+#pragma omp parallel for schedule(static)
+    for (int b = 1; b <= nv; ++b)
+        for (int c = 1; c <= nu; ++c) {
+            int64_t srci = (int64_t)src * sn + (int64_t)c * su + (int64_t)b * sv;
+            orc_point(T, srci + d.sg * sn, srci, sx, sy, F, ax, ay, az, hz,
+                      hx, hy, hxy, hxz, hyz);
+        }
+}
+
+/* One directional pass: all planes of direction dir in the driver's order. */
+void orc_pass(double *T, int nx, int ny, int nz, double dx, double dy,
+              double dz, double F, double a0, double a1, double a2, int dir)
+{
+    const int n[3] = {nx, ny, nz};
+    const orc_dir d = ORC_DIRS[dir];
+    const int nn = n[d.nrm];
+    if (d.sg > 0)
+        for (int s = 1; s < nn; ++s)
+            orc_plane(T, nx, ny, nz, dx, dy, dz, F, a0, a1, a2, dir, s);
+    else
+        for (int s = nn; s > 1; --s)
+            orc_plane(T, nx, ny, nz, dx, dy, dz, F, a0, a1, a2, dir, s);
+}
+
+/* Sweeps in the reference order (:1192-1237).  Runs exactly nsweeps sweeps
+ * when tol < 0; otherwise stops after the first sweep whose max|dT| <= tol
+ * (or at nsweeps).  Returns the number of sweeps run; *last_delta receives
+ * the max |T_after - T_before| over all cells of the last sweep. */
+int orc_solve(double *T, int nx, int ny, int nz, double dx, double dy,
+              double dz, double F, double a0, double a1, double a2,
+              int nsweeps, double tol, double *last_delta)
+{
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    double *prev = (double *)malloc(cells * sizeof(double));
+    if (!prev)
+        return -1;
+    int s = 0;
+    double delta = 0.0;
+    for (s = 0; s < nsweeps;) {
+        memcpy(prev, T, cells * sizeof(double));
+        for (int dir = 0; dir < 6; ++dir)
+            orc_pass(T, nx, ny, nz, dx, dy, dz, F, a0, a1, a2, dir);
+        ++s;
+        delta = 0.0;
+        for (size_t c = 0; c < cells; ++c) {
+            double e = fabs(T[c] - prev[c]);
+            if (e > delta)
+                delta = e;
+        }
+        if (tol >= 0.0 && delta <= tol)
+            break;
+    }
+    free(prev);
+    if (last_delta)
+        *last_delta = delta;
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Source initialisation                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* Exact point-source time of the homogeneous drift medium,
+ * Fold3dPMM.c:9-26. */
+double orc_fold_from_point(double F, double ax, double ay, double az, double x,
+                           double y, double z)
+{
+    double xsq = x * x + y * y + z * z;
+    double adotx = ax * x + ay * y + az * z;
+    double q = (F * F - (ax * ax + ay * ay + az * az)) * xsq + adotx * adotx;
+    if (q > 0.0) {
+        q = adotx + sqrt(q);
+        if (q > 0.0)
+            return xsq / q;
+    }
+    return 1.0 * ORC_MAXT;
+}
+
+/* Implicit surface whose zero level set is the source, Fold3dPMM.c:29-33. */
+double orc_surface(double x, double y, double z)
+{
+    return 5.0 + (sin(x) + cos(y + x) + sin(x + y + z)) * 0.4 - z +
+           (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
+}
+
+typedef struct {
+    double *T;
+    orc_grid g;
+    double F, a[3];
+} orc_seed_ctx;
+
+/* Fold3dPMM.c:35-54: min-update of one node from a surface point at
+ * (x, y, z) relative to it, sign preserved, drift reversed on the negative
+ * side. */
+static void orc_node(const orc_seed_ctx *s, double x, double y, double z,
+                     int i, int j, int k)
+{
+    double *T = s->T;
+    int64_t id = i + s->g.stride[1] * j + s->g.stride[2] * k;
+    double ax = s->a[0], ay = s->a[1], az = s->a[2], F = s->F;
+    if (T[id] < 0.0) {
+        ax *= -1;
+        ay *= -1;
+        az *= -1;
+    }
+    double tnew = orc_fold_from_point(F, ax, ay, az, -x, -y, -z);
+    if (tnew < fabs(T[id]))
+        T[id] = (osign(T[id]) * 1.0) * tnew;
+}
+
+/* The 44 node updates of updateVoxel (Fold3dPMM.c:62-110), in order.  Each
+ * row: multiples (of dxx,dyy,dzz) added to the surface point's position, and
+ * the node index offset.  Rows 17 and 21 (0-based) keep the reference's position/index
+ * mismatches (:82 and :86). */
+#define ORC_NVOXEL 44
+static const signed char ORC_VOXEL[ORC_NVOXEL][6] = {
+    {0, 0, 0, 0, 0, 0},    {-1, 0, 0, 1, 0, 0},   {0, -1, 0, 0, 1, 0},
+    {0, 0, -1, 0, 0, 1},   {-1, -1, 0, 1, 1, 0},  {-1, 0, -1, 1, 0, 1},
+    {0, -1, -1, 0, 1, 1},  {-1, -1, -1, 1, 1, 1}, {1, 0, 0, -1, 0, 0},
+    {1, -1, 0, -1, 1, 0},  {1, 0, -1, -1, 0, 1},  {1, -1, -1, -1, 1, 1},
+    {-2, 0, 0, 2, 0, 0},   {-2, -1, 0, 2, 1, 0},  {-2, 0, -1, 2, 0, 1},
+    {-2, -1, -1, 2, 1, 1}, {0, 1, 0, 0, -1, 0},   {-1, 1, 0, 1, 0, 0},
+    {0, 1, -1, 0, -1, 1},  {-1, 1, -1, 1, -1, 1}, {0, -2, 0, 0, 2, 0},
+    {-1, -2, 0, 2, 0, 0},  {0, -2, -1, 0, 2, 1},  {-1, -2, -1, 1, 2, 1},
+    {0, 0, 1, 0, 0, -1},   {-1, 0, 1, 1, 0, -1},  {0, -1, 1, 0, 1, -1},
+    {-1, -1, 1, 1, 1, -1}, {0, 0, -2, 0, 0, 2},   {-1, 0, -2, 1, 0, 2},
+    {0, -1, -2, 0, 1, 2},  {-1, -1, -2, 1, 1, 2}, {0, 1, 1, 0, -1, -1},
+    {1, 0, 1, -1, 0, -1},  {1, 1, 0, -1, -1, 0},  {0, -2, -2, 0, 2, 2},
+    {-2, 0, -2, 2, 0, 2},  {-2, -2, 0, 2, 2, 0},  {-1, 1, 1, 1, -1, -1},
+    {1, -1, 1, -1, 1, -1}, {1, 1, -1, -1, -1, 1}, {-1, -2, -2, 1, 2, 2},
+    {-2, -1, -2, 2, 1, 2}, {-2, -2, -1, 2, 2, 1},
+};
+
+static inline double orc_shift(double p, int m, double h)
+{
+    /* p, p+h, p-h, p-2*h exactly as the reference spells them */
+    if (m == 0) return p;
+    if (m == 1) return p + h;
+    if (m == -1) return p - h;
+    return p - 2 * h;
+}
+
+/* Fold3dPMM.c:56-112 */
+static void orc_voxel(const orc_seed_ctx *s, int i, int j, int k, double xp,
+                      double yp, double zp, double hx, double hy, double hz)
+{
+    for (int r = 0; r < ORC_NVOXEL; ++r) {
+        const signed char *e = ORC_VOXEL[r];
+        orc_node(s, orc_shift(xp, e[0], hx), orc_shift(yp, e[1], hy),
+                 orc_shift(zp, e[2], hz), i + e[3], j + e[4], k + e[5]);
+    }
+}
+
+/* Number of voxels in the last orc_init_implicit call with more than eight
+ * edge crossings (the reference's 8-entry buffers would overflow there). */
+static long orc_overfull_voxels = 0;
+long orc_last_overfull(void) { return orc_overfull_voxels; }
+
+/* Implicit-surface initialisation, ImplicitInitialiser (Fold3dPMM.c:129-389)
+ * with run-time sizes and medium.  T must hold (nx+2)(ny+2)(nz+2) doubles. */
+int orc_init_implicit(double *T, int nx, int ny, int nz, double hx, double hy,
+                      double hz, double F, double a0, double a1, double a2)
+{
+    orc_seed_ctx s;
+    s.T = T;
+    s.g = orc_make_grid(nx, ny, nz);
+    s.F = F;
+    s.a[0] = a0; s.a[1] = a1; s.a[2] = a2;
+    const int64_t sy = s.g.stride[1], sz = s.g.stride[2];
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    double *IF = (double *)malloc(cells * sizeof(double));
+    if (!IF)
+        return -1;
+    /* :137-147; the coordinate helpers x/y/z are :115-126 */
+    for (int i = 0; i < nx + 2; i++)
+        for (int j = 0; j < ny + 2; j++)
+            for (int k = 0; k < nz + 2; k++) {
+                int64_t id = i + sy * j + sz * k;
+                IF[id] = orc_surface((i - 1) * hx + 0., (j - 1) * hy + 0.,
+                                     (k - 1) * hz + 0.);
+                T[id] = (osign(IF[id]) * 1.0) * ORC_MAXT;
+            }
+    orc_overfull_voxels = 0;
+    for (int i = 1; i < nx; i++)
+        for (int j = 1; j < ny; j++)
+            for (int k = 1; k < nz; k++) {
+                const int64_t id = i + sy * j + sz * k;
+                const double f = IF[id], fx = IF[id + 1], fy = IF[id + sy],
+                             fz = IF[id + sz], fxy = IF[id + 1 + sy],
+                             fzx = IF[id + 1 + sz], fzy = IF[id + sy + sz],
+                             fxyz = IF[id + 1 + sy + sz];
+                double X[12], Y[12], Z[12];
+                int np = 0;
+                double p;
+#define ORC_CROSS(expr, H, px, py, pz)                                         \
+    p = (expr);                                                                \
+    if (0.0 <= p && p <= H) {                                                  \
+        X[np] = (px); Y[np] = (py); Z[np] = (pz); np += 1;                     \
+    }
+                /* edge crossings, :173-269, in the reference's order */
+                ORC_CROSS(hx * f / (f - fx), hx, p, 0.0, 0.0);
+                ORC_CROSS(hx * fz / (fz - fzx), hx, p, 0.0, hz);
+                ORC_CROSS(hx * fy / (fy - fxy), hx, p, hy, 0.0);
+                ORC_CROSS(hx * fzy / (fzy - fxyz), hx, p, hy, hz);
+                ORC_CROSS(hy * f / (f - fy), hy, 0.0, p, 0.0);
+                ORC_CROSS(hy * fz / (fz - fzy), hy, 0., p, hz);
+                ORC_CROSS(hy * fx / (fx - fxy), hy, hx, p, 0.0);
+                ORC_CROSS(hy * fzx / (fzx - fxyz), hy, hx, p, hz);
+                ORC_CROSS(hz * f / (f - fz), hz, 0.0, 0.0, p);
+                ORC_CROSS(hz * fxy / (fxy - fxyz), hz, hx, hy, p);
+                ORC_CROSS(hz * fx / (fx - fzx), hz, hx, 0.0, p);
+                ORC_CROSS(hz * fy / (fy - fzy), hz, 0.0, hy, p);
+#undef ORC_CROSS
+                if (np > 8)
+                    ++orc_overfull_voxels;
+                /* :271-383: every crossing, plus blends with earlier ones.
+                 * The blends' z coordinates take Y[l-2] / Y[l-3] where the
+                 * reference does (:309-379). */
+                for (int l = 0; l < np; l += 1) {
+                    orc_voxel(&s, i, j, k, X[l], Y[l], Z[l], hx, hy, hz);
+                    for (int b = 1; b <= 5 && b <= l; ++b) {
+                        orc_voxel(&s, i, j, k, (2 * X[l] + X[l - b]) / 3,
+                                  (2 * Y[l] + Y[l - b]) / 3,
+                                  (2 * Z[l] + Z[l - b]) / 3, hx, hy, hz);
+                        orc_voxel(&s, i, j, k, (X[l] + 2 * X[l - b]) / 3,
+                                  (Y[l] + 2 * Y[l - b]) / 3,
+                                  (Z[l] + 2 * Z[l - b]) / 3, hx, hy, hz);
+                        if (b == 3) { /* :307-322 */
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 3]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 3]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 3]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (2 * X[l] + X[l - 2] + X[l - 3]) / 4,
+                                      (2 * Y[l] + Y[l - 2] + Y[l - 3]) / 4,
+                                      (2 * Z[l] + Y[l - 2] + Z[l - 3]) / 4, hx,
+                                      hy, hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + 2 * X[l - 2] + X[l - 3]) / 4,
+                                      (Y[l] + 2 * Y[l - 2] + Y[l - 3]) / 4,
+                                      (Z[l] + 2 * Y[l - 2] + Z[l - 3]) / 4, hx,
+                                      hy, hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + 2 * X[l - 3]) / 4,
+                                      (Y[l] + Y[l - 2] + 2 * Y[l - 3]) / 4,
+                                      (Z[l] + Y[l - 2] + 2 * Z[l - 3]) / 4, hx,
+                                      hy, hz);
+                        }
+                        if (b == 4) { /* :336-347 */
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 3]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 3]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 3]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 4]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 4]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 4]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 3] + X[l - 4]) / 3,
+                                      (Y[l] + Y[l - 3] + Y[l - 4]) / 3,
+                                      (Z[l] + Y[l - 3] + Z[l - 4]) / 3, hx, hy,
+                                      hz);
+                        }
+                        if (b == 5) { /* :361-380 */
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 3]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 3]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 3]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 4]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 4]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 4]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 2] + X[l - 5]) / 3,
+                                      (Y[l] + Y[l - 2] + Y[l - 5]) / 3,
+                                      (Z[l] + Y[l - 2] + Z[l - 5]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 3] + X[l - 5]) / 3,
+                                      (Y[l] + Y[l - 3] + Y[l - 5]) / 3,
+                                      (Z[l] + Y[l - 3] + Z[l - 5]) / 3, hx, hy,
+                                      hz);
+                            orc_voxel(&s, i, j, k,
+                                      (X[l] + X[l - 3] + X[l - 4]) / 3,
+                                      (Y[l] + Y[l - 3] + Y[l - 4]) / 3,
+                                      (Z[l] + Y[l - 3] + Z[l - 4]) / 3, hx, hy,
+                                      hz);
+                        }
+                    }
+                }
+            }
+    free(IF);
+    return 0;
+}
+
+/* Point source: T = +MAXT everywhere, T[src] = 0. */
+void orc_init_point(double *T, int nx, int ny, int nz, int si, int sj, int sk)
+{
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    for (size_t c = 0; c < cells; ++c)
+        T[c] = ORC_MAXT;
+    T[si + (int64_t)(nx + 2) * (sj + (int64_t)(ny + 2) * sk)] = 0.0;
+}

@@ -1,0 +1,98 @@
+"""Generate tests/golden/ from the reference's OWN code.
+
+Run in a checkout where the reference sources are available; it builds
+oracle/_ref (oracle/build.py compiles Stencil-OpenACC/AN_ISO_1_OpenACC.c and
+Stencil-OpenACC/Fold3dPMM.c for the host at each size) and drives the
+reference's ImplicitInitialiser and six function_* sweeps in the order and
+with the arguments of its main (AN_ISO_1_OpenACC.c:1180-1237).
+
+Outputs:
+  ref_n8.npz, ref_n16.npz   full fields (float64, shape (n+2,)*3):
+      init            after ImplicitInitialiser
+      s1, s2, s8      after 1, 2 and 8 sweeps (implicit-surface source)
+      point_s8        point source at the centre (+MAXT elsewhere), 8 sweeps
+  digests.json      sha256 of the raw float64 bytes of larger reference
+                    results (the fields themselves would be too big), plus
+                    the md5 of the reference program's own text dump at 128^3
+                    (an_iso_1_openacc.txt, written by its unmodified main).
+
+    python tests/golden/make_golden.py            # everything but 128^3 dump
+    python tests/golden/make_golden.py --dump128  # also run the 128^3 program (~30 s)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import MAXT, RefLib, build  # noqa: E402
+
+
+def point_field(n):
+    T = np.full((n + 2,) * 3, MAXT)
+    c = n // 2 + 1
+    T[c, c, c] = 0.0
+    return T
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main():
+    out = {}
+    for n in (8, 16):
+        build.build_ref(n)
+        r = RefLib(n)
+        T = r.init_implicit()
+        f = {"init": T.copy()}
+        r.sweeps(T, 1)
+        f["s1"] = T.copy()
+        r.sweeps(T, 1)
+        f["s2"] = T.copy()
+        r.sweeps(T, 6)
+        f["s8"] = T.copy()
+        P = point_field(n)
+        r.sweeps(P, 8)
+        f["point_s8"] = P
+        np.savez_compressed(os.path.join(HERE, "ref_n%d.npz" % n), **f)
+    dig = {}
+    for n in (32, 64):
+        build.build_ref(n)
+        r = RefLib(n)
+        T = r.init_implicit()
+        dig["n%d_init" % n] = sha(T)
+        r.sweeps(T, 8)
+        dig["n%d_s8" % n] = sha(T)
+        P = point_field(n)
+        r.sweeps(P, 8)
+        dig["n%d_point_s8" % n] = sha(P)
+    if "--dump128" in sys.argv:
+        d = build.build_ref(128, with_program=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            subprocess.run([os.path.join(d, "an_iso_1_ref")], cwd=tmp, check=True,
+                           stdout=subprocess.DEVNULL)
+            with open(os.path.join(tmp, "an_iso_1_openacc.txt"), "rb") as fh:
+                dig["n128_s8_text_md5"] = hashlib.md5(fh.read()).hexdigest()
+    else:
+        old = os.path.join(HERE, "digests.json")
+        if os.path.exists(old):
+            prev = json.load(open(old))
+            if "n128_s8_text_md5" in prev:
+                dig["n128_s8_text_md5"] = prev["n128_s8_text_md5"]
+    with open(os.path.join(HERE, "digests.json"), "w") as fh:
+        json.dump(dig, fh, indent=1, sort_keys=True)
+    print(json.dumps(dig, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,101 @@
+"""CPU tests of the C-ABI: the library loads, exports every declared symbol,
+and rejects bad arguments with status codes (no compute calls)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    names = set()
+    for h in ("fold3dpmm.h", "fold3d_acc.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = "\n".join(ln for ln in src.splitlines() if not ln.lstrip().startswith("#"))
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", src):
+            name = m.group(1)
+            if name not in ("defined", "if", "sizeof"):
+                names.add(name)
+    return names
+
+
+def test_every_declared_symbol_is_exported(f3d):
+    decl = declared_functions()
+    assert len(decl) >= 25
+    out = subprocess.run(["nm", "-D", "--defined-only", f3d.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    missing = decl - exported
+    assert not missing, "declared but not exported: %s" % sorted(missing)
+    assert set(f3d.EXPORTED) == decl
+    # nothing else leaks from the library
+    extra = {s for s in exported if not s.startswith("_")} - decl
+    assert not extra, "exported but not declared: %s" % sorted(extra)
+
+
+def test_version_and_default_opts(f3d):
+    assert "sm_100a" in f3d.version()
+    o = f3d.opts()
+    assert o.max_sweeps == 1000 and o.fixed == 0 and o.tol == 0.0 and o.skip == 1
+
+
+def test_null_arguments_rejected(f3d):
+    L = f3d.lib()
+    g = f3d.grid(8, 8, 8, 1.0)
+    m = f3d.medium()
+    o = f3d.opts()
+    rc = L.fold3d_solve(None, C.byref(g), C.byref(m), C.c_void_p(16), C.byref(o), None, None)
+    assert rc == f3d.ERR_INVALID and "ctx" in f3d.last_error()
+    assert L.fold3d_create(None, 0) == f3d.ERR_INVALID
+
+
+@pytest.mark.parametrize("g,msg", [((1, 8, 8, 1.0), "sizes"), ((8, 8, 8, 0.0), "spacing"),
+                                   ((8, 8, 8, float("nan")), "spacing")])
+def test_bad_grid_rejected_before_any_launch(f3d, g, msg):
+    L = f3d.lib()
+    gr = f3d.Grid(g[0], g[1], g[2], g[3], g[3], g[3])
+    rc = L.fold3d_plane(C.byref(gr), C.byref(f3d.medium()), C.c_void_p(16), 0, 1, None)
+    assert rc == f3d.ERR_INVALID and msg in f3d.last_error()
+
+
+def test_bad_medium_direction_and_plane_rejected(f3d):
+    L = f3d.lib()
+    g = f3d.grid(8, 8, 8, 1.0)
+    bad = f3d.Medium(-1.0, 0, 0, 0)
+    assert L.fold3d_plane(C.byref(g), C.byref(bad), C.c_void_p(16), 0, 1, None) == f3d.ERR_INVALID
+    m = f3d.medium()
+    assert L.fold3d_plane(C.byref(g), C.byref(m), C.c_void_p(16), 6, 1, None) == f3d.ERR_INVALID
+    assert L.fold3d_plane(C.byref(g), C.byref(m), C.c_void_p(16), 0, 8, None) == f3d.ERR_INVALID
+    assert L.fold3d_plane(C.byref(g), C.byref(m), C.c_void_p(16), 1, 1, None) == f3d.ERR_INVALID
+    assert L.fold3d_plane(C.byref(g), C.byref(m), None, 0, 1, None) == f3d.ERR_INVALID
+
+
+def test_host_helpers_reject_bad_input(f3d):
+    L = f3d.lib()
+    g = f3d.grid(4, 4, 4, 1.0)
+    assert L.fold3d_init_point(None, C.byref(g), 1, 1, 1) == f3d.ERR_INVALID
+    import numpy as np
+
+    T = np.zeros((6, 6, 6))
+    assert L.fold3d_init_point(T.ctypes.data_as(C.c_void_p), C.byref(g), 0, 1, 1) == f3d.ERR_INVALID
+    assert L.fold3d_init_point(T.ctypes.data_as(C.c_void_p), C.byref(g), 1, 1, 5) == f3d.ERR_INVALID
+    assert L.fold3d_compat_set_grid(1, 5, 5) == f3d.ERR_INVALID
+    assert L.fold3d_compat_set_grid(0, 0, 0) == f3d.OK
+
+
+def test_create_without_gpu_fails_cleanly(f3d):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(f3d.Fold3dError) as e:
+        f3d.Context(0)
+    assert e.value.code in (f3d.ERR_CUDA, f3d.ERR_INVALID)
+
+
+def test_oracle_library_loads(orc):
+    assert orc.fold_from_point(1.1, 0, 0, 0, 1.1, 0, 0) == pytest.approx(1.0)

@@ -1,0 +1,232 @@
+"""GPU parity: the CUDA sweep against the reference's own outputs (golden
+fixtures and digests) and against the oracle, bit for bit.
+
+The bar is bit-exact equality of the float64 fields: every kernel follows
+the reference's operand order and is compiled without FMA contraction.
+"""
+import ctypes as C
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import assert_bitwise
+
+from oracle import REF_A, REF_F, ref_spacing
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = ["planes"]
+
+
+def engine_id(f3d, name):
+    return {"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT}[name]
+
+
+def gpu_solve(f3d, ctx, cuda, T, h, sweeps, *, fixed=True, tol=0.0, engine="planes", skip=False,
+              med=None):
+    d = cuda.from_numpy(T.copy()).cuda()
+    rep = ctx.solve(d, h, med, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol,
+                                         engine=engine_id(f3d, engine), skip=skip))
+    return d.cpu().numpy(), rep
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("n", [8, 16])
+def test_golden_implicit_surface(f3d, ctx, cuda, golden, n, engine):
+    h = (ref_spacing(n),) * 3
+    g = golden[n]
+    for k, key in ((1, "s1"), (2, "s2"), (8, "s8")):
+        out, rep = gpu_solve(f3d, ctx, cuda, g["init"], h, k, engine=engine)
+        assert rep.sweeps == k
+        assert_bitwise(out, g[key], "%s n=%d after %d sweeps" % (engine, n, k))
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("n", [8, 16])
+def test_golden_point_source(f3d, ctx, cuda, golden, n, engine):
+    h = (ref_spacing(n),) * 3
+    c = n // 2 + 1
+    T = f3d.init_point(n, n, n, (c, c, c))
+    out, _ = gpu_solve(f3d, ctx, cuda, T, h, 8, engine=engine)
+    assert_bitwise(out, golden[n]["point_s8"], "point source")
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+def test_digests_64(f3d, ctx, cuda, digests, engine):
+    n = 64
+    h = (ref_spacing(n),) * 3
+    T = f3d.init_implicit(n, n, n, h[0])
+    assert sha(T) == digests["n64_init"]
+    out, _ = gpu_solve(f3d, ctx, cuda, T, h, 8, engine=engine)
+    assert sha(out) == digests["n64_s8"]
+    c = n // 2 + 1
+    P = f3d.init_point(n, n, n, (c, c, c))
+    out, _ = gpu_solve(f3d, ctx, cuda, P, h, 8, engine=engine)
+    assert sha(out) == digests["n64_point_s8"]
+
+
+CASES = [
+    # dims, spacing, F, drift, source
+    ((13, 9, 11), (0.7, 0.9, 1.1), 1.3, (0.2, -0.5, 0.3), "implicit"),
+    ((24, 17, 30), (0.41, 0.33, 0.5), 1.0, (0.0, 0.0, 0.0), "point"),
+    ((31, 40, 19), (0.25, 0.3, 0.35), 2.0, (-0.9, 0.4, 1.1), "point"),
+    ((33, 20, 27), (0.3, 0.3, 0.3), 1.1, REF_A, "implicit"),
+    ((2, 5, 3), (1.0, 1.0, 1.0), 1.1, REF_A, "point"),
+]
+
+
+def make_case(f3d, orc, dims, h, F, a, src):
+    if src == "implicit":
+        return orc.init_implicit(*dims, h, F=F, a=a)
+    rng = np.random.default_rng(sum(dims))
+    s = tuple(int(rng.integers(1, d + 1)) for d in dims)
+    return orc.init_point(*dims, s)
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[0])) + c[4])
+def test_oracle_fixed_sweeps(f3d, orc, ctx, cuda, case, engine):
+    dims, h, F, a, src = case
+    T0 = make_case(f3d, orc, dims, h, F, a, src)
+    for k in (1, 3):
+        ref = T0.copy()
+        orc.solve(ref, h, k, F=F, a=a)
+        out, rep = gpu_solve(f3d, ctx, cuda, T0, h, k, engine=engine, med=f3d.medium(F, a))
+        assert_bitwise(out, ref, "%s %s %d sweeps" % (engine, dims, k))
+        assert rep.nominal_updates == k * 2 * ((dims[0] - 1) * dims[1] * dims[2] +
+                                               (dims[1] - 1) * dims[0] * dims[2] +
+                                               (dims[2] - 1) * dims[0] * dims[1])
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("case", CASES[:4], ids=lambda c: "x".join(map(str, c[0])) + c[4])
+def test_oracle_convergence(f3d, orc, ctx, cuda, case, engine):
+    """Run both to max|dT| == 0: same number of sweeps, same field."""
+    dims, h, F, a, src = case
+    T0 = make_case(f3d, orc, dims, h, F, a, src)
+    ref = T0.copy()
+    s_ref, d_ref = orc.solve(ref, h, 300, tol=0.0, F=F, a=a)
+    out, rep = gpu_solve(f3d, ctx, cuda, T0, h, 300, fixed=False, tol=0.0, engine=engine,
+                         med=f3d.medium(F, a))
+    assert d_ref == 0.0 and rep.max_delta == 0.0
+    assert rep.sweeps == s_ref
+    assert_bitwise(out, ref, "converged")
+
+
+def test_tolerance_stop_matches_oracle(f3d, orc, ctx, cuda):
+    n = 20
+    h = (ref_spacing(n),) * 3
+    T0 = orc.init_implicit(n, n, n, h)
+    ref = T0.copy()
+    s_ref, d_ref = orc.solve(ref, h, 300, tol=1e-3)
+    out, rep = gpu_solve(f3d, ctx, cuda, T0, h, 300, fixed=False, tol=1e-3)
+    assert rep.sweeps == s_ref and rep.max_delta == d_ref
+    assert_bitwise(out, ref, "tol stop")
+
+
+def test_host_path_equals_device_path(f3d, orc, ctx, cuda):
+    n = 24
+    h = (ref_spacing(n),) * 3
+    T0 = orc.init_implicit(n, n, n, h)
+    dev, _ = gpu_solve(f3d, ctx, cuda, T0, h, 4)
+    host = T0.copy()
+    rep = ctx.solve(host, h, None, f3d.opts(max_sweeps=4, fixed=True))
+    assert rep.sweeps == 4
+    assert_bitwise(host, dev, "host vs device")
+
+
+def test_plane_entry_point_matches_oracle(f3d, orc, cuda):
+    dims, h = (21, 14, 17), (0.5, 0.6, 0.7)
+    T0 = orc.init_implicit(*dims, h)
+    d = cuda.from_numpy(T0.copy()).cuda()
+    ref = T0.copy()
+    for dir_, src in ((0, 1), (0, 2), (1, 21), (2, 1), (3, 17), (4, 14), (5, 1), (5, 7)):
+        f3d.plane(d, h, dir_, src)
+        orc.plane(ref, h, dir_, src)
+    cuda.cuda.synchronize()
+    assert_bitwise(d.cpu().numpy(), ref, "plane steps")
+
+
+def test_reference_compatible_entry_points(f3d, golden, cuda):
+    """Drive the six function_* exactly as the reference's main does, on a
+    field allocated with the library's acc_malloc (which records the grid
+    size), and compare with the reference's own 8-sweep result."""
+    from oracle import _REF_CALLS, RefLib
+
+    n = 16
+    L = f3d.lib()
+    r = RefLib(n)  # only for the argument lists of the reference driver
+    T = golden[n]["init"].copy()
+    nbytes = T.nbytes
+    d = L.acc_malloc(nbytes)
+    assert d
+    try:
+        L.acc_memcpy_to_device(C.c_void_p(d), T.ctypes.data_as(C.c_void_p), nbytes)
+        for _ in range(8):
+            for entry in _REF_CALLS:
+                fn = getattr(L, entry[0])
+                args = r._args(entry)
+                planes = range(1, n) if entry[1] == "up" else range(n, 1, -1)
+                for p in planes:
+                    fn(C.c_void_p(d), p, *args)
+                assert f3d.last_error() == ""
+        out = np.empty_like(T)
+        L.acc_memcpy_from_device(out.ctypes.data_as(C.c_void_p), C.c_void_p(d), nbytes)
+    finally:
+        L.acc_free(C.c_void_p(d))
+    assert_bitwise(out, golden[n]["s8"], "function_* path")
+
+
+def test_compat_rejects_unknown_grid(f3d, cuda):
+    L = f3d.lib()
+    t = cuda.zeros(10 * 10 * 10, dtype=cuda.float64, device="cuda")
+    L.function_x_down(C.c_void_p(t.data_ptr()), 1, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+    assert "grid size unknown" in f3d.last_error()
+    assert L.fold3d_compat_set_grid(8, 8, 8) == f3d.OK
+    try:
+        L.function_x_down(C.c_void_p(t.data_ptr()), 1, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+        assert f3d.last_error() == ""
+        L.function_x_down(C.c_void_p(t.data_ptr()), 8, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+        assert "out of range" in f3d.last_error()
+    finally:
+        L.fold3d_compat_set_grid(0, 0, 0)
+
+
+def test_full_size_planes_512(f3d, orc, ctx, cuda):
+    """At the benchmark size (512^3, reference medium and source), the first
+    planes of every direction match the oracle bit for bit."""
+    n = 512
+    h = (ref_spacing(n),) * 3
+    T0 = f3d.init_implicit(n, n, n, h[0])
+    d = cuda.from_numpy(T0).cuda()
+    ref = T0.copy()
+    for dir_ in range(6):
+        first = 1 if dir_ in (0, 2, 5) else n
+        step = 1 if dir_ in (0, 2, 5) else -1
+        for p in range(3):
+            f3d.plane(d, h, dir_, first + step * p)
+            orc.plane(ref, h, dir_, first + step * p)
+    cuda.cuda.synchronize()
+    assert_bitwise(d.cpu().numpy(), ref, "512^3 planes")
+
+
+def test_full_size_properties_512(f3d, ctx, cuda):
+    """Size-independent properties at 512^3: deterministic (two runs equal
+    bit for bit), magnitudes never increase, signs never change."""
+    n = 512
+    h = (ref_spacing(n),) * 3
+    T0 = f3d.init_implicit(n, n, n, h[0])
+    a = cuda.from_numpy(T0).cuda()
+    b = a.clone()
+    o = f3d.opts(max_sweeps=2, fixed=True, engine=f3d.ENGINE_PLANES, skip=False)
+    ctx.solve(a, h, None, o)
+    ctx.solve(b, h, None, o)
+    assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+    t0 = cuda.from_numpy(T0).cuda()
+    assert bool((a.abs() <= t0.abs()).all())
+    assert bool(((a > 0) == (t0 > 0)).all())
