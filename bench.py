@@ -232,6 +232,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--prof-sweep", type=int, default=0,
+                    help="profiling aid: run sweeps 1..S-1, then sweep S inside a CUDA profiler range "
+                         "(for ncu --profile-from-start off), then exit")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -273,6 +276,24 @@ def main():
     def step():
         T_dev.copy_(T0_dev)
         return ctx.solve(T_dev, h, None, opts, stream=sp)
+
+    if args.prof_sweep > 0:
+        if args.prof_sweep > 1:
+            T_dev.copy_(T0_dev)
+            ctx.solve(T_dev, h, None, f3d.opts(max_sweeps=args.prof_sweep - 1, fixed=True, engine=engine,
+                                               skip=bool(args.skip)), stream=sp)
+        else:
+            T_dev.copy_(T0_dev)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        r1 = ctx.solve(T_dev, h, None, f3d.opts(max_sweeps=1, fixed=True, engine=engine, skip=bool(args.skip)),
+                       stream=sp)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"prof_sweep": args.prof_sweep, "sweep_ms": r1.elapsed_ms,
+                          "updates": r1.nominal_updates, "evaluated": r1.evaluated_updates}))
+        ctx.close()
+        return
 
     rep = None
     for _ in range(args.warmup):

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "fold3d_acc.h"
+#include "fold3d_fast.cuh"
 #include "fold3d_internal.h"
 
 namespace fold3d {
@@ -136,6 +137,7 @@ struct fold3d_ctx {
     double *key_T = nullptr;
     fold3d_grid key_g{};
     fold3d_medium key_m{};
+    int key_variant = -1;
     // buffer for fold3d_solve_host
     double *d_field = nullptr;
     size_t d_field_cells = 0;
@@ -171,6 +173,7 @@ void fold3d_default_opts(fold3d_opts *o)
     o->tol = 0.0;
     o->engine = FOLD3D_ENGINE_AUTO;
     o->skip = 1;
+    o->variant = 0;
 }
 
 int fold3d_create(fold3d_ctx **out, int device)
@@ -214,10 +217,11 @@ void fold3d_destroy(fold3d_ctx *c)
 }  // extern "C"
 
 // One sweep (max-delta reset + the 6 passes) captured into a graph.
-static int build_sweep_graph(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T)
+static int build_sweep_graph(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T,
+                             int variant)
 {
     if (c->sweep_exec && c->key_T == T && !memcmp(&c->key_g, &g, sizeof g) &&
-        !memcmp(&c->key_m, &m, sizeof m))
+        !memcmp(&c->key_m, &m, sizeof m) && c->key_variant == variant)
         return FOLD3D_OK;
     if (c->sweep_exec) {
         cudaGraphExecDestroy(c->sweep_exec);
@@ -229,9 +233,11 @@ static int build_sweep_graph(fold3d_ctx *c, const fold3d_grid &g, const fold3d_m
     for (int dir = 0; dir < 6 && le == cudaSuccess; ++dir) {
         const PlaneGeom pg = make_geom(g, dir);
         const LocalFrameH L = make_frame(g, m, dir);
+        DirTable tab;
+        build_dir_table(L, tab);
         int src = pass_first(pg, dir);
         for (int p = 0; p < pass_count(pg) && le == cudaSuccess; ++p, src += kDirs[dir].sg)
-            le = launch_plane(T, pg, L, src, c->d_maxd, c->stream);
+            le = launch_plane(T, pg, L, &tab, variant, src, c->d_maxd, c->stream);
     }
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(c->stream, &graph);
@@ -249,13 +255,14 @@ static int build_sweep_graph(fold3d_ctx *c, const fold3d_grid &g, const fold3d_m
     c->key_T = T;
     c->key_g = g;
     c->key_m = m;
+    c->key_variant = variant;
     return FOLD3D_OK;
 }
 
 static int solve_planes(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T,
                         const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
 {
-    int rc = build_sweep_graph(c, g, m, T);
+    int rc = build_sweep_graph(c, g, m, T, o.variant);
     if (rc) return rc;
     cudaError_t e;
     if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
@@ -306,6 +313,8 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
     if (o->engine < 0 || o->engine > FOLD3D_ENGINE_WAVEFRONT)
         return set_error(FOLD3D_ERR_INVALID, "unknown engine");
     if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (o->variant != kVariantFast && o->variant != kVariantLiteral)
+        return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     return solve_planes(c, *g, *m, T, *o, s, rep);
@@ -356,7 +365,10 @@ int fold3d_plane(const fold3d_grid *g, const fold3d_medium *m, double *T, int di
     const int tgt = src + kDirs[dir].sg;
     if (src < 1 || src > pg.nplanes || tgt < 1 || tgt > pg.nplanes)
         return set_error(FOLD3D_ERR_INVALID, "plane index out of range");
-    cudaError_t e = launch_plane(T, pg, make_frame(*g, *m, dir), src, nullptr, (cudaStream_t)stream);
+    const LocalFrameH L = make_frame(*g, *m, dir);
+    DirTable tab;
+    build_dir_table(L, tab);
+    cudaError_t e = launch_plane(T, pg, L, &tab, kVariantFast, src, nullptr, (cudaStream_t)stream);
     return e == cudaSuccess ? FOLD3D_OK : cuda_error(e, "plane launch");
 }
 
@@ -414,7 +426,9 @@ void compat_plane(int dir, double *T, int src, double dzz, double dxx, double dy
     // The caller's arguments are already in the direction's local frame
     // (the reference driver permutes them, AN_ISO_1_OpenACC.c:1198-1235).
     const LocalFrameH L = {F, ax, ay, az, dzz, dxx, dyy, dxy, dxz, dyz};
-    cudaError_t e = launch_plane(T, pg, L, src, nullptr, 0);
+    DirTable tab;
+    build_dir_table(L, tab);
+    cudaError_t e = launch_plane(T, pg, L, &tab, kVariantFast, src, nullptr, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) cuda_error(e, "function_*");
 }

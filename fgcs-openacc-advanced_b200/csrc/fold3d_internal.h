@@ -45,8 +45,19 @@ int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
 void clear_error();
 
-// Kernel launchers (fold3d_kernels.cu).
-cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, int src,
-                         unsigned long long *maxd, cudaStream_t s);
+struct DirTable;  // fold3d_fast.cuh
+
+// Per-direction solver constants, evaluated on the host (fold3d_tables.cpp).
+void build_dir_table(const LocalFrameH &L, DirTable &out);
+
+// Solver variants of the plane kernel.
+enum Variant {
+    kVariantFast = 0,     // host-folded constants (fold3d_fast.cuh), the default
+    kVariantLiteral = 1   // the reference's expressions point by point (fold3d_solver.cuh)
+};
+
+// Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
+cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,
+                         int variant, int src, unsigned long long *maxd, cudaStream_t s);
 
 }  // namespace fold3d

@@ -58,7 +58,10 @@ class Medium(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("max_sweeps", C.c_int), ("fixed", C.c_int), ("tol", C.c_double),
-                ("engine", C.c_int), ("skip", C.c_int)]
+                ("engine", C.c_int), ("skip", C.c_int), ("variant", C.c_int)]
+
+
+VARIANT_FAST, VARIANT_LITERAL = 0, 1
 
 
 class Report(C.Structure):
@@ -137,11 +140,12 @@ def medium(F=REF_F, a=REF_A) -> Medium:
     return Medium(float(F), float(a[0]), float(a[1]), float(a[2]))
 
 
-def opts(max_sweeps=1000, fixed=False, tol=0.0, engine=ENGINE_AUTO, skip=True) -> Opts:
+def opts(max_sweeps=1000, fixed=False, tol=0.0, engine=ENGINE_AUTO, skip=True, variant=VARIANT_FAST) -> Opts:
     o = Opts()
     lib().fold3d_default_opts(C.byref(o))
     o.max_sweeps, o.fixed, o.tol, o.engine, o.skip = int(max_sweeps), int(bool(fixed)), float(tol), \
         int(engine), int(bool(skip))
+    o.variant = int(variant)
     return o
 
 

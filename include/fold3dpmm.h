@@ -94,6 +94,9 @@ typedef struct {
     int skip;         /* non-zero: skip tiles whose inputs did not change since   */
                       /* their last update in that direction (result unchanged, */
                       /* bit for bit); wavefront engine only                     */
+    int variant;      /* local-solver form, same results bit for bit:            */
+                      /* 0 = per-direction constants folded on the host (fast),  */
+                      /* 1 = the reference's expressions point by point (check)  */
 } fold3d_opts;
 
 typedef struct {
@@ -118,7 +121,7 @@ const char *fold3d_last_error(void);
 const char *fold3d_version(void);
 
 /* Default options: fixed = 0, max_sweeps = 1000, tol = 0.0 (run until the
- * field stops changing), engine = AUTO, skip = 1. */
+ * field stops changing), engine = AUTO, skip = 1, variant = 0. */
 void fold3d_default_opts(fold3d_opts *o);
 
 /* Context: owns device scratch, graphs and events for one device.  One

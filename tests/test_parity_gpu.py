@@ -16,18 +16,22 @@ from oracle import REF_A, REF_F, ref_spacing
 
 pytestmark = pytest.mark.gpu
 
-ENGINES = ["planes"]
+ENGINES = ["planes", "planes-literal"]
 
 
-def engine_id(f3d, name):
-    return {"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT}[name]
+def engine_opts(f3d, name):
+    """'<engine>[-literal]': engine and solver variant."""
+    eng, _, var = name.partition("-")
+    return ({"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT}[eng],
+            f3d.VARIANT_LITERAL if var == "literal" else f3d.VARIANT_FAST)
 
 
 def gpu_solve(f3d, ctx, cuda, T, h, sweeps, *, fixed=True, tol=0.0, engine="planes", skip=False,
               med=None):
     d = cuda.from_numpy(T.copy()).cuda()
-    rep = ctx.solve(d, h, med, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol,
-                                         engine=engine_id(f3d, engine), skip=skip))
+    eng, var = engine_opts(f3d, engine)
+    rep = ctx.solve(d, h, med, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol, engine=eng, skip=skip,
+                                         variant=var))
     return d.cpu().numpy(), rep
 
 
@@ -230,3 +234,64 @@ def test_full_size_properties_512(f3d, ctx, cuda):
     t0 = cuda.from_numpy(T0).cuda()
     assert bool((a.abs() <= t0.abs()).all())
     assert bool(((a > 0) == (t0 > 0)).all())
+
+
+def test_variants_agree_full_size_512(f3d, ctx, cuda):
+    """At the benchmark size (512^3, 8 sweeps) the folded-constant solver and
+    the literal reference-expression solver give the same field bit for bit
+    (the literal one is pinned to the oracle by the tests above)."""
+    n = 512
+    h = (ref_spacing(n),) * 3
+    T0 = f3d.init_implicit(n, n, n, h[0])
+    a = cuda.from_numpy(T0).cuda()
+    b = a.clone()
+    ra = ctx.solve(a, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=f3d.ENGINE_PLANES,
+                                        variant=f3d.VARIANT_FAST))
+    rb = ctx.solve(b, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=f3d.ENGINE_PLANES,
+                                        variant=f3d.VARIANT_LITERAL))
+    assert ra.max_delta == rb.max_delta
+    assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+
+
+def test_division_by_constant_matches_ieee(f3d, cuda):
+    """div_by_const (Markstein's method, fold3d_fast.cuh) against CUDA's IEEE
+    division, bit for bit: the divisors of every solver table of several
+    media and grids, and random divisors, over quotient operands spanning
+    the safe range, zeros and out-of-range values."""
+    import os
+    import subprocess
+
+    from conftest import PKG, ROOT
+
+    so = os.path.join(ROOT, "tests", "_build", "libdivcheck.so")
+    src = os.path.join(ROOT, "tests", "csrc", "divcheck.cu")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        os.makedirs(os.path.dirname(so), exist_ok=True)
+        subprocess.run(["nvcc", "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "--fmad=false",
+                        "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(PKG, "csrc"), "-I",
+                        os.path.join(ROOT, "include"), "-o", so, src], check=True)
+    L = C.CDLL(so)
+    L.divcheck.argtypes = [C.c_void_p] * 3 + [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(11)
+    cs = [0.0196, 0.00391389432485323, 10.0 / 511, 1.21 - 0.16, 1.21 - 0.49, 0.5649, 1.0, 3.0, 0.7, 2.5e-7,
+          1e5, 1.0 / 3.0, np.sqrt(2.0) * 0.0196]
+    cs += list(rng.uniform(0.01, 10.0, 40)) + list(-rng.uniform(0.01, 10.0, 8))
+    cs += list(2.0 ** rng.uniform(-390, 390, 16))
+    c = np.array(cs, dtype=np.float64)
+    r = 1.0 / c
+    n = 1 << 25
+    mant = rng.uniform(1.0, 2.0, n)
+    ex = rng.integers(-60, 61, n)
+    x = np.ldexp(mant, ex) * rng.choice([-1.0, 1.0], n)
+    x[: n // 8] = np.ldexp(mant[: n // 8], rng.integers(-420, 421, n // 8))  # edges of the safe range
+    x[::997] = 0.0
+    x[1::1009] = 1e16 - x[1::1009]
+    dx = cuda.from_numpy(x).cuda()
+    dc = cuda.from_numpy(c).cuda()
+    dr = cuda.from_numpy(r).cuda()
+    mm = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    first = cuda.zeros(1, dtype=cuda.int64, device="cuda")
+    assert L.divcheck(dx.data_ptr(), dc.data_ptr(), dr.data_ptr(), n, len(c), mm.data_ptr(),
+                      first.data_ptr()) == 0
+    i = int(first.item())
+    assert int(mm.item()) == 0, "x=%r c=%r" % (x[i], c[i % len(c)])
