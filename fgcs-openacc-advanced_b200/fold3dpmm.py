@@ -33,7 +33,7 @@ REF_A = (-0.35, 0.4, 0.7)
 EXPORTED = (
     "fold3d_last_error", "fold3d_version", "fold3d_default_opts", "fold3d_create", "fold3d_destroy",
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
-    "fold3d_exact_time", "fold3d_compat_set_grid",
+    "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -95,6 +95,7 @@ def lib() -> C.CDLL:
     L.fold3d_solve.argtypes = [vp, P(Grid), P(Medium), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_host.argtypes = [vp, P(Grid), P(Medium), vp, vp, P(Opts), vp, P(Report)]
     L.fold3d_plane.argtypes = [P(Grid), P(Medium), vp, i, i, vp]
+    L.fold3d_solve_noalloc.argtypes = [P(Grid), P(Medium), vp, P(Opts), vp, P(Report)]
     L.fold3d_init_implicit.argtypes = [vp, P(Grid), P(Medium)]
     L.fold3d_init_point.argtypes = [vp, P(Grid), i, i, i]
     L.fold3d_exact_time.argtypes = [P(Medium), d, d, d]
@@ -241,6 +242,20 @@ class Context:
             _check(lib().fold3d_solve(self._h, C.byref(g), C.byref(med), _dev_ptr(T), C.byref(o), s,
                                       C.byref(rep)))
         return rep
+
+
+NOALLOC_MAX_SWEEPS = 4096
+
+
+def solve_noalloc(T, h, med: Medium | None = None, o: Opts | None = None, stream=None) -> Report:
+    """fold3d_solve_noalloc on a float64 CUDA tensor, in place: the solve
+    entry point that allocates no memory (see include/fold3dpmm.h)."""
+    nx, ny, nz = grid_of(T)
+    rep = Report()
+    _check(lib().fold3d_solve_noalloc(C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()), _dev_ptr(T),
+                                      C.byref(o or opts()), C.c_void_p(stream) if stream else None,
+                                      C.byref(rep)))
+    return rep
 
 
 def plane(T, h, dir_, src, med: Medium | None = None, stream=None):

@@ -161,6 +161,29 @@ int fold3d_init_point(double *T_host, const fold3d_grid *g, int si, int sj, int 
  * FOLD3D_MAXT where undefined (InitFoldFromPoint, Fold3dPMM.c:9-26). */
 double fold3d_exact_time(const fold3d_medium *m, double x, double y, double z);
 
+/* Whole solve that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that must not have device memory allocated for them: host
+ * programs whose device buffers all come from another runtime (an OpenACC
+ * driver using acc_malloc, a framework whose caching allocator already holds
+ * the GPU's memory) or plugin hosts that lend buffers and budget every byte.
+ * It runs the same per-plane kernels as fold3d_solve (engine and skip are
+ * ignored), needs no context, and calls no cudaMalloc, cudaFree or other
+ * allocating routine.  The caller passes the device field T_dev (in/out).
+ *
+ * Scratch: a static device array of FOLD3D_NOALLOC_MAX_SWEEPS 8-byte slots
+ * (32 KiB), one per sweep, that every GPU which loads the library holds until
+ * the process exits; calls with max_sweeps above that limit are rejected with
+ * FOLD3D_ERR_INVALID.  All calls share the array and it keeps the previous
+ * call's values: each sweep clears its own slot first, and calls whose work
+ * overlaps on the GPU race on it.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  Synchronous like
+ * fold3d_solve; rep->elapsed_ms is the call's host wall time. */
+#define FOLD3D_NOALLOC_MAX_SWEEPS 4096
+int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T_dev,
+                         const fold3d_opts *o, void *stream, fold3d_report *rep);
+
 /* Grid size the reference-compatible sweep functions assume for a device
  * field (they have no size argument, AN_ISO_1_OpenACC.c:180).  If never set,
  * the size is taken from the allocation made by this library's acc_malloc. */
