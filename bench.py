@@ -213,7 +213,7 @@ def run_reference(args):
 def workload_config(args):
     return {"workload": "fold-ref %d^3 implicit-surface source, %d sweeps" % (args.size, args.sweeps),
             "grid": args.size, "sweeps": args.sweeps, "medium": "F=1.1 a=(-0.35,0.4,0.7)",
-            "spacing": "h=10/(n-1)", "engine": args.engine, "skip": bool(args.skip),
+            "spacing": "h=10/(n-1)", "engine": args.engine, "skip": bool(args.skip), "variant": args.variant,
             "l2": "field %.2f GB > 126 MB L2; no flush needed" % ((args.size + 2) ** 3 * 8 / 1e9),
             "parallelism": "replicas" if args.gpus > 1 else "single"}
 
@@ -228,6 +228,8 @@ def main():
     ap.add_argument("--sweeps", type=int, default=8)
     ap.add_argument("--engine", choices=["planes", "wavefront", "auto"], default="auto")
     ap.add_argument("--skip", type=int, default=0, help="tile skipping (bit-exact); 0 = evaluate every update")
+    ap.add_argument("--variant", choices=["fast", "literal", "compact"], default="fast",
+                    help="local-solver form (identical results)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=4.0)
@@ -260,7 +262,8 @@ def main():
     n, sweeps = args.size, args.sweeps
     h = 10.0 / (n - 1.0)
     engine = {"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT, "auto": f3d.ENGINE_AUTO}[args.engine]
-    opts = f3d.opts(max_sweeps=sweeps, fixed=True, engine=engine, skip=bool(args.skip))
+    variant = {"fast": f3d.VARIANT_FAST, "literal": f3d.VARIANT_LITERAL, "compact": f3d.VARIANT_COMPACT}[args.variant]
+    opts = f3d.opts(max_sweeps=sweeps, fixed=True, engine=engine, skip=bool(args.skip), variant=variant)
 
     t0 = time.perf_counter()
     T0_host = f3d.init_implicit(n, n, n, h)
@@ -281,13 +284,13 @@ def main():
         if args.prof_sweep > 1:
             T_dev.copy_(T0_dev)
             ctx.solve(T_dev, h, None, f3d.opts(max_sweeps=args.prof_sweep - 1, fixed=True, engine=engine,
-                                               skip=bool(args.skip)), stream=sp)
+                                               skip=bool(args.skip), variant=variant), stream=sp)
         else:
             T_dev.copy_(T0_dev)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
-        r1 = ctx.solve(T_dev, h, None, f3d.opts(max_sweeps=1, fixed=True, engine=engine, skip=bool(args.skip)),
-                       stream=sp)
+        r1 = ctx.solve(T_dev, h, None, f3d.opts(max_sweeps=1, fixed=True, engine=engine, skip=bool(args.skip),
+                                                variant=variant), stream=sp)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
         print(json.dumps({"prof_sweep": args.prof_sweep, "sweep_ms": r1.elapsed_ms,

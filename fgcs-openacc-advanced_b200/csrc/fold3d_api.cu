@@ -313,7 +313,7 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
     if (o->engine < 0 || o->engine > FOLD3D_ENGINE_WAVEFRONT)
         return set_error(FOLD3D_ERR_INVALID, "unknown engine");
     if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (o->variant != kVariantFast && o->variant != kVariantLiteral)
+    if (o->variant != kVariantFast && o->variant != kVariantLiteral && o->variant != kVariantCompact)
         return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;

@@ -67,7 +67,10 @@ struct SideTable {
     double g, rg;       // F*F - az*az, RN(1/g)          (:147)
     double K1;          // 1-D candidate increment dzz*dzz/q (:225)
     int d1_ok;          // 1-D candidate defined (:219, :223)
-    int pad_;
+    // the per-call flags below as bit masks, bit k for call k
+    unsigned m_e1, m_e2, m_nblock;  // surf[k].e1, .e2, .nblock
+    unsigned m_nest_early;          // surf[k].nest.early
+    unsigned m_edge_early;          // edge[k].early
     SurfK surf[8];      // the eight FoldSurf3Points calls (:233-240), in order
     EdgeK edge[8];      // the eight FoldEdge2Points calls (:242-253), in order
 };
@@ -170,6 +173,56 @@ __device__ __forceinline__ double point_update_fast(double told, double st, doub
         }
     }
     return ((told > 0) ? 1.0 : -1.0) * tn;
+}
+
+// ---------------------------------------------------------------------------
+// Candidate values for the compacted kernel.  Each function returns the
+// smallest candidate its reference call would accept when entered with the
+// current time `th` -- or +infinity -- instead of updating a running time.
+// Every value returned is below th, so folding them with min gives the same
+// result as the reference's sequence of calls (see the header comment).  The
+// caller has already applied the call's entry gates.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double edge_cand(double th, double s0, double s1, const EdgeK &k, double F)
+{
+    double best = th;
+    const double d = div_by_const(s1 - s0, k.hx, k.rhx);
+    double c = (1.0 - d * k.ax);
+    double q = k.g * (c * c - d * d * k.ga);
+    if (0.0 < q) {
+        c = div_by_const(-k.az * c + sqrt(q), k.ga, k.rga);
+        q = s0 + k.hz * c;
+        if (q < best && q > kmin(s0, s1)) {
+            const double g = sqrt(div_by_const((d * d + c * c) * F * F, k.g, k.rg));
+            const double xe = -k.hz * (d + k.ax * g) / (c + k.az * g);
+            if (0.0 < xe && xe < k.hx) best = q;
+        }
+    }
+    if (best > s1 && k.fb_ok) best = kmin(best, s1 + k.K);
+    return best;
+}
+
+__device__ __forceinline__ double surf_cand(double th, double s0, double s1, double s2, const SurfK &k,
+                                            const SideTable &t)
+{
+    double best = th;
+    const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
+    const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
+    double dd = dx * dx + dy * dy;
+    double al = 1.0 - k.ax * dx - k.ay * dy;
+    double q = al * al - dd * t.g;
+    if (q > 0.0) {
+        al = div_by_const(-t.az * al + t.F * sqrt(q), t.g, t.rg);
+        const double g = s0 + t.hz * al;
+        if (g < best && g > kmin(kmin(s0, s1), s2)) {
+            q = sqrt(dd + al * al);
+            dd = -t.hz / (t.F * al + t.az * q);
+            const double xe = dd * (t.F * dx + k.ax * q);
+            const double ye = dd * (t.F * dy + k.ay * q);
+            if (0.0 <= kmin(xe, ye) && ye * k.hx <= xe * k.hy && xe <= k.hx) best = g;
+        }
+    }
+    return best;
 }
 #endif  // __CUDACC__
 

@@ -53,7 +53,8 @@ void build_dir_table(const LocalFrameH &L, DirTable &out);
 // Solver variants of the plane kernel.
 enum Variant {
     kVariantFast = 0,     // host-folded constants (fold3d_fast.cuh), the default
-    kVariantLiteral = 1   // the reference's expressions point by point (fold3d_solver.cuh)
+    kVariantLiteral = 1,  // the reference's expressions point by point (fold3d_solver.cuh)
+    kVariantCompact = 2   // host-folded constants, solver calls compacted across the block
 };
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.

@@ -71,7 +71,7 @@ extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m
                          "fold3d_solve_noalloc: max_sweeps exceeds FOLD3D_NOALLOC_MAX_SWEEPS (4096), the size of "
                          "its static per-sweep scratch; use fold3d_solve for longer solves");
     if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (o->variant != kVariantFast && o->variant != kVariantLiteral)
+    if (o->variant != kVariantFast && o->variant != kVariantLiteral && o->variant != kVariantCompact)
         return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -122,6 +122,14 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
     t.edge[5] = edge_consts(F, -(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz);
     t.edge[6] = edge_consts(F, -ay, ax, az, hy, hz);
     t.edge[7] = edge_consts(F, (ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz);
+    t.m_e1 = t.m_e2 = t.m_nblock = t.m_nest_early = t.m_edge_early = 0;
+    for (int k = 0; k < 8; ++k) {
+        t.m_e1 |= (unsigned)(t.surf[k].e1 != 0) << k;
+        t.m_e2 |= (unsigned)(t.surf[k].e2 != 0) << k;
+        t.m_nblock |= (unsigned)(t.surf[k].nblock != 0) << k;
+        t.m_nest_early |= (unsigned)(t.surf[k].nest.early != 0) << k;
+        t.m_edge_early |= (unsigned)(t.edge[k].early != 0) << k;
+    }
 }
 
 }  // namespace

@@ -61,7 +61,7 @@ class Opts(C.Structure):
                 ("engine", C.c_int), ("skip", C.c_int), ("variant", C.c_int)]
 
 
-VARIANT_FAST, VARIANT_LITERAL = 0, 1
+VARIANT_FAST, VARIANT_LITERAL, VARIANT_COMPACT = 0, 1, 2
 
 
 class Report(C.Structure):

@@ -96,7 +96,8 @@ typedef struct {
                       /* bit for bit); wavefront engine only                     */
     int variant;      /* local-solver form, same results bit for bit:            */
                       /* 0 = per-direction constants folded on the host (fast),  */
-                      /* 1 = the reference's expressions point by point (check)  */
+                      /* 1 = the reference's expressions point by point (check), */
+                      /* 2 = folded constants, calls compacted across the block  */
 } fold3d_opts;
 
 typedef struct {

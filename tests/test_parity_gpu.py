@@ -16,14 +16,14 @@ from oracle import REF_A, REF_F, ref_spacing
 
 pytestmark = pytest.mark.gpu
 
-ENGINES = ["planes", "planes-literal"]
+ENGINES = ["planes", "planes-literal", "planes-compact"]
 
 
 def engine_opts(f3d, name):
     """'<engine>[-literal]': engine and solver variant."""
     eng, _, var = name.partition("-")
     return ({"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT}[eng],
-            f3d.VARIANT_LITERAL if var == "literal" else f3d.VARIANT_FAST)
+            {"": f3d.VARIANT_FAST, "literal": f3d.VARIANT_LITERAL, "compact": f3d.VARIANT_COMPACT}[var])
 
 
 def gpu_solve(f3d, ctx, cuda, T, h, sweeps, *, fixed=True, tol=0.0, engine="planes", skip=False,
@@ -251,6 +251,11 @@ def test_variants_agree_full_size_512(f3d, ctx, cuda):
                                         variant=f3d.VARIANT_LITERAL))
     assert ra.max_delta == rb.max_delta
     assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+    c = cuda.from_numpy(T0).cuda()
+    rc = ctx.solve(c, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=f3d.ENGINE_PLANES,
+                                        variant=f3d.VARIANT_COMPACT))
+    assert rc.max_delta == ra.max_delta
+    assert cuda.equal(a.view(cuda.int64), c.view(cuda.int64))
 
 
 def test_division_by_constant_matches_ieee(f3d, cuda):
