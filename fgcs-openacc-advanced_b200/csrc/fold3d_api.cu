@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -141,6 +142,14 @@ struct fold3d_ctx {
     // buffer for fold3d_solve_host
     double *d_field = nullptr;
     size_t d_field_cells = 0;
+    // WAVEFRONT engine scratch, sized for the grid of key_wg
+    fold3d_grid key_wg{};
+    unsigned *w_flags = nullptr;
+    unsigned *w_mod[3] = {nullptr, nullptr, nullptr};
+    unsigned *w_counters = nullptr;          // [0] work, [1] status
+    unsigned long long *w_evaluated = nullptr;
+    unsigned epoch = 0;                      // passes run so far on this context
+    int sms = 0, wave_bps = 0;
 };
 
 namespace {
@@ -206,6 +215,11 @@ void fold3d_destroy(fold3d_ctx *c)
     DeviceGuard dg(c->device);
     if (c->sweep_exec) cudaGraphExecDestroy(c->sweep_exec);
     if (c->d_field) cudaFree(c->d_field);
+    if (c->w_flags) cudaFree(c->w_flags);
+    for (int b = 0; b < 3; ++b)
+        if (c->w_mod[b]) cudaFree(c->w_mod[b]);
+    if (c->w_counters) cudaFree(c->w_counters);
+    if (c->w_evaluated) cudaFree(c->w_evaluated);
     if (c->d_maxd) cudaFree(c->d_maxd);
     if (c->h_maxd) cudaFreeHost(c->h_maxd);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -297,6 +311,140 @@ static int solve_planes(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium
     return FOLD3D_OK;
 }
 
+// Tiles (32 x 8) per plane of the orientation with normal axis b.
+static void orient_tiles(const fold3d_grid &g, int b, int &ntu, int &ntv)
+{
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
+    ntu = (n[ub] + 31) / 32;
+    ntv = (n[vb] + 7) / 8;
+}
+
+static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
+{
+    if (c->w_flags && c->key_wg.nx == g.nx && c->key_wg.ny == g.ny && c->key_wg.nz == g.nz) return FOLD3D_OK;
+    if (c->w_flags) cudaFree(c->w_flags);
+    for (int b = 0; b < 3; ++b) {
+        if (c->w_mod[b]) cudaFree(c->w_mod[b]);
+        c->w_mod[b] = nullptr;
+    }
+    c->w_flags = nullptr;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    size_t flag_words = 0;
+    cudaError_t e;
+    for (int b = 0; b < 3; ++b) {
+        int ntu, ntv;
+        orient_tiles(g, b, ntu, ntv);
+        flag_words = std::max(flag_words, (size_t)(n[b] - 1) * ntu * ntv);
+        const size_t words = (size_t)(n[b] + 2) * ntu * ntv;
+        if ((e = cudaMalloc(&c->w_mod[b], words * 4)) != cudaSuccess ||
+            (e = cudaMemset(c->w_mod[b], 0, words * 4)) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+    }
+    if ((e = cudaMalloc(&c->w_flags, flag_words * 4)) != cudaSuccess ||
+        (e = cudaMemset(c->w_flags, 0, flag_words * 4)) != cudaSuccess)
+        return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+    if (!c->w_counters) {
+        if ((e = cudaMalloc(&c->w_counters, 2 * sizeof(unsigned))) != cudaSuccess ||
+            (e = cudaMalloc(&c->w_evaluated, sizeof(unsigned long long))) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+    }
+    if (!c->sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
+        c->wave_bps = wave_blocks_per_sm();
+    }
+    c->epoch = 0;  // fresh flags and maps
+    c->key_wg = g;
+    return FOLD3D_OK;
+}
+
+static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T,
+                           const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
+{
+    int rc = wave_scratch(c, g);
+    if (rc) return rc;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(c->w_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->w_evaluated, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+        return cuda_error(e, "cudaMemsetAsync");
+    WaveArgs a;
+    memset(&a, 0, sizeof a);
+    for (int b = 0; b < 3; ++b) {
+        int ntu, ntv;
+        orient_tiles(g, b, ntu, ntv);
+        a.mod[b] = c->w_mod[b];
+        a.mod_ntu[b] = ntu;
+        a.mod_ntiles[b] = ntu * ntv;
+    }
+    a.flags = c->w_flags;
+    a.work = c->w_counters;
+    a.status = c->w_counters + 1;
+    a.maxd = c->d_maxd;
+    a.evaluated = c->w_evaluated;
+    a.timeout_ns = 4000000000ull;
+    const unsigned e0 = c->epoch + 1;
+    a.skip_from = o.skip ? e0 + 6 : 0xffffffffu;
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    int sweeps = 0;
+    double delta = 0.0;
+    unsigned hstat[2] = {0, 0};
+    DirTable tab;
+    while (sweeps < o.max_sweeps) {
+        if ((e = cudaMemsetAsync(c->d_maxd, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+            return cuda_error(e, "cudaMemsetAsync");
+        for (int dir = 0; dir < 6; ++dir) {
+            const DirSpec &d = kDirs[dir];
+            a.pg = make_geom(g, dir);
+            a.nrm = d.nrm;
+            a.ua = (d.nrm == 0) ? 1 : 0;
+            a.va = (d.nrm == 2) ? 1 : 2;
+            a.sg = d.sg;
+            orient_tiles(g, d.nrm, a.ntu, a.ntv);
+            a.steps = pass_count(a.pg);
+            a.first_src = pass_first(a.pg, dir);
+            a.epoch = ++c->epoch;
+            build_dir_table(make_frame(g, m, dir), tab);
+            const long long items = (long long)a.steps * a.ntu * a.ntv;
+            const int grid = (int)std::min<long long>(items, (long long)c->sms * c->wave_bps);
+            if ((e = cudaMemsetAsync(a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
+                return cuda_error(e, "cudaMemsetAsync");
+            if ((e = launch_wave_pass(T, a, tab, grid, s)) != cudaSuccess) return cuda_error(e, "wavefront pass");
+        }
+        ++sweeps;
+        if (!o.fixed) {
+            if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(hstat, c->w_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+                return cuda_error(e, "cudaMemcpyAsync");
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "sweep");
+            if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "wavefront: a dependency wait gave up");
+            memcpy(&delta, c->h_maxd, 8);
+            if (delta <= o.tol) break;
+        }
+    }
+    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    unsigned long long evald = 0;
+    if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hstat, c->w_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&evald, c->w_evaluated, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_error(e, "cudaMemcpyAsync");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "solve");
+    if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "wavefront: a dependency wait gave up");
+    memcpy(&delta, c->h_maxd, 8);
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        rep->sweeps = sweeps;
+        rep->max_delta = delta;
+        rep->elapsed_ms = ms;
+        rep->nominal_updates = nominal_per_sweep(g) * (uint64_t)sweeps;
+        rep->evaluated_updates = evald;
+        rep->engine = FOLD3D_ENGINE_WAVEFRONT;
+    }
+    return FOLD3D_OK;
+}
+
 extern "C" {
 
 int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
@@ -317,7 +465,73 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
         return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if (o->engine == FOLD3D_ENGINE_WAVEFRONT) {
+        if (o->variant != kVariantFast)
+            return set_error(FOLD3D_ERR_UNSUPPORTED, "the wavefront engine runs the default solver variant only");
+        return solve_wavefront(c, *g, *m, T, *o, s, rep);
+    }
     return solve_planes(c, *g, *m, T, *o, s, rep);
+}
+
+int fold3d_selftest_wait_timeout(fold3d_ctx *c, double timeout_ms)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (!(timeout_ms > 0 && timeout_ms < 1000)) return set_error(FOLD3D_ERR_INVALID, "timeout_ms in (0, 1000)");
+    DeviceGuard dg(c->device);
+    const fold3d_grid g = {16, 16, 16, 1.0, 1.0, 1.0};
+    const fold3d_medium m = {1.1, -0.35, 0.4, 0.7};
+    int rc = wave_scratch(c, g);
+    if (rc) return rc;
+    cudaError_t e;
+    const size_t cells = field_cells(g);
+    if (c->d_field_cells < cells) {
+        if (c->d_field) cudaFree(c->d_field);
+        c->d_field = nullptr;
+        c->d_field_cells = 0;
+        c->key_T = nullptr;
+        if ((e = cudaMalloc(&c->d_field, cells * sizeof(double))) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "cudaMalloc");
+        c->d_field_cells = cells;
+    }
+    cudaStream_t s = c->stream;
+    WaveArgs a;
+    memset(&a, 0, sizeof a);
+    for (int b = 0; b < 3; ++b) {
+        int ntu, ntv;
+        orient_tiles(g, b, ntu, ntv);
+        a.mod[b] = c->w_mod[b];
+        a.mod_ntu[b] = ntu;
+        a.mod_ntiles[b] = ntu * ntv;
+    }
+    a.flags = c->w_flags;
+    a.work = c->w_counters;
+    a.status = c->w_counters + 1;
+    a.maxd = c->d_maxd;
+    a.evaluated = c->w_evaluated;
+    a.timeout_ns = (unsigned long long)(timeout_ms * 1e6);
+    a.skip_from = 0xffffffffu;
+    a.pg = make_geom(g, FOLD3D_K_UP);
+    a.nrm = 2;
+    a.ua = 0;
+    a.va = 1;
+    a.sg = 1;
+    orient_tiles(g, 2, a.ntu, a.ntv);
+    a.steps = pass_count(a.pg);
+    a.first_src = 1;
+    a.epoch = ++c->epoch;
+    DirTable tab;
+    build_dir_table(make_frame(g, m, FOLD3D_K_UP), tab);
+    // start the item counter after step 0: step 1 then waits for flags nothing sets
+    const unsigned start[2] = {(unsigned)(a.ntu * a.ntv), 0u};
+    unsigned hstat[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(c->w_counters, start, sizeof start, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = launch_wave_pass(c->d_field, a, tab, 4, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hstat, c->w_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_error(e, "selftest");
+    if (hstat[1] == 1) return set_error(FOLD3D_ERR_TIMEOUT, "wavefront: a dependency wait gave up (as intended)");
+    return set_error(FOLD3D_ERR_CUDA, "selftest: the waits did not give up");
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,
@@ -446,6 +660,16 @@ int fold3d_compat_set_grid(int nx, int ny, int nz)
     g_compat_n[1] = ny;
     g_compat_n[2] = nz;
     return FOLD3D_OK;
+}
+
+void fold3d_compat_plane(int dir, double *T, int p, double dzz, double dxx, double dyy, double dxy, double dxz,
+                         double dyz, double F, double ay, double ax, double az)
+{
+    if (dir < 0 || dir > 5) {
+        set_error(FOLD3D_ERR_INVALID, "fold3d_compat_plane: dir must be 0..5");
+        return;
+    }
+    compat_plane(dir, T, p, dzz, dxx, dyy, dxy, dxz, dyz, F, ay, ax, az);
 }
 
 #define FOLD3D_COMPAT(name, dir)                                                                    \

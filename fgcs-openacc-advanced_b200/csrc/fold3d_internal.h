@@ -57,6 +57,26 @@ enum Variant {
     kVariantCompact = 2   // host-folded constants, solver calls compacted across the block
 };
 
+// Arguments of one WAVEFRONT pass (fold3d_wavefront.cu).
+struct WaveArgs {
+    PlaneGeom pg;
+    int nrm, ua, va, sg;         // normal axis, in-plane u / v axes, step direction
+    int ntu, ntv;                // 32 x 8 tiles per plane (this orientation)
+    int steps, first_src;        // plane steps of the pass and the first source plane
+    unsigned epoch;              // number of this pass (monotonic per context)
+    unsigned skip_from;          // passes numbered below this never skip
+    unsigned long long timeout_ns;
+    unsigned *flags;             // [steps][tiles]: pass number when the item finished
+    unsigned *mod[3];            // per orientation: [plane 0..n+1][tile]: last pass a point changed
+    int mod_ntu[3], mod_ntiles[3];
+    unsigned *work;              // item counter (zeroed before each pass)
+    unsigned *status;            // 0, or 1 after a wait gave up
+    unsigned long long *maxd;    // max |dT| (IEEE bits) of the sweep
+    unsigned long long *evaluated;  // points evaluated
+};
+cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s);
+int wave_blocks_per_sm();
+
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,
                          int variant, int src, unsigned long long *maxd, cudaStream_t s);

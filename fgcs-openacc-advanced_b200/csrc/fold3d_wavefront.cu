@@ -1,0 +1,213 @@
+// fold3d_wavefront.cu -- the WAVEFRONT engine: one persistent launch per
+// directional pass, tile dataflow between consecutive planes, and tiles
+// skipped when their inputs did not change.
+//
+// Work items are (plane step p, tile t) pairs of a pass, tiles being 32 x 8
+// points of a plane, numbered plane-major.  Every CTA claims the next item
+// from an atomic counter.  Item (p, t) reads the source plane written by
+// step p-1 only within t's 1-point halo, i.e. from the 3 x 3 tiles around t,
+// so it waits for exactly those items (their completion flags), not for the
+// whole previous plane: consecutive planes overlap and no plane-wide barrier
+// or launch separates them.  Items are claimed in increasing order, so every
+// item an item waits for is held by a CTA that is already running; the
+// waits always end.  They are bounded anyway: after a time limit the CTA
+// raises the status word and every CTA leaves (FOLD3D_ERR_TIMEOUT).
+//
+// Skipping.  A point update is min(T_old, M(nine source values, side)) (see
+// fold3d_fast.cuh), so re-evaluating a tile whose source neighbourhood has
+// not changed since its previous evaluation in the same direction leaves
+// every target value unchanged, bit for bit.  Each orientation (plane normal
+// x, y or z) keeps a map with, per plane and tile, the last pass in which any
+// of its points changed; a pass writes the maps of all three orientations for
+// the points it changes.  From the second sweep of a solve on, item (p, t)
+// of pass e is skipped when no tile of the 3 x 3 neighbourhood of its source
+// plane changed in passes e-5 .. e (the previous evaluation of that tile in
+// this direction was in pass e-6, after the source plane's update of that
+// pass).
+//
+// Synchronisation: a CTA publishes an item with __syncthreads, a gpu-scope
+// fence and a release store of the pass number into the item's flag; a
+// waiting CTA's thread 0 polls with acquire loads and then releases its block
+// with __syncthreads.  Field values written inside the launch are read with
+// L2-cached loads (ld.global.cg), never through the non-coherent read-only
+// path.
+#include <cstring>
+
+#include "fold3d_fast.cuh"
+#include "fold3d_internal.h"
+
+namespace fold3d {
+
+namespace {
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
+
+}  // namespace
+
+__global__ void __launch_bounds__(256) wave_pass_kernel(double *__restrict__ T, WaveArgs a,
+                                                        const __grid_constant__ DirTable tab)
+{
+    __shared__ int s_item;
+    __shared__ int s_skip;
+    __shared__ double wmax[8];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const PlaneGeom &g = a.pg;
+    const int ntiles = a.ntu * a.ntv;
+    const long long total = (long long)a.steps * ntiles;
+    double dmax = 0.0;
+    unsigned long long evaluated = 0;
+
+    for (;;) {
+        if (tid == 0) {
+            int it = -1;
+            if (*(volatile unsigned *)a.status == 0) {
+                const unsigned w = atomicAdd(a.work, 1u);
+                if (w < total) it = (int)w;
+            }
+            s_item = it;
+        }
+        __syncthreads();
+        const int item = s_item;
+        if (item < 0) break;
+        const int p = item / ntiles, t = item - p * ntiles;
+        const int tu = t % a.ntu, tv = t / a.ntu;
+        const int src = a.first_src + p * a.sg;
+        const int tgt = src + a.sg;
+
+        // wait for the 3 x 3 tiles of step p-1 (they wrote this step's source plane)
+        if (tid == 0) {
+            int ok = 1;
+            if (p > 0) {
+                const unsigned *f = a.flags + (long long)(p - 1) * ntiles;
+                const unsigned long long t0 = global_ns();
+                for (int dv = -1; dv <= 1 && ok; ++dv)
+                    for (int du = -1; du <= 1 && ok; ++du) {
+                        const int nu = tu + du, nv = tv + dv;
+                        if (nu < 0 || nu >= a.ntu || nv < 0 || nv >= a.ntv) continue;
+                        const unsigned *fl = f + nv * a.ntu + nu;
+                        unsigned spins = 0;
+                        while (ld_acquire(fl) < a.epoch) {
+                            if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
+                                *(volatile unsigned *)a.status != 0) {
+                                atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                                ok = 0;
+                                break;
+                            }
+                            __nanosleep(64);
+                        }
+                    }
+            }
+            int skip = 0;
+            if (ok && a.epoch >= a.skip_from) {
+                // changed in passes epoch-5 .. epoch anywhere in the source neighbourhood?
+                const unsigned *m = a.mod[a.nrm] + (long long)src * ntiles;
+                unsigned last = 0;
+                for (int dv = -1; dv <= 1; ++dv)
+                    for (int du = -1; du <= 1; ++du) {
+                        const int nu = tu + du, nv = tv + dv;
+                        if (nu < 0 || nu >= a.ntu || nv < 0 || nv >= a.ntv) continue;
+                        last = max(last, __ldcg(m + nv * a.ntu + nu));
+                    }
+                skip = (last + 5u < a.epoch);
+            }
+            s_skip = ok ? skip : -1;
+        }
+        __syncthreads();
+        const int skip = s_skip;
+        if (skip < 0) break;  // timed out: leave without publishing
+
+        if (!skip) {
+            const int u = tu * 32 + lane + 1;
+            const int v = tv * 8 + warp + 1;
+            int changed = 0;
+            if (u <= g.nu && v <= g.nv) {
+                const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
+                const long long d = s + g.sn;
+                const double st = fabs(ld_cg(T + s));
+                const double xt = fabs(ld_cg(T + s + g.sx));
+                const double yt = fabs(ld_cg(T + s + g.sy));
+                const double xnt = fabs(ld_cg(T + s - g.sx));
+                const double ynt = fabs(ld_cg(T + s - g.sy));
+                const double txm = fabs(ld_cg(T + s + g.sx - g.sy));
+                const double txy = fabs(ld_cg(T + s + g.sx + g.sy));
+                const double tym = fabs(ld_cg(T + s - g.sx + g.sy));
+                const double txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
+                const double told = ld_cg(T + d);
+                const double tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
+                    T[d] = tnew;
+                    changed = 1;
+                    dmax = fmax(dmax, fabs(tnew - told));
+                    // mark the point's tile in the two other orientations
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int b = (q == 0) ? a.ua : a.va;
+                        const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
+                        const int cb = (q == 0) ? u : v;
+                        const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
+                        const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
+                        const int tile = ((cv - 1) >> 3) * a.mod_ntu[b] + ((cu - 1) >> 5);
+                        a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
+                    }
+                }
+                ++evaluated;
+            }
+            if (__syncthreads_or(changed) && tid == 0)
+                a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
+        }
+        // publish
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(a.flags + item, a.epoch);
+        }
+    }
+
+    // per-launch maximum |dT| and evaluated-point count
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if (lane == 0) wmax[warp] = dmax;
+    for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+    if (lane == 0 && evaluated) atomicAdd(a.evaluated, evaluated);
+    __syncthreads();
+    if (tid == 0) {
+        double m = 0.0;
+        for (int w = 0; w < 8; ++w) m = fmax(m, wmax[w]);
+        if (m > 0.0) atomicMax(a.maxd, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)
+{
+    wave_pass_kernel<<<grid, 256, 0, s>>>(T, a, tab);
+    return cudaGetLastError();
+}
+
+int wave_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel, 256, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+}  // namespace fold3d

@@ -33,7 +33,8 @@ REF_A = (-0.35, 0.4, 0.7)
 EXPORTED = (
     "fold3d_last_error", "fold3d_version", "fold3d_default_opts", "fold3d_create", "fold3d_destroy",
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
-    "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc",
+    "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
+    "fold3d_selftest_wait_timeout",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -101,6 +102,8 @@ def lib() -> C.CDLL:
     L.fold3d_exact_time.argtypes = [P(Medium), d, d, d]
     L.fold3d_exact_time.restype = d
     L.fold3d_compat_set_grid.argtypes = [i, i, i]
+    L.fold3d_compat_plane.argtypes = [i, vp, i] + [d] * 10
+    L.fold3d_selftest_wait_timeout.argtypes = [vp, d]
     L.InitFoldFromPoint.argtypes = [d] * 7
     L.InitFoldFromPoint.restype = d
     L.ImpSurfF.argtypes = [d] * 3

@@ -185,6 +185,22 @@ double fold3d_exact_time(const fold3d_medium *m, double x, double y, double z);
 int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T_dev,
                          const fold3d_opts *o, void *stream, fold3d_report *rep);
 
+/* The body of the six reference-compatible sweep functions below: one plane
+ * step of direction dir with the reference's argument conventions.  Programs
+ * that compile the reference's own sweep definitions (AN_ISO_1_OpenACC.c)
+ * and want this library's instead link the forwarders in
+ * fgcs-openacc-advanced_b200/dropin/fold3d_dropin.c, which call this. */
+void fold3d_compat_plane(int dir, double *T, int plane, double dzz, double dxx, double dyy,
+                         double dxy, double dxz, double dyz, double F, double ay, double ax,
+                         double az);
+
+/* Diagnostic: runs one WAVEFRONT pass on a small internal field whose first
+ * plane step is never published, with the dependency-wait limit set to
+ * timeout_ms, so every wait gives up.  Returns FOLD3D_ERR_TIMEOUT when the
+ * bounded waits and the status word work (the context stays usable), any
+ * other code otherwise.  Faults nothing and hangs nothing. */
+int fold3d_selftest_wait_timeout(fold3d_ctx *ctx, double timeout_ms);
+
 /* Grid size the reference-compatible sweep functions assume for a device
  * field (they have no size argument, AN_ISO_1_OpenACC.c:180).  If never set,
  * the size is taken from the allocation made by this library's acc_malloc. */

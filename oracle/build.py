@@ -143,6 +143,45 @@ def build_ref(n: int, with_program: bool = False, force: bool = False) -> str:
     return outdir
 
 
+SWEEPS = ("function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
+          "function_k_down")
+
+
+def dropin_path(n: int) -> str:
+    return os.path.join(REF_OUT, "n%d" % n, "an_iso_1_dropin")
+
+
+def build_dropin(n: int = 128, force: bool = False) -> str:
+    """The reference's unmodified single-GPU program (its own main) linked
+    against libfold3dpmm: its six sweep definitions are weakened in the
+    object file so that the strong forwarders of
+    fgcs-openacc-advanced_b200/dropin/fold3d_dropin.c take their place, and
+    ImplicitInitialiser and the acc_* runtime calls resolve to the library
+    (the reference's Fold3dPMM.c is not linked).  Needs libfold3dpmm.so."""
+    if not reference_available():
+        raise RuntimeError("reference sources not found under %s" % REF_ROOT)
+    root = os.path.dirname(HERE)
+    pkg = os.path.join(root, "fgcs-openacc-advanced_b200")
+    lib = os.path.join(pkg, "libfold3dpmm.so")
+    shim = os.path.join(pkg, "dropin", "fold3d_dropin.c")
+    acc = os.path.join(REF_DIR, "AN_ISO_1_OpenACC.c")
+    out = dropin_path(n)
+    if not force and _newer(out, acc, lib, shim, __file__):
+        return out
+    if not os.path.exists(lib):
+        raise RuntimeError("libfold3dpmm.so must be built first")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    with tempfile.TemporaryDirectory(prefix="fold3d_dropin_") as tmp:
+        hdr = _gen_header(n, tmp)
+        obj = os.path.join(tmp, "an_iso_1.o")
+        _run(["gcc", *CFLAGS, "-w", "-fPIC", "-fno-inline", "-include", hdr, "-c", acc, "-o", obj])
+        _run(["objcopy"] + ["--weaken-symbol=%s" % s for s in SWEEPS] + [obj])
+        rel = os.path.relpath(pkg, os.path.dirname(out))
+        _run(["gcc", *CFLAGS, "-o", out, obj, shim, "-I", os.path.join(root, "include"), "-L", pkg,
+              "-lfold3dpmm", "-Wl,-rpath,$ORIGIN/" + rel, "-lm"])
+    return out
+
+
 def ref_lib_path(n: int, omp: bool = False) -> str:
     return os.path.join(REF_OUT, "n%d" % n, "libref_omp.so" if omp else "libref.so")
 
@@ -152,10 +191,15 @@ DEFAULT_REF_SIZES = (8, 16, 32, 64, 128, 512)
 
 
 def build_all(sizes=DEFAULT_REF_SIZES) -> None:
+    """Oracle, the reference's host builds and, when libfold3dpmm.so exists,
+    the reference program linked against it (build the library first)."""
     build_oracle()
     if reference_available():
         for n in sizes:
             build_ref(n)
+        root = os.path.dirname(HERE)
+        if os.path.exists(os.path.join(root, "fgcs-openacc-advanced_b200", "libfold3dpmm.so")):
+            build_dropin(128)
 
 
 if __name__ == "__main__":

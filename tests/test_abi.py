@@ -99,3 +99,26 @@ def test_create_without_gpu_fails_cleanly(f3d):
 
 def test_oracle_library_loads(orc):
     assert orc.fold_from_point(1.1, 0, 0, 0, 1.1, 0, 0) == pytest.approx(1.0)
+
+
+def test_dropin_program_links_to_library():
+    """The reference's own program, linked with its sweeps replaced
+    (oracle/build.py:build_dropin): the six sweeps are strong definitions
+    from the forwarders, and ImplicitInitialiser and the OpenACC runtime
+    calls are left to libfold3dpmm.so."""
+    from oracle import build
+
+    exe = build.dropin_path(128)
+    if not os.path.exists(exe):
+        pytest.skip("drop-in program not built (needs the reference sources)")
+    out = subprocess.run(["nm", exe], capture_output=True, text=True, check=True).stdout
+    sym = {}
+    for ln in out.splitlines():
+        f = ln.split()
+        sym[f[-1]] = f[-2]
+    for s in build.SWEEPS:
+        assert sym.get(s) == "T", s
+    for s in ("ImplicitInitialiser", "acc_malloc", "acc_memcpy_to_device", "acc_memcpy_from_device"):
+        assert sym.get(s) == "U", s
+    ldd = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
+    assert "libfold3dpmm.so" in ldd and "libgomp" not in ldd

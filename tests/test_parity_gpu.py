@@ -16,20 +16,20 @@ from oracle import REF_A, REF_F, ref_spacing
 
 pytestmark = pytest.mark.gpu
 
-ENGINES = ["planes", "planes-literal", "planes-compact"]
+ENGINES = ["planes", "planes-literal", "planes-compact", "wavefront", "wavefront-skip"]
 
 
 def engine_opts(f3d, name):
-    """'<engine>[-literal]': engine and solver variant."""
+    """'<engine>[-literal|-compact|-skip]': engine, solver variant, skipping."""
     eng, _, var = name.partition("-")
     return ({"planes": f3d.ENGINE_PLANES, "wavefront": f3d.ENGINE_WAVEFRONT}[eng],
-            {"": f3d.VARIANT_FAST, "literal": f3d.VARIANT_LITERAL, "compact": f3d.VARIANT_COMPACT}[var])
+            {"literal": f3d.VARIANT_LITERAL, "compact": f3d.VARIANT_COMPACT}.get(var, f3d.VARIANT_FAST),
+            var == "skip")
 
 
-def gpu_solve(f3d, ctx, cuda, T, h, sweeps, *, fixed=True, tol=0.0, engine="planes", skip=False,
-              med=None):
+def gpu_solve(f3d, ctx, cuda, T, h, sweeps, *, fixed=True, tol=0.0, engine="planes", med=None):
     d = cuda.from_numpy(T.copy()).cuda()
-    eng, var = engine_opts(f3d, engine)
+    eng, var, skip = engine_opts(f3d, engine)
     rep = ctx.solve(d, h, med, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol, engine=eng, skip=skip,
                                          variant=var))
     return d.cpu().numpy(), rep
@@ -300,3 +300,68 @@ def test_division_by_constant_matches_ieee(f3d, cuda):
                       first.data_ptr()) == 0
     i = int(first.item())
     assert int(mm.item()) == 0, "x=%r c=%r" % (x[i], c[i % len(c)])
+
+
+def test_reference_program_runs_on_library(f3d, digests, cuda, tmp_path):
+    """The reference's unmodified single-GPU program (its own main,
+    AN_ISO_1_OpenACC.c:1150-1295) linked against libfold3dpmm: 8 sweeps at
+    128^3 through this library's ImplicitInitialiser, acc_* runtime and sweep
+    kernels write the reference's own output file, identical byte for byte
+    (md5 of an_iso_1_openacc.txt)."""
+    import os
+    import subprocess
+
+    from oracle import build
+
+    exe = build.dropin_path(128)
+    if not os.path.exists(exe):
+        pytest.skip("drop-in program not built (needs the reference sources at build time)")
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "Time taken for the 1 GPU" in r.stdout
+    data = (tmp_path / "an_iso_1_openacc.txt").read_bytes()
+    assert hashlib.md5(data).hexdigest() == digests["n128_s8_text_md5"]
+
+
+def test_wavefront_skip_matches_planes_full_size_512(f3d, ctx, cuda):
+    """512^3, 8 sweeps: the wavefront engine with tile skipping gives the
+    per-plane engine's field bit for bit, evaluating fewer points."""
+    n = 512
+    h = (ref_spacing(n),) * 3
+    T0 = f3d.init_implicit(n, n, n, h[0])
+    a = cuda.from_numpy(T0).cuda()
+    b = a.clone()
+    ra = ctx.solve(a, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=f3d.ENGINE_PLANES))
+    rb = ctx.solve(b, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=f3d.ENGINE_WAVEFRONT, skip=True))
+    assert rb.max_delta == ra.max_delta
+    assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+    assert rb.nominal_updates == ra.nominal_updates
+    assert 0 < rb.evaluated_updates <= rb.nominal_updates
+
+
+def test_wavefront_skip_converges_like_planes(f3d, ctx, cuda):
+    """Run to max|dT| == 0 at 96^3 (implicit surface and point source): same
+    sweep count and field as the per-plane engine; skipping evaluates far
+    fewer points once most of the field has settled."""
+    n = 96
+    h = (ref_spacing(n),) * 3
+    for T0 in (f3d.init_implicit(n, n, n, h[0]), f3d.init_point(n, n, n, (30, 50, 70))):
+        a = cuda.from_numpy(T0.copy()).cuda()
+        b = a.clone()
+        ra = ctx.solve(a, h, None, f3d.opts(max_sweeps=500, tol=0.0, engine=f3d.ENGINE_PLANES))
+        rb = ctx.solve(b, h, None, f3d.opts(max_sweeps=500, tol=0.0, engine=f3d.ENGINE_WAVEFRONT, skip=True))
+        assert ra.max_delta == 0.0 and rb.max_delta == 0.0
+        assert rb.sweeps == ra.sweeps
+        assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+        assert rb.evaluated_updates < 0.8 * rb.nominal_updates
+
+
+def test_wavefront_bounded_wait_times_out_cleanly(f3d, ctx, cuda, golden):
+    """A dependency wait that can never be satisfied gives up after its limit
+    and reports FOLD3D_ERR_TIMEOUT; the context keeps working afterwards."""
+    L = f3d.lib()
+    rc = L.fold3d_selftest_wait_timeout(ctx._h, 1.0)
+    assert rc == f3d.ERR_TIMEOUT, f3d.last_error()
+    n = 16
+    out, _ = gpu_solve(f3d, ctx, cuda, golden[n]["init"], (ref_spacing(n),) * 3, 8, engine="wavefront-skip")
+    assert_bitwise(out, golden[n]["s8"], "after the timeout")
