@@ -465,7 +465,12 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
         return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    if (o->engine == FOLD3D_ENGINE_WAVEFRONT) {
+    // AUTO: the wavefront engine for the default solver form, the per-plane
+    // engine for the cross-check forms.
+    const int engine = (o->engine == FOLD3D_ENGINE_AUTO)
+                           ? (o->variant == kVariantFast ? FOLD3D_ENGINE_WAVEFRONT : FOLD3D_ENGINE_PLANES)
+                           : o->engine;
+    if (engine == FOLD3D_ENGINE_WAVEFRONT) {
         if (o->variant != kVariantFast)
             return set_error(FOLD3D_ERR_UNSUPPORTED, "the wavefront engine runs the default solver variant only");
         return solve_wavefront(c, *g, *m, T, *o, s, rep);

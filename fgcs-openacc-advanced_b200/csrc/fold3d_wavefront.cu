@@ -25,10 +25,15 @@
 // this direction was in pass e-6, after the source plane's update of that
 // pass).
 //
+// The change marks of earlier passes are final when a pass starts; whether
+// step p-1 of the current pass changed the source plane comes with its
+// completion flags, which hold (pass << 1) | changed.
+//
 // Synchronisation: a CTA publishes an item with __syncthreads, a gpu-scope
-// fence and a release store of the pass number into the item's flag; a
-// waiting CTA's thread 0 polls with acquire loads and then releases its block
-// with __syncthreads.  Field values written inside the launch are read with
+// fence and a release store into the item's flag; in a waiting CTA, nine
+// threads poll the nine neighbour flags in parallel with acquire loads and
+// then release the block with __syncthreads.  Each CTA claims its next item
+// while it works on the current one.  Field values written inside the launch are read with
 // L2-cached loads (ld.global.cg), never through the non-coherent read-only
 // path.
 #include <cstring>
@@ -63,83 +68,77 @@ __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) wave_pass_kernel(double *__restrict__ T, WaveArgs a,
+__global__ void __launch_bounds__(256, 4) wave_pass_kernel(double *__restrict__ T, WaveArgs a,
                                                         const __grid_constant__ DirTable tab)
 {
-    __shared__ int s_item;
-    __shared__ int s_skip;
+    __shared__ int s_next;
     __shared__ double wmax[8];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const PlaneGeom &g = a.pg;
     const int ntiles = a.ntu * a.ntv;
     const long long total = (long long)a.steps * ntiles;
+    // flags hold (pass << 1) | changed
+    const unsigned want = a.epoch << 1;
+    const bool may_skip = a.epoch >= a.skip_from;
     double dmax = 0.0;
     unsigned long long evaluated = 0;
 
+    if (tid == 0) {
+        const unsigned w = atomicAdd(a.work, 1u);
+        s_next = (w < total) ? (int)w : -1;
+    }
+    __syncthreads();
     for (;;) {
-        if (tid == 0) {
+        const int item = s_next;
+        if (item < 0) break;
+        __syncthreads();  // every thread has read s_next
+        if (tid == 0) {   // claim the next item now; it is processed after this one
             int it = -1;
             if (*(volatile unsigned *)a.status == 0) {
                 const unsigned w = atomicAdd(a.work, 1u);
                 if (w < total) it = (int)w;
             }
-            s_item = it;
+            s_next = it;
         }
-        __syncthreads();
-        const int item = s_item;
-        if (item < 0) break;
         const int p = item / ntiles, t = item - p * ntiles;
         const int tu = t % a.ntu, tv = t / a.ntu;
         const int src = a.first_src + p * a.sg;
         const int tgt = src + a.sg;
 
-        // wait for the 3 x 3 tiles of step p-1 (they wrote this step's source plane)
-        if (tid == 0) {
-            int ok = 1;
-            if (p > 0) {
-                const unsigned *f = a.flags + (long long)(p - 1) * ntiles;
-                const unsigned long long t0 = global_ns();
-                for (int dv = -1; dv <= 1 && ok; ++dv)
-                    for (int du = -1; du <= 1 && ok; ++du) {
-                        const int nu = tu + du, nv = tv + dv;
-                        if (nu < 0 || nu >= a.ntu || nv < 0 || nv >= a.ntv) continue;
-                        const unsigned *fl = f + nv * a.ntu + nu;
-                        unsigned spins = 0;
-                        while (ld_acquire(fl) < a.epoch) {
-                            if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
-                                *(volatile unsigned *)a.status != 0) {
-                                atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
-                                ok = 0;
-                                break;
-                            }
-                            __nanosleep(64);
+        // Threads 0..8 each watch one tile of the 3 x 3 neighbourhood: its
+        // change mark from earlier passes, and its step p-1 flag (which also
+        // says whether that item changed the source plane).
+        int timed_out = 0, recent = 0;
+        if (tid < 9) {
+            const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
+            if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
+                const int nt = nv * a.ntu + nu;
+                if (may_skip) recent = (__ldcg(a.mod[a.nrm] + (long long)src * ntiles + nt) + 5u >= a.epoch);
+                if (p > 0) {
+                    const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nt;
+                    const unsigned long long t0 = global_ns();
+                    unsigned spins = 0, f;
+                    while ((f = ld_acquire(fl)) < want) {
+                        if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
+                            *(volatile unsigned *)a.status != 0) {
+                            atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                            timed_out = 1;
+                            break;
                         }
+                        __nanosleep(32);
                     }
+                    if (!timed_out) recent |= (int)(f & 1u);
+                }
             }
-            int skip = 0;
-            if (ok && a.epoch >= a.skip_from) {
-                // changed in passes epoch-5 .. epoch anywhere in the source neighbourhood?
-                const unsigned *m = a.mod[a.nrm] + (long long)src * ntiles;
-                unsigned last = 0;
-                for (int dv = -1; dv <= 1; ++dv)
-                    for (int du = -1; du <= 1; ++du) {
-                        const int nu = tu + du, nv = tv + dv;
-                        if (nu < 0 || nu >= a.ntu || nv < 0 || nv >= a.ntv) continue;
-                        last = max(last, __ldcg(m + nv * a.ntu + nu));
-                    }
-                skip = (last + 5u < a.epoch);
-            }
-            s_skip = ok ? skip : -1;
         }
-        __syncthreads();
-        const int skip = s_skip;
-        if (skip < 0) break;  // timed out: leave without publishing
+        if (__syncthreads_or(timed_out)) break;  // leave without publishing
+        const int skip = may_skip && !__syncthreads_or(recent);
 
+        int changed = 0;
         if (!skip) {
             const int u = tu * 32 + lane + 1;
             const int v = tv * 8 + warp + 1;
-            int changed = 0;
             if (u <= g.nu && v <= g.nv) {
                 const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
                 const long long d = s + g.sn;
@@ -172,14 +171,14 @@ __global__ void __launch_bounds__(256) wave_pass_kernel(double *__restrict__ T, 
                 }
                 ++evaluated;
             }
-            if (__syncthreads_or(changed) && tid == 0)
-                a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
+            changed = __syncthreads_or(changed);
+            if (changed && tid == 0) a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
         }
-        // publish
+        // publish (the barrier orders every thread's stores before thread 0's fence)
         __syncthreads();
         if (tid == 0) {
             __threadfence();
-            st_release(a.flags + item, a.epoch);
+            st_release(a.flags + item, want | (unsigned)changed);
         }
     }
 

@@ -67,7 +67,7 @@ enum fold3d_dir {
 
 /* Execution engines for a whole solve. */
 enum fold3d_engine {
-    FOLD3D_ENGINE_AUTO = 0,
+    FOLD3D_ENGINE_AUTO = 0,      /* WAVEFRONT for variant 0, PLANES otherwise          */
     FOLD3D_ENGINE_PLANES = 1,    /* one kernel per plane, each sweep a CUDA graph    */
     FOLD3D_ENGINE_WAVEFRONT = 2  /* one persistent kernel per pass, tile dataflow     */
 };
