@@ -48,7 +48,13 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, build_dir: str | None = None, lib: str | None = None,
+          defines=()) -> str:
+    """Compile into build_dir and link lib (defaults: _build/, libfold3dpmm.so);
+    defines: extra -D flags for every source."""
+    BUILD = build_dir or globals()["BUILD"]
+    LIB = lib or globals()["LIB"]
+    extra = ["-D%s" % d for d in defines]
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, h) for h in ("fold3dpmm.h", "fold3d_acc.h")] + [__file__]
     objs = []
@@ -58,11 +64,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
         if force or _stale(obj, [path] + hdrs):
             if src.endswith(".cu"):
-                cmd = [NVCC, *NVCC_FLAGS, "-c", path, "-o", obj]
+                cmd = [NVCC, *NVCC_FLAGS, *extra, "-c", path, "-o", obj]
                 if verbose:
                     cmd.insert(1, "-Xptxas=-v")
             else:
-                cmd = ["g++", *CXX_FLAGS, "-c", path, "-o", obj]
+                cmd = ["g++", *CXX_FLAGS, *extra, "-c", path, "-o", obj]
             r = _run(cmd)
             if verbose:
                 sys.stdout.write(r.stdout + r.stderr)

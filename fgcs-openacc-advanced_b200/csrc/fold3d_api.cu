@@ -311,13 +311,13 @@ static int solve_planes(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium
     return FOLD3D_OK;
 }
 
-// Tiles (32 x 8) per plane of the orientation with normal axis b.
+// WAVEFRONT tiles (32 x kWaveTV) per plane of the orientation with normal axis b.
 static void orient_tiles(const fold3d_grid &g, int b, int &ntu, int &ntv)
 {
     const int n[3] = {g.nx, g.ny, g.nz};
     const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
     ntu = (n[ub] + 31) / 32;
-    ntv = (n[vb] + 7) / 8;
+    ntv = (n[vb] + kWaveTV - 1) / kWaveTV;
 }
 
 static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)

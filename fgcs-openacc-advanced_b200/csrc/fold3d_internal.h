@@ -57,11 +57,19 @@ enum Variant {
     kVariantCompact = 2   // host-folded constants, solver calls compacted across the block
 };
 
+// WAVEFRONT tiles are 32 points along the plane's faster axis by
+// FOLD3D_WAVE_TV rows; one CTA of 32*FOLD3D_WAVE_TV threads works on a tile.
+#ifndef FOLD3D_WAVE_TV
+#define FOLD3D_WAVE_TV 4
+#endif
+constexpr int kWaveTV = FOLD3D_WAVE_TV;
+static_assert(kWaveTV == 1 || kWaveTV == 2 || kWaveTV == 4 || kWaveTV == 8, "tile rows");
+
 // Arguments of one WAVEFRONT pass (fold3d_wavefront.cu).
 struct WaveArgs {
     PlaneGeom pg;
     int nrm, ua, va, sg;         // normal axis, in-plane u / v axes, step direction
-    int ntu, ntv;                // 32 x 8 tiles per plane (this orientation)
+    int ntu, ntv;                // 32 x kWaveTV tiles per plane (this orientation)
     int steps, first_src;        // plane steps of the pass and the first source plane
     unsigned epoch;              // number of this pass (monotonic per context)
     unsigned skip_from;          // passes numbered below this never skip

@@ -2,8 +2,8 @@
 // directional pass, tile dataflow between consecutive planes, and tiles
 // skipped when their inputs did not change.
 //
-// Work items are (plane step p, tile t) pairs of a pass, tiles being 32 x 8
-// points of a plane, numbered plane-major.  Every CTA claims the next item
+// Work items are (plane step p, tile t) pairs of a pass, tiles being
+// 32 x kWaveTV points of a plane, numbered plane-major.  Every CTA claims the next item
 // from an atomic counter.  Item (p, t) reads the source plane written by
 // step p-1 only within t's 1-point halo, i.e. from the 3 x 3 tiles around t,
 // so it waits for exactly those items (their completion flags), not for the
@@ -68,11 +68,13 @@ __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
 
 }  // namespace
 
-__global__ void __launch_bounds__(256, 4) wave_pass_kernel(double *__restrict__ T, WaveArgs a,
-                                                        const __grid_constant__ DirTable tab)
+constexpr int kWaveThreads = 32 * kWaveTV;
+
+__global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
+    wave_pass_kernel(double *__restrict__ T, WaveArgs a, const __grid_constant__ DirTable tab)
 {
     __shared__ int s_next;
-    __shared__ double wmax[8];
+    __shared__ double wmax[kWaveTV];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const PlaneGeom &g = a.pg;
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(256, 4) wave_pass_kernel(double *__restrict__ 
         int changed = 0;
         if (!skip) {
             const int u = tu * 32 + lane + 1;
-            const int v = tv * 8 + warp + 1;
+            const int v = tv * kWaveTV + warp + 1;
             if (u <= g.nu && v <= g.nv) {
                 const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
                 const long long d = s + g.sn;
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(256, 4) wave_pass_kernel(double *__restrict__ 
                         const int cb = (q == 0) ? u : v;
                         const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
                         const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
-                        const int tile = ((cv - 1) >> 3) * a.mod_ntu[b] + ((cu - 1) >> 5);
+                        const int tile = ((cv - 1) / kWaveTV) * a.mod_ntu[b] + ((cu - 1) >> 5);
                         a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
                     }
                 }
@@ -191,21 +193,22 @@ __global__ void __launch_bounds__(256, 4) wave_pass_kernel(double *__restrict__ 
     __syncthreads();
     if (tid == 0) {
         double m = 0.0;
-        for (int w = 0; w < 8; ++w) m = fmax(m, wmax[w]);
+        for (int w = 0; w < kWaveTV; ++w) m = fmax(m, wmax[w]);
         if (m > 0.0) atomicMax(a.maxd, (unsigned long long)__double_as_longlong(m));
     }
 }
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)
 {
-    wave_pass_kernel<<<grid, 256, 0, s>>>(T, a, tab);
+    wave_pass_kernel<<<grid, kWaveThreads, 0, s>>>(T, a, tab);
     return cudaGetLastError();
 }
 
 int wave_blocks_per_sm()
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel, 256, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel, kWaveThreads, 0) != cudaSuccess)
+        return 1;
     return n > 0 ? n : 1;
 }
 

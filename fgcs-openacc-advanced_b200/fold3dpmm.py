@@ -18,7 +18,8 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfold3dpmm.so")
+# FOLD3D_LIBRARY may name another build of the same library.
+LIB_PATH = os.environ.get("FOLD3D_LIBRARY") or os.path.join(HERE, "libfold3dpmm.so")
 
 OK, ERR_INVALID, ERR_NOMEM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(6)
 MAXT = 10e15 * 1.0
