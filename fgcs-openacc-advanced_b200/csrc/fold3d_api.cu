@@ -11,6 +11,7 @@
 #include <string>
 
 #include "fold3d_acc.h"
+#include "fold3d_ellip.cuh"
 #include "fold3d_fast.cuh"
 #include "fold3d_internal.h"
 
@@ -149,7 +150,7 @@ struct fold3d_ctx {
     unsigned *w_counters = nullptr;          // [0] work, [1] status
     unsigned long long *w_evaluated = nullptr;
     unsigned epoch = 0;                      // passes run so far on this context
-    int sms = 0, wave_bps = 0;
+    int sms = 0, wave_bps = 0, wave_bps_ell = 0;
 };
 
 namespace {
@@ -353,15 +354,41 @@ static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
-        c->wave_bps = wave_blocks_per_sm();
+        c->wave_bps = wave_blocks_per_sm(kMediumDrift);
+        c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
     c->epoch = 0;  // fresh flags and maps
     c->key_wg = g;
     return FOLD3D_OK;
 }
 
-static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium &m, double *T,
-                           const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
+// Elliptical-medium constants of a sweep direction.
+static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int dir)
+{
+    const DirSpec &d = kDirs[dir];
+    const double h[3] = {g.dx, g.dy, g.dz};
+    static const int pair[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    EllipParam p;
+    memset(&p, 0, sizeof p);
+    p.dir.hx = h[d.xa];
+    p.dir.hy = h[d.ya];
+    p.dir.hz = h[d.nrm];
+    p.dir.sxy = d.xs * d.ys;
+    p.dir.sxz = d.xs * d.sg;
+    p.dir.syz = d.ys * d.sg;
+    p.dir.ixx = pair[d.xa][d.xa];
+    p.dir.iyy = pair[d.ya][d.ya];
+    p.dir.izz = pair[d.nrm][d.nrm];
+    p.dir.ixy = pair[d.xa][d.ya];
+    p.dir.ixz = pair[d.xa][d.nrm];
+    p.dir.iyz = pair[d.ya][d.nrm];
+    const float *arr[6] = {m.mxx, m.mxy, m.mxz, m.myy, m.myz, m.mzz};
+    for (int k = 0; k < 6; ++k) p.med.m[k] = arr[k];
+    return p;
+}
+
+static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
+                           double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
 {
     int rc = wave_scratch(c, g);
     if (rc) return rc;
@@ -405,12 +432,18 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
             a.steps = pass_count(a.pg);
             a.first_src = pass_first(a.pg, dir);
             a.epoch = ++c->epoch;
-            build_dir_table(make_frame(g, m, dir), tab);
             const long long items = (long long)a.steps * a.ntu * a.ntv;
-            const int grid = (int)std::min<long long>(items, (long long)c->sms * c->wave_bps);
+            const int bps = em ? c->wave_bps_ell : c->wave_bps;
+            const int grid = (int)std::min<long long>(items, (long long)c->sms * bps);
             if ((e = cudaMemsetAsync(a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
                 return cuda_error(e, "cudaMemsetAsync");
-            if ((e = launch_wave_pass(T, a, tab, grid, s)) != cudaSuccess) return cuda_error(e, "wavefront pass");
+            if (em) {
+                e = launch_wave_pass_ellip(T, a, ellip_param(g, *em, dir), grid, s);
+            } else {
+                build_dir_table(make_frame(g, *fm, dir), tab);
+                e = launch_wave_pass(T, a, tab, grid, s);
+            }
+            if (e != cudaSuccess) return cuda_error(e, "wavefront pass");
         }
         ++sweeps;
         if (!o.fixed) {
@@ -473,7 +506,7 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
     if (engine == FOLD3D_ENGINE_WAVEFRONT) {
         if (o->variant != kVariantFast)
             return set_error(FOLD3D_ERR_UNSUPPORTED, "the wavefront engine runs the default solver variant only");
-        return solve_wavefront(c, *g, *m, T, *o, s, rep);
+        return solve_wavefront(c, *g, m, nullptr, T, *o, s, rep);
     }
     return solve_planes(c, *g, *m, T, *o, s, rep);
 }
@@ -537,6 +570,36 @@ int fold3d_selftest_wait_timeout(fold3d_ctx *c, double timeout_ms)
         return cuda_error(e, "selftest");
     if (hstat[1] == 1) return set_error(FOLD3D_ERR_TIMEOUT, "wavefront: a dependency wait gave up (as intended)");
     return set_error(FOLD3D_ERR_CUDA, "selftest: the waits did not give up");
+}
+
+void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az, float out[6])
+{
+    if (!out) return;
+    const double nn = std::sqrt(ax * ax + ay * ay + az * az);
+    const double nx = ax / nn, ny = ay / nn, nz = az / nn;
+    const double a = 1.0 / (vz * vz * (1.0 + 2.0 * eps));
+    const double b = 1.0 / (vz * vz) - a;
+    const double m[6] = {a + b * nx * nx, b * nx * ny, b * nx * nz, a + b * ny * ny, b * ny * nz, a + b * nz * nz};
+    for (int k = 0; k < 6; ++k) out[k] = (float)m[k];
+}
+
+int fold3d_solve_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T, const fold3d_opts *o,
+                       void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (!T || !m || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (!m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
+        return set_error(FOLD3D_ERR_INVALID, "metric array is NULL");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "the elliptical medium runs on the wavefront engine, variant 0");
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return solve_wavefront(c, *g, nullptr, m, T, *o, s, rep);
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,

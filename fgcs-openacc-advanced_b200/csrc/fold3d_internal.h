@@ -82,8 +82,15 @@ struct WaveArgs {
     unsigned long long *maxd;    // max |dT| (IEEE bits) of the sweep
     unsigned long long *evaluated;  // points evaluated
 };
+// Media of the local solver.
+enum Medium { kMediumDrift = 0, kMediumEllip = 1 };
+
+struct EllipDir;     // fold3d_ellip.cuh
+struct EllipParam;   // below, once EllipDir is complete
+
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s);
-int wave_blocks_per_sm();
+cudaError_t launch_wave_pass_ellip(double *T, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s);
+int wave_blocks_per_sm(int medium);
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,

@@ -38,6 +38,7 @@
 // path.
 #include <cstring>
 
+#include "fold3d_ellip.cuh"
 #include "fold3d_fast.cuh"
 #include "fold3d_internal.h"
 
@@ -70,8 +71,19 @@ __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
 
 constexpr int kWaveThreads = 32 * kWaveTV;
 
+// Medium-dependent launch parameters: the drift medium's constant table, or
+// the elliptical medium's direction constants and metric arrays.
+template <int MED> struct WaveMedium;
+template <> struct WaveMedium<kMediumDrift> {
+    using type = DirTable;
+};
+template <> struct WaveMedium<kMediumEllip> {
+    using type = EllipParam;
+};
+
+template <int MED>
 __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
-    wave_pass_kernel(double *__restrict__ T, WaveArgs a, const __grid_constant__ DirTable tab)
+    wave_pass_kernel(double *__restrict__ T, WaveArgs a, const __grid_constant__ typename WaveMedium<MED>::type tab)
 {
     __shared__ int s_next;
     __shared__ double wmax[kWaveTV];
@@ -154,7 +166,13 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
                 const double tym = fabs(ld_cg(T + s - g.sx + g.sy));
                 const double txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
                 const double told = ld_cg(T + d);
-                const double tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                double tnew;
+                if constexpr (MED == kMediumDrift) {
+                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                } else {
+                    const double nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
+                    tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d));
+                }
                 if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
                     T[d] = tnew;
                     changed = 1;
@@ -200,15 +218,25 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)
 {
-    wave_pass_kernel<<<grid, kWaveThreads, 0, s>>>(T, a, tab);
+    wave_pass_kernel<kMediumDrift><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
     return cudaGetLastError();
 }
 
-int wave_blocks_per_sm()
+cudaError_t launch_wave_pass_ellip(double *T, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s)
+{
+    wave_pass_kernel<kMediumEllip><<<grid, kWaveThreads, 0, s>>>(T, a, p);
+    return cudaGetLastError();
+}
+
+int wave_blocks_per_sm(int medium)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel, kWaveThreads, 0) != cudaSuccess)
-        return 1;
+    cudaError_t e = (medium == kMediumEllip)
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip>,
+                                                                        kWaveThreads, 0)
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumDrift>,
+                                                                        kWaveThreads, 0);
+    if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 

@@ -35,7 +35,7 @@ EXPORTED = (
     "fold3d_last_error", "fold3d_version", "fold3d_default_opts", "fold3d_create", "fold3d_destroy",
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
-    "fold3d_selftest_wait_timeout",
+    "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -56,6 +56,10 @@ class Grid(C.Structure):
 
 class Medium(C.Structure):
     _fields_ = [("F", C.c_double), ("ax", C.c_double), ("ay", C.c_double), ("az", C.c_double)]
+
+
+class Ellip(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("mxx", "mxy", "mxz", "myy", "myz", "mzz")]
 
 
 class Opts(C.Structure):
@@ -105,6 +109,8 @@ def lib() -> C.CDLL:
     L.fold3d_compat_set_grid.argtypes = [i, i, i]
     L.fold3d_compat_plane.argtypes = [i, vp, i] + [d] * 10
     L.fold3d_selftest_wait_timeout.argtypes = [vp, d]
+    L.fold3d_ellip_metric.argtypes = [d, d, d, d, d, C.POINTER(C.c_float)]
+    L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
     L.InitFoldFromPoint.restype = d
     L.ImpSurfF.argtypes = [d] * 3
@@ -248,6 +254,24 @@ class Context:
         return rep
 
 
+def ellip_metric(vz, eps, axis):
+    """The six float metric entries (xx, xy, xz, yy, yz, zz) of a tilted
+    elliptical cell (fold3d_ellip_metric)."""
+    out = (C.c_float * 6)()
+    lib().fold3d_ellip_metric(float(vz), float(eps), float(axis[0]), float(axis[1]), float(axis[2]), out)
+    return list(out)
+
+
+def ellip(M):
+    """fold3d_ellip from six contiguous float32 CUDA tensors (xx xy xz yy yz zz)."""
+    import torch
+
+    for m in M:
+        if m.dtype != torch.float32 or not m.is_cuda or not m.is_contiguous():
+            raise ValueError("metric arrays must be contiguous float32 CUDA tensors")
+    return Ellip(*(C.c_void_p(m.data_ptr()) for m in M))
+
+
 NOALLOC_MAX_SWEEPS = 4096
 
 
@@ -259,6 +283,17 @@ def solve_noalloc(T, h, med: Medium | None = None, o: Opts | None = None, stream
     _check(lib().fold3d_solve_noalloc(C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()), _dev_ptr(T),
                                       C.byref(o or opts()), C.c_void_p(stream) if stream else None,
                                       C.byref(rep)))
+    return rep
+
+
+def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> Report:
+    """Solve in place on a float64 CUDA tensor with an elliptical medium M
+    (six float32 CUDA tensors in the field layout)."""
+    nx, ny, nz = grid_of(T)
+    rep = Report()
+    e = ellip(M)
+    _check(lib().fold3d_solve_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), _dev_ptr(T),
+                                    C.byref(o or opts()), C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 

@@ -1,0 +1,99 @@
+"""Seeded synthetic media for the elliptical (tilted transversely isotropic)
+solver.
+
+The benchmark configurations name no public model, so media are generated
+here from a seed.  A medium is the per-cell metric M = a I + b n n^T of a
+tilted elliptical cell (a = 1/(Vz^2 (1 + 2 eps)), b = 1/Vz^2 - a, n the
+symmetry axis), returned as six float32 arrays (xx, xy, xz, yy, yz, zz in the
+i, j, k axes) in the field layout, shape (nz+2, ny+2, nx+2), ghost layer
+copied from the nearest interior cell.
+
+heterogeneous_tti() follows the construction of the 512^3 configuration:
+Vz = 1500 + 0.8 * depth (m), times 1 + the sum of 16 Gaussian anomalies of
++-15 % (sigma 20-60 cells at 512^3, centres uniform); eps uniform in
+[0, 0.25] smoothed by a Gaussian of sigma 8 cells; tilt uniform in
+[0, 45] degrees and azimuth uniform in [0, 360) degrees, smoothed likewise
+through their unit vectors (no wrap-around).  Lengths in cells scale with
+n / 512.  k is the depth axis.  Smoothing is an FFT convolution with a
+periodic Gaussian, in float64.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+
+def metric_from(vz, eps, n_axis):
+    """M = a I + b n n^T (float64 tensors) -> six float32 tensors."""
+    nx, ny, nz = n_axis
+    nn = torch.sqrt(nx * nx + ny * ny + nz * nz)
+    nx, ny, nz = nx / nn, ny / nn, nz / nn
+    a = 1.0 / (vz * vz * (1.0 + 2.0 * eps))
+    b = 1.0 / (vz * vz) - a
+    comps = (a + b * nx * nx, b * nx * ny, b * nx * nz, a + b * ny * ny, b * ny * nz, a + b * nz * nz)
+    return [c.to(torch.float32) for c in comps]
+
+
+def _pad(t):
+    """(nz, ny, nx) interior -> (nz+2, ny+2, nx+2), ghosts copied from the nearest interior cell."""
+    return torch.nn.functional.pad(t[None, None], (1, 1, 1, 1, 1, 1), mode="replicate")[0, 0].contiguous()
+
+
+def homogeneous_ellip(nx, ny, nz, vz, eps, tilt_deg, azimuth_deg, device="cpu"):
+    th, ph = math.radians(tilt_deg), math.radians(azimuth_deg)
+    shape = (nz + 2, ny + 2, nx + 2)
+    f = lambda v: torch.full(shape, float(v), dtype=torch.float64, device=device)
+    return metric_from(f(vz), f(eps), (f(math.sin(th) * math.cos(ph)), f(math.sin(th) * math.sin(ph)),
+                                       f(math.cos(th))))
+
+
+def _smooth(x, sigma):
+    """Periodic Gaussian smoothing of a float64 (nz, ny, nx) tensor."""
+    if sigma <= 0:
+        return x
+    spec = torch.fft.rfftn(x)
+    k = [torch.fft.fftfreq(n, device=x.device, dtype=torch.float64) for n in x.shape[:2]]
+    k.append(torch.fft.rfftfreq(x.shape[2], device=x.device, dtype=torch.float64))
+    kz, ky, kx = torch.meshgrid(*k, indexing="ij")
+    g = torch.exp(-2.0 * (math.pi * sigma) ** 2 * (kx * kx + ky * ky + kz * kz))
+    return torch.fft.irfftn(spec * g, s=x.shape)
+
+
+def heterogeneous_tti(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
+    """Six float32 metric arrays of the seeded heterogeneous TTI medium."""
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    scale = max(nx, ny, nz) / 512.0
+    shape = (nz, ny, nx)
+    dev = torch.device(device)
+    k = torch.arange(nz, dtype=torch.float64, device=dev)
+    depth = (k * h).view(nz, 1, 1)
+    vz = (1500.0 + 0.8 * depth).expand(shape).clone()
+    zz, yy, xx = torch.meshgrid(*(torch.arange(n, dtype=torch.float64, device=dev) for n in shape), indexing="ij")
+    pert = torch.zeros(shape, dtype=torch.float64, device=dev)
+    for _ in range(anomalies):
+        c = torch.rand(3, generator=gen, dtype=torch.float64) * torch.tensor([nz, ny, nx], dtype=torch.float64)
+        sig = (20.0 + 40.0 * torch.rand(1, generator=gen, dtype=torch.float64).item()) * scale
+        amp = 0.15 if torch.rand(1, generator=gen).item() < 0.5 else -0.15
+        r2 = (zz - c[0].item()) ** 2 + (yy - c[1].item()) ** 2 + (xx - c[2].item()) ** 2
+        pert += amp * torch.exp(-r2 / (2.0 * sig * sig))
+    del zz, yy, xx
+    vz = vz * (1.0 + pert)
+    del pert
+    sig = 8.0 * scale
+    eps = _smooth((0.25 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev), sig)
+    th = torch.deg2rad(45.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev)
+    ph = torch.deg2rad(360.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev)
+    ax = _smooth(torch.sin(th) * torch.cos(ph), sig)
+    ay = _smooth(torch.sin(th) * torch.sin(ph), sig)
+    az = _smooth(torch.cos(th), sig)
+    del th, ph
+    M = metric_from(vz, eps.clamp(0.0, 0.25), (ax, ay, az))
+    return [_pad(m) for m in M]
+
+
+def exact_time(M6, dx, dy, dz):
+    """sqrt(d^T M d) for one homogeneous metric (six floats) and offset d."""
+    xx, xy, xz, yy, yz, zz = (float(m) for m in M6)
+    q = xx * dx * dx + yy * dy * dy + zz * dz * dz + 2 * (xy * dx * dy + xz * dx * dz + yz * dy * dz)
+    return math.sqrt(q)

@@ -150,6 +150,28 @@ int fold3d_solve_host(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_medium
 int fold3d_plane(const fold3d_grid *g, const fold3d_medium *m, double *T_dev, int dir,
                  int src, void *stream);
 
+/* A per-cell elliptical (tilted transversely isotropic) medium.  No
+ * counterpart in the reference, whose solver only knows the drift medium.
+ * The travel time along a short straight segment d is sqrt(d^T M d), M the
+ * cell's symmetric positive definite metric (slowness squared); the six
+ * arrays hold M's entries in the i, j, k axes, as float, in the field layout
+ * ((nx+2)(ny+2)(nz+2), only interior cells are read), on the device. */
+typedef struct {
+    const float *mxx, *mxy, *mxz, *myy, *myz, *mzz;
+} fold3d_ellip;
+
+/* Metric of a tilted elliptical cell: vertical speed vz, Thomsen epsilon eps
+ * (horizontal speed vz*sqrt(1+2*eps)) and symmetry axis (ax, ay, az) (need
+ * not be normalised): M = a I + b n n^T with a = 1/(vz^2 (1+2 eps)),
+ * b = 1/vz^2 - a.  out = {xx, xy, xz, yy, yz, zz}. */
+void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az, float out[6]);
+
+/* Solve in place on a device field with an elliptical medium (engine
+ * WAVEFRONT; opts.variant must be 0).  Same sweep order, stopping rules and
+ * report as fold3d_solve. */
+int fold3d_solve_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, double *T_dev,
+                       const fold3d_opts *o, void *stream, fold3d_report *rep);
+
 /* Implicit-surface source initialisation of a host field (the reference's
  * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).
  * Uses all host cores. */

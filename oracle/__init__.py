@@ -77,6 +77,10 @@ class Oracle:
         L.orc_surface.argtypes = [_dbl] * 3
         L.orc_surface.restype = _dbl
         L.orc_last_overfull.restype = C.c_long
+        L.orc_ell_solve.argtypes = [_ptr, C.POINTER(C.c_void_p), _int, _int, _int, _dbl, _dbl, _dbl, _int, _dbl,
+                                    C.POINTER(_dbl)]
+        L.orc_ell_solve.restype = _int
+        L.orc_ell_plane.argtypes = [_ptr, C.POINTER(C.c_void_p), _int, _int, _int, _dbl, _dbl, _dbl, _int, _int]
         self.L = L
 
     @staticmethod
@@ -108,6 +112,22 @@ class Oracle:
         s = self.L.orc_solve(_p(T), *self._dims(T), h[0], h[1], h[2], F, *a, nsweeps, tol, C.byref(d))
         if s < 0:
             raise MemoryError("orc_solve failed")
+        return s, d.value
+
+    @staticmethod
+    def _metric(M):
+        arrs = [np.ascontiguousarray(m, dtype=np.float32) for m in M]
+        ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in arrs))
+        return arrs, ptrs
+
+    def ell_solve(self, T, M, h, nsweeps, tol=-1.0):
+        """Elliptical medium (six float32 metric arrays, field layout), in
+        place.  Returns (sweeps_run, max|dT| of the last sweep)."""
+        arrs, ptrs = self._metric(M)
+        d = _dbl(0.0)
+        s = self.L.orc_ell_solve(_p(T), ptrs, *self._dims(T), h[0], h[1], h[2], nsweeps, tol, C.byref(d))
+        if s < 0:
+            raise MemoryError("orc_ell_solve failed")
         return s, d.value
 
     def fold_from_point(self, F, ax, ay, az, x, y, z) -> float:

@@ -538,3 +538,200 @@ void orc_init_point(double *T, int nx, int ny, int nz, int si, int sj, int sk)
         T[c] = ORC_MAXT;
     T[si + (int64_t)(nx + 2) * (sj + (int64_t)(ny + 2) * sk)] = 0.0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Elliptical (tilted) medium                                                */
+/* ------------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference (its local solver only knows the drift
+ * medium).  This is the CPU statement of this repository's own solver for a
+ * per-cell Riemannian metric M (travel time of a short straight segment d is
+ * sqrt(d^T M d)); the GPU kernel (csrc/fold3d_ellip.cuh) follows it operation
+ * by operation, so the two agree bit for bit.
+ *
+ * In a sweep direction's local frame (x, y in the source plane, z towards
+ * the target; unit vectors xs*e[xa], ys*e[ya], sg*e[nrm]) the target X sits
+ * at (0, 0, hz) above the source point st, and the eight neighbours at
+ * (i*hx, j*hy, 0), i, j in {-1, 0, 1}.  With t linear on each vertex, edge
+ * and triangle of that 3 x 3 fan, the new time is
+ *     min over the fan of  t(p) + ||X - p||_M,
+ * found as: the 9 vertex values, the interior stationary points of the 16
+ * edges (8 spokes st-P, 8 rim edges between adjacent neighbours) and of the
+ * 8 triangles (st, neighbour, next neighbour), in closed form.  Each
+ * candidate exceeds the smallest time it is built from, so a candidate is
+ * only computed while the running time is above that smallest time.
+ */
+
+/* The metric in a direction's local frame, scaled by the spacings:
+ * Axx = M'xx hx hx, Axy = M'xy hx hy, Axz = M'xz hx hz, and so on. */
+typedef struct { double xx, yy, zz, xy, xz, yz; } orc_aq;
+
+/* u^T M' v for u = (ui hx, uj hy, uk hz), v likewise (integer coefficients). */
+static double orc_bf(const orc_aq *A, int ui, int uj, int uk, int vi, int vj, int vk)
+{
+    return (double)(ui * vi) * A->xx + (double)(uj * vj) * A->yy + (double)(uk * vk) * A->zz +
+           (double)(ui * vj + uj * vi) * A->xy + (double)(ui * vk + uk * vi) * A->xz +
+           (double)(uj * vk + uk * vj) * A->yz;
+}
+
+/* neighbour offsets in the local frame, st first, then the rim in order */
+static const int ORC_RIM[8][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, -1}};
+
+static void orc_ell_vertex(double *tn, const orc_aq *A, double tp, int i, int j)
+{
+    if (!(*tn > tp)) return;
+    double c = orc_bf(A, -i, -j, 1, -i, -j, 1);
+    if (c > 0.0) {
+        double cand = tp + sqrt(c);
+        if (cand < *tn) *tn = cand;
+    }
+}
+
+/* edge from P (pi,pj) with time tp to Q (qi,qj) with time tq */
+static void orc_ell_edge(double *tn, const orc_aq *A, double tp, double tq, int pi, int pj, int qi, int qj)
+{
+    if (!(*tn > omin(tp, tq))) return;
+    const int ei = qi - pi, ej = qj - pj;
+    double a = orc_bf(A, ei, ej, 0, ei, ej, 0);
+    double b = orc_bf(A, ei, ej, 0, -pi, -pj, 1);
+    double c = orc_bf(A, -pi, -pj, 1, -pi, -pj, 1);
+    double d = tq - tp;
+    double den = a - d * d;
+    double disc = a * c - b * b;
+    if (den > 0.0 && disc > 0.0) {
+        double n = sqrt(disc / den);
+        double lam = (b - d * n) / a;
+        if (lam > 0.0 && lam < 1.0) {
+            double cand = tp + lam * d + n;
+            if (cand < *tn) *tn = cand;
+        }
+    }
+}
+
+/* triangle st (origin, time t0) - A (ai,aj, time ta) - B (bi,bj, time tb) */
+static void orc_ell_tri(double *tn, const orc_aq *A, double t0, double ta, double tb, int ai, int aj, int bi,
+                        int bj)
+{
+    if (!(*tn > omin(t0, omin(ta, tb)))) return;
+    double p11 = orc_bf(A, ai, aj, 0, ai, aj, 0);
+    double p12 = orc_bf(A, ai, aj, 0, bi, bj, 0);
+    double p22 = orc_bf(A, bi, bj, 0, bi, bj, 0);
+    double q1 = orc_bf(A, ai, aj, 0, 0, 0, 1);
+    double q2 = orc_bf(A, bi, bj, 0, 0, 0, 1);
+    double c = A->zz;
+    double d1 = ta - t0, d2 = tb - t0;
+    double det = p11 * p22 - p12 * p12;
+    if (!(det > 0.0)) return;
+    double u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
+    double w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
+    double s = (d1 * u1 + d2 * u2) / det;
+    double r = c - (q1 * w1 + q2 * w2) / det;
+    if (s < 1.0 && r > 0.0) {
+        double n = sqrt(r / (1.0 - s));
+        double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
+        if (l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0) {
+            double cand = t0 + (l1 * d1 + l2 * d2) + n;
+            if (cand < *tn) *tn = cand;
+        }
+    }
+}
+
+/* New signed value of a target from st and the rim values nb[8] (ORC_RIM order). */
+static double orc_ell_point(double told, double st, const double nb[8], const orc_aq *A)
+{
+    double tn = fabs(told);
+    orc_ell_vertex(&tn, A, st, 0, 0);
+    double m = st;
+    for (int r = 0; r < 8; ++r) m = omin(m, nb[r]);
+    if (tn > m) {
+        for (int r = 0; r < 8; ++r) orc_ell_vertex(&tn, A, nb[r], ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) orc_ell_edge(&tn, A, st, nb[r], 0, 0, ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) {
+            const int s = (r + 1) & 7;
+            orc_ell_edge(&tn, A, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0], ORC_RIM[s][1]);
+        }
+        for (int r = 0; r < 8; ++r) {
+            const int s = (r + 1) & 7;
+            orc_ell_tri(&tn, A, st, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0], ORC_RIM[s][1]);
+        }
+    }
+    return ((told > 0) ? 1.0 : -1.0) * tn;
+}
+
+/* index of the global metric component (p,q), arrays ordered xx xy xz yy yz zz */
+static int orc_mi(int p, int q)
+{
+    if (p > q) { int t = p; p = q; q = t; }
+    static const int tab[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    return tab[p][q];
+}
+
+/* One plane step of the elliptical medium.  M: six float arrays (xx, xy, xz,
+ * yy, yz, zz of the metric in the i, j, k axes) in the field layout. */
+void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                   int dir, int src)
+{
+    const orc_grid g = orc_make_grid(nx, ny, nz);
+    const orc_dir d = ORC_DIRS[dir];
+    const double h[3] = {dx, dy, dz};
+    const double hz = h[d.nrm], hx = h[d.xa], hy = h[d.ya];
+    const int ax[3] = {d.xa, d.ya, d.nrm};
+    const int sgn[3] = {d.xs, d.ys, d.sg};
+    const int64_t sn = g.stride[d.nrm];
+    const int64_t sx = d.xs * g.stride[d.xa], sy = d.ys * g.stride[d.ya];
+    int u = (d.nrm == 0) ? 1 : 0;
+    int v = (d.nrm == 2) ? 1 : 2;
+    const int nu = g.n[u], nv = g.n[v];
+    const int64_t su = g.stride[u], sv = g.stride[v];
+#pragma omp parallel for schedule(static)
+    for (int b = 1; b <= nv; ++b)
+        for (int c = 1; c <= nu; ++c) {
+            const int64_t s = (int64_t)src * sn + (int64_t)c * su + (int64_t)b * sv;
+            const int64_t t = s + d.sg * sn;
+            /* local metric M'_pq = s_p s_q M[ax_p][ax_q], scaled by the spacings */
+            orc_aq A;
+            A.xx = (double)M[orc_mi(ax[0], ax[0])][t] * hx * hx;
+            A.yy = (double)M[orc_mi(ax[1], ax[1])][t] * hy * hy;
+            A.zz = (double)M[orc_mi(ax[2], ax[2])][t] * hz * hz;
+            A.xy = (double)(sgn[0] * sgn[1]) * (double)M[orc_mi(ax[0], ax[1])][t] * hx * hy;
+            A.xz = (double)(sgn[0] * sgn[2]) * (double)M[orc_mi(ax[0], ax[2])][t] * hx * hz;
+            A.yz = (double)(sgn[1] * sgn[2]) * (double)M[orc_mi(ax[1], ax[2])][t] * hy * hz;
+            double nb[8];
+            for (int r = 0; r < 8; ++r) nb[r] = fabs(T[s + ORC_RIM[r][0] * sx + ORC_RIM[r][1] * sy]);
+            T[t] = orc_ell_point(T[t], fabs(T[s]), nb, &A);
+        }
+}
+
+/* Sweeps of the elliptical medium in the reference's direction order;
+ * semantics as orc_solve. */
+int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                  int nsweeps, double tol, double *last_delta)
+{
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    const int n[3] = {nx, ny, nz};
+    double *prev = (double *)malloc(cells * sizeof(double));
+    if (!prev) return -1;
+    int s = 0;
+    double delta = 0.0;
+    for (s = 0; s < nsweeps;) {
+        memcpy(prev, T, cells * sizeof(double));
+        for (int dir = 0; dir < 6; ++dir) {
+            const orc_dir d = ORC_DIRS[dir];
+            const int nn = n[d.nrm];
+            if (d.sg > 0)
+                for (int p = 1; p < nn; ++p) orc_ell_plane(T, M, nx, ny, nz, dx, dy, dz, dir, p);
+            else
+                for (int p = nn; p > 1; --p) orc_ell_plane(T, M, nx, ny, nz, dx, dy, dz, dir, p);
+        }
+        ++s;
+        delta = 0.0;
+        for (size_t c = 0; c < cells; ++c) {
+            double e = fabs(T[c] - prev[c]);
+            if (e > delta) delta = e;
+        }
+        if (tol >= 0.0 && delta <= tol) break;
+    }
+    free(prev);
+    if (last_delta) *last_delta = delta;
+    return s;
+}

@@ -147,3 +147,83 @@ def test_product_point_init(f3d):
     assert T[1, 3, 2] == 0.0
     T[1, 3, 2] = MAXT
     assert np.all(T == MAXT)
+
+
+# -- elliptical (tilted) medium: the project's own solver -------------------
+
+def _ellip_errors(T, M6, c, n, h, rmin):
+    import media
+
+    errs = []
+    for kk in range(1, n + 1, 3):
+        for jj in range(1, n + 1, 3):
+            for ii in range(1, n + 1, 3):
+                ex = media.exact_time(M6, (ii - c) * h, (jj - c) * h, (kk - c) * h)
+                if ex > rmin:
+                    errs.append(abs(abs(T[kk, jj, ii]) - ex) / ex)
+    return max(errs), float(np.mean(errs))
+
+
+def test_oracle_ellip_matches_closed_form():
+    """Point source in the tilted ellipse of the 128^3 configuration (Vz 2000,
+    Vx = Vy = 2400 m/s, tilt 30, azimuth 45 degrees; here 40^3, h = 10 m):
+    the converged solve agrees with t = sqrt(x^T M x) to first-order accuracy
+    (reported: max and mean relative error away from the source)."""
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    n, h = 40, 10.0
+    eps = ((2400.0 / 2000.0) ** 2 - 1.0) / 2.0
+    M = [m.numpy() for m in media.homogeneous_ellip(n, n, n, 2000.0, eps, 30.0, 45.0)]
+    c = n // 2 + 1
+    T = o.init_point(n, n, n, (c, c, c))
+    s, d = o.ell_solve(T, M, (h, h, h), 100, tol=1e-10)
+    assert d <= 1e-10 and s < 10
+    mx, mean = _ellip_errors(T, [M[k][c, c, c] for k in range(6)], c, n, h, 0.05)
+    assert mx < 0.05 and mean < 0.02, (mx, mean)
+
+
+def test_oracle_ellip_isotropic_symmetry():
+    """Isotropic metric: the converged field is symmetric under the grid's
+    reflections (the sweep order is not, so this checks the solver)."""
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    n = 21
+    M = [m.numpy() for m in media.homogeneous_ellip(n, n, n, 1500.0, 0.0, 0.0, 0.0)]
+    T = o.init_point(n, n, n, (11, 11, 11))
+    o.ell_solve(T, M, (5.0, 5.0, 5.0), 100, tol=0.0)
+    inner = T[1:-1, 1:-1, 1:-1]
+    for ax in range(3):
+        assert np.allclose(inner, np.flip(inner, axis=ax), rtol=1e-12, atol=0)
+    assert np.allclose(inner, inner.transpose(2, 1, 0), rtol=1e-12, atol=0)
+
+
+def test_ellip_metric_helper_matches_generator(f3d):
+    import math
+
+    import media
+    import torch
+
+    th, ph = math.radians(30.0), math.radians(45.0)
+    ref = media.metric_from(torch.tensor(2000.0, dtype=torch.float64), torch.tensor(0.22, dtype=torch.float64),
+                            tuple(torch.tensor(v, dtype=torch.float64) for v in
+                                  (math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th))))
+    got = f3d.ellip_metric(2000.0, 0.22, (math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)))
+    assert [float(r) for r in ref] == got
+
+
+def test_heterogeneous_tti_generator_is_seeded_and_spd():
+    import media
+    import torch
+
+    a = media.heterogeneous_tti(24, 20, 28, 10.0, seed=0)
+    b = media.heterogeneous_tti(24, 20, 28, 10.0, seed=0)
+    c = media.heterogeneous_tti(24, 20, 28, 10.0, seed=1)
+    assert all(torch.equal(x, y) for x, y in zip(a, b))
+    assert not torch.equal(a[0], c[0])
+    xx, xy, xz, yy, yz, zz = (m.double() for m in a)
+    det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * xz) + xz * (xy * yz - yy * xz)
+    assert bool((xx > 0).all()) and bool((xx * yy - xy * xy > 0).all()) and bool((det > 0).all())

@@ -365,3 +365,62 @@ def test_wavefront_bounded_wait_times_out_cleanly(f3d, ctx, cuda, golden):
     n = 16
     out, _ = gpu_solve(f3d, ctx, cuda, golden[n]["init"], (ref_spacing(n),) * 3, 8, engine="wavefront-skip")
     assert_bitwise(out, golden[n]["s8"], "after the timeout")
+
+
+# -- elliptical (tilted) medium ----------------------------------------------
+
+def _ell_case(kind, dims, h, seed=0):
+    import media
+
+    nx, ny, nz = dims
+    if kind == "homog":
+        eps = ((2400.0 / 2000.0) ** 2 - 1.0) / 2.0
+        return media.homogeneous_ellip(nx, ny, nz, 2000.0, eps, 30.0, 45.0)
+    return media.heterogeneous_tti(nx, ny, nz, h, seed=seed)
+
+
+@pytest.mark.parametrize("kind,dims,src", [("homog", (40, 40, 40), (21, 21, 21)),
+                                           ("tti", (37, 29, 33), (5, 20, 9)),
+                                           ("tti", (64, 64, 64), (33, 33, 9))])
+@pytest.mark.parametrize("skip", [False, True])
+def test_ellip_matches_oracle(f3d, orc, ctx, cuda, kind, dims, src, skip):
+    """The elliptical solver on the GPU (wavefront engine) equals the FP64 CPU
+    statement bit for bit, after 3 fixed sweeps and when run to
+    max|dT| <= 1e-10."""
+    h = (10.0, 10.0, 10.0)
+    M = _ell_case(kind, dims, h[0])
+    Md = [m.cuda() for m in M]
+    Mh = [m.numpy() for m in M]
+    T0 = orc.init_point(*dims, src)
+    for fixed, sweeps, tol in ((True, 3, 0.0), (False, 300, 1e-10)):
+        ref = T0.copy()
+        s_ref, d_ref = orc.ell_solve(ref, Mh, h, sweeps, tol=(-1.0 if fixed else tol))
+        d = cuda.from_numpy(T0.copy()).cuda()
+        rep = f3d.solve_ellip(ctx, d, h, Md, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol, skip=skip))
+        assert rep.sweeps == s_ref
+        assert rep.max_delta == d_ref
+        assert_bitwise(d.cpu().numpy(), ref, "%s %s fixed=%s" % (kind, dims, fixed))
+
+
+def test_ellip_full_size_skip_exact_512(f3d, ctx, cuda):
+    """512^3 heterogeneous TTI medium (seed 0), source at depth 64: the run to
+    max|dT| <= 1e-10 with tile skipping equals the run without, bit for bit,
+    and skipping evaluates fewer points."""
+    import media
+
+    n = 512
+    M = [m.cuda() for m in media.heterogeneous_tti(n, n, n, 10.0, seed=0, device="cuda")]
+    T0 = torch_point(cuda, n, (257, 257, 65))
+    a, b = T0.clone(), T0
+    o = dict(max_sweeps=200, fixed=False, tol=1e-10)
+    ra = f3d.solve_ellip(ctx, a, 10.0, M, f3d.opts(skip=False, **o))
+    rb = f3d.solve_ellip(ctx, b, 10.0, M, f3d.opts(skip=True, **o))
+    assert ra.sweeps == rb.sweeps and ra.max_delta == rb.max_delta <= 1e-10
+    assert cuda.equal(a.view(cuda.int64), b.view(cuda.int64))
+    assert rb.evaluated_updates < ra.evaluated_updates
+
+
+def torch_point(cuda, n, src):
+    T = cuda.full((n + 2,) * 3, 10e15 * 1.0, dtype=cuda.float64, device="cuda")
+    T[src[2], src[1], src[0]] = 0.0
+    return T
