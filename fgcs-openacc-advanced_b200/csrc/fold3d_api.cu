@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <cstring>
 #include <map>
+#include <numeric>
+#include <vector>
 #include <mutex>
 #include <string>
 
@@ -149,8 +151,16 @@ struct fold3d_ctx {
     unsigned *w_mod[3] = {nullptr, nullptr, nullptr};
     unsigned *w_counters = nullptr;          // [0] work, [1] status
     unsigned long long *w_evaluated = nullptr;
-    unsigned epoch = 0;                      // passes run so far on this context
-    int sms = 0, wave_bps = 0, wave_bps_ell = 0;
+    unsigned epoch = 0;                      // passes run so far on this context (never decreases)
+    int sms = 0, wave_bps = 0, wave_bps_ell = 0, batch_bps = 0;
+    // batched solves: per-instance scratch and per-direction staging
+    std::vector<int> bkey;                   // dims of the instances the scratch is sized for
+    unsigned *b_scratch = nullptr;           // flags and change maps of all instances
+    std::vector<size_t> b_flag_off, b_mod_off[3];
+    unsigned long long *b_slots = nullptr;   // [2n]: max|dT| and evaluated points per instance
+    unsigned *b_counters = nullptr;          // work, status
+    char *b_stage_d = nullptr, *b_stage_h = nullptr;
+    size_t b_stage_bytes = 0;
 };
 
 namespace {
@@ -221,6 +231,11 @@ void fold3d_destroy(fold3d_ctx *c)
         if (c->w_mod[b]) cudaFree(c->w_mod[b]);
     if (c->w_counters) cudaFree(c->w_counters);
     if (c->w_evaluated) cudaFree(c->w_evaluated);
+    if (c->b_scratch) cudaFree(c->b_scratch);
+    if (c->b_slots) cudaFree(c->b_slots);
+    if (c->b_counters) cudaFree(c->b_counters);
+    if (c->b_stage_d) cudaFree(c->b_stage_d);
+    if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
     if (c->d_maxd) cudaFree(c->d_maxd);
     if (c->h_maxd) cudaFreeHost(c->h_maxd);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -321,6 +336,27 @@ static void orient_tiles(const fold3d_grid &g, int b, int &ntu, int &ntv)
     ntv = (n[vb] + kWaveTV - 1) / kWaveTV;
 }
 
+// Pass numbers travel as (pass << 1) | changed in 32-bit flags.  Far before
+// that overflows, every flag and change map is cleared and numbering restarts.
+static int reserve_passes(fold3d_ctx *c, unsigned passes)
+{
+    if (c->epoch + passes < (1u << 30)) return FOLD3D_OK;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_error(e, "cudaDeviceSynchronize");
+    if (c->w_flags) {
+        c->key_wg = fold3d_grid{};
+        cudaFree(c->w_flags);
+        c->w_flags = nullptr;
+    }
+    if (c->b_scratch) {
+        cudaFree(c->b_scratch);
+        c->b_scratch = nullptr;
+    }
+    c->bkey.clear();
+    c->epoch = 0;
+    return FOLD3D_OK;
+}
+
 static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
 {
     if (c->w_flags && c->key_wg.nx == g.nx && c->key_wg.ny == g.ny && c->key_wg.nz == g.nz) return FOLD3D_OK;
@@ -357,8 +393,7 @@ static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
         c->wave_bps = wave_blocks_per_sm(kMediumDrift);
         c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
-    c->epoch = 0;  // fresh flags and maps
-    c->key_wg = g;
+    c->key_wg = g;  // fresh flags and maps are zero, below every pass number to come
     return FOLD3D_OK;
 }
 
@@ -390,8 +425,9 @@ static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int d
 static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
                            double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
 {
-    int rc = wave_scratch(c, g);
+    int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
     if (rc) return rc;
+    if ((rc = wave_scratch(c, g))) return rc;
     cudaError_t e;
     if ((e = cudaMemsetAsync(c->w_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess ||
         (e = cudaMemsetAsync(c->w_evaluated, 0, sizeof(unsigned long long), s)) != cudaSuccess)
@@ -478,7 +514,260 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
     return FOLD3D_OK;
 }
 
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+static int batch_scratch(fold3d_ctx *c, int n, const fold3d_instance *in)
+{
+    std::vector<int> key(3 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        key[3 * i] = in[i].grid.nx;
+        key[3 * i + 1] = in[i].grid.ny;
+        key[3 * i + 2] = in[i].grid.nz;
+    }
+    if (c->b_scratch && key == c->bkey) return FOLD3D_OK;
+    if (c->b_scratch) cudaFree(c->b_scratch);
+    if (c->b_slots) cudaFree(c->b_slots);
+    if (c->b_stage_d) cudaFree(c->b_stage_d);
+    if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
+    c->b_scratch = nullptr;
+    c->b_slots = nullptr;
+    c->b_stage_d = c->b_stage_h = nullptr;
+    c->bkey.clear();
+    size_t words = 0;
+    int max_steps = 0;
+    c->b_flag_off.assign(n, 0);
+    for (int b = 0; b < 3; ++b) c->b_mod_off[b].assign(n, 0);
+    for (int i = 0; i < n; ++i) {
+        const fold3d_grid &g = in[i].grid;
+        const int dims[3] = {g.nx, g.ny, g.nz};
+        size_t fw = 0;
+        for (int b = 0; b < 3; ++b) {
+            int ntu, ntv;
+            orient_tiles(g, b, ntu, ntv);
+            fw = std::max(fw, (size_t)(dims[b] - 1) * ntu * ntv);
+            c->b_mod_off[b][i] = words;
+            words += (size_t)(dims[b] + 2) * ntu * ntv;
+            max_steps = std::max(max_steps, dims[b] - 1);
+        }
+        c->b_flag_off[i] = words;
+        words += fw;
+    }
+    cudaError_t e;
+    if ((e = cudaMalloc(&c->b_scratch, words * 4)) != cudaSuccess ||
+        (e = cudaMemset(c->b_scratch, 0, words * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&c->b_slots, 2 * (size_t)n * 8)) != cudaSuccess)
+        return set_error(FOLD3D_ERR_NOMEM, std::string("batch scratch: ") + cudaGetErrorString(e));
+    if (!c->b_counters && (e = cudaMalloc(&c->b_counters, 2 * sizeof(unsigned))) != cudaSuccess)
+        return set_error(FOLD3D_ERR_NOMEM, std::string("batch scratch: ") + cudaGetErrorString(e));
+    // per direction: inst[n], step_off[max_steps+1], step_k[max_steps], tile_pre[n+1]
+    const size_t per = align_up((size_t)n * sizeof(BatchInst), 256) + align_up((max_steps + 1) * 8, 256) +
+                       align_up((size_t)max_steps * 4, 256) + align_up(((size_t)n + 1) * 8, 256);
+    c->b_stage_bytes = per;
+    if ((e = cudaMalloc(&c->b_stage_d, 6 * per)) != cudaSuccess ||
+        (e = cudaMallocHost(&c->b_stage_h, 6 * per)) != cudaSuccess)
+        return set_error(FOLD3D_ERR_NOMEM, std::string("batch staging: ") + cudaGetErrorString(e));
+    if (!c->sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
+        c->wave_bps = wave_blocks_per_sm(kMediumDrift);
+        c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
+    }
+    if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm();
+    c->bkey = key;
+    return FOLD3D_OK;
+}
+
+// Staging layout of direction dir: pointers into the host or device copy.
+struct BatchStage {
+    BatchInst *inst;
+    long long *step_off;
+    int *step_k;
+    long long *tile_pre;
+};
+static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
+{
+    int max_steps = 0;
+    for (size_t i = 0; i < c->bkey.size(); ++i) max_steps = std::max(max_steps, c->bkey[i] - 1);
+    char *p = base + (size_t)dir * c->b_stage_bytes;
+    BatchStage s;
+    s.inst = reinterpret_cast<BatchInst *>(p);
+    p += align_up((size_t)n * sizeof(BatchInst), 256);
+    s.step_off = reinterpret_cast<long long *>(p);
+    p += align_up((max_steps + 1) * 8, 256);
+    s.step_k = reinterpret_cast<int *>(p);
+    p += align_up((size_t)max_steps * 4, 256);
+    s.tile_pre = reinterpret_cast<long long *>(p);
+    return s;
+}
+
+static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts &o, cudaStream_t s,
+                       fold3d_report *reps)
+{
+    int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
+    if (rc) return rc;
+    if ((rc = batch_scratch(c, n, in))) return rc;
+    cudaError_t e;
+    std::vector<char> active(n, 1);
+    std::vector<int> sweeps(n, 0);
+    std::vector<double> delta(n, 0.0);
+    std::vector<unsigned long long> slots(2 * (size_t)n);
+    if ((e = cudaMemsetAsync(c->b_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_slots + n, 0, (size_t)n * 8, s)) != cudaSuccess)
+        return cuda_error(e, "cudaMemsetAsync");
+    const unsigned e0 = c->epoch + 1;
+    const unsigned skip_from = o.skip ? e0 + 6 : 0xffffffffu;
+    int max_steps = 0;
+    for (int v : c->bkey) max_steps = std::max(max_steps, v - 1);
+    BatchArgs args[6];
+    // (re)build the six directions' staging for the current active set
+    auto stage = [&]() -> int {
+        for (int dir = 0; dir < 6; ++dir) {
+            const DirSpec &d = kDirs[dir];
+            BatchStage h = batch_stage(c, c->b_stage_h, dir, n);
+            BatchStage dv = batch_stage(c, c->b_stage_d, dir, n);
+            std::vector<int> order;
+            for (int i = 0; i < n; ++i)
+                if (active[i]) order.push_back(i);
+            auto steps_of = [&](int i) {
+                const int dims[3] = {in[i].grid.nx, in[i].grid.ny, in[i].grid.nz};
+                return dims[d.nrm] - 1;
+            };
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return steps_of(x) > steps_of(y); });
+            const int k = (int)order.size();
+            h.tile_pre[0] = 0;
+            for (int q = 0; q < k; ++q) {
+                const int i = order[q];
+                const fold3d_grid &g = in[i].grid;
+                BatchInst &bi = h.inst[q];
+                memset(&bi, 0, sizeof bi);
+                WaveArgs &a = bi.a;
+                a.pg = make_geom(g, dir);
+                a.nrm = d.nrm;
+                a.ua = (d.nrm == 0) ? 1 : 0;
+                a.va = (d.nrm == 2) ? 1 : 2;
+                a.sg = d.sg;
+                orient_tiles(g, d.nrm, a.ntu, a.ntv);
+                a.steps = pass_count(a.pg);
+                a.first_src = pass_first(a.pg, dir);
+                a.timeout_ns = 4000000000ull;
+                a.flags = c->b_scratch + c->b_flag_off[i];
+                for (int b = 0; b < 3; ++b) {
+                    int ntu, ntv;
+                    orient_tiles(g, b, ntu, ntv);
+                    a.mod[b] = c->b_scratch + c->b_mod_off[b][i];
+                    a.mod_ntu[b] = ntu;
+                    a.mod_ntiles[b] = ntu * ntv;
+                }
+                a.work = c->b_counters;
+                a.status = c->b_counters + 1;
+                a.maxd = c->b_slots + i;
+                a.evaluated = c->b_slots + n + i;
+                bi.p = ellip_param(g, in[i].medium, dir);
+                bi.T = in[i].T;
+                h.tile_pre[q + 1] = h.tile_pre[q] + (long long)a.ntu * a.ntv;
+            }
+            h.step_off[0] = 0;
+            for (int p = 0; p < max_steps; ++p) {
+                int kk = 0;
+                while (kk < k && steps_of(order[kk]) > p) ++kk;
+                h.step_k[p] = kk;
+                h.step_off[p + 1] = h.step_off[p] + h.tile_pre[kk];
+            }
+            if (h.step_off[max_steps] >= (1ll << 31)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
+            args[dir].inst = dv.inst;
+            args[dir].step_off = dv.step_off;
+            args[dir].step_k = dv.step_k;
+            args[dir].tile_pre = dv.tile_pre;
+            args[dir].max_steps = max_steps;
+            args[dir].total = (unsigned)h.step_off[max_steps];
+            args[dir].work = c->b_counters;
+            args[dir].status = c->b_counters + 1;
+            args[dir].skip_from = skip_from;
+        }
+        cudaError_t ce = cudaMemcpyAsync(c->b_stage_d, c->b_stage_h, 6 * c->b_stage_bytes, cudaMemcpyHostToDevice, s);
+        return ce == cudaSuccess ? FOLD3D_OK : cuda_error(ce, "batch staging upload");
+    };
+    if ((rc = stage())) return rc;
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    int sweep = 0, left = n;
+    unsigned hstat[2] = {0, 0};
+    while (sweep < o.max_sweeps && left > 0) {
+        if ((e = cudaMemsetAsync(c->b_slots, 0, (size_t)n * 8, s)) != cudaSuccess) return cuda_error(e, "memset");
+        for (int dir = 0; dir < 6; ++dir) {
+            args[dir].epoch = ++c->epoch;
+            const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_bps);
+            if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
+                return cuda_error(e, "memset");
+            if (grid > 0 && (e = launch_batch_pass(args[dir], grid, s)) != cudaSuccess)
+                return cuda_error(e, "batch pass");
+        }
+        ++sweep;
+        for (int i = 0; i < n; ++i)
+            if (active[i]) ++sweeps[i];
+        if (!o.fixed || sweep == o.max_sweeps) {
+            if ((e = cudaMemcpyAsync(slots.data(), c->b_slots, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpyAsync(hstat, c->b_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+                return cuda_error(e, "cudaMemcpyAsync");
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "sweep");
+            if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "batch: a dependency wait gave up");
+            bool changed = false;
+            for (int i = 0; i < n; ++i) {
+                if (!active[i]) continue;
+                memcpy(&delta[i], &slots[i], 8);
+                if (!o.fixed && delta[i] <= o.tol) {
+                    active[i] = 0;
+                    --left;
+                    changed = true;
+                }
+            }
+            if (changed && left > 0 && (rc = stage())) return rc;
+        }
+    }
+    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    if ((e = cudaMemcpyAsync(slots.data() + n, c->b_slots + n, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_error(e, "batch");
+    if (reps) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        for (int i = 0; i < n; ++i) {
+            reps[i].sweeps = sweeps[i];
+            reps[i].max_delta = delta[i];
+            reps[i].elapsed_ms = ms;
+            reps[i].nominal_updates = nominal_per_sweep(in[i].grid) * (uint64_t)sweeps[i];
+            reps[i].evaluated_updates = slots[n + i];
+            reps[i].engine = FOLD3D_ENGINE_WAVEFRONT;
+        }
+    }
+    return FOLD3D_OK;
+}
+
 extern "C" {
+
+int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts *o, void *stream,
+                       fold3d_report *reps)
+{
+    clear_error();
+    if (!c || !in || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (n < 1) return set_error(FOLD3D_ERR_INVALID, "n must be >= 1");
+    for (int i = 0; i < n; ++i) {
+        int rc = check_grid(&in[i].grid);
+        if (rc) return rc;
+        const fold3d_ellip &m = in[i].medium;
+        if (!in[i].T || !m.mxx || !m.mxy || !m.mxz || !m.myy || !m.myz || !m.mzz)
+            return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
+    }
+    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "batched solves run on the wavefront engine, variant 0");
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return solve_batch(c, n, in, *o, s, reps);
+}
 
 int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
                  const fold3d_opts *o, void *stream, fold3d_report *rep)

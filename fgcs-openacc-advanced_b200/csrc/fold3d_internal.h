@@ -92,6 +92,35 @@ cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, 
 cudaError_t launch_wave_pass_ellip(double *T, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s);
 int wave_blocks_per_sm(int medium);
 
+}  // namespace fold3d
+#include "fold3d_ellip.cuh"
+namespace fold3d {
+
+// One instance of a batched pass (fold3d_wavefront.cu): its pass arguments,
+// elliptical-medium constants and field.
+struct BatchInst {
+    WaveArgs a;
+    EllipParam p;
+    double *T;
+};
+static_assert(sizeof(BatchInst) % 4 == 0, "BatchInst is copied in words");
+
+// One batched pass: the active instances sorted by step count (descending),
+// the first global item of each step, the number of instances with a step p,
+// and the prefix sums of the instances' tiles per plane.
+struct BatchArgs {
+    const BatchInst *inst;
+    const long long *step_off;  // [max_steps + 1]
+    const int *step_k;          // [max_steps]
+    const long long *tile_pre;  // [active + 1]
+    int max_steps;
+    unsigned total;
+    unsigned *work, *status;
+    unsigned epoch, skip_from;  // pass number and first pass that may skip
+};
+cudaError_t launch_batch_pass(const BatchArgs &b, int grid, cudaStream_t s);
+int batch_blocks_per_sm();
+
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,
                          int variant, int src, unsigned long long *maxd, cudaStream_t s);

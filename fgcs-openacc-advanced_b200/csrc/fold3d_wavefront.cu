@@ -81,24 +81,142 @@ template <> struct WaveMedium<kMediumEllip> {
     using type = EllipParam;
 };
 
+// One work item (step p, tile t) of one grid, for all threads of the CTA:
+// wait for the 3 x 3 tiles of step p-1, then skip or update the tile, then
+// publish its flag.  Adds each changed point's |dT| into dmax and the
+// evaluated points into evaluated.  Returns false if a wait gave up (the
+// item is then left unpublished and the caller must leave).
+template <int MED>
+__device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs &a,
+                                          const typename WaveMedium<MED>::type &tab, int item, double &dmax,
+                                          unsigned long long &evaluated)
+{
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const PlaneGeom &g = a.pg;
+    const int ntiles = a.ntu * a.ntv;
+    const unsigned want = a.epoch << 1;  // flags hold (pass << 1) | changed
+    const bool may_skip = a.epoch >= a.skip_from;
+    const int p = item / ntiles, t = item - p * ntiles;
+    const int tu = t % a.ntu, tv = t / a.ntu;
+    const int src = a.first_src + p * a.sg;
+    const int tgt = src + a.sg;
+
+    // Threads 0..8 each watch one tile of the 3 x 3 neighbourhood: its change
+    // mark from earlier passes, and its step p-1 flag (which also says whether
+    // that item changed the source plane).
+    int timed_out = 0, recent = 0;
+    if (tid < 9) {
+        const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
+        if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
+            const int nt = nv * a.ntu + nu;
+            if (may_skip) recent = (__ldcg(a.mod[a.nrm] + (long long)src * ntiles + nt) + 5u >= a.epoch);
+            if (p > 0) {
+                const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nt;
+                const unsigned long long t0 = global_ns();
+                unsigned spins = 0, f;
+                while ((f = ld_acquire(fl)) < want) {
+                    if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
+                        *(volatile unsigned *)a.status != 0) {
+                        atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                        timed_out = 1;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (!timed_out) recent |= (int)(f & 1u);
+            }
+        }
+    }
+    if (__syncthreads_or(timed_out)) return false;
+    const int skip = may_skip && !__syncthreads_or(recent);
+
+    int changed = 0;
+    if (!skip) {
+        const int u = tu * 32 + lane + 1;
+        const int v = tv * kWaveTV + warp + 1;
+        if (u <= g.nu && v <= g.nv) {
+            const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
+            const long long d = s + g.sn;
+            const double st = fabs(ld_cg(T + s));
+            const double xt = fabs(ld_cg(T + s + g.sx));
+            const double yt = fabs(ld_cg(T + s + g.sy));
+            const double xnt = fabs(ld_cg(T + s - g.sx));
+            const double ynt = fabs(ld_cg(T + s - g.sy));
+            const double txm = fabs(ld_cg(T + s + g.sx - g.sy));
+            const double txy = fabs(ld_cg(T + s + g.sx + g.sy));
+            const double tym = fabs(ld_cg(T + s - g.sx + g.sy));
+            const double txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
+            const double told = ld_cg(T + d);
+            double tnew;
+            if constexpr (MED == kMediumDrift) {
+                tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+            } else {
+                const double nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
+                tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d));
+            }
+            if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
+                T[d] = tnew;
+                changed = 1;
+                dmax = fmax(dmax, fabs(tnew - told));
+                // mark the point's tile in the two other orientations
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int b = (q == 0) ? a.ua : a.va;
+                    const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
+                    const int cb = (q == 0) ? u : v;
+                    const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
+                    const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
+                    const int tile = ((cv - 1) / kWaveTV) * a.mod_ntu[b] + ((cu - 1) >> 5);
+                    a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
+                }
+            }
+            ++evaluated;
+        }
+        changed = __syncthreads_or(changed);
+        if (changed && tid == 0) a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
+    }
+    // publish (the barrier orders every thread's stores before thread 0's fence)
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        st_release(a.flags + item, want | (unsigned)changed);
+    }
+    return true;
+}
+
+// Block-wide maximum of d into *out (IEEE bits) and sum of e into *sum.
+__device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsigned long long *out,
+                                           unsigned long long *sum)
+{
+    __shared__ double wmax[kWaveTV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (lane == 0) {
+        wmax[warp] = d;
+        if (e) atomicAdd(sum, e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < kWaveTV; ++w) m = fmax(m, wmax[w]);
+        if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+}
+
 template <int MED>
 __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
     wave_pass_kernel(double *__restrict__ T, WaveArgs a, const __grid_constant__ typename WaveMedium<MED>::type tab)
 {
     __shared__ int s_next;
-    __shared__ double wmax[kWaveTV];
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    const PlaneGeom &g = a.pg;
-    const int ntiles = a.ntu * a.ntv;
-    const long long total = (long long)a.steps * ntiles;
-    // flags hold (pass << 1) | changed
-    const unsigned want = a.epoch << 1;
-    const bool may_skip = a.epoch >= a.skip_from;
+    const long long total = (long long)a.steps * a.ntu * a.ntv;
     double dmax = 0.0;
     unsigned long long evaluated = 0;
-
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         const unsigned w = atomicAdd(a.work, 1u);
         s_next = (w < total) ? (int)w : -1;
     }
@@ -107,7 +225,7 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
         const int item = s_next;
         if (item < 0) break;
         __syncthreads();  // every thread has read s_next
-        if (tid == 0) {   // claim the next item now; it is processed after this one
+        if (threadIdx.x == 0) {  // claim the next item now; it is processed after this one
             int it = -1;
             if (*(volatile unsigned *)a.status == 0) {
                 const unsigned w = atomicAdd(a.work, 1u);
@@ -115,105 +233,89 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
             }
             s_next = it;
         }
-        const int p = item / ntiles, t = item - p * ntiles;
-        const int tu = t % a.ntu, tv = t / a.ntu;
-        const int src = a.first_src + p * a.sg;
-        const int tgt = src + a.sg;
-
-        // Threads 0..8 each watch one tile of the 3 x 3 neighbourhood: its
-        // change mark from earlier passes, and its step p-1 flag (which also
-        // says whether that item changed the source plane).
-        int timed_out = 0, recent = 0;
-        if (tid < 9) {
-            const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
-            if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
-                const int nt = nv * a.ntu + nu;
-                if (may_skip) recent = (__ldcg(a.mod[a.nrm] + (long long)src * ntiles + nt) + 5u >= a.epoch);
-                if (p > 0) {
-                    const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nt;
-                    const unsigned long long t0 = global_ns();
-                    unsigned spins = 0, f;
-                    while ((f = ld_acquire(fl)) < want) {
-                        if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
-                            *(volatile unsigned *)a.status != 0) {
-                            atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
-                            timed_out = 1;
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                    if (!timed_out) recent |= (int)(f & 1u);
-                }
-            }
-        }
-        if (__syncthreads_or(timed_out)) break;  // leave without publishing
-        const int skip = may_skip && !__syncthreads_or(recent);
-
-        int changed = 0;
-        if (!skip) {
-            const int u = tu * 32 + lane + 1;
-            const int v = tv * kWaveTV + warp + 1;
-            if (u <= g.nu && v <= g.nv) {
-                const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
-                const long long d = s + g.sn;
-                const double st = fabs(ld_cg(T + s));
-                const double xt = fabs(ld_cg(T + s + g.sx));
-                const double yt = fabs(ld_cg(T + s + g.sy));
-                const double xnt = fabs(ld_cg(T + s - g.sx));
-                const double ynt = fabs(ld_cg(T + s - g.sy));
-                const double txm = fabs(ld_cg(T + s + g.sx - g.sy));
-                const double txy = fabs(ld_cg(T + s + g.sx + g.sy));
-                const double tym = fabs(ld_cg(T + s - g.sx + g.sy));
-                const double txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
-                const double told = ld_cg(T + d);
-                double tnew;
-                if constexpr (MED == kMediumDrift) {
-                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
-                } else {
-                    const double nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
-                    tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d));
-                }
-                if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
-                    T[d] = tnew;
-                    changed = 1;
-                    dmax = fmax(dmax, fabs(tnew - told));
-                    // mark the point's tile in the two other orientations
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const int b = (q == 0) ? a.ua : a.va;
-                        const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
-                        const int cb = (q == 0) ? u : v;
-                        const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
-                        const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
-                        const int tile = ((cv - 1) / kWaveTV) * a.mod_ntu[b] + ((cu - 1) >> 5);
-                        a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
-                    }
-                }
-                ++evaluated;
-            }
-            changed = __syncthreads_or(changed);
-            if (changed && tid == 0) a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
-        }
-        // publish (the barrier orders every thread's stores before thread 0's fence)
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release(a.flags + item, want | (unsigned)changed);
-        }
+        if (!wave_item<MED>(T, a, tab, item, dmax, evaluated)) break;
     }
+    wave_flush(dmax, evaluated, a.maxd, a.evaluated);
+}
 
-    // per-launch maximum |dT| and evaluated-point count
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    if (lane == 0) wmax[warp] = dmax;
-    for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-    if (lane == 0 && evaluated) atomicAdd(a.evaluated, evaluated);
+// ---------------------------------------------------------------------------
+// Batched passes: the items of one pass of many independent grids (the
+// elliptical medium) in one launch.  Items are ordered step-major across the
+// instances (step p of every instance that has one, then step p+1), the
+// instances sorted by their number of steps, so that the active instances of
+// a step are a prefix of the list; every item's predecessors (step p-1 of the
+// same instance) come earlier in that order, and the launch's claimed items
+// spread over many instances at once.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads) batch_pass_kernel(BatchArgs b)
+{
+    __shared__ int s_next;
+    __shared__ int s_loc[2];
+    __shared__ BatchInst s_inst;
+    if (threadIdx.x == 0) {
+        const unsigned w = atomicAdd(b.work, 1u);
+        s_next = (w < b.total) ? (int)w : -1;
+    }
     __syncthreads();
-    if (tid == 0) {
-        double m = 0.0;
-        for (int w = 0; w < kWaveTV; ++w) m = fmax(m, wmax[w]);
-        if (m > 0.0) atomicMax(a.maxd, (unsigned long long)__double_as_longlong(m));
+    for (;;) {
+        const int gitem = s_next;
+        if (gitem < 0) break;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int it = -1;
+            if (*(volatile unsigned *)b.status == 0) {
+                const unsigned w = atomicAdd(b.work, 1u);
+                if (w < b.total) it = (int)w;
+            }
+            s_next = it;
+            // step p: last step start <= gitem; instance: last tile prefix <= rest
+            int lo = 0, hi = b.max_steps;  // step_off[lo] <= gitem < step_off[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (b.step_off[mid] <= gitem) lo = mid; else hi = mid;
+            }
+            const int p = lo;
+            const long long r = gitem - b.step_off[p];
+            int il = 0, ih = b.step_k[p];
+            while (ih - il > 1) {
+                const int mid = (il + ih) >> 1;
+                if (b.tile_pre[mid] <= r) il = mid; else ih = mid;
+            }
+            const BatchInst &bi = b.inst[il];
+            s_loc[0] = il;
+            s_loc[1] = p * (bi.a.ntu * bi.a.ntv) + (int)(r - b.tile_pre[il]);
+        }
+        __syncthreads();
+        {
+            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + s_loc[0]);
+            unsigned *dst = reinterpret_cast<unsigned *>(&s_inst);
+            for (int w = threadIdx.x; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = src[w];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {  // the pass number is per launch, not per staged instance
+            s_inst.a.epoch = b.epoch;
+            s_inst.a.skip_from = b.skip_from;
+        }
+        __syncthreads();
+        double dmax = 0.0;
+        unsigned long long evaluated = 0;
+        if (!wave_item<kMediumEllip>(s_inst.T, s_inst.a, s_inst.p, s_loc[1], dmax, evaluated)) break;
+        wave_flush(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
     }
+}
+
+cudaError_t launch_batch_pass(const BatchArgs &b, int grid, cudaStream_t s)
+{
+    batch_pass_kernel<<<grid, kWaveThreads, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+int batch_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel, kWaveThreads, 0) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
 }
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)

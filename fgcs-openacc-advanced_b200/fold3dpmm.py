@@ -35,7 +35,7 @@ EXPORTED = (
     "fold3d_last_error", "fold3d_version", "fold3d_default_opts", "fold3d_create", "fold3d_destroy",
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
-    "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip",
+    "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -60,6 +60,10 @@ class Medium(C.Structure):
 
 class Ellip(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("mxx", "mxy", "mxz", "myy", "myz", "mzz")]
+
+
+class Instance(C.Structure):
+    _fields_ = [("grid", Grid), ("medium", Ellip), ("T", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -111,6 +115,7 @@ def lib() -> C.CDLL:
     L.fold3d_selftest_wait_timeout.argtypes = [vp, d]
     L.fold3d_ellip_metric.argtypes = [d, d, d, d, d, C.POINTER(C.c_float)]
     L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
+    L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
     L.InitFoldFromPoint.restype = d
     L.ImpSurfF.argtypes = [d] * 3
@@ -295,6 +300,23 @@ def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> 
     _check(lib().fold3d_solve_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), _dev_ptr(T),
                                     C.byref(o or opts()), C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
+
+
+def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream=None) -> list:
+    """fold3d_solve_batch: fields[i] (float64 CUDA tensors, in place), hs[i]
+    spacings, media[i] six float32 CUDA metric tensors.  Returns the
+    per-instance reports."""
+    n = len(fields)
+    arr = (Instance * n)()
+    for i, (T, h, M) in enumerate(zip(fields, hs, media)):
+        nx, ny, nz = grid_of(T)
+        arr[i].grid = grid(nx, ny, nz, h)
+        arr[i].medium = ellip(M)
+        arr[i].T = _dev_ptr(T)
+    reps = (Report * n)()
+    _check(lib().fold3d_solve_batch(ctx._h, n, arr, C.byref(o or opts()), C.c_void_p(stream) if stream else None,
+                                    reps))
+    return list(reps)
 
 
 def plane(T, h, dir_, src, med: Medium | None = None, stream=None):

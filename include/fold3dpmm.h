@@ -172,6 +172,24 @@ void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az,
 int fold3d_solve_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, double *T_dev,
                        const fold3d_opts *o, void *stream, fold3d_report *rep);
 
+/* One instance of a batched solve: its grid, elliptical medium and device
+ * field (in/out). */
+typedef struct {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    double *T;
+} fold3d_instance;
+
+/* Solves n independent instances (grids of any sizes, elliptical media) at
+ * once: every directional pass of all instances that are still running is
+ * one launch, whose CTAs take tiles of all instances from one queue.  No
+ * counterpart in the reference.  Unless opts.fixed, each instance stops
+ * after its first sweep with max|dT| <= opts.tol, the others go on.  Results
+ * are bit-identical to solving the instances one by one with
+ * fold3d_solve_ellip.  reps: n reports, or NULL. */
+int fold3d_solve_batch(fold3d_ctx *ctx, int n, const fold3d_instance *inst, const fold3d_opts *o,
+                       void *stream, fold3d_report *reps);
+
 /* Implicit-surface source initialisation of a host field (the reference's
  * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).
  * Uses all host cores. */

@@ -424,3 +424,56 @@ def torch_point(cuda, n, src):
     T = cuda.full((n + 2,) * 3, 10e15 * 1.0, dtype=cuda.float64, device="cuda")
     T[src[2], src[1], src[0]] = 0.0
     return T
+
+
+# -- batched solves -----------------------------------------------------------
+
+def _batch_instances(cuda, count, lo, hi, seed):
+    import media
+
+    rng = np.random.default_rng(seed)
+    inst = []
+    for i in range(count):
+        dims = tuple(int(v) for v in rng.integers(lo, hi + 1, 3))
+        M = [m.cuda() for m in media.heterogeneous_tti(*dims, 10.0, seed=100 + i)]
+        src = tuple(int(rng.integers(1, d + 1)) for d in dims)
+        T = torch_point_dims(cuda, dims, src)
+        inst.append((T, M))
+    return inst
+
+
+def torch_point_dims(cuda, dims, src):
+    nx, ny, nz = dims
+    T = cuda.full((nz + 2, ny + 2, nx + 2), 10e15 * 1.0, dtype=cuda.float64, device="cuda")
+    T[src[2], src[1], src[0]] = 0.0
+    return T
+
+
+@pytest.mark.parametrize("fixed", [True, False])
+def test_batch_equals_one_by_one(f3d, ctx, cuda, fixed):
+    """A batch of instances with different (non-cubic) grids, media and
+    sources gives each instance exactly the field and sweep count of its own
+    fold3d_solve_ellip (3 fixed sweeps, or per-instance convergence to
+    max|dT| <= 1e-10 with instances stopping at different sweeps)."""
+    inst = _batch_instances(cuda, 7, 9, 41, seed=5)
+    o = f3d.opts(max_sweeps=3, fixed=True) if fixed else f3d.opts(max_sweeps=300, tol=1e-10)
+    alone = []
+    for T, M in inst:
+        t = T.clone()
+        r = f3d.solve_ellip(ctx, t, 10.0, M, o)
+        alone.append((t, r))
+    fields = [T.clone() for T, _ in inst]
+    reps = f3d.solve_batch(ctx, fields, [10.0] * len(inst), [M for _, M in inst], o)
+    sweeps = set()
+    for (t, r), f, rb in zip(alone, fields, reps):
+        assert rb.sweeps == r.sweeps and rb.max_delta == r.max_delta
+        assert rb.nominal_updates == r.nominal_updates
+        assert cuda.equal(t.view(cuda.int64), f.view(cuda.int64))
+        sweeps.add(r.sweeps)
+    if not fixed:
+        assert len(sweeps) > 1  # instances did stop at different sweeps
+
+
+def test_batch_rejects_bad_input(f3d, ctx, cuda):
+    L = f3d.lib()
+    assert L.fold3d_solve_batch(ctx._h, 0, None, C.byref(f3d.opts()), None, None) == f3d.ERR_INVALID
