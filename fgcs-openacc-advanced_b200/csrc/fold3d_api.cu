@@ -159,6 +159,8 @@ struct fold3d_ctx {
     std::vector<size_t> b_flag_off, b_mod_off[3];
     unsigned long long *b_slots = nullptr;   // [2n]: max|dT| and evaluated points per instance
     unsigned *b_counters = nullptr;          // work, status
+    double *adj_pushed = nullptr;            // adjoint: lambda already pushed, per cell
+    size_t adj_cells = 0;
     char *b_stage_d = nullptr, *b_stage_h = nullptr;
     size_t b_stage_bytes = 0;
 };
@@ -234,6 +236,7 @@ void fold3d_destroy(fold3d_ctx *c)
     if (c->b_scratch) cudaFree(c->b_scratch);
     if (c->b_slots) cudaFree(c->b_slots);
     if (c->b_counters) cudaFree(c->b_counters);
+    if (c->adj_pushed) cudaFree(c->adj_pushed);
     if (c->b_stage_d) cudaFree(c->b_stage_d);
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
     if (c->d_maxd) cudaFree(c->d_maxd);
@@ -423,7 +426,8 @@ static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int d
 }
 
 static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
-                           double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep)
+                           double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep,
+                           unsigned short *winners = nullptr)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
     if (rc) return rc;
@@ -468,6 +472,8 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
             a.steps = pass_count(a.pg);
             a.first_src = pass_first(a.pg, dir);
             a.epoch = ++c->epoch;
+            a.dir = dir;
+            a.winners = winners;
             const long long items = (long long)a.steps * a.ntu * a.ntv;
             const int bps = em ? c->wave_bps_ell : c->wave_bps;
             const int grid = (int)std::min<long long>(items, (long long)c->sms * bps);
@@ -889,6 +895,101 @@ int fold3d_solve_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     return solve_wavefront(c, *g, nullptr, m, T, *o, s, rep);
+}
+
+int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T,
+                              unsigned short *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!W) return set_error(FOLD3D_ERR_INVALID, "winner array is NULL");
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    cudaError_t e = cudaMemsetAsync(W, 0xff, field_cells(*g) * sizeof(unsigned short), s);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
+    if (!T || !m || !o || !m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
+        return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "the elliptical medium runs on the wavefront engine, variant 0");
+    return solve_wavefront(c, *g, nullptr, m, T, *o, s, rep, W);
+}
+
+int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const double *T,
+                         const unsigned short *W, const double *dLdT, double *lam, double *dLdM, int max_sweeps,
+                         void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!c || !m || !T || !W || !dLdT || !lam || !dLdM) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    const size_t cells = field_cells(*g);
+    cudaError_t e;
+    if (c->adj_cells < cells) {
+        if (c->adj_pushed) cudaFree(c->adj_pushed);
+        c->adj_pushed = nullptr;
+        c->adj_cells = 0;
+        if ((e = cudaMalloc(&c->adj_pushed, cells * sizeof(double))) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "adjoint scratch");
+        c->adj_cells = cells;
+    }
+    if ((e = cudaMemcpyAsync(lam, dLdT, cells * sizeof(double), cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->adj_pushed, 0, cells * sizeof(double), s)) != cudaSuccess)
+        return cuda_error(e, "adjoint setup");
+    AdjGeom geo;
+    memset(&geo, 0, sizeof geo);
+    EllipParam ep[6];
+    for (int d = 0; d < 6; ++d) {
+        geo.pg[d] = make_geom(*g, d);
+        ep[d] = ellip_param(*g, *m, d);
+        geo.d[d] = ep[d].dir;
+    }
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    int sweeps = 0;
+    double delta = 0.0;
+    while (sweeps < max_sweeps) {
+        if ((e = cudaMemsetAsync(c->d_maxd, 0, 8, s)) != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
+        for (int d = 5; d >= 0; --d) {  // the forward order reversed
+            const PlaneGeom &pg = geo.pg[d];
+            // forward targets of direction d: first+sg .. ; walk them backwards
+            const int sg = kDirs[d].sg;
+            const int first_tgt = pass_first(pg, d) + sg;
+            const int last_tgt = pass_first(pg, d) + sg * pass_count(pg);
+            for (int t = last_tgt, q = 0; q < pass_count(pg); ++q, t -= sg)
+                if ((e = launch_adj_push(T, lam, c->adj_pushed, W, pg, ep[d], d, t, c->d_maxd, s)) != cudaSuccess)
+                    return cuda_error(e, "adjoint push");
+            (void)first_tgt;
+        }
+        ++sweeps;
+        if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_error(e, "adjoint sweep");
+        memcpy(&delta, c->h_maxd, 8);
+        if (delta == 0.0) break;
+    }
+    EllipMedium med;
+    const float *arr[6] = {m->mxx, m->mxy, m->mxz, m->myy, m->myz, m->mzz};
+    for (int k = 0; k < 6; ++k) med.m[k] = arr[k];
+    if ((e = launch_adj_grad(T, lam, W, geo, med, *g, dLdM, s)) != cudaSuccess) return cuda_error(e, "gradient");
+    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_error(e, "adjoint");
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        rep->sweeps = sweeps;
+        rep->max_delta = delta;
+        rep->elapsed_ms = ms;
+        rep->nominal_updates = nominal_per_sweep(*g) * (uint64_t)sweeps;
+        rep->evaluated_updates = 0;
+        rep->engine = FOLD3D_ENGINE_PLANES;
+    }
+    return FOLD3D_OK;
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,

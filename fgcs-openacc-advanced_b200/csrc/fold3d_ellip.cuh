@@ -59,18 +59,24 @@ __device__ __forceinline__ double ell_bf(const EllipA &A, int ui, int uj, int uk
 
 __device__ __forceinline__ double ell_min(double a, double b) { return (a < b) ? a : b; }
 
-__device__ __forceinline__ void ell_vertex(double &tn, const EllipA &A, double tp, int i, int j)
+// Candidate ids (the adjoint's winner record): 0 vertex st, 1+r rim vertex r,
+// 9+r spoke st-rim[r], 17+r rim edge rim[r]-rim[r+1], 25+r triangle
+// (st, rim[r], rim[r+1]).  Each routine sets win when it lowers tn.
+__device__ __forceinline__ void ell_vertex(double &tn, int &win, int id, const EllipA &A, double tp, int i, int j)
 {
     if (!(tn > tp)) return;
     const double c = ell_bf(A, -i, -j, 1, -i, -j, 1);
     if (c > 0.0) {
         const double cand = tp + sqrt(c);
-        if (cand < tn) tn = cand;
+        if (cand < tn) {
+            tn = cand;
+            win = id;
+        }
     }
 }
 
-__device__ __forceinline__ void ell_edge(double &tn, const EllipA &A, double tp, double tq, int pi, int pj, int qi,
-                                         int qj)
+__device__ __forceinline__ void ell_edge(double &tn, int &win, int id, const EllipA &A, double tp, double tq, int pi,
+                                         int pj, int qi, int qj)
 {
     if (!(tn > ell_min(tp, tq))) return;
     const int ei = qi - pi, ej = qj - pj;
@@ -85,13 +91,16 @@ __device__ __forceinline__ void ell_edge(double &tn, const EllipA &A, double tp,
         const double lam = (b - d * n) / a;
         if (lam > 0.0 && lam < 1.0) {
             const double cand = tp + lam * d + n;
-            if (cand < tn) tn = cand;
+            if (cand < tn) {
+                tn = cand;
+                win = id;
+            }
         }
     }
 }
 
-__device__ __forceinline__ void ell_tri(double &tn, const EllipA &A, double t0, double ta, double tb, int ai,
-                                        int aj, int bi, int bj)
+__device__ __forceinline__ void ell_tri(double &tn, int &win, int id, const EllipA &A, double t0, double ta, double tb,
+                                        int ai, int aj, int bi, int bj)
 {
     if (!(tn > ell_min(t0, ell_min(ta, tb)))) return;
     const double p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
@@ -112,7 +121,10 @@ __device__ __forceinline__ void ell_tri(double &tn, const EllipA &A, double t0, 
         const double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
         if (l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0) {
             const double cand = t0 + (l1 * d1 + l2 * d2) + n;
-            if (cand < tn) tn = cand;
+            if (cand < tn) {
+                tn = cand;
+                win = id;
+            }
         }
     }
 }
@@ -135,28 +147,31 @@ __device__ __forceinline__ EllipA ell_local(const EllipMedium &M, const EllipDir
     return A;
 }
 
-// New signed value of a target from st and its rim values (rim order above).
-__device__ __forceinline__ double point_update_ellip(double told, double st, const double nb[8], const EllipA &A)
+// New signed value of a target from st and its rim values (rim order above);
+// win: id of the candidate that set it, -1 if none did.
+__device__ __forceinline__ double point_update_ellip(double told, double st, const double nb[8], const EllipA &A,
+                                                     int &win)
 {
     double tn = fabs(told);
-    ell_vertex(tn, A, st, 0, 0);
+    win = -1;
+    ell_vertex(tn, win, 0, A, st, 0, 0);
     double m = st;
 #pragma unroll
     for (int r = 0; r < 8; ++r) m = ell_min(m, nb[r]);
     if (tn > m) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) ell_vertex(tn, A, nb[r], ell_ri(r), ell_rj(r));
+        for (int r = 0; r < 8; ++r) ell_vertex(tn, win, 1 + r, A, nb[r], ell_ri(r), ell_rj(r));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) ell_edge(tn, A, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
+        for (int r = 0; r < 8; ++r) ell_edge(tn, win, 9 + r, A, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            ell_edge(tn, A, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
+            ell_edge(tn, win, 17 + r, A, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            ell_tri(tn, A, st, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
+            ell_tri(tn, win, 25 + r, A, st, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
     }
     return ((told > 0) ? 1.0 : -1.0) * tn;

@@ -81,6 +81,8 @@ struct WaveArgs {
     unsigned *status;            // 0, or 1 after a wait gave up
     unsigned long long *maxd;    // max |dT| (IEEE bits) of the sweep
     unsigned long long *evaluated;  // points evaluated
+    unsigned short *winners;     // elliptical medium: winner records, or NULL
+    int dir;                     // direction of the pass (for the winner records)
 };
 // Media of the local solver.
 enum Medium { kMediumDrift = 0, kMediumEllip = 1 };
@@ -120,6 +122,17 @@ struct BatchArgs {
 };
 cudaError_t launch_batch_pass(const BatchArgs &b, int grid, cudaStream_t s);
 int batch_blocks_per_sm();
+
+// Adjoint of the elliptical solver (fold3d_adjoint.cu).
+struct AdjGeom {
+    PlaneGeom pg[6];
+    EllipDir d[6];
+};
+cudaError_t launch_adj_push(const double *T, double *lam, double *pushed, const unsigned short *W,
+                            const PlaneGeom &pg, const EllipParam &ep, int dir, int tgt, unsigned long long *maxd,
+                            cudaStream_t s);
+cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned short *W, const AdjGeom &geo,
+                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s);
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,

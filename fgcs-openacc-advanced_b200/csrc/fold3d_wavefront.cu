@@ -153,7 +153,10 @@ __device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs
                 tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
             } else {
                 const double nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
-                tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d));
+                int win;
+                tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d), win);
+                if (a.winners && __double_as_longlong(tnew) != __double_as_longlong(told))
+                    a.winners[d] = (win < 0) ? (unsigned short)0xffffu : (unsigned short)((a.dir << 6) | win);
             }
             if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
                 T[d] = tnew;

@@ -36,6 +36,7 @@ EXPORTED = (
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
     "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
+    "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -116,6 +117,8 @@ def lib() -> C.CDLL:
     L.fold3d_ellip_metric.argtypes = [d, d, d, d, d, C.POINTER(C.c_float)]
     L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
+    L.fold3d_solve_ellip_record.argtypes = [vp, P(Grid), P(Ellip), vp, vp, P(Opts), vp, P(Report)]
+    L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
     L.InitFoldFromPoint.restype = d
     L.ImpSurfF.argtypes = [d] * 3
@@ -299,6 +302,29 @@ def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> 
     e = ellip(M)
     _check(lib().fold3d_solve_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), _dev_ptr(T),
                                     C.byref(o or opts()), C.c_void_p(stream) if stream else None, C.byref(rep)))
+    return rep
+
+
+def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream=None) -> Report:
+    """solve_ellip that also fills W (an int16 CUDA tensor shaped like T)
+    with each cell's winner record (the adjoint's checkpoint)."""
+    nx, ny, nz = grid_of(T)
+    rep = Report()
+    _check(lib().fold3d_solve_ellip_record(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
+                                           C.c_void_p(W.data_ptr()), C.byref(o or opts()),
+                                           C.c_void_p(stream) if stream else None, C.byref(rep)))
+    return rep
+
+
+def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, stream=None) -> Report:
+    """fold3d_adjoint_ellip: lam <- dL/dT (total), dLdM (shape (6,)+T.shape,
+    float64) <- dL/dM, from the converged T, its winner record W and dLdT."""
+    nx, ny, nz = grid_of(T)
+    rep = Report()
+    _check(lib().fold3d_adjoint_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
+                                      C.c_void_p(W.data_ptr()), _dev_ptr(dLdT), _dev_ptr(lam),
+                                      C.c_void_p(dLdM.data_ptr()), int(max_sweeps),
+                                      C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 

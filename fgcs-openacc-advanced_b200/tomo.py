@@ -1,0 +1,52 @@
+"""Traveltime-tomography harness: the elliptical solver as a differentiable
+torch operation.  torch is used here only as the harness; the forward solve
+and its adjoint run in libfold3dpmm (fold3d_solve_ellip_record,
+fold3d_adjoint_ellip).
+
+EllipSolve.apply(T0, h, max_sweeps, tol, *M) returns the converged field for
+the initial field T0 (a point source) and a float64 metric M (six CUDA
+tensors, xx xy xz yy yz zz, field layout; the solver stores it as float32).
+Its backward pass returns dL/dM in float64, so torch carries the gradient on
+to whatever produced M (slowness, epsilon and axis through
+media.metric_from).
+"""
+from __future__ import annotations
+
+import torch
+
+import fold3dpmm as f3d
+
+_ctx = {}
+
+
+def context(device=None) -> f3d.Context:
+    dev = torch.cuda.current_device() if device is None else device
+    if dev not in _ctx:
+        _ctx[dev] = f3d.Context(dev)
+    return _ctx[dev]
+
+
+class EllipSolve(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, T0, h, max_sweeps, tol, *M):
+        M32 = [m.detach().to(torch.float32).contiguous() for m in M]
+        T = T0.detach().clone()
+        W = torch.empty(T.shape, dtype=torch.int16, device=T.device)
+        rep = f3d.solve_ellip_record(context(), T, h, M32, W,
+                                     f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol))
+        ctx.save_for_backward(T, W, *M32)
+        ctx.h = h
+        ctx.sweeps = rep.sweeps
+        return T
+
+    @staticmethod
+    def backward(ctx, gT):
+        T, W, *M32 = ctx.saved_tensors
+        lam = torch.empty_like(T)
+        dLdM = torch.empty((6,) + tuple(T.shape), dtype=torch.float64, device=T.device)
+        f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM)
+        return (None, None, None, None) + tuple(dLdM[m] for m in range(6))
+
+
+def solve(T0, h, M, max_sweeps=1000, tol=0.0):
+    return EllipSolve.apply(T0, h, max_sweeps, tol, *M)

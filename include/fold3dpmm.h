@@ -172,6 +172,29 @@ void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az,
 int fold3d_solve_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, double *T_dev,
                        const fold3d_opts *o, void *stream, fold3d_report *rep);
 
+/* fold3d_solve_ellip that also records, per cell, the candidate that last
+ * set its time -- (direction << 6) | candidate id, or 0xffff if none did --
+ * into winners_dev (one unsigned short per field cell, device memory; the
+ * call first sets it to 0xffff).  This record is the checkpoint of the
+ * adjoint; it replaces the history of the field. */
+int fold3d_solve_ellip_record(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, double *T_dev,
+                              unsigned short *winners_dev, const fold3d_opts *o, void *stream,
+                              fold3d_report *rep);
+
+/* Adjoint of a converged elliptical solve.  No counterpart in the reference.
+ * Given the converged field T_dev, its winner record and dLdT_dev = dL/dT
+ * (device, field layout), writes lambda_dev = the total derivative dL/dT
+ * (device, field layout) and dLdM_dev = dL/dM, six arrays of doubles in the
+ * field layout, component-major (xx xy xz yy yz zz), every cell written (0 on
+ * ghosts and on cells without a winner).  Backward sweeps repeat
+ * until one changes nothing, at most max_sweeps; rep->sweeps counts them and
+ * rep->max_delta is the largest pushed amount of the last one (0 when done).
+ * lambda is accumulated with floating-point atomics: results agree with the
+ * FP64 CPU statement to rounding, not bit for bit. */
+int fold3d_adjoint_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, const double *T_dev,
+                         const unsigned short *winners_dev, const double *dLdT_dev, double *lambda_dev,
+                         double *dLdM_dev, int max_sweeps, void *stream, fold3d_report *rep);
+
 /* One instance of a batched solve: its grid, elliptical medium and device
  * field (in/out). */
 typedef struct {

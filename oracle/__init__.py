@@ -81,6 +81,12 @@ class Oracle:
                                     C.POINTER(_dbl)]
         L.orc_ell_solve.restype = _int
         L.orc_ell_plane.argtypes = [_ptr, C.POINTER(C.c_void_p), _int, _int, _int, _dbl, _dbl, _dbl, _int, _int]
+        L.orc_ell_solve_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _int,
+                                        _dbl, C.POINTER(_dbl)]
+        L.orc_ell_solve_rec.restype = _int
+        L.orc_ell_adjoint_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _ptr,
+                                          _ptr, _ptr]
+        L.orc_ell_adjoint_rec.restype = C.c_long
         self.L = L
 
     @staticmethod
@@ -129,6 +135,28 @@ class Oracle:
         if s < 0:
             raise MemoryError("orc_ell_solve failed")
         return s, d.value
+
+    def ell_solve_rec(self, T, M, h, nsweeps, tol=-1.0):
+        """ell_solve that also returns the winner record (uint16, field layout;
+        0xffff where no candidate set the value)."""
+        arrs, ptrs = self._metric(M)
+        W = np.full(T.shape, 0xFFFF, dtype=np.uint16)
+        d = _dbl(0.0)
+        s = self.L.orc_ell_solve_rec(_p(T), ptrs, W.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2], nsweeps,
+                                     tol, C.byref(d))
+        return s, d.value, W
+
+    def ell_adjoint(self, T, M, h, W, r):
+        """FP64 adjoint from the winner record: (lambda, dL/dM (6, ...),
+        number of non-causal weights)."""
+        arrs, ptrs = self._metric(M)
+        lam = np.zeros_like(T)
+        g = np.zeros((6,) + T.shape)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        Wc = np.ascontiguousarray(W, dtype=np.uint16)
+        nc = self.L.orc_ell_adjoint_rec(_p(T), ptrs, Wc.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2],
+                                        r.ctypes.data_as(_ptr), lam.ctypes.data_as(_ptr), g.ctypes.data_as(_ptr))
+        return lam, g, nc
 
     def fold_from_point(self, F, ax, ay, az, x, y, z) -> float:
         return self.L.orc_fold_from_point(F, ax, ay, az, x, y, z)

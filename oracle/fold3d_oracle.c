@@ -577,18 +577,21 @@ static double orc_bf(const orc_aq *A, int ui, int uj, int uk, int vi, int vj, in
 /* neighbour offsets in the local frame, st first, then the rim in order */
 static const int ORC_RIM[8][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, -1}};
 
-static void orc_ell_vertex(double *tn, const orc_aq *A, double tp, int i, int j)
+/* Each candidate routine sets *win to its id (see the adjoint below) when it
+ * lowers the time, so *win ends as the id of the candidate that set it. */
+static void orc_ell_vertex(double *tn, int *win, int id, const orc_aq *A, double tp, int i, int j)
 {
     if (!(*tn > tp)) return;
     double c = orc_bf(A, -i, -j, 1, -i, -j, 1);
     if (c > 0.0) {
         double cand = tp + sqrt(c);
-        if (cand < *tn) *tn = cand;
+        if (cand < *tn) { *tn = cand; *win = id; }
     }
 }
 
 /* edge from P (pi,pj) with time tp to Q (qi,qj) with time tq */
-static void orc_ell_edge(double *tn, const orc_aq *A, double tp, double tq, int pi, int pj, int qi, int qj)
+static void orc_ell_edge(double *tn, int *win, int id, const orc_aq *A, double tp, double tq, int pi, int pj,
+                         int qi, int qj)
 {
     if (!(*tn > omin(tp, tq))) return;
     const int ei = qi - pi, ej = qj - pj;
@@ -603,14 +606,14 @@ static void orc_ell_edge(double *tn, const orc_aq *A, double tp, double tq, int 
         double lam = (b - d * n) / a;
         if (lam > 0.0 && lam < 1.0) {
             double cand = tp + lam * d + n;
-            if (cand < *tn) *tn = cand;
+            if (cand < *tn) { *tn = cand; *win = id; }
         }
     }
 }
 
 /* triangle st (origin, time t0) - A (ai,aj, time ta) - B (bi,bj, time tb) */
-static void orc_ell_tri(double *tn, const orc_aq *A, double t0, double ta, double tb, int ai, int aj, int bi,
-                        int bj)
+static void orc_ell_tri(double *tn, int *win, int id, const orc_aq *A, double t0, double ta, double tb, int ai,
+                        int aj, int bi, int bj)
 {
     if (!(*tn > omin(t0, omin(ta, tb)))) return;
     double p11 = orc_bf(A, ai, aj, 0, ai, aj, 0);
@@ -631,32 +634,40 @@ static void orc_ell_tri(double *tn, const orc_aq *A, double t0, double ta, doubl
         double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
         if (l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0) {
             double cand = t0 + (l1 * d1 + l2 * d2) + n;
-            if (cand < *tn) *tn = cand;
+            if (cand < *tn) { *tn = cand; *win = id; }
         }
     }
 }
 
-/* New signed value of a target from st and the rim values nb[8] (ORC_RIM order). */
-static double orc_ell_point(double told, double st, const double nb[8], const orc_aq *A)
+/* New signed value of a target from st and the rim values nb[8] (ORC_RIM
+ * order); *win: id of the candidate that set it, -1 if none did. */
+static double orc_ell_point(double told, double st, const double nb[8], const orc_aq *A, int *win)
 {
     double tn = fabs(told);
-    orc_ell_vertex(&tn, A, st, 0, 0);
+    *win = -1;
+    orc_ell_vertex(&tn, win, 0, A, st, 0, 0);
     double m = st;
     for (int r = 0; r < 8; ++r) m = omin(m, nb[r]);
     if (tn > m) {
-        for (int r = 0; r < 8; ++r) orc_ell_vertex(&tn, A, nb[r], ORC_RIM[r][0], ORC_RIM[r][1]);
-        for (int r = 0; r < 8; ++r) orc_ell_edge(&tn, A, st, nb[r], 0, 0, ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) orc_ell_vertex(&tn, win, 1 + r, A, nb[r], ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) orc_ell_edge(&tn, win, 9 + r, A, st, nb[r], 0, 0, ORC_RIM[r][0], ORC_RIM[r][1]);
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            orc_ell_edge(&tn, A, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0], ORC_RIM[s][1]);
+            orc_ell_edge(&tn, win, 17 + r, A, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0],
+                         ORC_RIM[s][1]);
         }
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            orc_ell_tri(&tn, A, st, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0], ORC_RIM[s][1]);
+            orc_ell_tri(&tn, win, 25 + r, A, st, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0],
+                        ORC_RIM[s][1]);
         }
     }
     return ((told > 0) ? 1.0 : -1.0) * tn;
 }
+
+/* Winner record of a cell: (direction << 6) | candidate id; FOLD_NOWIN when no
+ * candidate set its value (a source, or never reached). */
+#define ORC_NOWIN 0xffffu
 
 /* index of the global metric component (p,q), arrays ordered xx xy xz yy yz zz */
 static int orc_mi(int p, int q)
@@ -668,8 +679,8 @@ static int orc_mi(int p, int q)
 
 /* One plane step of the elliptical medium.  M: six float arrays (xx, xy, xz,
  * yy, yz, zz of the metric in the i, j, k axes) in the field layout. */
-void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
-                   int dir, int src)
+void orc_ell_plane_rec(double *T, const float *const *M, unsigned short *W, int nx, int ny, int nz, double dx,
+                       double dy, double dz, int dir, int src)
 {
     const orc_grid g = orc_make_grid(nx, ny, nz);
     const orc_dir d = ORC_DIRS[dir];
@@ -698,14 +709,24 @@ void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, dou
             A.yz = (double)(sgn[1] * sgn[2]) * (double)M[orc_mi(ax[1], ax[2])][t] * hy * hz;
             double nb[8];
             for (int r = 0; r < 8; ++r) nb[r] = fabs(T[s + ORC_RIM[r][0] * sx + ORC_RIM[r][1] * sy]);
-            T[t] = orc_ell_point(T[t], fabs(T[s]), nb, &A);
+            int win;
+            const double nv = orc_ell_point(T[t], fabs(T[s]), nb, &A, &win);
+            if (W && memcmp(&nv, &T[t], sizeof nv) != 0)
+                W[t] = (win < 0) ? ORC_NOWIN : (unsigned short)((dir << 6) | win);
+            T[t] = nv;
         }
+}
+
+void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                   int dir, int src)
+{
+    orc_ell_plane_rec(T, M, NULL, nx, ny, nz, dx, dy, dz, dir, src);
 }
 
 /* Sweeps of the elliptical medium in the reference's direction order;
  * semantics as orc_solve. */
-int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
-                  int nsweeps, double tol, double *last_delta)
+int orc_ell_solve_rec(double *T, const float *const *M, unsigned short *W, int nx, int ny, int nz, double dx,
+                      double dy, double dz, int nsweeps, double tol, double *last_delta)
 {
     const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
     const int n[3] = {nx, ny, nz};
@@ -719,9 +740,9 @@ int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, doub
             const orc_dir d = ORC_DIRS[dir];
             const int nn = n[d.nrm];
             if (d.sg > 0)
-                for (int p = 1; p < nn; ++p) orc_ell_plane(T, M, nx, ny, nz, dx, dy, dz, dir, p);
+                for (int p = 1; p < nn; ++p) orc_ell_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
             else
-                for (int p = nn; p > 1; --p) orc_ell_plane(T, M, nx, ny, nz, dx, dy, dz, dir, p);
+                for (int p = nn; p > 1; --p) orc_ell_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
         }
         ++s;
         delta = 0.0;
@@ -734,4 +755,315 @@ int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, doub
     free(prev);
     if (last_delta) *last_delta = delta;
     return s;
+}
+
+int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                  int nsweeps, double tol, double *last_delta)
+{
+    return orc_ell_solve_rec(T, M, NULL, nx, ny, nz, dx, dy, dz, nsweeps, tol, last_delta);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Adjoint of the elliptical solver                                          */
+/* ------------------------------------------------------------------------ */
+/*
+ * At convergence every reached cell's time equals one candidate of one sweep
+ * direction (re-evaluating any direction leaves it unchanged).  That
+ * candidate -- the "winner" -- is t(footpoint) + ||X - footpoint||_M with the
+ * footpoint on a vertex, edge or triangle of the direction's source plane;
+ * by the envelope theorem its derivative with respect to each source time is
+ * that source's barycentric weight at the footpoint, and with respect to the
+ * local metric entry A_ij it is c_i c_j / (2 n) (c the footpoint-to-target
+ * vector in spacing units, n its length; off-diagonal entries count twice).
+ *
+ * Winner ids: 0 the source point st (vertex), 1..8 rim vertices, 9..16
+ * spokes st-rim[r], 17..24 rim edges rim[r]-rim[r+1], 25..32 triangles
+ * (st, rim[r], rim[r+1]).  The winner is the first (direction in sweep
+ * order, then id) whose value equals |T| bit for bit.
+ */
+typedef struct {
+    int dir, id, np;         /* np source points (0 if none: source or unreached) */
+    int64_t src[3];          /* their field indices */
+    double w[3];             /* their weights */
+    double dM[6];            /* d(time)/d(metric entry xx xy xz yy yz zz), global axes */
+} orc_winner;
+
+static const int ORC_RIMX[9] = {0, 1, 1, 0, -1, -1, -1, 0, 1}; /* point 0 = st, 1..8 = rim */
+static const int ORC_RIMY[9] = {0, 0, 1, 1, 1, 0, -1, -1, -1};
+
+/* Evaluate candidate `id` without gates; returns its value (or +inf) and
+ * fills the footpoint weights over points pt[] (0 = st, 1..8 = rim) and the
+ * vector c (spacing units). */
+static double orc_ell_cand(const orc_aq *A, const double tv[9], int id, int pt[3], double w[3], int *np,
+                           double c[3], double *nlen)
+{
+    *np = 0;
+    if (id <= 8) { /* vertex */
+        const int i = ORC_RIMX[id], j = ORC_RIMY[id];
+        double q = orc_bf(A, -i, -j, 1, -i, -j, 1);
+        if (!(q > 0.0)) return INFINITY;
+        *np = 1; pt[0] = id; w[0] = 1.0;
+        c[0] = -i; c[1] = -j; c[2] = 1.0;
+        *nlen = sqrt(q);
+        return tv[id] + *nlen;
+    }
+    if (id <= 24) { /* edge */
+        int P, Q;
+        if (id <= 16) { P = 0; Q = id - 8; } else { P = id - 16; Q = (id - 16) % 8 + 1; }
+        const int pi = ORC_RIMX[P], pj = ORC_RIMY[P], qi = ORC_RIMX[Q], qj = ORC_RIMY[Q];
+        const int ei = qi - pi, ej = qj - pj;
+        double a = orc_bf(A, ei, ej, 0, ei, ej, 0);
+        double b = orc_bf(A, ei, ej, 0, -pi, -pj, 1);
+        double cc = orc_bf(A, -pi, -pj, 1, -pi, -pj, 1);
+        double d = tv[Q] - tv[P];
+        double den = a - d * d;
+        double disc = a * cc - b * b;
+        if (!(den > 0.0 && disc > 0.0)) return INFINITY;
+        double n = sqrt(disc / den);
+        double lam = (b - d * n) / a;
+        if (!(lam > 0.0 && lam < 1.0)) return INFINITY;
+        *np = 2; pt[0] = P; pt[1] = Q; w[0] = 1.0 - lam; w[1] = lam;
+        c[0] = -pi - lam * ei; c[1] = -pj - lam * ej; c[2] = 1.0;
+        *nlen = n;
+        return tv[P] + lam * d + n;
+    }
+    { /* triangle st, rim[r], rim[r+1] */
+        const int r = id - 25, Pa = r + 1, Pb = (r + 1) % 8 + 1;
+        const int ai = ORC_RIMX[Pa], aj = ORC_RIMY[Pa], bi = ORC_RIMX[Pb], bj = ORC_RIMY[Pb];
+        double p11 = orc_bf(A, ai, aj, 0, ai, aj, 0);
+        double p12 = orc_bf(A, ai, aj, 0, bi, bj, 0);
+        double p22 = orc_bf(A, bi, bj, 0, bi, bj, 0);
+        double q1 = orc_bf(A, ai, aj, 0, 0, 0, 1);
+        double q2 = orc_bf(A, bi, bj, 0, 0, 0, 1);
+        double cz = A->zz;
+        double d1 = tv[Pa] - tv[0], d2 = tv[Pb] - tv[0];
+        double det = p11 * p22 - p12 * p12;
+        if (!(det > 0.0)) return INFINITY;
+        double u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
+        double w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
+        double s = (d1 * u1 + d2 * u2) / det;
+        double rr = cz - (q1 * w1 + q2 * w2) / det;
+        if (!(s < 1.0 && rr > 0.0)) return INFINITY;
+        double n = sqrt(rr / (1.0 - s));
+        double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
+        if (!(l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0)) return INFINITY;
+        *np = 3; pt[0] = 0; pt[1] = Pa; pt[2] = Pb;
+        w[0] = 1.0 - l1 - l2; w[1] = l1; w[2] = l2;
+        c[0] = -l1 * ai - l2 * bi; c[1] = -l1 * aj - l2 * bj; c[2] = 1.0;
+        *nlen = n;
+        return tv[0] + (l1 * d1 + l2 * d2) + n;
+    }
+}
+
+static void orc_ell_local(const float *const *M, int64_t t, const orc_dir *d, const double h[3], orc_aq *A,
+                          double *hx, double *hy, double *hz)
+{
+    const int ax[3] = {d->xa, d->ya, d->nrm};
+    const int sgn[3] = {d->xs, d->ys, d->sg};
+    *hz = h[d->nrm]; *hx = h[d->xa]; *hy = h[d->ya];
+    A->xx = (double)M[orc_mi(ax[0], ax[0])][t] * *hx * *hx;
+    A->yy = (double)M[orc_mi(ax[1], ax[1])][t] * *hy * *hy;
+    A->zz = (double)M[orc_mi(ax[2], ax[2])][t] * *hz * *hz;
+    A->xy = (double)(sgn[0] * sgn[1]) * (double)M[orc_mi(ax[0], ax[1])][t] * *hx * *hy;
+    A->xz = (double)(sgn[0] * sgn[2]) * (double)M[orc_mi(ax[0], ax[2])][t] * *hx * *hz;
+    A->yz = (double)(sgn[1] * sgn[2]) * (double)M[orc_mi(ax[1], ax[2])][t] * *hy * *hz;
+}
+
+/* Winner of interior cell (i,j,k) of a converged field. */
+static void orc_ell_winner_at(const double *T, const float *const *M, const orc_grid *g, const double h[3], int i,
+                              int j, int k, orc_winner *wn)
+{
+    memset(wn, 0, sizeof *wn);
+    wn->dir = -1;
+    const int64_t x = i + g->stride[1] * j + g->stride[2] * k;
+    const double tx = fabs(T[x]);
+    if (!(tx > 0.0) || tx >= ORC_MAXT) return;
+    const int c3[3] = {i, j, k};
+    double best = INFINITY;
+    int bdir = -1, bid = -1;
+    /* first pass: the first exact match, else the smallest candidate */
+    for (int dir = 0; dir < 6 && !(best == tx); ++dir) {
+        const orc_dir d = ORC_DIRS[dir];
+        const int sc = c3[d.nrm] - d.sg;
+        if (sc < 1 || sc > g->n[d.nrm]) continue;
+        const int64_t st = x - d.sg * g->stride[d.nrm];
+        const int64_t sx = d.xs * g->stride[d.xa], sy = d.ys * g->stride[d.ya];
+        double tv[9];
+        for (int p = 0; p < 9; ++p) tv[p] = fabs(T[st + ORC_RIMX[p] * sx + ORC_RIMY[p] * sy]);
+        orc_aq A;
+        double hx, hy, hz;
+        orc_ell_local(M, x, &d, h, &A, &hx, &hy, &hz);
+        for (int id = 0; id <= 32; ++id) {
+            int pt[3], np;
+            double w[3], cv[3], n;
+            double v = orc_ell_cand(&A, tv, id, pt, w, &np, cv, &n);
+            if (v == tx || v < best) {
+                best = v;
+                bdir = dir;
+                bid = id;
+                if (v == tx) break;
+            }
+        }
+    }
+    if (bdir < 0) return;
+    for (int dir = bdir; dir <= bdir; ++dir) {
+        const orc_dir d = ORC_DIRS[dir];
+        const int sc = c3[d.nrm] - d.sg; /* source plane coordinate */
+        if (sc < 1 || sc > g->n[d.nrm]) continue;
+        const int64_t st = x - d.sg * g->stride[d.nrm];
+        const int64_t sx = d.xs * g->stride[d.xa], sy = d.ys * g->stride[d.ya];
+        int64_t idx[9];
+        double tv[9];
+        for (int p = 0; p < 9; ++p) {
+            idx[p] = st + ORC_RIMX[p] * sx + ORC_RIMY[p] * sy;
+            tv[p] = fabs(T[idx[p]]);
+        }
+        orc_aq A;
+        double hx, hy, hz;
+        orc_ell_local(M, x, &d, h, &A, &hx, &hy, &hz);
+        for (int id = bid; id <= bid; ++id) {
+            int pt[3], np;
+            double w[3], cv[3], n;
+            orc_ell_cand(&A, tv, id, pt, w, &np, cv, &n);
+            {
+                wn->dir = dir;
+                wn->id = id;
+                wn->np = np;
+                for (int q = 0; q < np; ++q) { wn->src[q] = idx[pt[q]]; wn->w[q] = w[q]; }
+                /* d/dA_ij, then to the global entries through A = s_p s_q M h_p h_q */
+                const double hh[3] = {hx, hy, hz};
+                const int ax[3] = {d.xa, d.ya, d.nrm};
+                const int sgn[3] = {d.xs, d.ys, d.sg};
+                for (int p = 0; p < 3; ++p)
+                    for (int q = p; q < 3; ++q) {
+                        double dA = cv[p] * cv[q] / ((p == q ? 2.0 : 1.0) * n);
+                        wn->dM[orc_mi(ax[p], ax[q])] += dA * (double)(sgn[p] * sgn[q]) * hh[p] * hh[q];
+                    }
+                return;
+            }
+        }
+    }
+}
+
+/* Weights and metric derivative of the recorded winner (dir, id) of cell x,
+ * evaluated with the final field. */
+static void orc_ell_weights(const double *T, const float *const *M, const orc_grid *g, const double h[3], int64_t x,
+                            int dir, int id, orc_winner *wn)
+{
+    memset(wn, 0, sizeof *wn);
+    wn->dir = dir;
+    wn->id = id;
+    const orc_dir d = ORC_DIRS[dir];
+    const int64_t st = x - d.sg * g->stride[d.nrm];
+    const int64_t sx = d.xs * g->stride[d.xa], sy = d.ys * g->stride[d.ya];
+    int64_t idx[9];
+    double tv[9];
+    for (int p = 0; p < 9; ++p) {
+        idx[p] = st + ORC_RIMX[p] * sx + ORC_RIMY[p] * sy;
+        tv[p] = fabs(T[idx[p]]);
+    }
+    orc_aq A;
+    double hx, hy, hz;
+    orc_ell_local(M, x, &d, h, &A, &hx, &hy, &hz);
+    int pt[3], np;
+    double w[3], cv[3], n;
+    double v = orc_ell_cand(&A, tv, id, pt, w, &np, cv, &n);
+    if (!(v < INFINITY)) return; /* no longer a valid footpoint: no dependency */
+    wn->np = np;
+    for (int q = 0; q < np; ++q) { wn->src[q] = idx[pt[q]]; wn->w[q] = w[q]; }
+    const double hh[3] = {hx, hy, hz};
+    const int ax[3] = {d.xa, d.ya, d.nrm};
+    const int sgn[3] = {d.xs, d.ys, d.sg};
+    for (int p = 0; p < 3; ++p)
+        for (int q = p; q < 3; ++q) {
+            double dA = cv[p] * cv[q] / ((p == q ? 2.0 : 1.0) * n);
+            wn->dM[orc_mi(ax[p], ax[q])] += dA * (double)(sgn[p] * sgn[q]) * hh[p] * hh[q];
+        }
+}
+
+static const double *orc_sort_T;
+static int orc_cmp_desc(const void *a, const void *b)
+{
+    const double x = fabs(orc_sort_T[*(const int64_t *)a]), y = fabs(orc_sort_T[*(const int64_t *)b]);
+    return (x < y) - (x > y);
+}
+
+/* Winners of all interior cells: dir/id (-1 if none) and weights, for tests. */
+void orc_ell_winners(const double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                     int *dir_out, int *id_out, double *w_out /* 3 per cell */)
+{
+    const orc_grid g = orc_make_grid(nx, ny, nz);
+    const double h[3] = {dx, dy, dz};
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    for (size_t c = 0; c < cells; ++c) { dir_out[c] = -1; id_out[c] = -1; w_out[3 * c] = w_out[3 * c + 1] = w_out[3 * c + 2] = 0.0; }
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                orc_winner wn;
+                orc_ell_winner_at(T, M, &g, h, i, j, k, &wn);
+                const int64_t x = i + g.stride[1] * j + g.stride[2] * k;
+                dir_out[x] = wn.dir;
+                id_out[x] = wn.id;
+                for (int q = 0; q < 3; ++q) w_out[3 * x + q] = wn.w[q];
+            }
+}
+
+/* FP64 adjoint: given the converged field T and r = dL/dT (field layout),
+ * returns lambda (dL/dT total) and dL/dM (6 arrays, component-major, field
+ * layout).  Cells are processed by decreasing time; the return value is the
+ * number of winner weights that point to a source point whose time is not
+ * smaller (0 for a causal field, for which the order is exact). */
+long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned short *rec, int nx, int ny, int nz,
+                         double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
+{
+    const orc_grid g = orc_make_grid(nx, ny, nz);
+    const double h[3] = {dx, dy, dz};
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    orc_winner *W = (orc_winner *)malloc(cells * sizeof(orc_winner));
+    int64_t *order = (int64_t *)malloc(cells * sizeof(int64_t));
+    if (!W || !order) { free(W); free(order); return -1; }
+    memset(W, 0, cells * sizeof(orc_winner));
+    size_t nint = 0;
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) order[nint++] = i + g.stride[1] * j + g.stride[2] * k;
+#pragma omp parallel for schedule(static)
+    for (size_t q = 0; q < nint; ++q) {
+        const int64_t x = order[q];
+        const int k = (int)(x / g.stride[2]), j = (int)((x % g.stride[2]) / g.stride[1]), i = (int)(x % g.stride[1]);
+        if (rec) {
+            if (rec[x] != ORC_NOWIN) orc_ell_weights(T, M, &g, h, x, rec[x] >> 6, rec[x] & 63, &W[x]);
+        } else {
+            orc_ell_winner_at(T, M, &g, h, i, j, k, &W[x]);
+        }
+    }
+    orc_sort_T = T;
+    qsort(order, nint, sizeof(int64_t), orc_cmp_desc);
+    memcpy(lambda, r, cells * sizeof(double));
+    long noncausal = 0;
+    for (size_t q = 0; q < nint; ++q) {
+        const int64_t x = order[q];
+        const orc_winner *wn = &W[x];
+        for (int s = 0; s < wn->np; ++s) {
+            if (wn->w[s] > 0.0 && !(fabs(T[wn->src[s]]) < fabs(T[x]))) ++noncausal;
+            lambda[wn->src[s]] += wn->w[s] * lambda[x];
+        }
+    }
+    for (size_t c = 0; c < 6 * cells; ++c) dLdM[c] = 0.0;
+    for (size_t q = 0; q < nint; ++q) {
+        const int64_t x = order[q];
+        for (int m = 0; m < 6; ++m) dLdM[m * cells + x] = lambda[x] * W[x].dM[m];
+    }
+    free(W);
+    free(order);
+    return noncausal;
+}
+
+/* Adjoint with winners found from the converged field (first candidate, in
+ * direction and id order, equal to the time; else the closest). */
+long orc_ell_adjoint(const double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                     const double *r, double *lambda, double *dLdM)
+{
+    return orc_ell_adjoint_rec(T, M, NULL, nx, ny, nz, dx, dy, dz, r, lambda, dLdM);
 }

@@ -477,3 +477,139 @@ def test_batch_equals_one_by_one(f3d, ctx, cuda, fixed):
 def test_batch_rejects_bad_input(f3d, ctx, cuda):
     L = f3d.lib()
     assert L.fold3d_solve_batch(ctx._h, 0, None, C.byref(f3d.opts()), None, None) == f3d.ERR_INVALID
+
+
+# -- adjoint of the elliptical solver ----------------------------------------
+
+def _adj_case(cuda, dims=(23, 19, 27), seed=4, src=(12, 9, 5)):
+    import media
+
+    M = media.heterogeneous_tti(*dims, 10.0, seed=seed)
+    T0 = torch_point_dims(cuda, dims, src)
+    rec = (slice(1, 2), slice(1, -1, 2), slice(1, -1, 2))  # receivers on the k = 1 face
+    return M, T0, rec
+
+
+def test_winner_record_matches_oracle(f3d, orc, ctx, cuda):
+    M, T0, _ = _adj_case(cuda)
+    Md = [m.cuda() for m in M]
+    T = T0.clone()
+    W = cuda.empty(T.shape, dtype=cuda.int16, device="cuda")
+    rep = f3d.solve_ellip_record(ctx, T, 10.0, Md, W, f3d.opts(max_sweeps=300, tol=0.0))
+    ref = T0.cpu().numpy()
+    s, d, Wref = orc.ell_solve_rec(ref, [m.numpy() for m in M], (10.0,) * 3, 300, tol=0.0)
+    assert rep.sweeps == s
+    assert_bitwise(T.cpu().numpy(), ref, "field")
+    assert np.array_equal(W.cpu().numpy().view(np.uint16), Wref)
+    assert (Wref != 0xFFFF).sum() > 0.9 * Wref[1:-1, 1:-1, 1:-1].size
+
+
+def test_adjoint_matches_cpu_adjoint(f3d, orc, ctx, cuda):
+    """lambda and dL/dM of the GPU adjoint against the FP64 CPU adjoint (which
+    processes cells by decreasing time and finds the winner graph causal)."""
+    M, T0, rec = _adj_case(cuda)
+    Md = [m.cuda() for m in M]
+    T = T0.clone()
+    W = cuda.empty(T.shape, dtype=cuda.int16, device="cuda")
+    f3d.solve_ellip_record(ctx, T, 10.0, Md, W, f3d.opts(max_sweeps=300, tol=0.0))
+    r = cuda.zeros_like(T)
+    r[rec] = T[rec] * 0.01 + 1.0
+    lam = cuda.full_like(T, float("nan"))
+    g = cuda.full((6,) + tuple(T.shape), float("nan"), dtype=cuda.float64, device="cuda")  # every cell is written
+    rep = f3d.adjoint_ellip(ctx, T, 10.0, Md, W, r, lam, g)
+    assert rep.max_delta == 0.0 and rep.sweeps >= 2
+    lr, gr, nc = orc.ell_adjoint(T.cpu().numpy(), [m.numpy() for m in M], (10.0,) * 3,
+                                 W.cpu().numpy().view(np.uint16), r.cpu().numpy())
+    assert nc == 0
+    np.testing.assert_allclose(lam.cpu().numpy(), lr, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(g.cpu().numpy(), gr, rtol=1e-9, atol=1e-12 * np.abs(gr).max())
+
+
+def test_adjoint_matches_finite_differences(f3d, ctx, cuda):
+    """dL/dM from the adjoint against central differences of the loss
+    L = 1/2 sum over receivers (T - t_obs)^2, step 1e-6 relative on the
+    solver's own (float32) metric entries, at 32 random cells."""
+    import tomo
+
+    M, T0, rec = _adj_case(cuda)
+    Md = [m.double().cuda().requires_grad_(True) for m in M]
+    T = tomo.solve(T0, 10.0, Md)
+    tobs = (T[rec] * 0.97).detach()
+    L = 0.5 * ((T[rec] - tobs) ** 2).sum()
+    L.backward()
+    G = [m.grad for m in Md]
+
+    def loss(Mx):
+        with cuda.no_grad():
+            Tx = tomo.solve(T0, 10.0, Mx)
+            return float(0.5 * ((Tx[rec] - tobs) ** 2).sum())
+
+    rng = np.random.default_rng(7)
+    base = [m.detach().float().cuda() for m in Md]
+    cand = cuda.nonzero(G[0].abs() > 0).cpu().numpy()
+    errs = []
+    for q in rng.choice(len(cand), 32, replace=False):
+        k, j, i = (int(v) for v in cand[q])
+        comp = int(rng.integers(0, 6))
+        v = float(base[comp][k, j, i])
+        step = abs(v) * 1e-6 if v != 0 else 1e-12
+        up = [b.clone() for b in base]
+        dn = [b.clone() for b in base]
+        up[comp][k, j, i] = v + step
+        dn[comp][k, j, i] = v - step
+        dv = float(up[comp][k, j, i]) - float(dn[comp][k, j, i])  # the float32 difference actually applied
+        fd = (loss([u.double() for u in up]) - loss([d.double() for d in dn])) / dv
+        ad = float(G[comp][k, j, i])
+        errs.append(abs(fd - ad) / max(abs(ad), abs(fd), 1e-300))
+    assert np.median(errs) < 1e-6 and max(errs) < 1e-4, (np.median(errs), max(errs))
+
+
+def test_adjoint_chain_to_slowness_and_epsilon(cuda):
+    """Through torch's chain rule, gradients with respect to per-cell
+    slowness and epsilon agree with central differences (relative step 1e-3:
+    the metric is stored as float32, so smaller steps in these parameters are
+    lost to rounding)."""
+    import math
+
+    import media
+    import tomo
+
+    dims, h = (21, 17, 19), 10.0
+    nx, ny, nz = dims
+    shape = (nz + 2, ny + 2, nx + 2)
+    gen = cuda.Generator(device="cpu").manual_seed(3)
+    s0 = (1.0 / (1800.0 + 400.0 * cuda.rand(shape, generator=gen, dtype=cuda.float64))).cuda()
+    e0 = (0.2 * cuda.rand(shape, generator=gen, dtype=cuda.float64)).cuda()
+    th, ph = math.radians(25.0), math.radians(60.0)
+    axis = tuple(cuda.full(shape, v, dtype=cuda.float64, device="cuda")
+                 for v in (math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)))
+    T0 = torch_point_dims(cuda, dims, (11, 9, 3))
+    rec = (slice(1, 2), slice(1, -1, 2), slice(1, -1, 2))
+
+    def metric(s, e):
+        return [m.double() for m in media.metric_from(1.0 / s, e, axis)]
+
+    s = s0.clone().requires_grad_(True)
+    e = e0.clone().requires_grad_(True)
+    T = tomo.solve(T0, h, metric(s, e))
+    tobs = (T[rec] * 0.98).detach()
+    (0.5 * ((T[rec] - tobs) ** 2).sum()).backward()
+
+    def loss(sv, ev):
+        with cuda.no_grad():
+            Tx = tomo.solve(T0, h, metric(sv, ev))
+            return float(0.5 * ((Tx[rec] - tobs) ** 2).sum())
+
+    rng = np.random.default_rng(1)
+    cells = cuda.nonzero(s.grad.abs() > 1e-3 * s.grad.abs().max()).cpu().numpy()
+    for q in rng.choice(len(cells), 8, replace=False):
+        k, j, i = (int(v) for v in cells[q])
+        for var, g, base in (("s", s.grad, s0), ("eps", e.grad, e0)):
+            step = 1e-3 * float(base[k, j, i]) if float(base[k, j, i]) != 0 else 1e-4
+            up, dn = base.clone(), base.clone()
+            up[k, j, i] += step
+            dn[k, j, i] -= step
+            fd = (loss(up, e0) - loss(dn, e0)) / (2 * step) if var == "s" else \
+                (loss(s0, up) - loss(s0, dn)) / (2 * step)
+            ad = float(g[k, j, i])
+            assert abs(fd - ad) <= 2e-2 * max(abs(ad), abs(fd)) + 1e-9 * float(g.abs().max()), (var, fd, ad)
