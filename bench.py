@@ -438,6 +438,117 @@ def run_batch(args):
     ctx.close()
 
 
+def run_adjoint(args):
+    """--medium adjoint: traveltime tomography at --adj-size^3 (256), h=10 m.
+    True medium: the seeded heterogeneous TTI construction (seed 2); starting
+    medium: its slowness, eps and axis smoothed by a Gaussian of 16 cells.
+    64 sources on a jittered 8 x 8 grid 10 cells below the top face (k = 11),
+    4096 receivers on a 64 x 64 grid on the top face (k = 1).  Observed times
+    come from solves in the true medium (untimed).  One step = the loss
+    1/2 sum (t - t_obs)^2 over all sources and receivers and its gradient with
+    respect to per-cell slowness and eps: per source a recording forward solve
+    (to max|dT| <= 1e-10) and the adjoint, through tomo.EllipSolve (torch
+    autograd over the C-ABI), then torch's chain rule from the metric to
+    slowness and eps.  The forward and adjoint library calls are also timed
+    on their own (CUDA events inside the library)."""
+    import numpy as np
+    import torch
+
+    import media
+    import tomo
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n, h = args.adj_size, 10.0
+    nsrc_side, nrec_side = 8, 64
+    t0 = time.perf_counter()
+    vz_t, eps_t, ax_t = media.tti_params(n, n, n, h, seed=2, device="cuda", pad=True)
+    M_true = [m.double() for m in media.metric_from(vz_t, eps_t, ax_t)]
+    vz0, eps0, ax0 = media.smooth_params(vz_t, eps_t, ax_t, 16.0)
+    del vz_t, eps_t, ax_t
+    rng = np.random.default_rng(2)
+    cell = n / nsrc_side
+    srcs = []
+    for b in range(nsrc_side):
+        for a in range(nsrc_side):
+            i = int((a + 0.5) * cell + rng.uniform(-cell / 4, cell / 4)) + 1
+            j = int((b + 0.5) * cell + rng.uniform(-cell / 4, cell / 4)) + 1
+            srcs.append((min(max(i, 1), n), min(max(j, 1), n), 11))
+    ridx = torch.tensor([1 + (n // nrec_side) // 2 + (n // nrec_side) * q for q in range(nrec_side)],
+                        device="cuda")
+    rec = (1, ridx.view(-1, 1), ridx.view(1, -1))  # (k, j, i): top face
+
+    def t0_of(sp_):
+        t = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=torch.float64, device="cuda")
+        t[sp_[2], sp_[1], sp_[0]] = 0.0
+        return t
+
+    tol = 1e-10
+    tobs = []
+    with torch.no_grad():
+        for sp_ in srcs:
+            tobs.append(tomo.solve(t0_of(sp_), h, M_true, tol=tol)[rec].clone())
+    del M_true
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    reps = []
+    tomo.collect_reports(reps)
+
+    def step():
+        s = (1.0 / vz0).requires_grad_(True)
+        e = eps0.clone().requires_grad_(True)
+        Mg = [m.double() for m in media.metric_from(1.0 / s, e, ax0)]
+        Ml = [m.detach().requires_grad_(True) for m in Mg]
+        loss = torch.zeros((), dtype=torch.float64, device="cuda")
+        for sp_, to in zip(srcs, tobs):
+            T = tomo.solve(t0_of(sp_), h, Ml, tol=tol)
+            Ls = 0.5 * ((T[rec] - to) ** 2).sum()
+            Ls.backward()
+            loss += Ls.detach()
+        torch.autograd.backward(Mg, [m.grad for m in Ml])
+        return float(loss), s.grad, e.grad
+
+    for _ in range(args.warmup):
+        step()
+    reps.clear()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            loss, gs, ge = step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    tomo.collect_reports(None)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    nsrc = len(srcs)
+    fr = [r for k, r in reps if k == "forward"]
+    ar = [r for k, r in reps if k == "adjoint"]
+    fwd = sum(r.elapsed_ms for r in fr) / len(fr)
+    adj = sum(r.elapsed_ms for r in ar) / len(ar)
+    # wavefront: one launch per direction pass; adjoint: one per target plane and direction, plus the gradient
+    launches = sum(6 * r.sweeps for r in fr) + sum(6 * n * r.sweeps + 1 for r in ar)
+    out = {
+        "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded heterogeneous TTI true medium (seed 2), smoothed starting medium",
+        "config": {"workload": "tomography gradient %d^3 h=10 m, %d sources (jittered %dx%d, k=11), %d receivers "
+                               "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
+                               % (n, nsrc, nsrc_side, nsrc_side, nrec_side ** 2, nrec_side, nrec_side),
+                   "grid": n, "sources": nsrc, "receivers": nrec_side ** 2,
+                   "gradient": "slowness and eps (torch autograd over the C-ABI)"},
+        "forward_ms_per_source": fwd, "adjoint_ms_per_source": adj, "adjoint_over_forward": adj / fwd,
+        "forward_sweeps": [min(r.sweeps for r in fr), max(r.sweeps for r in fr)],
+        "adjoint_sweeps": [min(r.sweeps for r in ar), max(r.sweeps for r in ar)],
+        "harness_ms_per_source": ms / nsrc - fwd - adj, "loss": loss,
+        "grad_norms": {"slowness": float(gs.norm()), "eps": float(ge.norm())},
+        "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": launches,
+    }
+    print(json.dumps(out))
+
+
 def workload_config(args):
     what = "run to max|dT| = 0" if getattr(args, "converge", False) else "%d sweeps" % args.sweeps
     return {"workload": "fold-ref %d^3 implicit-surface source, %s" % (args.size, what),
@@ -463,7 +574,8 @@ def main():
                     help="local-solver form (identical results)")
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
-    ap.add_argument("--medium", choices=["fold", "tti", "batch"], default="fold",
+    ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
+    ap.add_argument("--medium", choices=["fold", "tti", "batch", "adjoint"], default="fold",
                     help="fold: the reference's drift medium and source (default); tti: the "
                          "heterogeneous tilted-elliptical configuration")
     ap.add_argument("--converge", action="store_true",
@@ -480,6 +592,8 @@ def main():
         return run_reference(args)
     if args.medium == "tti":
         return run_tti(args)
+    if args.medium == "adjoint":
+        return run_adjoint(args)
     if args.medium == "batch":
         return run_batch(args)
 

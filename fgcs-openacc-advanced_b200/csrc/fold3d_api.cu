@@ -957,14 +957,12 @@ int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip
         if ((e = cudaMemsetAsync(c->d_maxd, 0, 8, s)) != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
         for (int d = 5; d >= 0; --d) {  // the forward order reversed
             const PlaneGeom &pg = geo.pg[d];
-            // forward targets of direction d: first+sg .. ; walk them backwards
+            // the forward targets of direction d, last first
             const int sg = kDirs[d].sg;
-            const int first_tgt = pass_first(pg, d) + sg;
             const int last_tgt = pass_first(pg, d) + sg * pass_count(pg);
             for (int t = last_tgt, q = 0; q < pass_count(pg); ++q, t -= sg)
                 if ((e = launch_adj_push(T, lam, c->adj_pushed, W, pg, ep[d], d, t, c->d_maxd, s)) != cudaSuccess)
                     return cuda_error(e, "adjoint push");
-            (void)first_tgt;
         }
         ++sweeps;
         if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

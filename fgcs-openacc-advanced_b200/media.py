@@ -62,6 +62,13 @@ def _smooth(x, sigma):
 
 def heterogeneous_tti(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
     """Six float32 metric arrays of the seeded heterogeneous TTI medium."""
+    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies)
+    return [_pad(m) for m in metric_from(vz, eps, axis)]
+
+
+def tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, pad=False):
+    """The parameters of heterogeneous_tti(): float64 (vz, eps, (ax, ay, az))
+    on the interior (nz, ny, nx), or in the field layout with pad=True."""
     gen = torch.Generator(device="cpu").manual_seed(seed)
     scale = max(nx, ny, nz) / 512.0
     shape = (nz, ny, nx)
@@ -88,8 +95,29 @@ def heterogeneous_tti(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
     ay = _smooth(torch.sin(th) * torch.sin(ph), sig)
     az = _smooth(torch.cos(th), sig)
     del th, ph
-    M = metric_from(vz, eps.clamp(0.0, 0.25), (ax, ay, az))
-    return [_pad(m) for m in M]
+    eps = eps.clamp(0.0, 0.25)
+    if pad:
+        return _pad(vz), _pad(eps), (_pad(ax), _pad(ay), _pad(az))
+    return vz, eps, (ax, ay, az)
+
+
+def _smooth_edges(x, sigma):
+    """Gaussian smoothing without wrap-around: the (nz, ny, nx) tensor is
+    extended by 3 sigma of edge copies on every side, smoothed periodically
+    and cropped."""
+    p = int(math.ceil(3.0 * sigma))
+    big = torch.nn.functional.pad(x[None, None], (p,) * 6, mode="replicate")[0, 0]
+    return _smooth(big, sigma)[p:-p, p:-p, p:-p].contiguous()
+
+
+def smooth_params(vz, eps, axis, sigma):
+    """Gaussian smoothing (sigma in cells, no wrap-around) of padded
+    parameters: slowness and eps are smoothed, the axis through its
+    components; ghosts re-copied."""
+    inner = lambda t: t[1:-1, 1:-1, 1:-1]
+    s = _smooth_edges(inner(1.0 / vz), sigma)
+    return (_pad(1.0 / s), _pad(_smooth_edges(inner(eps), sigma)),
+            tuple(_pad(_smooth_edges(inner(a), sigma)) for a in axis))
 
 
 def exact_time(M6, dx, dy, dz):

@@ -17,6 +17,20 @@ import torch
 import fold3dpmm as f3d
 
 _ctx = {}
+_reports = None
+
+
+def collect_reports(lst):
+    """Append ("forward" | "adjoint", fold3d_report) of every later library
+    call to lst (None stops collecting)."""
+    global _reports
+    _reports = lst
+
+
+def _note(kind, rep):
+    if _reports is not None:
+        _reports.append((kind, rep))
+    return rep
 
 
 def context(device=None) -> f3d.Context:
@@ -32,8 +46,8 @@ class EllipSolve(torch.autograd.Function):
         M32 = [m.detach().to(torch.float32).contiguous() for m in M]
         T = T0.detach().clone()
         W = torch.empty(T.shape, dtype=torch.int16, device=T.device)
-        rep = f3d.solve_ellip_record(context(), T, h, M32, W,
-                                     f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol))
+        rep = _note("forward", f3d.solve_ellip_record(context(), T, h, M32, W,
+                                                      f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol)))
         ctx.save_for_backward(T, W, *M32)
         ctx.h = h
         ctx.sweeps = rep.sweeps
@@ -44,7 +58,7 @@ class EllipSolve(torch.autograd.Function):
         T, W, *M32 = ctx.saved_tensors
         lam = torch.empty_like(T)
         dLdM = torch.empty((6,) + tuple(T.shape), dtype=torch.float64, device=T.device)
-        f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM)
+        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM))
         return (None, None, None, None) + tuple(dLdM[m] for m in range(6))
 
 

@@ -12,7 +12,7 @@ import pytest
 
 from conftest import assert_bitwise
 
-from oracle import REF_A, REF_F, ref_spacing
+from oracle import MAXT, REF_A, REF_F, ref_spacing
 
 pytestmark = pytest.mark.gpu
 
@@ -481,6 +481,26 @@ def test_batch_rejects_bad_input(f3d, ctx, cuda):
 
 # -- adjoint of the elliptical solver ----------------------------------------
 
+_DIAG_OF = {0: (0, 0), 1: (0, 3), 2: (0, 5), 3: (3, 3), 4: (3, 5), 5: (5, 5)}
+
+
+def _fd_pair(base, comp, k, j, i, rel=1e-6):
+    """Metric component comp of cell (k, j, i) moved up and down by rel times
+    the cell's metric scale sqrt(M_ii M_jj) (the entry itself for diagonal
+    entries; off-diagonal entries can be many orders smaller than the
+    metric, so a step relative to them alone drowns in rounding of the loss).
+    Returns the two float64 metrics and the float32 difference applied."""
+    a, b = _DIAG_OF[comp]
+    scale = (float(base[a][k, j, i]) * float(base[b][k, j, i])) ** 0.5
+    v = float(base[comp][k, j, i])
+    up, dn = base[comp].clone(), base[comp].clone()
+    up[k, j, i] = v + rel * scale
+    dn[k, j, i] = v - rel * scale
+    dv = float(up[k, j, i]) - float(dn[k, j, i])
+    Mu = [x.double() if c != comp else up.double() for c, x in enumerate(base)]
+    Md = [x.double() if c != comp else dn.double() for c, x in enumerate(base)]
+    return Mu, Md, dv
+
 def _adj_case(cuda, dims=(23, 19, 27), seed=4, src=(12, 9, 5)):
     import media
 
@@ -527,8 +547,9 @@ def test_adjoint_matches_cpu_adjoint(f3d, orc, ctx, cuda):
 
 def test_adjoint_matches_finite_differences(f3d, ctx, cuda):
     """dL/dM from the adjoint against central differences of the loss
-    L = 1/2 sum over receivers (T - t_obs)^2, step 1e-6 relative on the
-    solver's own (float32) metric entries, at 32 random cells."""
+    L = 1/2 sum over receivers (T - t_obs)^2, step 1e-6 relative (of the
+    cell's metric scale) on the solver's own float32 metric entries, divided
+    by the float32 difference actually applied, at 32 random cells."""
     import tomo
 
     M, T0, rec = _adj_case(cuda)
@@ -551,14 +572,8 @@ def test_adjoint_matches_finite_differences(f3d, ctx, cuda):
     for q in rng.choice(len(cand), 32, replace=False):
         k, j, i = (int(v) for v in cand[q])
         comp = int(rng.integers(0, 6))
-        v = float(base[comp][k, j, i])
-        step = abs(v) * 1e-6 if v != 0 else 1e-12
-        up = [b.clone() for b in base]
-        dn = [b.clone() for b in base]
-        up[comp][k, j, i] = v + step
-        dn[comp][k, j, i] = v - step
-        dv = float(up[comp][k, j, i]) - float(dn[comp][k, j, i])  # the float32 difference actually applied
-        fd = (loss([u.double() for u in up]) - loss([d.double() for d in dn])) / dv
+        Mu, Md, dv = _fd_pair(base, comp, k, j, i)
+        fd = (loss(Mu) - loss(Md)) / dv
         ad = float(G[comp][k, j, i])
         errs.append(abs(fd - ad) / max(abs(ad), abs(fd), 1e-300))
     assert np.median(errs) < 1e-6 and max(errs) < 1e-4, (np.median(errs), max(errs))
@@ -613,3 +628,46 @@ def test_adjoint_chain_to_slowness_and_epsilon(cuda):
                 (loss(s0, up) - loss(s0, dn)) / (2 * step)
             ad = float(g[k, j, i])
             assert abs(fd - ad) <= 2e-2 * max(abs(ad), abs(fd)) + 1e-9 * float(g.abs().max()), (var, fd, ad)
+
+
+def test_adjoint_finite_differences_256(f3d, cuda):
+    """Full tomography size: 256^3 seeded heterogeneous TTI medium (seed 2),
+    one source 10 cells below the top face, 4096 receivers on the top face.
+    dL/dM from the adjoint against central differences (1e-6 relative to
+    the cell's metric scale, float32-exact, on the solver's metric entries)
+    at 32 random cells among those whose gradient is at least 1e-3 of the
+    largest.  Median relative error below 1e-6; every sample below 1e-5 (the
+    rounding of a loss summed over 4096 receivers is a few 1e-16 of it,
+    against differences of about 1e-10 of it)."""
+    import media
+    import tomo
+
+    n, h = 256, 10.0
+    M = [m.double().requires_grad_(True) for m in media.heterogeneous_tti(n, n, n, h, seed=2, device="cuda")]
+    T0 = cuda.full((n + 2,) * 3, MAXT, dtype=cuda.float64, device="cuda")
+    T0[11, 100, 140] = 0.0
+    ridx = cuda.arange(3, n + 1, 4, device="cuda")
+    rec = (1, ridx.view(-1, 1), ridx.view(1, -1))
+    T = tomo.solve(T0, h, M)
+    tobs = (T[rec] * 0.97).detach()
+    (0.5 * ((T[rec] - tobs) ** 2).sum()).backward()
+    G = [m.grad for m in M]
+
+    def loss(Mx):
+        with cuda.no_grad():
+            Tx = tomo.solve(T0, h, Mx)
+            return float(0.5 * ((Tx[rec] - tobs) ** 2).sum())
+
+    base = [m.detach().float() for m in M]
+    gmax = max(float(g.abs().max()) for g in G)
+    rng = np.random.default_rng(11)
+    errs = []
+    for q in range(32):
+        comp = int(rng.integers(0, 6))
+        cand = cuda.nonzero(G[comp].abs() >= 1e-3 * gmax)
+        k, j, i = (int(v) for v in cand[int(rng.integers(0, len(cand)))].tolist())
+        Mu, Md, dv = _fd_pair(base, comp, k, j, i)
+        fd = (loss(Mu) - loss(Md)) / dv
+        ad = float(G[comp][k, j, i])
+        errs.append(abs(fd - ad) / max(abs(ad), abs(fd)))
+    assert np.median(errs) < 1e-6 and max(errs) < 1e-5, (np.median(errs), max(errs))
