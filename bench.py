@@ -501,7 +501,7 @@ def run_adjoint(args):
         Ml = [m.detach().requires_grad_(True) for m in Mg]
         loss = torch.zeros((), dtype=torch.float64, device="cuda")
         for sp_, to in zip(srcs, tobs):
-            T = tomo.solve(t0_of(sp_), h, Ml, tol=tol)
+            T = tomo.solve(t0_of(sp_), h, Ml, tol=tol, adj_tol=args.adj_tol)
             Ls = 0.5 * ((T[rec] - to) ** 2).sum()
             Ls.backward()
             loss += Ls.detach()
@@ -538,7 +538,7 @@ def run_adjoint(args):
                                "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
                                % (n, nsrc, nsrc_side, nsrc_side, nrec_side ** 2, nrec_side, nrec_side),
                    "grid": n, "sources": nsrc, "receivers": nrec_side ** 2,
-                   "gradient": "slowness and eps (torch autograd over the C-ABI)"},
+                   "gradient": "slowness and eps (torch autograd over the C-ABI)", "adjoint_tol": args.adj_tol},
         "forward_ms_per_source": fwd, "adjoint_ms_per_source": adj, "adjoint_over_forward": adj / fwd,
         "forward_sweeps": [min(r.sweeps for r in fr), max(r.sweeps for r in fr)],
         "adjoint_sweeps": [min(r.sweeps for r in ar), max(r.sweeps for r in ar)],
@@ -575,6 +575,9 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
+    ap.add_argument("--adj-tol", type=float, default=1e-12,
+                    help="--medium adjoint: backward sweeps stop once one pushes at most this fraction of the "
+                         "first sweep's largest push (0: until nothing is pushed)")
     ap.add_argument("--medium", choices=["fold", "tti", "batch", "adjoint"], default="fold",
                     help="fold: the reference's drift medium and source (default); tti: the "
                          "heterogeneous tilted-elliptical configuration")

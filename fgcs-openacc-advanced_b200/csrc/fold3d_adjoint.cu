@@ -21,12 +21,20 @@
 // chain of winners of one direction is done in one pass; backward sweeps
 // (all six directions, reversed) repeat until a sweep pushes nothing.
 // Finally dL/dM(x) = lambda(x) * d(time)/dM(x).
+//
+// A backward pass is one persistent launch over (step, 32 x kWaveTV tile)
+// items, like a forward WAVEFRONT pass run the other way: the cells of step
+// p's target plane receive their pushes from the 3 x 3 tiles around them at
+// step p-1 (the plane behind them in this walk), so item (p, t) waits for
+// exactly those items' completion flags (bounded waits), then pushes and
+// publishes its own flag.
 #include <math_constants.h>
 
 #include <cstring>
 
 #include "fold3d_ellip.cuh"
 #include "fold3d_internal.h"
+#include "fold3d_sync.cuh"
 
 namespace fold3d {
 
@@ -122,50 +130,119 @@ __device__ double ell_cand(const EllipA &A, const double tv[9], int id, int pt[3
     return tv[0] + (l1 * d1 + l2 * d2) + n;
 }
 
-// Fan times and field indices of the winner's direction for target x.
-__device__ __forceinline__ void fan_of(const double *T, long long x, const PlaneGeom &g, long long idx[9], double tv[9])
+// Fan times of the winner's direction for target x (source point first,
+// then the rim in order).
+__device__ __forceinline__ void fan_times(const double *T, long long x, const PlaneGeom &g, double tv[9])
 {
     const long long st = x - g.sn;
 #pragma unroll
-    for (int p = 0; p < 9; ++p) {
-        idx[p] = st + fan_i(p) * g.sx + fan_j(p) * g.sy;
-        tv[p] = fabs(T[idx[p]]);
-    }
+    for (int p = 0; p < 9; ++p) tv[p] = fabs(T[st + fan_i(p) * g.sx + fan_j(p) * g.sy]);
+}
+
+// Field index of fan point p of target x.
+__device__ __forceinline__ long long fan_index(long long x, const PlaneGeom &g, int p)
+{
+    return x - g.sn + fan_i(p) * g.sx + fan_j(p) * g.sy;
 }
 }  // namespace
 
-// One backward step of direction dir: the cells of one target plane whose
-// winner came from this direction push what they have not pushed yet.
-__global__ void __launch_bounds__(256) adj_push_kernel(const double *__restrict__ T, double *lam, double *pushed,
-                                                       const unsigned short *__restrict__ W, PlaneGeom g,
-                                                       EllipParam ep, int dir, long long tgt_off,
-                                                       unsigned long long *maxd)
+constexpr int kAdjThreads = 32 * kWaveTV;
+
+// One backward pass of direction b.a.dir (see the top of the file).
+__global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads)
+    adj_pass_kernel(AdjWaveArgs b, const __grid_constant__ EllipParam ep)
 {
-    const int u = blockIdx.x * 32 + threadIdx.x + 1;
-    const int v = blockIdx.y * 8 + threadIdx.y + 1;
+    __shared__ int s_next;
+    const WaveArgs &a = b.a;
+    const PlaneGeom &g = a.pg;
+    const int ntiles = a.ntu * a.ntv;
+    const long long total = (long long)a.steps * ntiles;
+    const unsigned want = a.epoch << 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double dmax = 0.0;
-    if (u <= g.nu && v <= g.nv) {
-        const long long x = tgt_off + (long long)u * g.su + (long long)v * g.sv;
-        const unsigned w = W[x];
-        if (w != kNoWinner && (int)(w >> 6) == dir) {
-            const double L = lam[x];
-            const double D = L - pushed[x];
-            if (D != 0.0) {
-                pushed[x] = L;
-                long long idx[9];
-                double tv[9];
-                fan_of(T, x, g, idx, tv);
-                int pt[3], np;
-                double wt[3], c[3], n;
-                if (ell_cand(ell_local(ep.med, ep.dir, x), tv, (int)(w & 63u), pt, wt, np, c, n) < CUDART_INF)
-                    for (int q = 0; q < np; ++q) atomicAdd(lam + idx[pt[q]], wt[q] * D);
-                dmax = fabs(D);
+    if (tid == 0) {
+        const unsigned w = atomicAdd(a.work, 1u);
+        s_next = (w < total) ? (int)w : -1;
+    }
+    __syncthreads();
+    for (;;) {
+        const int item = s_next;
+        if (item < 0) break;
+        __syncthreads();  // every thread has read s_next
+        if (tid == 0) {  // claim the next item now; it is processed after this one
+            int it = -1;
+            if (*(volatile unsigned *)a.status == 0) {
+                const unsigned w = atomicAdd(a.work, 1u);
+                if (w < total) it = (int)w;
             }
+            s_next = it;
+        }
+        const int p = item / ntiles, t = item - p * ntiles;
+        const int tu = t % a.ntu, tv = t / a.ntu;
+        const int tgt = a.first_src - p * a.sg;
+        // Everything but lambda is fixed during the adjoint: find this
+        // thread's cell, its winner's source points and weights, and what it
+        // pushed before, while the items it waits for are still running.
+        const int u = tu * 32 + lane + 1;
+        const int v = tv * kWaveTV + warp + 1;
+        long long x = -1, src[3] = {0, 0, 0};
+        double wt[3] = {0.0, 0.0, 0.0}, P = 0.0;
+        int np = 0;
+        if (u <= g.nu && v <= g.nv) {
+            const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
+            const unsigned w = b.W[xc];
+            if (w != kNoWinner && (int)(w >> 6) == a.dir) {
+                x = xc;
+                P = b.pushed[x];
+                double tv9[9], c[3], n;
+                int pt[3];
+                fan_times(b.T, x, g, tv9);
+                if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w & 63u), pt, wt, np, c, n) < CUDART_INF))
+                    np = 0;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
+            }
+        }
+        int timed_out = 0;
+        if (tid < 9 && p > 0) {
+            const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
+            if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
+                const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nv * a.ntu + nu;
+                const unsigned long long t0 = global_ns();
+                unsigned spins = 0;
+                while (ld_acquire(fl) < want) {
+                    if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
+                        *(volatile unsigned *)a.status != 0) {
+                        atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                        timed_out = 1;
+                        break;
+                    }
+                    if (kPollNs) __nanosleep(kPollNs);
+                }
+            }
+        }
+        if (__syncthreads_or(timed_out)) break;
+        if (x >= 0) {
+            const double L = __ldcg(b.lam + x);
+            const double D = L - P;
+            if (D != 0.0) {
+                b.pushed[x] = L;
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+                    if (q < np) atomicAdd(b.lam + src[q], wt[q] * D);
+                dmax = fmax(dmax, fabs(D));
+            }
+        }
+        // publish (the barrier orders every thread's atomics before thread 0's fence)
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(a.flags + item, want);
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    if ((threadIdx.x & 31) == 0 && dmax > 0.0) atomicMax(maxd, (unsigned long long)__double_as_longlong(dmax));
+    if (lane == 0 && dmax > 0.0) atomicMax(a.maxd, (unsigned long long)__double_as_longlong(dmax));
 }
 
 // dL/dM(x) = lambda(x) d(time(x))/dM(x), six arrays (component-major) in the
@@ -187,9 +264,8 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict_
         if (w != kNoWinner && (w >> 6) < 6u) {
             const int dir = (int)(w >> 6);
             const EllipDir &D = geo.d[dir];
-            long long idx[9];
             double tv[9];
-            fan_of(T, x, geo.pg[dir], idx, tv);
+            fan_times(T, x, geo.pg[dir], tv);
             int pt[3], np;
             double wt[3], c[3], n;
             if (ell_cand(ell_local(med, D, x), tv, (int)(w & 63u), pt, wt, np, c, n) < CUDART_INF) {
@@ -211,14 +287,17 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict_
     }
 }
 
-cudaError_t launch_adj_push(const double *T, double *lam, double *pushed, const unsigned short *W,
-                            const PlaneGeom &pg, const EllipParam &ep, int dir, int tgt, unsigned long long *maxd,
-                            cudaStream_t s)
+cudaError_t launch_adj_pass(const AdjWaveArgs &b, const EllipParam &ep, int grid, cudaStream_t s)
 {
-    dim3 block(32, 8);
-    dim3 grid((pg.nu + 31) / 32, (pg.nv + 7) / 8);
-    adj_push_kernel<<<grid, block, 0, s>>>(T, lam, pushed, W, pg, ep, dir, (long long)tgt * pg.s_nrm, maxd);
+    adj_pass_kernel<<<grid, kAdjThreads, 0, s>>>(b, ep);
     return cudaGetLastError();
+}
+
+int adj_blocks_per_sm()
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adj_pass_kernel, kAdjThreads, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
 }
 
 cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned short *W, const AdjGeom &geo,

@@ -161,6 +161,7 @@ struct fold3d_ctx {
     unsigned *b_counters = nullptr;          // work, status
     double *adj_pushed = nullptr;            // adjoint: lambda already pushed, per cell
     size_t adj_cells = 0;
+    int adj_bps = 0;
     char *b_stage_d = nullptr, *b_stage_h = nullptr;
     size_t b_stage_bytes = 0;
 };
@@ -920,13 +921,14 @@ int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_
 
 int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const double *T,
                          const unsigned short *W, const double *dLdT, double *lam, double *dLdM, int max_sweeps,
-                         void *stream, fold3d_report *rep)
+                         double tol, void *stream, fold3d_report *rep)
 {
     clear_error();
     if (!c || !m || !T || !W || !dLdT || !lam || !dLdM) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
     int rc = check_grid(g);
     if (rc) return rc;
     if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     const size_t cells = field_cells(*g);
@@ -942,6 +944,9 @@ int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip
     if ((e = cudaMemcpyAsync(lam, dLdT, cells * sizeof(double), cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(c->adj_pushed, 0, cells * sizeof(double), s)) != cudaSuccess)
         return cuda_error(e, "adjoint setup");
+    if ((rc = reserve_passes(c, 6u * (unsigned)std::min(max_sweeps, 1 << 20) + 12u))) return rc;
+    if ((rc = wave_scratch(c, *g))) return rc;
+    if (!c->adj_bps) c->adj_bps = adj_blocks_per_sm();
     AdjGeom geo;
     memset(&geo, 0, sizeof geo);
     EllipParam ep[6];
@@ -950,26 +955,50 @@ int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip
         ep[d] = ellip_param(*g, *m, d);
         geo.d[d] = ep[d].dir;
     }
+    AdjWaveArgs b;
+    memset(&b, 0, sizeof b);
+    b.T = T;
+    b.lam = lam;
+    b.pushed = c->adj_pushed;
+    b.W = W;
+    b.a.flags = c->w_flags;
+    b.a.work = c->w_counters;
+    b.a.status = c->w_counters + 1;
+    b.a.maxd = c->d_maxd;
+    b.a.timeout_ns = 4000000000ull;
+    if ((e = cudaMemsetAsync(c->w_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess)
+        return cuda_error(e, "cudaMemsetAsync");
     if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
     int sweeps = 0;
-    double delta = 0.0;
+    double delta = 0.0, first = 0.0;
+    unsigned hstat[2] = {0, 0};
     while (sweeps < max_sweeps) {
         if ((e = cudaMemsetAsync(c->d_maxd, 0, 8, s)) != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
         for (int d = 5; d >= 0; --d) {  // the forward order reversed
-            const PlaneGeom &pg = geo.pg[d];
-            // the forward targets of direction d, last first
-            const int sg = kDirs[d].sg;
-            const int last_tgt = pass_first(pg, d) + sg * pass_count(pg);
-            for (int t = last_tgt, q = 0; q < pass_count(pg); ++q, t -= sg)
-                if ((e = launch_adj_push(T, lam, c->adj_pushed, W, pg, ep[d], d, t, c->d_maxd, s)) != cudaSuccess)
-                    return cuda_error(e, "adjoint push");
+            const DirSpec &ds = kDirs[d];
+            b.a.pg = geo.pg[d];
+            b.a.nrm = ds.nrm;
+            b.a.sg = ds.sg;
+            orient_tiles(*g, ds.nrm, b.a.ntu, b.a.ntv);
+            b.a.steps = pass_count(b.a.pg);
+            b.a.first_src = pass_first(b.a.pg, d) + ds.sg * pass_count(b.a.pg);  // the forward pass's last target
+            b.a.epoch = ++c->epoch;
+            b.a.dir = d;
+            const long long items = (long long)b.a.steps * b.a.ntu * b.a.ntv;
+            const int grid = (int)std::min<long long>(items, (long long)c->sms * c->adj_bps);
+            if ((e = cudaMemsetAsync(b.a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
+                return cuda_error(e, "cudaMemsetAsync");
+            if ((e = launch_adj_pass(b, ep[d], grid, s)) != cudaSuccess) return cuda_error(e, "adjoint pass");
         }
         ++sweeps;
         if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(hstat, c->w_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
             return cuda_error(e, "adjoint sweep");
+        if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "adjoint: a dependency wait gave up");
         memcpy(&delta, c->h_maxd, 8);
-        if (delta == 0.0) break;
+        if (sweeps == 1) first = delta;
+        if (delta <= tol * first) break;
     }
     EllipMedium med;
     const float *arr[6] = {m->mxx, m->mxy, m->mxz, m->myy, m->myz, m->mzz};

@@ -59,6 +59,12 @@ enum Variant {
 
 // WAVEFRONT tiles are 32 points along the plane's faster axis by
 // FOLD3D_WAVE_TV rows; one CTA of 32*FOLD3D_WAVE_TV threads works on a tile.
+// Pause between two polls of a dependency flag (ns; 0 polls back to back).
+#ifndef FOLD3D_POLL_NS
+#define FOLD3D_POLL_NS 32
+#endif
+constexpr unsigned kPollNs = FOLD3D_POLL_NS;
+
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4
 #endif
@@ -128,9 +134,17 @@ struct AdjGeom {
     PlaneGeom pg[6];
     EllipDir d[6];
 };
-cudaError_t launch_adj_push(const double *T, double *lam, double *pushed, const unsigned short *W,
-                            const PlaneGeom &pg, const EllipParam &ep, int dir, int tgt, unsigned long long *maxd,
-                            cudaStream_t s);
+// One backward pass of direction a.dir: a.first_src holds the first target
+// plane of the pass (the forward pass's last), a.steps the planes, a.maxd
+// receives max |pushed amount|, a.epoch numbers the pass like a forward pass.
+struct AdjWaveArgs {
+    WaveArgs a;
+    const double *T;
+    double *lam, *pushed;
+    const unsigned short *W;
+};
+cudaError_t launch_adj_pass(const AdjWaveArgs &b, const EllipParam &ep, int grid, cudaStream_t s);
+int adj_blocks_per_sm();
 cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned short *W, const AdjGeom &geo,
                             const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s);
 

@@ -41,29 +41,11 @@
 #include "fold3d_ellip.cuh"
 #include "fold3d_fast.cuh"
 #include "fold3d_internal.h"
+#include "fold3d_sync.cuh"
 
 namespace fold3d {
 
 namespace {
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
 __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
 
@@ -122,7 +104,7 @@ __device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs
                         timed_out = 1;
                         break;
                     }
-                    __nanosleep(32);
+                    if (kPollNs) __nanosleep(kPollNs);
                 }
                 if (!timed_out) recent |= (int)(f & 1u);
             }

@@ -118,7 +118,7 @@ def lib() -> C.CDLL:
     L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
     L.fold3d_solve_ellip_record.argtypes = [vp, P(Grid), P(Ellip), vp, vp, P(Opts), vp, P(Report)]
-    L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, vp, P(Report)]
+    L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
     L.InitFoldFromPoint.restype = d
     L.ImpSurfF.argtypes = [d] * 3
@@ -316,14 +316,16 @@ def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream
     return rep
 
 
-def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, stream=None) -> Report:
+def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, tol=0.0, stream=None) -> Report:
     """fold3d_adjoint_ellip: lam <- dL/dT (total), dLdM (shape (6,)+T.shape,
-    float64) <- dL/dM, from the converged T, its winner record W and dLdT."""
+    float64) <- dL/dM, from the converged T, its winner record W and dLdT.
+    Backward sweeps stop once one pushes at most tol times the first sweep's
+    largest push (tol 0: once one pushes nothing)."""
     nx, ny, nz = grid_of(T)
     rep = Report()
     _check(lib().fold3d_adjoint_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
                                       C.c_void_p(W.data_ptr()), _dev_ptr(dLdT), _dev_ptr(lam),
-                                      C.c_void_p(dLdM.data_ptr()), int(max_sweeps),
+                                      C.c_void_p(dLdM.data_ptr()), int(max_sweeps), float(tol),
                                       C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 

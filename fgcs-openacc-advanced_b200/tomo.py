@@ -3,9 +3,11 @@ torch operation.  torch is used here only as the harness; the forward solve
 and its adjoint run in libfold3dpmm (fold3d_solve_ellip_record,
 fold3d_adjoint_ellip).
 
-EllipSolve.apply(T0, h, max_sweeps, tol, *M) returns the converged field for
-the initial field T0 (a point source) and a float64 metric M (six CUDA
-tensors, xx xy xz yy yz zz, field layout; the solver stores it as float32).
+EllipSolve.apply(T0, h, max_sweeps, tol, adj_tol, *M) returns the converged
+field for the initial field T0 (a point source) and a float64 metric M (six
+CUDA tensors, xx xy xz yy yz zz, field layout; the solver stores it as
+float32).  tol stops the forward sweeps (max |dT| <= tol), adj_tol the
+backward ones (fold3d_adjoint_ellip's tol).
 Its backward pass returns dL/dM in float64, so torch carries the gradient on
 to whatever produced M (slowness, epsilon and axis through
 media.metric_from).
@@ -42,7 +44,7 @@ def context(device=None) -> f3d.Context:
 
 class EllipSolve(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, T0, h, max_sweeps, tol, *M):
+    def forward(ctx, T0, h, max_sweeps, tol, adj_tol, *M):
         M32 = [m.detach().to(torch.float32).contiguous() for m in M]
         T = T0.detach().clone()
         W = torch.empty(T.shape, dtype=torch.int16, device=T.device)
@@ -51,6 +53,7 @@ class EllipSolve(torch.autograd.Function):
         ctx.save_for_backward(T, W, *M32)
         ctx.h = h
         ctx.sweeps = rep.sweeps
+        ctx.adj_tol = adj_tol
         return T
 
     @staticmethod
@@ -58,9 +61,10 @@ class EllipSolve(torch.autograd.Function):
         T, W, *M32 = ctx.saved_tensors
         lam = torch.empty_like(T)
         dLdM = torch.empty((6,) + tuple(T.shape), dtype=torch.float64, device=T.device)
-        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM))
-        return (None, None, None, None) + tuple(dLdM[m] for m in range(6))
+        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM,
+                                           tol=ctx.adj_tol))
+        return (None, None, None, None, None) + tuple(dLdM[m] for m in range(6))
 
 
-def solve(T0, h, M, max_sweeps=1000, tol=0.0):
-    return EllipSolve.apply(T0, h, max_sweeps, tol, *M)
+def solve(T0, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):
+    return EllipSolve.apply(T0, h, max_sweeps, tol, adj_tol, *M)

@@ -186,14 +186,17 @@ int fold3d_solve_ellip_record(fold3d_ctx *ctx, const fold3d_grid *g, const fold3
  * (device, field layout), writes lambda_dev = the total derivative dL/dT
  * (device, field layout) and dLdM_dev = dL/dM, six arrays of doubles in the
  * field layout, component-major (xx xy xz yy yz zz), every cell written (0 on
- * ghosts and on cells without a winner).  Backward sweeps repeat
- * until one changes nothing, at most max_sweeps; rep->sweeps counts them and
- * rep->max_delta is the largest pushed amount of the last one (0 when done).
+ * ghosts and on cells without a winner).  Backward sweeps repeat until one
+ * pushes at most tol times the largest amount the first sweep pushed (tol 0:
+ * until one pushes nothing), at most max_sweeps; rep->sweeps counts them and
+ * rep->max_delta is the largest pushed amount of the last one.  The gradient
+ * converges geometrically over the sweeps; tol 1e-12 typically leaves a
+ * relative error of that order.
  * lambda is accumulated with floating-point atomics: results agree with the
  * FP64 CPU statement to rounding, not bit for bit. */
 int fold3d_adjoint_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, const double *T_dev,
                          const unsigned short *winners_dev, const double *dLdT_dev, double *lambda_dev,
-                         double *dLdM_dev, int max_sweeps, void *stream, fold3d_report *rep);
+                         double *dLdM_dev, int max_sweeps, double tol, void *stream, fold3d_report *rep);
 
 /* One instance of a batched solve: its grid, elliptical medium and device
  * field (in/out). */

@@ -671,3 +671,24 @@ def test_adjoint_finite_differences_256(f3d, cuda):
         ad = float(G[comp][k, j, i])
         errs.append(abs(fd - ad) / max(abs(ad), abs(fd)))
     assert np.median(errs) < 1e-6 and max(errs) < 1e-5, (np.median(errs), max(errs))
+
+
+def test_adjoint_tolerance_stops_early(f3d, ctx, cuda):
+    """A relative tolerance ends the backward sweeps early with the gradient
+    still within ~1e-9 of the exact (tol 0) one."""
+    M, T0, rec = _adj_case(cuda, dims=(40, 36, 44), seed=9, src=(20, 18, 6))
+    Md = [m.cuda() for m in M]
+    T = T0.clone()
+    W = cuda.empty(T.shape, dtype=cuda.int16, device="cuda")
+    f3d.solve_ellip_record(ctx, T, 10.0, Md, W, f3d.opts(max_sweeps=300, tol=0.0))
+    r = cuda.zeros_like(T)
+    r[rec] = 1.0
+    out = {}
+    for tol in (0.0, 1e-12):
+        lam = cuda.empty_like(T)
+        g = cuda.empty((6,) + tuple(T.shape), dtype=cuda.float64, device="cuda")
+        out[tol] = (f3d.adjoint_ellip(ctx, T, 10.0, Md, W, r, lam, g, tol=tol), g)
+    assert out[1e-12][0].sweeps <= out[0.0][0].sweeps
+    assert out[0.0][0].max_delta == 0.0
+    err = float((out[1e-12][1] - out[0.0][1]).norm() / out[0.0][1].norm())
+    assert err < 1e-9, err
