@@ -233,12 +233,10 @@ __global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads)
                 dmax = fmax(dmax, fabs(D));
             }
         }
-        // publish (the barrier orders every thread's atomics before thread 0's fence)
+        // publish: the barrier makes every thread's atomics precede thread 0's
+        // release store, which orders them (cumulatively) before the flag
         __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_release(a.flags + item, want);
-        }
+        if (tid == 0) st_release(a.flags + item, want);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));

@@ -29,8 +29,8 @@
 // step p-1 of the current pass changed the source plane comes with its
 // completion flags, which hold (pass << 1) | changed.
 //
-// Synchronisation: a CTA publishes an item with __syncthreads, a gpu-scope
-// fence and a release store into the item's flag; in a waiting CTA, nine
+// Synchronisation: a CTA publishes an item with __syncthreads and a
+// gpu-scope release store into the item's flag; in a waiting CTA, nine
 // threads poll the nine neighbour flags in parallel with acquire loads and
 // then release the block with __syncthreads.  Each CTA claims its next item
 // while it works on the current one.  Field values written inside the launch are read with
@@ -161,12 +161,10 @@ __device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs
         changed = __syncthreads_or(changed);
         if (changed && tid == 0) a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
     }
-    // publish (the barrier orders every thread's stores before thread 0's fence)
+    // publish: the barrier makes every thread's stores precede thread 0's
+    // release store, which orders them (cumulatively) before the flag
     __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        st_release(a.flags + item, want | (unsigned)changed);
-    }
+    if (tid == 0) st_release(a.flags + item, want | (unsigned)changed);
     return true;
 }
 
