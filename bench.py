@@ -722,8 +722,11 @@ def main():
     alg_bytes = BYTES_PER_UPDATE * upd
     launches = launches_per_step * args.steps
     achieved = alg_bytes / (solve_ms / 1e3) / 1e9
+    # DRAM bytes (read + write) of one pass from an ncu capture of this workload
+    # (profiles/wave_pass_kernel_fold512_dram.md); other sizes: not measured
+    traffic = 1090855424 + 178331648 if (n == 512 and rep.engine == f3d.ENGINE_WAVEFRONT) else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_kind": peak_kind,
+                "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "plane_kernel" if rep.engine == f3d.ENGINE_PLANES else "wavefront_kernel",
                 "alg_bytes_per_launch": alg_bytes / launches_per_step,
                 "avg_launch_us": solve_ms * 1e3 / launches_per_step,

@@ -2,7 +2,7 @@
 // elliptical-medium solve.  No counterpart in the reference.
 //
 // The forward solve records, per cell, the candidate that last set its time
-// (its "winner": sweep direction and candidate id, 2 bytes).  At convergence
+// (its "winner": sweep direction and candidate id, 1 byte).  At convergence
 // a cell's time is that candidate, t(footpoint) + ||X - footpoint||_M, with
 // the footpoint on a vertex, edge or triangle of the direction's source
 // plane.  By the envelope theorem its derivative with respect to each source
@@ -39,7 +39,6 @@
 namespace fold3d {
 
 namespace {
-constexpr unsigned short kNoWinner = 0xffffu;
 
 // Point p of the fan: 0 the source point st, 1..8 rim point p-1.
 __device__ __forceinline__ int fan_i(int p) { return p == 0 ? 0 : ell_ri(p - 1); }
@@ -191,13 +190,13 @@ __global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads)
         if (u <= g.nu && v <= g.nv) {
             const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
             const unsigned w = b.W[xc];
-            if (w != kNoWinner && (int)(w >> 6) == a.dir) {
+            if (w != kNoWinner && (int)(w / kEllipCands) == a.dir) {
                 x = xc;
                 P = b.pushed[x];
                 double tv9[9], c[3], n;
                 int pt[3];
                 fan_times(b.T, x, g, tv9);
-                if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w & 63u), pt, wt, np, c, n) < CUDART_INF))
+                if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF))
                     np = 0;
 #pragma unroll
                 for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
@@ -247,7 +246,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads)
 // field layout, accumulated in the order of the CPU statement.  Every cell is
 // written: ghosts and cells without a winner get 0.
 __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict__ T, const double *__restrict__ lam,
-                                                       const unsigned short *__restrict__ W,
+                                                       const unsigned char *__restrict__ W,
                                                        const __grid_constant__ AdjGeom geo, EllipMedium med, int nx,
                                                        int ny, int nz, double *dLdM)
 {
@@ -259,14 +258,14 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict_
         const bool interior = i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nz;
         double dM[6] = {0, 0, 0, 0, 0, 0};
         const unsigned w = interior ? W[x] : kNoWinner;
-        if (w != kNoWinner && (w >> 6) < 6u) {
-            const int dir = (int)(w >> 6);
+        if (w < 6u * kEllipCands) {
+            const int dir = (int)(w / kEllipCands);
             const EllipDir &D = geo.d[dir];
             double tv[9];
             fan_times(T, x, geo.pg[dir], tv);
             int pt[3], np;
             double wt[3], c[3], n;
-            if (ell_cand(ell_local(med, D, x), tv, (int)(w & 63u), pt, wt, np, c, n) < CUDART_INF) {
+            if (ell_cand(ell_local(med, D, x), tv, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF) {
                 const double hh[3] = {D.hx, D.hy, D.hz};
                 const int sxy[3][3] = {{1, D.sxy, D.sxz}, {D.sxy, 1, D.syz}, {D.sxz, D.syz, 1}};
                 const int comp[3][3] = {{D.ixx, D.ixy, D.ixz}, {D.ixy, D.iyy, D.iyz}, {D.ixz, D.iyz, D.izz}};
@@ -298,7 +297,7 @@ int adj_blocks_per_sm()
     return n > 0 ? n : 1;
 }
 
-cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned short *W, const AdjGeom &geo,
+cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
                             const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s)
 {
     adj_grad_kernel<<<148 * 8, 256, 0, s>>>(T, lam, W, geo, med, g.nx, g.ny, g.nz, dLdM);

@@ -428,7 +428,7 @@ static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int d
 
 static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
                            double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep,
-                           unsigned short *winners = nullptr)
+                           unsigned char *winners = nullptr)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
     if (rc) return rc;
@@ -899,7 +899,7 @@ int fold3d_solve_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *
 }
 
 int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T,
-                              unsigned short *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
+                              unsigned char *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
     clear_error();
     if (!W) return set_error(FOLD3D_ERR_INVALID, "winner array is NULL");
@@ -908,7 +908,7 @@ int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_
     if (rc) return rc;
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    cudaError_t e = cudaMemsetAsync(W, 0xff, field_cells(*g) * sizeof(unsigned short), s);
+    cudaError_t e = cudaMemsetAsync(W, 0xff, field_cells(*g), s);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
     if (!T || !m || !o || !m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
         return set_error(FOLD3D_ERR_INVALID, "NULL argument");
@@ -920,7 +920,7 @@ int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_
 }
 
 int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const double *T,
-                         const unsigned short *W, const double *dLdT, double *lam, double *dLdM, int max_sweeps,
+                         const unsigned char *W, const double *dLdT, double *lam, double *dLdM, int max_sweeps,
                          double tol, void *stream, fold3d_report *rep)
 {
     clear_error();

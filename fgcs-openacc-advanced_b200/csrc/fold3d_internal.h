@@ -87,11 +87,17 @@ struct WaveArgs {
     unsigned *status;            // 0, or 1 after a wait gave up
     unsigned long long *maxd;    // max |dT| (IEEE bits) of the sweep
     unsigned long long *evaluated;  // points evaluated
-    unsigned short *winners;     // elliptical medium: winner records, or NULL
+    unsigned char *winners;      // elliptical medium: winner records, or NULL
     int dir;                     // direction of the pass (for the winner records)
 };
 // Media of the local solver.
 enum Medium { kMediumDrift = 0, kMediumEllip = 1 };
+
+// Winner record of a cell (elliptical medium): direction * kEllipCands +
+// candidate id (candidate ids 0..32 of the fan solver), kNoWinner if no
+// candidate set the cell's time.  One byte per cell.
+constexpr unsigned kEllipCands = 33;
+constexpr unsigned kNoWinner = 0xffu;
 
 struct EllipDir;     // fold3d_ellip.cuh
 struct EllipParam;   // below, once EllipDir is complete
@@ -141,11 +147,11 @@ struct AdjWaveArgs {
     WaveArgs a;
     const double *T;
     double *lam, *pushed;
-    const unsigned short *W;
+    const unsigned char *W;
 };
 cudaError_t launch_adj_pass(const AdjWaveArgs &b, const EllipParam &ep, int grid, cudaStream_t s);
 int adj_blocks_per_sm();
-cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned short *W, const AdjGeom &geo,
+cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
                             const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s);
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.

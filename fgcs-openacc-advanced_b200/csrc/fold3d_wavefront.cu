@@ -138,7 +138,7 @@ __device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs
                 int win;
                 tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d), win);
                 if (a.winners && __double_as_longlong(tnew) != __double_as_longlong(told))
-                    a.winners[d] = (win < 0) ? (unsigned short)0xffffu : (unsigned short)((a.dir << 6) | win);
+                    a.winners[d] = (win < 0) ? (unsigned char)kNoWinner : (unsigned char)(a.dir * kEllipCands + win);
             }
             if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
                 T[d] = tnew;

@@ -305,9 +305,20 @@ def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> 
     return rep
 
 
+def _check_like(name, X, T, itemsize, lead=()):
+    """X must be a contiguous CUDA tensor of shape lead + T.shape with
+    itemsize-byte elements (the library writes that many bytes)."""
+    if not (X.is_cuda and X.is_contiguous() and X.element_size() == itemsize
+            and tuple(X.shape) == tuple(lead) + tuple(T.shape)):
+        raise ValueError("%s: need a contiguous CUDA tensor of shape %s with %d-byte elements"
+                         % (name, tuple(lead) + tuple(T.shape), itemsize))
+
+
 def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream=None) -> Report:
-    """solve_ellip that also fills W (an int16 CUDA tensor shaped like T)
-    with each cell's winner record (the adjoint's checkpoint)."""
+    """solve_ellip that also fills W (a uint8 CUDA tensor shaped like T) with
+    each cell's winner record (the adjoint's checkpoint): direction * 33 +
+    candidate id, 0xff where no candidate set the cell's time."""
+    _check_like("W", W, T, 1)
     nx, ny, nz = grid_of(T)
     rep = Report()
     _check(lib().fold3d_solve_ellip_record(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
@@ -321,6 +332,10 @@ def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, 
     float64) <- dL/dM, from the converged T, its winner record W and dLdT.
     Backward sweeps stop once one pushes at most tol times the first sweep's
     largest push (tol 0: once one pushes nothing)."""
+    _check_like("W", W, T, 1)
+    _check_like("dLdT", dLdT, T, 8)
+    _check_like("lam", lam, T, 8)
+    _check_like("dLdM", dLdM, T, 8, lead=(6,))
     nx, ny, nz = grid_of(T)
     rep = Report()
     _check(lib().fold3d_adjoint_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),

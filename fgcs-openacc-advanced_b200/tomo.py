@@ -47,7 +47,7 @@ class EllipSolve(torch.autograd.Function):
     def forward(ctx, T0, h, max_sweeps, tol, adj_tol, *M):
         M32 = [m.detach().to(torch.float32).contiguous() for m in M]
         T = T0.detach().clone()
-        W = torch.empty(T.shape, dtype=torch.int16, device=T.device)
+        W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         rep = _note("forward", f3d.solve_ellip_record(context(), T, h, M32, W,
                                                       f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol)))
         ctx.save_for_backward(T, W, *M32)

@@ -173,12 +173,13 @@ int fold3d_solve_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip
                        const fold3d_opts *o, void *stream, fold3d_report *rep);
 
 /* fold3d_solve_ellip that also records, per cell, the candidate that last
- * set its time -- (direction << 6) | candidate id, or 0xffff if none did --
- * into winners_dev (one unsigned short per field cell, device memory; the
- * call first sets it to 0xffff).  This record is the checkpoint of the
+ * set its time -- direction * 33 + candidate id (directions 0..5 as in
+ * fold3d_dir, candidate ids 0..32 of the fan solver), or 0xff if none did --
+ * into winners_dev (one byte per field cell, device memory; the call first
+ * sets it to 0xff).  This record is the checkpoint of the
  * adjoint; it replaces the history of the field. */
 int fold3d_solve_ellip_record(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, double *T_dev,
-                              unsigned short *winners_dev, const fold3d_opts *o, void *stream,
+                              unsigned char *winners_dev, const fold3d_opts *o, void *stream,
                               fold3d_report *rep);
 
 /* Adjoint of a converged elliptical solve.  No counterpart in the reference.
@@ -195,7 +196,7 @@ int fold3d_solve_ellip_record(fold3d_ctx *ctx, const fold3d_grid *g, const fold3
  * lambda is accumulated with floating-point atomics: results agree with the
  * FP64 CPU statement to rounding, not bit for bit. */
 int fold3d_adjoint_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, const double *T_dev,
-                         const unsigned short *winners_dev, const double *dLdT_dev, double *lambda_dev,
+                         const unsigned char *winners_dev, const double *dLdT_dev, double *lambda_dev,
                          double *dLdM_dev, int max_sweeps, double tol, void *stream, fold3d_report *rep);
 
 /* One instance of a batched solve: its grid, elliptical medium and device

@@ -137,10 +137,10 @@ class Oracle:
         return s, d.value
 
     def ell_solve_rec(self, T, M, h, nsweeps, tol=-1.0):
-        """ell_solve that also returns the winner record (uint16, field layout;
-        0xffff where no candidate set the value)."""
+        """ell_solve that also returns the winner record (uint8, field layout:
+        direction * 33 + candidate id, 0xff where no candidate set the value)."""
         arrs, ptrs = self._metric(M)
-        W = np.full(T.shape, 0xFFFF, dtype=np.uint16)
+        W = np.full(T.shape, 0xFF, dtype=np.uint8)
         d = _dbl(0.0)
         s = self.L.orc_ell_solve_rec(_p(T), ptrs, W.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2], nsweeps,
                                      tol, C.byref(d))
@@ -153,7 +153,7 @@ class Oracle:
         lam = np.zeros_like(T)
         g = np.zeros((6,) + T.shape)
         r = np.ascontiguousarray(r, dtype=np.float64)
-        Wc = np.ascontiguousarray(W, dtype=np.uint16)
+        Wc = np.ascontiguousarray(W, dtype=np.uint8)
         nc = self.L.orc_ell_adjoint_rec(_p(T), ptrs, Wc.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2],
                                         r.ctypes.data_as(_ptr), lam.ctypes.data_as(_ptr), g.ctypes.data_as(_ptr))
         return lam, g, nc

@@ -665,9 +665,10 @@ static double orc_ell_point(double told, double st, const double nb[8], const or
     return ((told > 0) ? 1.0 : -1.0) * tn;
 }
 
-/* Winner record of a cell: (direction << 6) | candidate id; FOLD_NOWIN when no
- * candidate set its value (a source, or never reached). */
-#define ORC_NOWIN 0xffffu
+/* Winner record of a cell, one byte: direction * ORC_NCAND + candidate id;
+ * ORC_NOWIN when no candidate set its value (a source, or never reached). */
+#define ORC_NCAND 33
+#define ORC_NOWIN 0xffu
 
 /* index of the global metric component (p,q), arrays ordered xx xy xz yy yz zz */
 static int orc_mi(int p, int q)
@@ -679,7 +680,7 @@ static int orc_mi(int p, int q)
 
 /* One plane step of the elliptical medium.  M: six float arrays (xx, xy, xz,
  * yy, yz, zz of the metric in the i, j, k axes) in the field layout. */
-void orc_ell_plane_rec(double *T, const float *const *M, unsigned short *W, int nx, int ny, int nz, double dx,
+void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
                        double dy, double dz, int dir, int src)
 {
     const orc_grid g = orc_make_grid(nx, ny, nz);
@@ -712,7 +713,7 @@ void orc_ell_plane_rec(double *T, const float *const *M, unsigned short *W, int 
             int win;
             const double nv = orc_ell_point(T[t], fabs(T[s]), nb, &A, &win);
             if (W && memcmp(&nv, &T[t], sizeof nv) != 0)
-                W[t] = (win < 0) ? ORC_NOWIN : (unsigned short)((dir << 6) | win);
+                W[t] = (win < 0) ? ORC_NOWIN : (unsigned char)(dir * ORC_NCAND + win);
             T[t] = nv;
         }
 }
@@ -725,7 +726,7 @@ void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, dou
 
 /* Sweeps of the elliptical medium in the reference's direction order;
  * semantics as orc_solve. */
-int orc_ell_solve_rec(double *T, const float *const *M, unsigned short *W, int nx, int ny, int nz, double dx,
+int orc_ell_solve_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
                       double dy, double dz, int nsweeps, double tol, double *last_delta)
 {
     const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
@@ -1014,7 +1015,7 @@ void orc_ell_winners(const double *T, const float *const *M, int nx, int ny, int
  * layout).  Cells are processed by decreasing time; the return value is the
  * number of winner weights that point to a source point whose time is not
  * smaller (0 for a causal field, for which the order is exact). */
-long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned short *rec, int nx, int ny, int nz,
+long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned char *rec, int nx, int ny, int nz,
                          double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
 {
     const orc_grid g = orc_make_grid(nx, ny, nz);
@@ -1033,7 +1034,7 @@ long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned 
         const int64_t x = order[q];
         const int k = (int)(x / g.stride[2]), j = (int)((x % g.stride[2]) / g.stride[1]), i = (int)(x % g.stride[1]);
         if (rec) {
-            if (rec[x] != ORC_NOWIN) orc_ell_weights(T, M, &g, h, x, rec[x] >> 6, rec[x] & 63, &W[x]);
+            if (rec[x] < 6 * ORC_NCAND) orc_ell_weights(T, M, &g, h, x, rec[x] / ORC_NCAND, rec[x] % ORC_NCAND, &W[x]);
         } else {
             orc_ell_winner_at(T, M, &g, h, i, j, k, &W[x]);
         }

@@ -227,3 +227,53 @@ def test_heterogeneous_tti_generator_is_seeded_and_spd():
     xx, xy, xz, yy, yz, zz = (m.double() for m in a)
     det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * xz) + xz * (xy * yz - yy * xz)
     assert bool((xx > 0).all()) and bool((xx * yy - xy * xy > 0).all()) and bool((det > 0).all())
+
+
+def test_oracle_adjoint_matches_finite_differences():
+    """The FP64 CPU adjoint (winner records from the CPU solve, cells pushed
+    by decreasing time) against central differences of the CPU solve: step
+    1e-6 of the cell's metric scale on the float32 metric entries, divided by
+    the float32 difference applied."""
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    dims, h = (14, 12, 16), (10.0,) * 3
+    M = [m.numpy() for m in media.heterogeneous_tti(*dims, 10.0, seed=5)]
+    nx, ny, nz = dims
+    T0 = o.init_point(nx, ny, nz, (7, 6, 3))
+    T = T0.copy()
+    s, d, W = o.ell_solve_rec(T, M, h, 300, tol=0.0)
+    inner = W[1:-1, 1:-1, 1:-1]
+    assert d == 0.0 and W.dtype == np.uint8
+    assert (inner == 0xFF).sum() == 1 and W[3, 6, 7] == 0xFF  # only the source has no winner
+    assert int(inner[inner != 0xFF].max()) < 6 * 33
+    rec = (1, slice(1, -1, 2), slice(1, -1, 2))
+    tobs = T[rec] * 0.97
+    r = np.zeros_like(T)
+    r[rec] = T[rec] - tobs
+    lam, G, nc = o.ell_adjoint(T, M, h, W, r)
+    assert nc == 0
+
+    def loss(Mx):
+        Tx = T0.copy()
+        o.ell_solve(Tx, Mx, h, 300, tol=0.0)
+        return 0.5 * float(((Tx[rec] - tobs) ** 2).sum())
+
+    diag = {0: (0, 0), 1: (0, 3), 2: (0, 5), 3: (3, 3), 4: (3, 5), 5: (5, 5)}
+    rng = np.random.default_rng(2)
+    errs = []
+    for _ in range(12):
+        comp = int(rng.integers(0, 6))
+        cand = np.argwhere(np.abs(G[comp]) >= 1e-3 * np.abs(G).max())
+        k, j, i = cand[int(rng.integers(0, len(cand)))]
+        a, b = diag[comp]
+        step = 1e-6 * float(np.sqrt(M[a][k, j, i] * M[b][k, j, i]))
+        up = [m.copy() for m in M]
+        dn = [m.copy() for m in M]
+        up[comp][k, j, i] = np.float32(M[comp][k, j, i] + step)
+        dn[comp][k, j, i] = np.float32(M[comp][k, j, i] - step)
+        dv = float(up[comp][k, j, i]) - float(dn[comp][k, j, i])
+        fd = (loss(up) - loss(dn)) / dv
+        errs.append(abs(fd - G[comp][k, j, i]) / max(abs(fd), abs(G[comp][k, j, i])))
+    assert np.median(errs) < 1e-6 and max(errs) < 1e-4, (np.median(errs), max(errs))
