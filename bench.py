@@ -127,6 +127,33 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+def init_ranks(local, backend="nccl"):
+    """One process per GPU under torchrun: join the process group (short
+    timeout, so ranks that wait for a missing peer end with an error).
+    Returns torch.distributed, or None for a single process."""
+    if int(os.environ.get("WORLD_SIZE", "1")) <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300), **kw)
+    return dist
+
+
+def max_over_ranks(ms, dist, device="cuda"):
+    """The largest of every rank's ms (identity for a single process)."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None):
     """Time the reference's own sweep functions (oracle/_ref, OpenMP
     transform on `threads` cores) on the first planes of each of the six
@@ -225,14 +252,7 @@ def run_tti(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    dist = init_ranks(local)
     n, h = args.size, 10.0
     t0 = time.perf_counter()
     M = media.heterogeneous_tti(n, n, n, h, seed=0, device="cuda")
@@ -264,10 +284,7 @@ def run_tti(args):
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     upd = rep.nominal_updates
     value = world * upd * args.steps / (ms / 1e3) / 1e9
     e2e = None
@@ -609,14 +626,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    dist = init_ranks(local)
 
     n, sweeps = args.size, args.sweeps
     h = 10.0 / (n - 1.0)
@@ -680,10 +690,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     clocks = clk.summary()
     if args.converge:
         sweeps = rep.sweeps
@@ -707,10 +714,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, dist)
         nb = T0_pin.numel() * 8
         e2e = {"value": world * upd * args.steps / (ems / 1e3) / 1e9, "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb, "ms_per_step": ems / args.steps}

@@ -1,0 +1,56 @@
+"""Multi-process plumbing of bench.py on the CPU: world size 2 over gloo
+(127.0.0.1).  The GPU runs use the same helpers with NCCL."""
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import bench
+
+    dist = bench.init_ranks(rank, backend="gloo")
+    v = bench.max_over_ranks(1.5 + rank, dist, device="cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+    with open(os.path.join(out_dir, "rank%d" % rank), "w") as f:
+        f.write(repr(v))
+
+
+def test_max_over_ranks_world_2(tmp_path):
+    """Each rank times a different value; every rank ends with the largest."""
+    import torch.multiprocessing as mp
+
+    mp.start_processes(_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
+    assert [float((tmp_path / ("rank%d" % r)).read_text()) for r in range(2)] == [2.5, 2.5]
+
+
+def test_single_process_needs_no_group(monkeypatch):
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.init_ranks(0) is None
+    assert bench.max_over_ranks(3.25, None) == 3.25
+
+
+def test_reference_arm_runs_on_rank_0_only():
+    """Under torchrun the reference arm's other ranks exit 0 without work."""
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference"], env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.strip() == ""
