@@ -511,17 +511,30 @@ def run_adjoint(args):
     reps = []
     tomo.collect_reports(reps)
 
+    B = max(1, min(args.adj_batch, len(srcs)))
+    if B > 1:
+        T0s = torch.stack([t0_of(sp_) for sp_ in srcs])
+        tobs_s = torch.stack(tobs)
+        brec = (slice(None),) + rec
+
     def step():
         s = (1.0 / vz0).requires_grad_(True)
         e = eps0.clone().requires_grad_(True)
         Mg = [m.double() for m in media.metric_from(1.0 / s, e, ax0)]
         Ml = [m.detach().requires_grad_(True) for m in Mg]
         loss = torch.zeros((), dtype=torch.float64, device="cuda")
-        for sp_, to in zip(srcs, tobs):
-            T = tomo.solve(t0_of(sp_), h, Ml, tol=tol, adj_tol=args.adj_tol)
-            Ls = 0.5 * ((T[rec] - to) ** 2).sum()
-            Ls.backward()
-            loss += Ls.detach()
+        if B > 1:  # B sources per batched forward solve and batched adjoint
+            for c0 in range(0, len(srcs), B):
+                T = tomo.solve_batch(T0s[c0:c0 + B], h, Ml, tol=tol, adj_tol=args.adj_tol)
+                Ls = 0.5 * ((T[brec] - tobs_s[c0:c0 + B]) ** 2).sum()
+                Ls.backward()
+                loss += Ls.detach()
+        else:
+            for sp_, to in zip(srcs, tobs):
+                T = tomo.solve(t0_of(sp_), h, Ml, tol=tol, adj_tol=args.adj_tol)
+                Ls = 0.5 * ((T[rec] - to) ** 2).sum()
+                Ls.backward()
+                loss += Ls.detach()
         torch.autograd.backward(Mg, [m.grad for m in Ml])
         return float(loss), s.grad, e.grad
 
@@ -540,12 +553,23 @@ def run_adjoint(args):
     tomo.collect_reports(None)
     ms = ev0.elapsed_time(ev1) / args.steps
     nsrc = len(srcs)
-    fr = [r for k, r in reps if k == "forward"]
-    ar = [r for k, r in reps if k == "adjoint"]
-    fwd = sum(r.elapsed_ms for r in fr) / len(fr)
-    adj = sum(r.elapsed_ms for r in ar) / len(ar)
-    # wavefront: one launch per direction pass; adjoint: one per target plane and direction, plus the gradient
-    launches = sum(6 * r.sweeps for r in fr) + sum(6 * n * r.sweeps + 1 for r in ar)
+    if B > 1:
+        fr = [r for k, r in reps if k == "forward_batch"]
+        ar = [r for k, r in reps if k == "adjoint_batch"]
+        # a batch's reports share its elapsed time; count it once per batch
+        per_batch = lambda rs: [rs[q:q + B] for q in range(0, len(rs), B)]
+        fwd = sum(g[0].elapsed_ms for g in per_batch(fr)) / len(fr)
+        adj = sum(g[0].elapsed_ms for g in per_batch(ar)) / len(ar)
+        # one launch per direction pass of the slowest instance, plus one gradient launch per source
+        launches = sum(6 * max(r.sweeps for r in g) for g in per_batch(fr)) + \
+            sum(6 * max(r.sweeps for r in g) + len(g) for g in per_batch(ar))
+    else:
+        fr = [r for k, r in reps if k == "forward"]
+        ar = [r for k, r in reps if k == "adjoint"]
+        fwd = sum(r.elapsed_ms for r in fr) / len(fr)
+        adj = sum(r.elapsed_ms for r in ar) / len(ar)
+        # one launch per direction pass (forward and backward), plus the gradient
+        launches = sum(6 * r.sweeps for r in fr) + sum(6 * r.sweeps + 1 for r in ar)
     out = {
         "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -555,7 +579,8 @@ def run_adjoint(args):
                                "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
                                % (n, nsrc, nsrc_side, nsrc_side, nrec_side ** 2, nrec_side, nrec_side),
                    "grid": n, "sources": nsrc, "receivers": nrec_side ** 2,
-                   "gradient": "slowness and eps (torch autograd over the C-ABI)", "adjoint_tol": args.adj_tol},
+                   "gradient": "slowness and eps (torch autograd over the C-ABI)", "adjoint_tol": args.adj_tol,
+                   "sources_per_batch": B},
         "forward_ms_per_source": fwd, "adjoint_ms_per_source": adj, "adjoint_over_forward": adj / fwd,
         "forward_sweeps": [min(r.sweeps for r in fr), max(r.sweeps for r in fr)],
         "adjoint_sweeps": [min(r.sweeps for r in ar), max(r.sweeps for r in ar)],
@@ -592,6 +617,8 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
+    ap.add_argument("--adj-batch", type=int, default=64,
+                    help="--medium adjoint: sources per batched forward solve and adjoint (1: one by one)")
     ap.add_argument("--adj-tol", type=float, default=1e-12,
                     help="--medium adjoint: backward sweeps stop once one pushes at most this fraction of the "
                          "first sweep's largest push (0: until nothing is pushed)")

@@ -147,108 +147,223 @@ __device__ __forceinline__ long long fan_index(long long x, const PlaneGeom &g, 
 
 constexpr int kAdjThreads = 32 * kWaveTV;
 
-// One backward pass of direction b.a.dir (see the top of the file).
-__global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads)
-    adj_pass_kernel(AdjWaveArgs b, const __grid_constant__ EllipParam ep)
+// One item (step p, tile t) of a backward pass, for all threads of the CTA:
+// prepare the pushes, wait for those of the 3 x 3 tiles of step p-1 that
+// have work, push, publish.
+// Adds the largest pushed |amount| into dmax.  Returns false if a wait gave
+// up (the item is then left unpublished and the caller must leave).
+__device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam &ep, int item, double &dmax)
 {
-    __shared__ int s_next;
     const WaveArgs &a = b.a;
     const PlaneGeom &g = a.pg;
     const int ntiles = a.ntu * a.ntv;
-    const long long total = (long long)a.steps * ntiles;
     const unsigned want = a.epoch << 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double dmax = 0.0;
-    if (tid == 0) {
-        const unsigned w = atomicAdd(a.work, 1u);
-        s_next = (w < total) ? (int)w : -1;
+    const int p = item / ntiles, t = item - p * ntiles;
+    const int tu = t % a.ntu, tv = t / a.ntu;
+    const int tgt = a.first_src - p * a.sg;
+    // Everything but lambda is fixed during the adjoint: find this thread's
+    // cell, its winner's source points and weights, and what it pushed
+    // before, while the items it waits for are still running.
+    const int u = tu * 32 + lane + 1;
+    const int v = tv * kWaveTV + warp + 1;
+    long long x = -1, src[3] = {0, 0, 0};
+    double wt[3] = {0.0, 0.0, 0.0}, P = 0.0;
+    int np = 0;
+    if (u <= g.nu && v <= g.nv) {
+        const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
+        const unsigned w = b.W[xc];
+        if (w != kNoWinner && (int)(w / kEllipCands) == a.dir) {
+            x = xc;
+            P = b.pushed[x];
+            double tv9[9], c[3], n;
+            int pt[3];
+            fan_times(b.T, x, g, tv9);
+            if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF))
+                np = 0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
+        }
+    }
+    int timed_out = 0;
+    if (tid < 9 && p > 0) {
+        const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
+        // step p-1 works on plane tgt + sg; its tiles without work are not
+        // in the queue and never publish (nor push)
+        if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv &&
+            b.has[(long long)(tgt + a.sg) * ntiles + nv * a.ntu + nu]) {
+            const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nv * a.ntu + nu;
+            const unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_acquire(fl) < want) {
+                if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns || *(volatile unsigned *)a.status != 0) {
+                    atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                    timed_out = 1;
+                    break;
+                }
+                if (kPollNs) __nanosleep(kPollNs);
+            }
+        }
+    }
+    if (__syncthreads_or(timed_out)) return false;
+    if (x >= 0) {
+        const double L = __ldcg(b.lam + x);
+        const double D = L - P;
+        if (D != 0.0) {
+            b.pushed[x] = L;
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (q < np) atomicAdd(b.lam + src[q], wt[q] * D);
+            dmax = fmax(dmax, fabs(D));
+        }
+    }
+    // publish: the barrier makes every thread's atomics precede thread 0's
+    // release store, which orders them (cumulatively) before the flag
+    __syncthreads();
+    if (tid == 0) st_release(a.flags + item, want);
+    return true;
+}
+
+// Work map (see AdjTiles): every interior cell with a winner marks its tile
+// in its winner direction's orientation.
+__global__ void __launch_bounds__(256) adj_tiles_kernel(const unsigned char *__restrict__ W, int nx, int ny, int nz,
+                                                        AdjTiles t)
+{
+    const long long sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
+    const long long cells = sz * (nz + 2);
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < cells;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int c[3] = {(int)(x % sy), (int)((x / sy) % (ny + 2)), (int)(x / sz)};
+        if (c[0] < 1 || c[0] > nx || c[1] < 1 || c[1] > ny || c[2] < 1 || c[2] > nz) continue;
+        const unsigned w = W[x];
+        if (w >= 6u * kEllipCands) continue;
+        const int d = (int)(w / kEllipCands);
+        const int nrm = t.nrm[d];
+        const int ub = (nrm == 0) ? 1 : 0, vb = (nrm == 2) ? 1 : 2;
+        const int tile = ((c[vb] - 1) / kWaveTV) * t.ntu[nrm] + ((c[ub] - 1) >> 5);
+        t.has[d][(long long)c[nrm] * t.ntiles[nrm] + tile] = 1;
+    }
+}
+
+// Warp maximum of d into *out (IEEE bits of a non-negative double).
+__device__ __forceinline__ void adj_flush(double d, unsigned long long *out)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0 && d > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(d));
+}
+
+// Backward passes of one direction of one or many instances in one launch.
+// The items are listed in ba.items (instance slot << 40 | item within the
+// instance's pass), tiles with work only, ordered step-major across the
+// instances: every item an item waits for comes earlier in the list.
+__global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads) batch_adj_pass_kernel(BatchAdjArgs ba)
+{
+    __shared__ long long s_next;
+    __shared__ int s_il;
+    __shared__ BatchAdjInst s_inst;
+    if (threadIdx.x == 0) {
+        const unsigned w = atomicAdd(ba.work, 1u);
+        s_next = (w < ba.total) ? (long long)ba.items[w] : -1ll;
+        s_il = -1;
     }
     __syncthreads();
     for (;;) {
-        const int item = s_next;
-        if (item < 0) break;
-        __syncthreads();  // every thread has read s_next
-        if (tid == 0) {  // claim the next item now; it is processed after this one
-            int it = -1;
-            if (*(volatile unsigned *)a.status == 0) {
-                const unsigned w = atomicAdd(a.work, 1u);
-                if (w < total) it = (int)w;
+        const long long e = s_next;
+        if (e < 0) break;
+        const int il = (int)(e >> 40), local = (int)(e & ((1ll << 40) - 1));
+        __syncthreads();  // every thread has read s_next and s_il
+        if (threadIdx.x == 0) {  // claim the next item now; it is processed after this one
+            long long it = -1;
+            if (*(volatile unsigned *)ba.status == 0) {
+                const unsigned w = atomicAdd(ba.work, 1u);
+                if (w < ba.total) it = (long long)ba.items[w];
             }
             s_next = it;
         }
-        const int p = item / ntiles, t = item - p * ntiles;
-        const int tu = t % a.ntu, tv = t / a.ntu;
-        const int tgt = a.first_src - p * a.sg;
-        // Everything but lambda is fixed during the adjoint: find this
-        // thread's cell, its winner's source points and weights, and what it
-        // pushed before, while the items it waits for are still running.
-        const int u = tu * 32 + lane + 1;
-        const int v = tv * kWaveTV + warp + 1;
-        long long x = -1, src[3] = {0, 0, 0};
-        double wt[3] = {0.0, 0.0, 0.0}, P = 0.0;
-        int np = 0;
-        if (u <= g.nu && v <= g.nv) {
-            const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
-            const unsigned w = b.W[xc];
-            if (w != kNoWinner && (int)(w / kEllipCands) == a.dir) {
-                x = xc;
-                P = b.pushed[x];
-                double tv9[9], c[3], n;
-                int pt[3];
-                fan_times(b.T, x, g, tv9);
-                if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF))
-                    np = 0;
-#pragma unroll
-                for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
+        if (il != s_il) {  // consecutive items mostly share their instance
+            const unsigned *src = reinterpret_cast<const unsigned *>(ba.inst + il);
+            unsigned *dst = reinterpret_cast<unsigned *>(&s_inst);
+            for (int w = threadIdx.x; w < (int)(sizeof(BatchAdjInst) / 4); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_inst.b.a.epoch = ba.epoch;  // the pass number is per launch
+                s_il = il;
             }
+            __syncthreads();
         }
-        int timed_out = 0;
-        if (tid < 9 && p > 0) {
-            const int nu = tu + tid % 3 - 1, nv = tv + tid / 3 - 1;
-            if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
-                const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nv * a.ntu + nu;
-                const unsigned long long t0 = global_ns();
-                unsigned spins = 0;
-                while (ld_acquire(fl) < want) {
-                    if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
-                        *(volatile unsigned *)a.status != 0) {
-                        atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
-                        timed_out = 1;
-                        break;
-                    }
-                    if (kPollNs) __nanosleep(kPollNs);
-                }
-            }
-        }
-        if (__syncthreads_or(timed_out)) break;
-        if (x >= 0) {
-            const double L = __ldcg(b.lam + x);
-            const double D = L - P;
-            if (D != 0.0) {
-                b.pushed[x] = L;
-#pragma unroll
-                for (int q = 0; q < 3; ++q)
-                    if (q < np) atomicAdd(b.lam + src[q], wt[q] * D);
-                dmax = fmax(dmax, fabs(D));
-            }
-        }
-        // publish: the barrier makes every thread's atomics precede thread 0's
-        // release store, which orders them (cumulatively) before the flag
-        __syncthreads();
-        if (tid == 0) st_release(a.flags + item, want);
+        double dmax = 0.0;
+        if (!adj_item(s_inst.b, s_inst.ep, local, dmax)) break;
+        adj_flush(dmax, s_inst.b.a.maxd);
     }
+}
+
+// The item list of one backward pass (see batch_adj_pass_kernel), built in
+// two steps over blocks (step p, instance slot q): count the tiles of step p
+// that have work, then (after an exclusive scan of the counts in step-major
+// order, on the host) write their items in tile order.
+constexpr int kListThreads = 256;
+
+__device__ __forceinline__ const unsigned char *step_tiles(const AdjWaveArgs &b, int p)
+{
+    return b.has + (long long)(b.a.first_src - p * b.a.sg) * (b.a.ntu * b.a.ntv);
+}
+
+__global__ void __launch_bounds__(kListThreads) adj_count_kernel(const BatchAdjInst *inst, int k, int *cnt)
+{
+    const int p = blockIdx.x, q = blockIdx.y;
+    const AdjWaveArgs &b = inst[q].b;
+    const int ntiles = b.a.ntu * b.a.ntv;
+    int c = 0;
+    if (p < b.a.steps) {
+        const unsigned char *h = step_tiles(b, p);
+        for (int t0 = 0; t0 < ntiles; t0 += kListThreads) {
+            const int t = t0 + threadIdx.x;
+            c += __syncthreads_count(t < ntiles && h[t]);
+        }
+    }
+    if (threadIdx.x == 0) cnt[(long long)p * k + q] = c;
+}
+
+__global__ void __launch_bounds__(kListThreads) adj_fill_kernel(const BatchAdjInst *inst, int k, const long long *off,
+                                                                unsigned long long *items)
+{
+    __shared__ int wcnt[kListThreads / 32];
+    const int p = blockIdx.x, q = blockIdx.y;
+    const AdjWaveArgs &b = inst[q].b;
+    if (p >= b.a.steps) return;
+    const int ntiles = b.a.ntu * b.a.ntv;
+    const unsigned char *h = step_tiles(b, p);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long long base = off[(long long)p * k + q];
+    for (int t0 = 0; t0 < ntiles; t0 += kListThreads) {
+        const int t = t0 + threadIdx.x;
+        const bool f = t < ntiles && h[t];
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wcnt[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    if (lane == 0 && dmax > 0.0) atomicMax(a.maxd, (unsigned long long)__double_as_longlong(dmax));
+        for (int w = 0; w < kListThreads / 32; ++w) {
+            before += (w < warp) ? wcnt[w] : 0;
+            total += wcnt[w];
+        }
+        if (f)
+            items[base + before + __popc(m & ((1u << lane) - 1u))] =
+                ((unsigned long long)q << 40) | (unsigned long long)((long long)p * ntiles + t);
+        base += total;
+        __syncthreads();
+    }
 }
 
 // dL/dM(x) = lambda(x) d(time(x))/dM(x), six arrays (component-major) in the
 // field layout, accumulated in the order of the CPU statement.  Every cell is
-// written: ghosts and cells without a winner get 0.
+// written (ghosts and cells without a winner get 0), or, with accumulate,
+// added to.
 __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict__ T, const double *__restrict__ lam,
                                                        const unsigned char *__restrict__ W,
                                                        const __grid_constant__ AdjGeom geo, EllipMedium med, int nx,
-                                                       int ny, int nz, double *dLdM)
+                                                       int ny, int nz, double *dLdM, int accumulate)
 {
     const long long sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
     const long long cells = sz * (nz + 2);
@@ -280,28 +395,47 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict_
         }
         const double L = interior ? lam[x] : 0.0;
 #pragma unroll
-        for (int m = 0; m < 6; ++m) dLdM[m * cells + x] = L * dM[m];
+        for (int m = 0; m < 6; ++m) {
+            double *o = dLdM + m * cells + x;
+            *o = accumulate ? *o + L * dM[m] : L * dM[m];
+        }
     }
 }
 
-cudaError_t launch_adj_pass(const AdjWaveArgs &b, const EllipParam &ep, int grid, cudaStream_t s)
+cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
+                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, int accumulate, cudaStream_t s)
 {
-    adj_pass_kernel<<<grid, kAdjThreads, 0, s>>>(b, ep);
+    adj_grad_kernel<<<148 * 8, 256, 0, s>>>(T, lam, W, geo, med, g.nx, g.ny, g.nz, dLdM, accumulate);
     return cudaGetLastError();
 }
 
-int adj_blocks_per_sm()
+cudaError_t launch_adj_tiles(const unsigned char *W, const fold3d_grid &g, const AdjTiles &t, cudaStream_t s)
+{
+    adj_tiles_kernel<<<148 * 8, 256, 0, s>>>(W, g.nx, g.ny, g.nz, t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, int grid, cudaStream_t s)
+{
+    batch_adj_pass_kernel<<<grid, kAdjThreads, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_list(const BatchAdjInst *inst, int k, int max_steps, int *cnt, const long long *off,
+                            unsigned long long *items, cudaStream_t s)
+{
+    const dim3 grid(max_steps, k);
+    if (!off) adj_count_kernel<<<grid, kListThreads, 0, s>>>(inst, k, cnt);
+    else adj_fill_kernel<<<grid, kListThreads, 0, s>>>(inst, k, off, items);
+    return cudaGetLastError();
+}
+
+int batch_adj_blocks_per_sm()
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adj_pass_kernel, kAdjThreads, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_adj_pass_kernel, kAdjThreads, 0) != cudaSuccess)
+        return 1;
     return n > 0 ? n : 1;
-}
-
-cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
-                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s)
-{
-    adj_grad_kernel<<<148 * 8, 256, 0, s>>>(T, lam, W, geo, med, g.nx, g.ny, g.nz, dLdM);
-    return cudaGetLastError();
 }
 
 }  // namespace fold3d

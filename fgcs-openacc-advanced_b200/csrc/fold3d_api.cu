@@ -152,7 +152,7 @@ struct fold3d_ctx {
     unsigned *w_counters = nullptr;          // [0] work, [1] status
     unsigned long long *w_evaluated = nullptr;
     unsigned epoch = 0;                      // passes run so far on this context (never decreases)
-    int sms = 0, wave_bps = 0, wave_bps_ell = 0, batch_bps = 0;
+    int sms = 0, wave_bps = 0, wave_bps_ell = 0, batch_bps = 0, batch_adj_bps = 0;
     // batched solves: per-instance scratch and per-direction staging
     std::vector<int> bkey;                   // dims of the instances the scratch is sized for
     unsigned *b_scratch = nullptr;           // flags and change maps of all instances
@@ -161,7 +161,13 @@ struct fold3d_ctx {
     unsigned *b_counters = nullptr;          // work, status
     double *adj_pushed = nullptr;            // adjoint: lambda already pushed, per cell
     size_t adj_cells = 0;
-    int adj_bps = 0;
+    unsigned char *adj_has = nullptr;        // adjoint work maps (AdjTiles)
+    size_t adj_has_bytes = 0;
+    unsigned long long *adj_items = nullptr; // adjoint item lists, six directions
+    size_t adj_items_cap = 0;
+    int *adj_cnt = nullptr;                  // per (step, slot) counts, then offsets
+    long long *adj_off = nullptr;
+    size_t adj_cnt_cap = 0;
     char *b_stage_d = nullptr, *b_stage_h = nullptr;
     size_t b_stage_bytes = 0;
 };
@@ -238,6 +244,10 @@ void fold3d_destroy(fold3d_ctx *c)
     if (c->b_slots) cudaFree(c->b_slots);
     if (c->b_counters) cudaFree(c->b_counters);
     if (c->adj_pushed) cudaFree(c->adj_pushed);
+    if (c->adj_has) cudaFree(c->adj_has);
+    if (c->adj_items) cudaFree(c->adj_items);
+    if (c->adj_cnt) cudaFree(c->adj_cnt);
+    if (c->adj_off) cudaFree(c->adj_off);
     if (c->b_stage_d) cudaFree(c->b_stage_d);
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
     if (c->d_maxd) cudaFree(c->d_maxd);
@@ -522,14 +532,16 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
 }
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static constexpr size_t kStageInst = sizeof(BatchInst) > sizeof(BatchAdjInst) ? sizeof(BatchInst) : sizeof(BatchAdjInst);
 
-static int batch_scratch(fold3d_ctx *c, int n, const fold3d_instance *in)
+static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
 {
+    const int n = (int)grids.size();
     std::vector<int> key(3 * (size_t)n);
     for (int i = 0; i < n; ++i) {
-        key[3 * i] = in[i].grid.nx;
-        key[3 * i + 1] = in[i].grid.ny;
-        key[3 * i + 2] = in[i].grid.nz;
+        key[3 * i] = grids[i].nx;
+        key[3 * i + 1] = grids[i].ny;
+        key[3 * i + 2] = grids[i].nz;
     }
     if (c->b_scratch && key == c->bkey) return FOLD3D_OK;
     if (c->b_scratch) cudaFree(c->b_scratch);
@@ -545,7 +557,7 @@ static int batch_scratch(fold3d_ctx *c, int n, const fold3d_instance *in)
     c->b_flag_off.assign(n, 0);
     for (int b = 0; b < 3; ++b) c->b_mod_off[b].assign(n, 0);
     for (int i = 0; i < n; ++i) {
-        const fold3d_grid &g = in[i].grid;
+        const fold3d_grid &g = grids[i];
         const int dims[3] = {g.nx, g.ny, g.nz};
         size_t fw = 0;
         for (int b = 0; b < 3; ++b) {
@@ -567,7 +579,7 @@ static int batch_scratch(fold3d_ctx *c, int n, const fold3d_instance *in)
     if (!c->b_counters && (e = cudaMalloc(&c->b_counters, 2 * sizeof(unsigned))) != cudaSuccess)
         return set_error(FOLD3D_ERR_NOMEM, std::string("batch scratch: ") + cudaGetErrorString(e));
     // per direction: inst[n], step_off[max_steps+1], step_k[max_steps], tile_pre[n+1]
-    const size_t per = align_up((size_t)n * sizeof(BatchInst), 256) + align_up((max_steps + 1) * 8, 256) +
+    const size_t per = align_up((size_t)n * kStageInst, 256) + align_up((max_steps + 1) * 8, 256) +
                        align_up((size_t)max_steps * 4, 256) + align_up(((size_t)n + 1) * 8, 256);
     c->b_stage_bytes = per;
     if ((e = cudaMalloc(&c->b_stage_d, 6 * per)) != cudaSuccess ||
@@ -581,13 +593,15 @@ static int batch_scratch(fold3d_ctx *c, int n, const fold3d_instance *in)
         c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
     if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm();
+    if (!c->batch_adj_bps) c->batch_adj_bps = batch_adj_blocks_per_sm();
     c->bkey = key;
     return FOLD3D_OK;
 }
 
 // Staging layout of direction dir: pointers into the host or device copy.
+// The instance table holds BatchInst (forward) or BatchAdjInst (adjoint).
 struct BatchStage {
-    BatchInst *inst;
+    void *inst;
     long long *step_off;
     int *step_k;
     long long *tile_pre;
@@ -598,8 +612,8 @@ static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
     for (size_t i = 0; i < c->bkey.size(); ++i) max_steps = std::max(max_steps, c->bkey[i] - 1);
     char *p = base + (size_t)dir * c->b_stage_bytes;
     BatchStage s;
-    s.inst = reinterpret_cast<BatchInst *>(p);
-    p += align_up((size_t)n * sizeof(BatchInst), 256);
+    s.inst = p;
+    p += align_up((size_t)n * kStageInst, 256);
     s.step_off = reinterpret_cast<long long *>(p);
     p += align_up((max_steps + 1) * 8, 256);
     s.step_k = reinterpret_cast<int *>(p);
@@ -613,7 +627,9 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
     if (rc) return rc;
-    if ((rc = batch_scratch(c, n, in))) return rc;
+    std::vector<fold3d_grid> grids(n);
+    for (int i = 0; i < n; ++i) grids[i] = in[i].grid;
+    if ((rc = batch_scratch(c, grids))) return rc;
     cudaError_t e;
     std::vector<char> active(n, 1);
     std::vector<int> sweeps(n, 0);
@@ -646,7 +662,7 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
             for (int q = 0; q < k; ++q) {
                 const int i = order[q];
                 const fold3d_grid &g = in[i].grid;
-                BatchInst &bi = h.inst[q];
+                BatchInst &bi = static_cast<BatchInst *>(h.inst)[q];
                 memset(&bi, 0, sizeof bi);
                 WaveArgs &a = bi.a;
                 a.pg = make_geom(g, dir);
@@ -670,6 +686,8 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
                 a.status = c->b_counters + 1;
                 a.maxd = c->b_slots + i;
                 a.evaluated = c->b_slots + n + i;
+                a.dir = dir;
+                a.winners = in[i].winners;
                 bi.p = ellip_param(g, in[i].medium, dir);
                 bi.T = in[i].T;
                 h.tile_pre[q + 1] = h.tile_pre[q] + (long long)a.ntu * a.ntv;
@@ -682,7 +700,7 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
                 h.step_off[p + 1] = h.step_off[p] + h.tile_pre[kk];
             }
             if (h.step_off[max_steps] >= (1ll << 31)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
-            args[dir].inst = dv.inst;
+            args[dir].inst = static_cast<const BatchInst *>(dv.inst);
             args[dir].step_off = dv.step_off;
             args[dir].step_k = dv.step_k;
             args[dir].tile_pre = dv.tile_pre;
@@ -752,6 +770,269 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
     return FOLD3D_OK;
 }
 
+// Adjoint scratch (lambda already pushed) for `cells` cells.
+static int adj_scratch(fold3d_ctx *c, size_t cells)
+{
+    if (c->adj_cells >= cells) return FOLD3D_OK;
+    if (c->adj_pushed) cudaFree(c->adj_pushed);
+    c->adj_pushed = nullptr;
+    c->adj_cells = 0;
+    if (cudaMalloc(&c->adj_pushed, cells * sizeof(double)) != cudaSuccess)
+        return set_error(FOLD3D_ERR_NOMEM, "adjoint scratch");
+    c->adj_cells = cells;
+    return FOLD3D_OK;
+}
+
+// Bytes of one grid's adjoint work maps (six directions).
+static size_t adj_tiles_bytes(const fold3d_grid &g)
+{
+    const int n[3] = {g.nx, g.ny, g.nz};
+    size_t bytes = 0;
+    for (int d = 0; d < 6; ++d) {
+        int ntu, ntv;
+        orient_tiles(g, kDirs[d].nrm, ntu, ntv);
+        bytes += (size_t)(n[kDirs[d].nrm] + 2) * ntu * ntv;
+    }
+    return bytes;
+}
+
+// Lays out one grid's work maps at base, clears them and fills them from its
+// winner record.
+static int adj_tiles(const fold3d_grid &g, const unsigned char *W, unsigned char *base, AdjTiles &t, cudaStream_t s)
+{
+    const int n[3] = {g.nx, g.ny, g.nz};
+    for (int b = 0; b < 3; ++b) {
+        int ntv;
+        orient_tiles(g, b, t.ntu[b], ntv);
+        t.ntiles[b] = t.ntu[b] * ntv;
+    }
+    size_t at = 0;
+    for (int d = 0; d < 6; ++d) {
+        t.nrm[d] = kDirs[d].nrm;
+        t.has[d] = base + at;
+        at += (size_t)(n[t.nrm[d]] + 2) * t.ntiles[t.nrm[d]];
+    }
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(base, 0, at, s)) != cudaSuccess ||
+        (e = launch_adj_tiles(W, g, t, s)) != cudaSuccess)
+        return cuda_error(e, "adjoint work map");
+    return FOLD3D_OK;
+}
+
+static int adj_has_scratch(fold3d_ctx *c, size_t bytes)
+{
+    if (c->adj_has_bytes >= bytes) return FOLD3D_OK;
+    if (c->adj_has) cudaFree(c->adj_has);
+    c->adj_has = nullptr;
+    c->adj_has_bytes = 0;
+    if (cudaMalloc(&c->adj_has, bytes) != cudaSuccess) return set_error(FOLD3D_ERR_NOMEM, "adjoint work maps");
+    c->adj_has_bytes = bytes;
+    return FOLD3D_OK;
+}
+
+static int adj_list_scratch(fold3d_ctx *c, size_t items, size_t counts)
+{
+    if (c->adj_items_cap < items) {
+        if (c->adj_items) cudaFree(c->adj_items);
+        c->adj_items = nullptr;
+        c->adj_items_cap = 0;
+        if (cudaMalloc(&c->adj_items, items * 8) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "adjoint item lists");
+        c->adj_items_cap = items;
+    }
+    if (c->adj_cnt_cap < counts) {
+        if (c->adj_cnt) cudaFree(c->adj_cnt);
+        if (c->adj_off) cudaFree(c->adj_off);
+        c->adj_cnt = nullptr;
+        c->adj_off = nullptr;
+        c->adj_cnt_cap = 0;
+        if (cudaMalloc(&c->adj_cnt, counts * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&c->adj_off, counts * sizeof(long long)) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "adjoint item lists");
+        c->adj_cnt_cap = counts;
+    }
+    return FOLD3D_OK;
+}
+
+static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,
+                         int accumulate, cudaStream_t s, fold3d_report *reps)
+{
+    int rc = reserve_passes(c, 6u * (unsigned)std::min(max_sweeps, 1 << 20) + 12u);
+    if (rc) return rc;
+    std::vector<fold3d_grid> grids(n);
+    for (int i = 0; i < n; ++i) grids[i] = in[i].grid;
+    if ((rc = batch_scratch(c, grids))) return rc;
+    std::vector<size_t> off(n + 1, 0);
+    for (int i = 0; i < n; ++i) off[i + 1] = off[i] + field_cells(in[i].grid);
+    if ((rc = adj_scratch(c, off[n]))) return rc;
+    std::vector<size_t> hoff(n + 1, 0);
+    for (int i = 0; i < n; ++i) hoff[i + 1] = hoff[i] + adj_tiles_bytes(in[i].grid);
+    if ((rc = adj_has_scratch(c, hoff[n]))) return rc;
+    std::vector<AdjTiles> tiles(n);
+    for (int i = 0; i < n; ++i)
+        if ((rc = adj_tiles(in[i].grid, in[i].winners, c->adj_has + hoff[i], tiles[i], s))) return rc;
+    // item lists: direction dir's at item_off[dir], at most every (step, tile) of every instance
+    size_t item_off[7] = {0};
+    for (int dir = 0; dir < 6; ++dir) {
+        size_t cap = 0;
+        for (int i = 0; i < n; ++i) {
+            const int dims[3] = {in[i].grid.nx, in[i].grid.ny, in[i].grid.nz};
+            int ntu, ntv;
+            orient_tiles(in[i].grid, kDirs[dir].nrm, ntu, ntv);
+            cap += (size_t)(dims[kDirs[dir].nrm] - 1) * ntu * ntv;
+        }
+        item_off[dir + 1] = item_off[dir] + cap;
+    }
+    cudaError_t e;
+    for (int i = 0; i < n; ++i)
+        if ((e = cudaMemcpyAsync(in[i].lambda, in[i].dLdT, field_cells(in[i].grid) * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+            return cuda_error(e, "adjoint setup");
+    if ((e = cudaMemsetAsync(c->adj_pushed, 0, off[n] * sizeof(double), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess)
+        return cuda_error(e, "adjoint setup");
+    std::vector<char> active(n, 1);
+    std::vector<int> sweeps(n, 0);
+    std::vector<double> delta(n, 0.0), first(n, 0.0);
+    std::vector<unsigned long long> slots(n);
+    int max_steps = 0;
+    for (int v : c->bkey) max_steps = std::max(max_steps, v - 1);
+    if ((rc = adj_list_scratch(c, item_off[6], (size_t)max_steps * n + 1))) return rc;
+    std::vector<int> cnt((size_t)max_steps * n);
+    std::vector<long long> offs((size_t)max_steps * n + 1);
+    BatchAdjArgs args[6];
+    int slots_k[6] = {0, 0, 0, 0, 0, 0};
+    auto stage = [&]() -> int {
+        for (int dir = 0; dir < 6; ++dir) {
+            const DirSpec &d = kDirs[dir];
+            BatchStage h = batch_stage(c, c->b_stage_h, dir, n);
+            BatchStage dv = batch_stage(c, c->b_stage_d, dir, n);
+            std::vector<int> order;  // the active instances (the item lists order steps across them)
+            for (int i = 0; i < n; ++i)
+                if (active[i]) order.push_back(i);
+            const int k = (int)order.size();
+            for (int q = 0; q < k; ++q) {
+                const int i = order[q];
+                const fold3d_grid &g = in[i].grid;
+                BatchAdjInst &bi = static_cast<BatchAdjInst *>(h.inst)[q];
+                memset(&bi, 0, sizeof bi);
+                WaveArgs &a = bi.b.a;
+                a.pg = make_geom(g, dir);
+                a.nrm = d.nrm;
+                a.sg = d.sg;
+                orient_tiles(g, d.nrm, a.ntu, a.ntv);
+                a.steps = pass_count(a.pg);
+                a.first_src = pass_first(a.pg, dir) + d.sg * pass_count(a.pg);  // the forward pass's last target
+                a.timeout_ns = 4000000000ull;
+                a.flags = c->b_scratch + c->b_flag_off[i];
+                a.work = c->b_counters;
+                a.status = c->b_counters + 1;
+                a.maxd = c->b_slots + i;
+                a.dir = dir;
+                bi.b.T = in[i].T;
+                bi.b.lam = in[i].lambda;
+                bi.b.pushed = c->adj_pushed + off[i];
+                bi.b.W = in[i].winners;
+                bi.b.has = tiles[i].has[dir];
+                bi.ep = ellip_param(g, in[i].medium, dir);
+            }
+            args[dir].inst = static_cast<const BatchAdjInst *>(dv.inst);
+            args[dir].items = c->adj_items + item_off[dir];
+            args[dir].total = 0;
+            args[dir].work = c->b_counters;
+            args[dir].status = c->b_counters + 1;
+            slots_k[dir] = k;
+        }
+        cudaError_t ce = cudaMemcpyAsync(c->b_stage_d, c->b_stage_h, 6 * c->b_stage_bytes, cudaMemcpyHostToDevice, s);
+        if (ce != cudaSuccess) return cuda_error(ce, "batch staging upload");
+        // the six item lists: counts, exclusive scan (step-major, slot-minor), fill
+        for (int dir = 0; dir < 6; ++dir) {
+            const int k = slots_k[dir];
+            if (k == 0) continue;
+            if ((ce = launch_adj_list(args[dir].inst, k, max_steps, c->adj_cnt, nullptr, nullptr, s)) != cudaSuccess ||
+                (ce = cudaMemcpyAsync(cnt.data(), c->adj_cnt, (size_t)max_steps * k * sizeof(int),
+                                      cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (ce = cudaStreamSynchronize(s)) != cudaSuccess)
+                return cuda_error(ce, "adjoint item counts");
+            offs[0] = 0;
+            for (size_t q = 0; q < (size_t)max_steps * k; ++q) offs[q + 1] = offs[q] + cnt[q];
+            if (offs[(size_t)max_steps * k] >= (1ll << 32)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
+            args[dir].total = (unsigned)offs[(size_t)max_steps * k];
+            if ((ce = cudaMemcpyAsync(c->adj_off, offs.data(), ((size_t)max_steps * k + 1) * sizeof(long long),
+                                      cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+                (ce = launch_adj_list(args[dir].inst, k, max_steps, nullptr, c->adj_off,
+                                      const_cast<unsigned long long *>(args[dir].items), s)) != cudaSuccess ||
+                (ce = cudaStreamSynchronize(s)) != cudaSuccess)  // offs is reused by the next direction
+                return cuda_error(ce, "adjoint item lists");
+        }
+        return FOLD3D_OK;
+    };
+    if ((rc = stage())) return rc;
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    int sweep = 0, left = n;
+    unsigned hstat[2] = {0, 0};
+    while (sweep < max_sweeps && left > 0) {
+        if ((e = cudaMemsetAsync(c->b_slots, 0, (size_t)n * 8, s)) != cudaSuccess) return cuda_error(e, "memset");
+        for (int dir = 5; dir >= 0; --dir) {  // the forward order reversed
+            args[dir].epoch = ++c->epoch;
+            const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_adj_bps);
+            if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
+                return cuda_error(e, "memset");
+            if (grid > 0 && (e = launch_batch_adj_pass(args[dir], grid, s)) != cudaSuccess)
+                return cuda_error(e, "batched adjoint pass");
+        }
+        ++sweep;
+        if ((e = cudaMemcpyAsync(slots.data(), c->b_slots, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(hstat, c->b_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_error(e, "batched adjoint sweep");
+        if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "batched adjoint: a dependency wait gave up");
+        bool changed = false;
+        for (int i = 0; i < n; ++i) {
+            if (!active[i]) continue;
+            ++sweeps[i];
+            memcpy(&delta[i], &slots[i], 8);
+            if (sweeps[i] == 1) first[i] = delta[i];
+            if (delta[i] <= tol * first[i]) {
+                active[i] = 0;
+                --left;
+                changed = true;
+            }
+        }
+        if (changed && left > 0 && (rc = stage())) return rc;
+    }
+    for (int i = 0; i < n; ++i) {
+        AdjGeom geo;
+        memset(&geo, 0, sizeof geo);
+        for (int d = 0; d < 6; ++d) {
+            geo.pg[d] = make_geom(in[i].grid, d);
+            geo.d[d] = ellip_param(in[i].grid, in[i].medium, d).dir;
+        }
+        EllipMedium med;
+        const float *arr[6] = {in[i].medium.mxx, in[i].medium.mxy, in[i].medium.mxz,
+                               in[i].medium.myy, in[i].medium.myz, in[i].medium.mzz};
+        for (int k = 0; k < 6; ++k) med.m[k] = arr[k];
+        if ((e = launch_adj_grad(in[i].T, in[i].lambda, in[i].winners, geo, med, in[i].grid, in[i].dLdM, accumulate,
+                                 s)) != cudaSuccess)
+            return cuda_error(e, "gradient");
+    }
+    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_error(e, "batched adjoint");
+    if (reps) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        for (int i = 0; i < n; ++i) {
+            reps[i].sweeps = sweeps[i];
+            reps[i].max_delta = delta[i];
+            reps[i].elapsed_ms = ms;
+            reps[i].nominal_updates = nominal_per_sweep(in[i].grid) * (uint64_t)sweeps[i];
+            reps[i].evaluated_updates = 0;
+            reps[i].engine = FOLD3D_ENGINE_WAVEFRONT;
+        }
+    }
+    return FOLD3D_OK;
+}
+
 extern "C" {
 
 int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts *o, void *stream,
@@ -773,7 +1054,33 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
         return set_error(FOLD3D_ERR_UNSUPPORTED, "batched solves run on the wavefront engine, variant 0");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    for (int i = 0; i < n; ++i)
+        if (in[i].winners) {
+            cudaError_t e = cudaMemsetAsync(in[i].winners, 0xff, field_cells(in[i].grid), s);
+            if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
+        }
     return solve_batch(c, n, in, *o, s, reps);
+}
+
+int fold3d_adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,
+                         int accumulate, void *stream, fold3d_report *reps)
+{
+    clear_error();
+    if (!c || !in) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (n < 1) return set_error(FOLD3D_ERR_INVALID, "n must be >= 1");
+    if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    for (int i = 0; i < n; ++i) {
+        int rc = check_grid(&in[i].grid);
+        if (rc) return rc;
+        const fold3d_ellip &m = in[i].medium;
+        if (!in[i].T || !in[i].winners || !in[i].dLdT || !in[i].lambda || !in[i].dLdM || !m.mxx || !m.mxy ||
+            !m.mxz || !m.myy || !m.myz || !m.mzz)
+            return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
+    }
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return adjoint_batch(c, n, in, max_sweeps, tol, accumulate, s, reps);
 }
 
 int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
@@ -924,99 +1231,17 @@ int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip
                          double tol, void *stream, fold3d_report *rep)
 {
     clear_error();
-    if (!c || !m || !T || !W || !dLdT || !lam || !dLdM) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (!c || !g || !m || !T || !W || !dLdT || !lam || !dLdM) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
     int rc = check_grid(g);
     if (rc) return rc;
     if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
     if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (!m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
+        return set_error(FOLD3D_ERR_INVALID, "NULL metric array");
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    const size_t cells = field_cells(*g);
-    cudaError_t e;
-    if (c->adj_cells < cells) {
-        if (c->adj_pushed) cudaFree(c->adj_pushed);
-        c->adj_pushed = nullptr;
-        c->adj_cells = 0;
-        if ((e = cudaMalloc(&c->adj_pushed, cells * sizeof(double))) != cudaSuccess)
-            return set_error(FOLD3D_ERR_NOMEM, "adjoint scratch");
-        c->adj_cells = cells;
-    }
-    if ((e = cudaMemcpyAsync(lam, dLdT, cells * sizeof(double), cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
-        (e = cudaMemsetAsync(c->adj_pushed, 0, cells * sizeof(double), s)) != cudaSuccess)
-        return cuda_error(e, "adjoint setup");
-    if ((rc = reserve_passes(c, 6u * (unsigned)std::min(max_sweeps, 1 << 20) + 12u))) return rc;
-    if ((rc = wave_scratch(c, *g))) return rc;
-    if (!c->adj_bps) c->adj_bps = adj_blocks_per_sm();
-    AdjGeom geo;
-    memset(&geo, 0, sizeof geo);
-    EllipParam ep[6];
-    for (int d = 0; d < 6; ++d) {
-        geo.pg[d] = make_geom(*g, d);
-        ep[d] = ellip_param(*g, *m, d);
-        geo.d[d] = ep[d].dir;
-    }
-    AdjWaveArgs b;
-    memset(&b, 0, sizeof b);
-    b.T = T;
-    b.lam = lam;
-    b.pushed = c->adj_pushed;
-    b.W = W;
-    b.a.flags = c->w_flags;
-    b.a.work = c->w_counters;
-    b.a.status = c->w_counters + 1;
-    b.a.maxd = c->d_maxd;
-    b.a.timeout_ns = 4000000000ull;
-    if ((e = cudaMemsetAsync(c->w_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess)
-        return cuda_error(e, "cudaMemsetAsync");
-    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
-    int sweeps = 0;
-    double delta = 0.0, first = 0.0;
-    unsigned hstat[2] = {0, 0};
-    while (sweeps < max_sweeps) {
-        if ((e = cudaMemsetAsync(c->d_maxd, 0, 8, s)) != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
-        for (int d = 5; d >= 0; --d) {  // the forward order reversed
-            const DirSpec &ds = kDirs[d];
-            b.a.pg = geo.pg[d];
-            b.a.nrm = ds.nrm;
-            b.a.sg = ds.sg;
-            orient_tiles(*g, ds.nrm, b.a.ntu, b.a.ntv);
-            b.a.steps = pass_count(b.a.pg);
-            b.a.first_src = pass_first(b.a.pg, d) + ds.sg * pass_count(b.a.pg);  // the forward pass's last target
-            b.a.epoch = ++c->epoch;
-            b.a.dir = d;
-            const long long items = (long long)b.a.steps * b.a.ntu * b.a.ntv;
-            const int grid = (int)std::min<long long>(items, (long long)c->sms * c->adj_bps);
-            if ((e = cudaMemsetAsync(b.a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
-                return cuda_error(e, "cudaMemsetAsync");
-            if ((e = launch_adj_pass(b, ep[d], grid, s)) != cudaSuccess) return cuda_error(e, "adjoint pass");
-        }
-        ++sweeps;
-        if ((e = cudaMemcpyAsync(c->h_maxd, c->d_maxd, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(hstat, c->w_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-            (e = cudaStreamSynchronize(s)) != cudaSuccess)
-            return cuda_error(e, "adjoint sweep");
-        if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "adjoint: a dependency wait gave up");
-        memcpy(&delta, c->h_maxd, 8);
-        if (sweeps == 1) first = delta;
-        if (delta <= tol * first) break;
-    }
-    EllipMedium med;
-    const float *arr[6] = {m->mxx, m->mxy, m->mxz, m->myy, m->myz, m->mzz};
-    for (int k = 0; k < 6; ++k) med.m[k] = arr[k];
-    if ((e = launch_adj_grad(T, lam, W, geo, med, *g, dLdM, s)) != cudaSuccess) return cuda_error(e, "gradient");
-    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
-        return cuda_error(e, "adjoint");
-    if (rep) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        rep->sweeps = sweeps;
-        rep->max_delta = delta;
-        rep->elapsed_ms = ms;
-        rep->nominal_updates = nominal_per_sweep(*g) * (uint64_t)sweeps;
-        rep->evaluated_updates = 0;
-        rep->engine = FOLD3D_ENGINE_PLANES;
-    }
-    return FOLD3D_OK;
+    const fold3d_adjoint_instance one = {*g, *m, T, W, dLdT, lam, dLdM};
+    return adjoint_batch(c, 1, &one, max_sweeps, tol, 0, s, rep);
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,

@@ -148,11 +148,43 @@ struct AdjWaveArgs {
     const double *T;
     double *lam, *pushed;
     const unsigned char *W;
+    const unsigned char *has;  // [plane][tile] of this pass's orientation: 1 if a cell's winner is a.dir
 };
-cudaError_t launch_adj_pass(const AdjWaveArgs &b, const EllipParam &ep, int grid, cudaStream_t s);
-int adj_blocks_per_sm();
+
+// Work map of the adjoint: per direction d, one byte per (plane, tile) of d's
+// orientation, 1 when a cell of the tile has its winner in direction d (set
+// to 0 before launch_adj_tiles).  Backward items of tiles marked 0 push
+// nothing, so they publish at once, without waiting.
+struct AdjTiles {
+    unsigned char *has[6];
+    int nrm[6];              // normal axis of each direction
+    int ntu[3], ntiles[3];   // tiles per orientation
+};
+cudaError_t launch_adj_tiles(const unsigned char *W, const fold3d_grid &g, const AdjTiles &t, cudaStream_t s);
+
+// Batched backward passes: one instance's pass arguments and medium; the
+// item tables are laid out as for BatchArgs.
+struct BatchAdjInst {
+    AdjWaveArgs b;
+    EllipParam ep;
+};
+static_assert(sizeof(BatchAdjInst) % 4 == 0, "BatchAdjInst is copied in words");
+struct BatchAdjArgs {
+    const BatchAdjInst *inst;
+    const unsigned long long *items;  // slot << 40 | item, tiles with work only, step-major
+    unsigned total;                   // items in the list
+    unsigned *work, *status;
+    unsigned epoch;
+};
+cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, int grid, cudaStream_t s);
+// Item list of a backward pass over k instance slots: with off == NULL,
+// cnt[p * k + q] <- tiles with work at step p of slot q; else items[] <- the
+// list, off[p * k + q] being the exclusive prefix of cnt in that order.
+cudaError_t launch_adj_list(const BatchAdjInst *inst, int k, int max_steps, int *cnt, const long long *off,
+                            unsigned long long *items, cudaStream_t s);
+int batch_adj_blocks_per_sm();
 cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
-                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, cudaStream_t s);
+                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, int accumulate, cudaStream_t s);
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,

@@ -251,22 +251,7 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads) batch_pass_
                 if (w < b.total) it = (int)w;
             }
             s_next = it;
-            // step p: last step start <= gitem; instance: last tile prefix <= rest
-            int lo = 0, hi = b.max_steps;  // step_off[lo] <= gitem < step_off[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (b.step_off[mid] <= gitem) lo = mid; else hi = mid;
-            }
-            const int p = lo;
-            const long long r = gitem - b.step_off[p];
-            int il = 0, ih = b.step_k[p];
-            while (ih - il > 1) {
-                const int mid = (il + ih) >> 1;
-                if (b.tile_pre[mid] <= r) il = mid; else ih = mid;
-            }
-            const BatchInst &bi = b.inst[il];
-            s_loc[0] = il;
-            s_loc[1] = p * (bi.a.ntu * bi.a.ntv) + (int)(r - b.tile_pre[il]);
+            batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, gitem, s_loc[0], s_loc[1]);
         }
         __syncthreads();
         {

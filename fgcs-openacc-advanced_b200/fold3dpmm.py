@@ -36,6 +36,7 @@ EXPORTED = (
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
     "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
+    "fold3d_adjoint_batch",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
@@ -64,7 +65,12 @@ class Ellip(C.Structure):
 
 
 class Instance(C.Structure):
-    _fields_ = [("grid", Grid), ("medium", Ellip), ("T", C.c_void_p)]
+    _fields_ = [("grid", Grid), ("medium", Ellip), ("T", C.c_void_p), ("winners", C.c_void_p)]
+
+
+class AdjInstance(C.Structure):
+    _fields_ = [("grid", Grid), ("medium", Ellip), ("T", C.c_void_p), ("winners", C.c_void_p),
+                ("dLdT", C.c_void_p), ("lambda_", C.c_void_p), ("dLdM", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -117,6 +123,7 @@ def lib() -> C.CDLL:
     L.fold3d_ellip_metric.argtypes = [d, d, d, d, d, C.POINTER(C.c_float)]
     L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
+    L.fold3d_adjoint_batch.argtypes = [vp, i, P(AdjInstance), i, d, i, vp, P(Report)]
     L.fold3d_solve_ellip_record.argtypes = [vp, P(Grid), P(Ellip), vp, vp, P(Opts), vp, P(Report)]
     L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
@@ -345,10 +352,11 @@ def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, 
     return rep
 
 
-def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream=None) -> list:
+def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream=None, winners=None) -> list:
     """fold3d_solve_batch: fields[i] (float64 CUDA tensors, in place), hs[i]
-    spacings, media[i] six float32 CUDA metric tensors.  Returns the
-    per-instance reports."""
+    spacings, media[i] six float32 CUDA metric tensors, winners[i] (optional)
+    uint8 winner records shaped like fields[i].  Returns the per-instance
+    reports."""
     n = len(fields)
     arr = (Instance * n)()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
@@ -356,9 +364,39 @@ def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream
         arr[i].grid = grid(nx, ny, nz, h)
         arr[i].medium = ellip(M)
         arr[i].T = _dev_ptr(T)
+        if winners is not None and winners[i] is not None:
+            _check_like("winners[%d]" % i, winners[i], T, 1)
+            arr[i].winners = winners[i].data_ptr()
     reps = (Report * n)()
     _check(lib().fold3d_solve_batch(ctx._h, n, arr, C.byref(o or opts()), C.c_void_p(stream) if stream else None,
                                     reps))
+    return list(reps)
+
+
+def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, max_sweeps=1000, tol=0.0,
+                  accumulate=False, stream=None) -> list:
+    """fold3d_adjoint_batch: per instance i the arguments of adjoint_ellip
+    (fields[i] converged, winners[i] its record, dLdT[i], lam[i], dLdM[i]).
+    accumulate: dLdM[i] += the gradient (instances may share one dLdM).
+    Returns the per-instance reports."""
+    n = len(fields)
+    arr = (AdjInstance * n)()
+    for i, (T, h, M) in enumerate(zip(fields, hs, media)):
+        _check_like("winners[%d]" % i, winners[i], T, 1)
+        _check_like("dLdT[%d]" % i, dLdT[i], T, 8)
+        _check_like("lam[%d]" % i, lam[i], T, 8)
+        _check_like("dLdM[%d]" % i, dLdM[i], T, 8, lead=(6,))
+        nx, ny, nz = grid_of(T)
+        arr[i].grid = grid(nx, ny, nz, h)
+        arr[i].medium = ellip(M)
+        arr[i].T = _dev_ptr(T)
+        arr[i].winners = winners[i].data_ptr()
+        arr[i].dLdT = _dev_ptr(dLdT[i])
+        arr[i].lambda_ = _dev_ptr(lam[i])
+        arr[i].dLdM = dLdM[i].data_ptr()
+    reps = (Report * n)()
+    _check(lib().fold3d_adjoint_batch(ctx._h, n, arr, int(max_sweeps), float(tol), int(bool(accumulate)),
+                                      C.c_void_p(stream) if stream else None, reps))
     return list(reps)
 
 

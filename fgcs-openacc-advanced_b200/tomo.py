@@ -23,8 +23,9 @@ _reports = None
 
 
 def collect_reports(lst):
-    """Append ("forward" | "adjoint", fold3d_report) of every later library
-    call to lst (None stops collecting)."""
+    """Append (kind, fold3d_report) of every later library call to lst, kind
+    "forward" | "adjoint" | "forward_batch" | "adjoint_batch" (one report per
+    instance of a batch); None stops collecting."""
     global _reports
     _reports = lst
 
@@ -68,3 +69,45 @@ class EllipSolve(torch.autograd.Function):
 
 def solve(T0, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):
     return EllipSolve.apply(T0, h, max_sweeps, tol, adj_tol, *M)
+
+
+class EllipSolveBatch(torch.autograd.Function):
+    """Many sources in one medium: T0s (S, nz+2, ny+2, nx+2) initial fields,
+    one per source.  The forward solves all S at once (fold3d_solve_batch
+    with winner records), the backward runs their adjoints at once
+    (fold3d_adjoint_batch) and sums the S gradients into one dL/dM."""
+
+    @staticmethod
+    def forward(ctx, T0s, h, max_sweeps, tol, adj_tol, *M):
+        M32 = [m.detach().to(torch.float32).contiguous() for m in M]
+        T = T0s.detach().clone().contiguous()
+        W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
+        S = T.shape[0]
+        reps = f3d.solve_batch(context(), [T[s] for s in range(S)], [h] * S, [M32] * S,
+                               f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol),
+                               winners=[W[s] for s in range(S)])
+        for r in reps:
+            _note("forward_batch", r)
+        ctx.save_for_backward(T, W, *M32)
+        ctx.h = h
+        ctx.adj_tol = adj_tol
+        return T
+
+    @staticmethod
+    def backward(ctx, gT):
+        T, W, *M32 = ctx.saved_tensors
+        S = T.shape[0]
+        gT = gT.contiguous()
+        lam = torch.empty_like(T)
+        dLdM = torch.zeros((6,) + tuple(T.shape[1:]), dtype=torch.float64, device=T.device)
+        reps = f3d.adjoint_batch(context(), [T[s] for s in range(S)], [ctx.h] * S, [M32] * S,
+                                 [W[s] for s in range(S)], [gT[s] for s in range(S)], [lam[s] for s in range(S)],
+                                 [dLdM] * S, tol=ctx.adj_tol, accumulate=True)
+        for r in reps:
+            _note("adjoint_batch", r)
+        return (None, None, None, None, None) + tuple(dLdM[m] for m in range(6))
+
+
+def solve_batch(T0s, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):
+    """Fields of all sources (S, ...) in medium M, differentiable in M."""
+    return EllipSolveBatch.apply(T0s, h, max_sweeps, tol, adj_tol, *M)

@@ -200,11 +200,13 @@ int fold3d_adjoint_ellip(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ell
                          double *dLdM_dev, int max_sweeps, double tol, void *stream, fold3d_report *rep);
 
 /* One instance of a batched solve: its grid, elliptical medium and device
- * field (in/out). */
+ * field (in/out).  winners: NULL, or a device winner record of one byte per
+ * field cell, filled as by fold3d_solve_ellip_record. */
 typedef struct {
     fold3d_grid grid;
     fold3d_ellip medium;
     double *T;
+    unsigned char *winners;
 } fold3d_instance;
 
 /* Solves n independent instances (grids of any sizes, elliptical media) at
@@ -216,6 +218,28 @@ typedef struct {
  * fold3d_solve_ellip.  reps: n reports, or NULL. */
 int fold3d_solve_batch(fold3d_ctx *ctx, int n, const fold3d_instance *inst, const fold3d_opts *o,
                        void *stream, fold3d_report *reps);
+
+/* One instance of a batched adjoint: the arguments of fold3d_adjoint_ellip
+ * (device pointers, field layout; dLdM: six arrays, component-major). */
+typedef struct {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    const double *T;
+    const unsigned char *winners;
+    const double *dLdT;
+    double *lambda;
+    double *dLdM;
+} fold3d_adjoint_instance;
+
+/* The adjoints of n converged elliptical solves at once (no counterpart in
+ * the reference): every backward pass of all instances still running is one
+ * launch.  Each instance stops as fold3d_adjoint_ellip would with the same
+ * max_sweeps and tol.  accumulate = 0: dLdM is written as by
+ * fold3d_adjoint_ellip; accumulate != 0: dLdM += the instance's gradient, so
+ * instances of one grid may share one dLdM (the sum over sources of a
+ * tomography loss).  reps: n reports, or NULL. */
+int fold3d_adjoint_batch(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance *inst, int max_sweeps, double tol,
+                         int accumulate, void *stream, fold3d_report *reps);
 
 /* Implicit-surface source initialisation of a host field (the reference's
  * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).

@@ -187,7 +187,7 @@ def ref_lib_path(n: int, omp: bool = False) -> str:
 
 
 # Sizes the tests and the CPU-baseline legs use.
-DEFAULT_REF_SIZES = (8, 16, 32, 64, 128, 512)
+DEFAULT_REF_SIZES = (8, 16, 32, 64, 128, 512, 1280)
 
 
 def build_all(sizes=DEFAULT_REF_SIZES) -> None:
