@@ -53,6 +53,13 @@ double surface(double x, double y, double z)
            (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
 }
 
+// surface() with sin(x) and cos(y + x) given (the same values, computed once
+// per node column and row of the grid).
+inline double surface_tab(double x, double y, double z, double sin_x, double cos_yx)
+{
+    return 5.0 + (sin_x + cos_yx + std::sin(x + y + z)) * 0.4 - z + (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
+}
+
 // Node updates of one seeding point (updateVoxel, Fold3dPMM.c:62-110, in
 // order): position shift in multiples of the spacing (+1, -1 or -2), then the
 // node offset.  Two rows keep the reference's position/index mismatch
@@ -139,6 +146,23 @@ struct Seeder {
         const double f = IF[id], fx = IF[id + 1], fy = IF[id + sy], fz = IF[id + sz];
         const double fxy = IF[id + 1 + sy], fzx = IF[id + 1 + sz], fzy = IF[id + sy + sz];
         const double fxyz = IF[id + 1 + sy + sz];
+        // Skip voxels no edge of which can report a crossing.  An edge (a, b)
+        // reports one when p = h*a/(a-b) lands in [0, h].  For a and b of the
+        // same strict sign that needs a - b to round to a (one value below
+        // ~2^-52 of the other); with every corner of one sign and within a
+        // factor 2^40 of every other, each p lies strictly outside [0, h].
+        {
+            const double c[8] = {f, fx, fy, fz, fxy, fzx, fzy, fxyz};
+            bool pos = true, neg = true;
+            double lo = std::fabs(f), hi = lo;
+            for (int q = 0; q < 8; ++q) {
+                pos = pos && c[q] > 0.0;
+                neg = neg && c[q] < 0.0;
+                lo = std::min(lo, std::fabs(c[q]));
+                hi = std::max(hi, std::fabs(c[q]));
+            }
+            if ((pos || neg) && lo > hi * 0x1p-40) return;
+        }
         const double hx = h[0], hy = h[1], hz = h[2];
         double P[12][3];
         int np = 0;
@@ -245,19 +269,34 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
     const int nth = host_threads();
     const double hx = g->dx, hy = g->dy, hz = g->dz;
     // :137-147, node coordinates from x/y/z (:115-126)
+    std::vector<double> sin_x, cos_yx;
+    try {
+        sin_x.resize(nx + 2);
+        cos_yx.resize((size_t)sy * (ny + 2));
+    } catch (...) {
+        return FOLD3D_ERR_NOMEM;
+    }
+    for (int i = 0; i < nx + 2; ++i) sin_x[i] = std::sin((i - 1) * hx + 0.);
+    parallel_for(0, ny + 2, nth, [&](int j) {
+        const double y = (j - 1) * hy + 0.;
+        for (int i = 0; i < nx + 2; ++i) cos_yx[(size_t)j * sy + i] = std::cos(y + ((i - 1) * hx + 0.));
+    });
     parallel_for(0, nz + 2, nth, [&](int k) {
         const double z = (k - 1) * hz + 0.;
         for (int j = 0; j < ny + 2; ++j) {
             const double y = (j - 1) * hy + 0.;
             for (int i = 0; i < nx + 2; ++i) {
                 const long long id = i + sy * j + sz * k;
-                IF[id] = surface((i - 1) * hx + 0., y, z);
+                IF[id] = surface_tab((i - 1) * hx + 0., y, z, sin_x[i], cos_yx[(size_t)j * sy + i]);
                 T[id] = (side(IF[id]) * 1.0) * kMaxT;
             }
         }
     });
     Seeder s{T, sy, sz, m->F, {m->ax, m->ay, m->az}, {hx, hy, hz}};
-    // Voxels i = 1..nx-1 in slabs of >= 4, even slabs then odd slabs.
+    // Voxels i = 1..nx-1 in slabs of >= 4 (the surface crosses every slab,
+    // which balances the threads), even slabs then odd slabs: a voxel
+    // min-updates nodes within 2 cells of it, so slabs of one phase never
+    // touch the same node, and min-updates commute.  x innermost.
     const int nvox = nx - 1;
     int width = std::max(4, (nvox + 2 * nth - 1) / (2 * nth));
     const int nslabs = (nvox + width - 1) / width;
@@ -266,9 +305,9 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
         parallel_for(0, count, nth, [&](int q) {
             const int slab = 2 * q + phase;
             const int i0 = 1 + slab * width, i1 = std::min(nx - 1, i0 + width - 1);
-            for (int i = i0; i <= i1; ++i)
+            for (int k = 1; k < nz; ++k)
                 for (int j = 1; j < ny; ++j)
-                    for (int k = 1; k < nz; ++k) s.seed_voxel(IF.data(), i, j, k);
+                    for (int i = i0; i <= i1; ++i) s.seed_voxel(IF.data(), i, j, k);
         });
     }
     return FOLD3D_OK;
