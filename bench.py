@@ -675,6 +675,15 @@ def main():
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
 
+    # the same initial field built on the device (fold3d_init_implicit_device)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f3d.init_implicit_device(ctx, T_dev, h, stream=sp)
+    torch.cuda.synchronize()
+    init_dev_s = time.perf_counter() - t0
+    if not torch.equal(T_dev.view(torch.int64), T0_dev.view(torch.int64)):
+        raise RuntimeError("device initialiser differs from the host initialiser")
+
     def step():
         T_dev.copy_(T0_dev)
         return ctx.solve(T_dev, h, None, opts, stream=sp)
@@ -782,7 +791,7 @@ def main():
         "config": workload_config(args) | {"engine": engine_ran},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
         "clocks": clocks, "solve_ms": solve_ms, "evaluated_updates_per_step": evaluated / args.steps,
-        "init_s": init_s, "host_threads": host_threads(),
+        "init_s": init_s, "init_device_s": init_dev_s, "host_threads": host_threads(),
     }
     if rank == 0:
         print(json.dumps(out))

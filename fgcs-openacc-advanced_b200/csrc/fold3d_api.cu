@@ -165,6 +165,10 @@ struct fold3d_ctx {
     size_t adj_has_bytes = 0;
     unsigned long long *adj_items = nullptr; // adjoint item lists, six directions
     size_t adj_items_cap = 0;
+    double *i_if = nullptr;                  // device initialiser: the surface on the device
+    size_t i_if_cells = 0;
+    double *i_stage[2] = {nullptr, nullptr}; // ... and two pinned slabs of it on the host
+    size_t i_stage_bytes = 0;
     int *adj_cnt = nullptr;                  // per (step, slot) counts, then offsets
     long long *adj_off = nullptr;
     size_t adj_cnt_cap = 0;
@@ -247,6 +251,9 @@ void fold3d_destroy(fold3d_ctx *c)
     if (c->adj_has) cudaFree(c->adj_has);
     if (c->adj_items) cudaFree(c->adj_items);
     if (c->adj_cnt) cudaFree(c->adj_cnt);
+    if (c->i_if) cudaFree(c->i_if);
+    for (int b = 0; b < 2; ++b)
+        if (c->i_stage[b]) cudaFreeHost(c->i_stage[b]);
     if (c->adj_off) cudaFree(c->adj_off);
     if (c->b_stage_d) cudaFree(c->b_stage_d);
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
@@ -1060,6 +1067,41 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
             if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
         }
     return solve_batch(c, n, in, *o, s, reps);
+}
+
+int fold3d_init_implicit_device(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
+                                void *stream)
+{
+    clear_error();
+    if (!c || !g || !m || !T) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2) return set_error(FOLD3D_ERR_INVALID, "grid needs >= 2 points per axis");
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    const size_t cells = field_cells(*g), plane = (size_t)(g->nx + 2) * (g->ny + 2) * sizeof(double);
+    if (c->i_if_cells < cells) {
+        if (c->i_if) cudaFree(c->i_if);
+        c->i_if = nullptr;
+        c->i_if_cells = 0;
+        if (cudaMalloc(&c->i_if, cells * sizeof(double)) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "device initialiser scratch");
+        c->i_if_cells = cells;
+    }
+    // two slabs of about 256 MB of node planes (at least one plane, at most the field)
+    const size_t bytes = std::min(std::max((size_t)256 << 20, plane) / plane * plane, cells * sizeof(double));
+    if (c->i_stage_bytes < bytes) {
+        for (int b = 0; b < 2; ++b) {
+            if (c->i_stage[b]) cudaFreeHost(c->i_stage[b]);
+            c->i_stage[b] = nullptr;
+        }
+        c->i_stage_bytes = 0;
+        for (int b = 0; b < 2; ++b)
+            if (cudaMallocHost(&c->i_stage[b], bytes) != cudaSuccess)
+                return set_error(FOLD3D_ERR_NOMEM, "device initialiser staging");
+        c->i_stage_bytes = bytes;
+    }
+    return init_implicit_device(*g, *m, T, c->i_if, c->i_stage, c->i_stage_bytes / plane, s);
 }
 
 int fold3d_adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,

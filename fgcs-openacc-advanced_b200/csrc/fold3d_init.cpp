@@ -25,26 +25,15 @@
 #include <thread>
 #include <vector>
 
+#include "fold3d_internal.h"
+#include "fold3d_seed.h"
 #include "fold3dpmm.h"
 
 namespace {
 
-constexpr double kMaxT = 10e15 * 1.0;  // Fold3dPMM.h:6
-
-inline double side(double a) { return (a > 0) ? 1.0 : -1.0; }  // sign(), 0 -> -1
-
-// Fold3dPMM.c:9-26
-double exact_time(double F, double ax, double ay, double az, double x, double y, double z)
-{
-    double xsq = x * x + y * y + z * z;
-    double adotx = ax * x + ay * y + az * z;
-    double q = (F * F - (ax * ax + ay * ay + az * az)) * xsq + adotx * adotx;
-    if (q > 0.0) {
-        q = adotx + std::sqrt(q);
-        if (q > 0.0) return xsq / q;
-    }
-    return 1.0 * kMaxT;
-}
+using fold3d_seed::exact_time;
+using fold3d_seed::kMaxT;
+using fold3d_seed::side;
 
 // Fold3dPMM.c:29-33
 double surface(double x, double y, double z)
@@ -60,67 +49,16 @@ inline double surface_tab(double x, double y, double z, double sin_x, double cos
     return 5.0 + (sin_x + cos_yx + std::sin(x + y + z)) * 0.4 - z + (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
 }
 
-// Node updates of one seeding point (updateVoxel, Fold3dPMM.c:62-110, in
-// order): position shift in multiples of the spacing (+1, -1 or -2), then the
-// node offset.  Two rows keep the reference's position/index mismatch
-// (:82 shifts y by +1 but writes node j; :86 shifts x by -1, y by -2 but
-// writes node i+2, j).
-struct NodeStep {
-    signed char px, py, pz, di, dj, dk;
-};
-constexpr NodeStep kSteps[44] = {
-    {0, 0, 0, 0, 0, 0},     {-1, 0, 0, 1, 0, 0},    {0, -1, 0, 0, 1, 0},    {0, 0, -1, 0, 0, 1},
-    {-1, -1, 0, 1, 1, 0},   {-1, 0, -1, 1, 0, 1},   {0, -1, -1, 0, 1, 1},   {-1, -1, -1, 1, 1, 1},
-    {1, 0, 0, -1, 0, 0},    {1, -1, 0, -1, 1, 0},   {1, 0, -1, -1, 0, 1},   {1, -1, -1, -1, 1, 1},
-    {-2, 0, 0, 2, 0, 0},    {-2, -1, 0, 2, 1, 0},   {-2, 0, -1, 2, 0, 1},   {-2, -1, -1, 2, 1, 1},
-    {0, 1, 0, 0, -1, 0},    {-1, 1, 0, 1, 0, 0},    {0, 1, -1, 0, -1, 1},   {-1, 1, -1, 1, -1, 1},
-    {0, -2, 0, 0, 2, 0},    {-1, -2, 0, 2, 0, 0},   {0, -2, -1, 0, 2, 1},   {-1, -2, -1, 1, 2, 1},
-    {0, 0, 1, 0, 0, -1},    {-1, 0, 1, 1, 0, -1},   {0, -1, 1, 0, 1, -1},   {-1, -1, 1, 1, 1, -1},
-    {0, 0, -2, 0, 0, 2},    {-1, 0, -2, 1, 0, 2},   {0, -1, -2, 0, 1, 2},   {-1, -1, -2, 1, 1, 2},
-    {0, 1, 1, 0, -1, -1},   {1, 0, 1, -1, 0, -1},   {1, 1, 0, -1, -1, 0},   {0, -2, -2, 0, 2, 2},
-    {-2, 0, -2, 2, 0, 2},   {-2, -2, 0, 2, 2, 0},   {-1, 1, 1, 1, -1, -1},  {1, -1, 1, -1, 1, -1},
-    {1, 1, -1, -1, -1, 1},  {-1, -2, -2, 1, 2, 2},  {-2, -1, -2, 2, 1, 2},  {-2, -2, -1, 2, 2, 1},
-};
+constexpr fold3d_seed::NodeStep kSteps[fold3d_seed::kNodeSteps] = FOLD3D_SEED_STEPS;
+constexpr fold3d_seed::Blend kBlends[fold3d_seed::kBlendCount] = FOLD3D_SEED_BLENDS;
 
-inline double shifted(double p, int m, double h)
-{
-    switch (m) {
-    case 0: return p;
-    case 1: return p + h;
-    case -1: return p - h;
-    default: return p - 2 * h;
-    }
-}
-
-// Blends of crossing l with earlier crossings (:274-382), in order.  A blend
-// is (sum of w[t] * P[l - off[t]]) / div; its z coordinate takes the y
-// coordinate of term `zy` instead of the z coordinate (the reference's
-// ypos[l-2] / ypos[l-3] in the zp lines, :309-379), or -1 for none.
-struct Blend {
-    int minl, div, n, off[3], w[3], zy;
-};
-constexpr Blend kBlends[] = {
-    {1, 3, 2, {0, 1, 0}, {2, 1, 0}, -1}, {1, 3, 2, {0, 1, 0}, {1, 2, 0}, -1},
-    {2, 3, 2, {0, 2, 0}, {2, 1, 0}, -1}, {2, 3, 2, {0, 2, 0}, {1, 2, 0}, -1},
-    {3, 3, 2, {0, 3, 0}, {2, 1, 0}, -1}, {3, 3, 2, {0, 3, 0}, {1, 2, 0}, -1},
-    {3, 3, 3, {0, 2, 3}, {1, 1, 1}, 1},  {3, 4, 3, {0, 2, 3}, {2, 1, 1}, 1},
-    {3, 4, 3, {0, 2, 3}, {1, 2, 1}, 1},  {3, 4, 3, {0, 2, 3}, {1, 1, 2}, 1},
-    {4, 3, 2, {0, 4, 0}, {2, 1, 0}, -1}, {4, 3, 2, {0, 4, 0}, {1, 2, 0}, -1},
-    {4, 3, 3, {0, 2, 3}, {1, 1, 1}, 1},  {4, 3, 3, {0, 2, 4}, {1, 1, 1}, 1},
-    {4, 3, 3, {0, 3, 4}, {1, 1, 1}, 1},  {5, 3, 2, {0, 5, 0}, {2, 1, 0}, -1},
-    {5, 3, 2, {0, 5, 0}, {1, 2, 0}, -1}, {5, 3, 3, {0, 2, 3}, {1, 1, 1}, 1},
-    {5, 3, 3, {0, 2, 4}, {1, 1, 1}, 1},  {5, 3, 3, {0, 2, 5}, {1, 1, 1}, 1},
-    {5, 3, 3, {0, 3, 5}, {1, 1, 1}, 1},  {5, 3, 3, {0, 3, 4}, {1, 1, 1}, 1},
-};
-
-struct Seeder {
+// InitNode (Fold3dPMM.c:35-54) on the host field.
+struct HostNode {
     double *T;
     long long sy, sz;
     double F, a[3];
-    double h[3];
 
-    // InitNode, Fold3dPMM.c:35-54
-    void node(double x, double y, double z, int i, int j, int k) const
+    void operator()(double x, double y, double z, int i, int j, int k) const
     {
         double *t = T + i + sy * j + sz * k;
         double ax = a[0], ay = a[1], az = a[2];
@@ -131,79 +69,6 @@ struct Seeder {
         }
         double tn = exact_time(F, ax, ay, az, -x, -y, -z);
         if (tn < std::fabs(*t)) *t = (side(*t) * 1.0) * tn;
-    }
-
-    void voxel(int i, int j, int k, double xp, double yp, double zp) const
-    {
-        for (const NodeStep &s : kSteps)
-            node(shifted(xp, s.px, h[0]), shifted(yp, s.py, h[1]), shifted(zp, s.pz, h[2]), i + s.di,
-                 j + s.dj, k + s.dk);
-    }
-
-    void seed_voxel(const double *IF, int i, int j, int k) const
-    {
-        const long long id = i + sy * j + sz * k;
-        const double f = IF[id], fx = IF[id + 1], fy = IF[id + sy], fz = IF[id + sz];
-        const double fxy = IF[id + 1 + sy], fzx = IF[id + 1 + sz], fzy = IF[id + sy + sz];
-        const double fxyz = IF[id + 1 + sy + sz];
-        // Skip voxels no edge of which can report a crossing.  An edge (a, b)
-        // reports one when p = h*a/(a-b) lands in [0, h].  For a and b of the
-        // same strict sign that needs a - b to round to a (one value below
-        // ~2^-52 of the other); with every corner of one sign and within a
-        // factor 2^40 of every other, each p lies strictly outside [0, h].
-        {
-            const double c[8] = {f, fx, fy, fz, fxy, fzx, fzy, fxyz};
-            bool pos = true, neg = true;
-            double lo = std::fabs(f), hi = lo;
-            for (int q = 0; q < 8; ++q) {
-                pos = pos && c[q] > 0.0;
-                neg = neg && c[q] < 0.0;
-                lo = std::min(lo, std::fabs(c[q]));
-                hi = std::max(hi, std::fabs(c[q]));
-            }
-            if ((pos || neg) && lo > hi * 0x1p-40) return;
-        }
-        const double hx = h[0], hy = h[1], hz = h[2];
-        double P[12][3];
-        int np = 0;
-        auto cross = [&](double p, double lim, double x, double y, double z) {
-            if (0.0 <= p && p <= lim) {
-                P[np][0] = x;
-                P[np][1] = y;
-                P[np][2] = z;
-                ++np;
-            }
-        };
-        double p;
-        p = hx * f / (f - fx);       cross(p, hx, p, 0.0, 0.0);
-        p = hx * fz / (fz - fzx);    cross(p, hx, p, 0.0, hz);
-        p = hx * fy / (fy - fxy);    cross(p, hx, p, hy, 0.0);
-        p = hx * fzy / (fzy - fxyz); cross(p, hx, p, hy, hz);
-        p = hy * f / (f - fy);       cross(p, hy, 0.0, p, 0.0);
-        p = hy * fz / (fz - fzy);    cross(p, hy, 0.0, p, hz);
-        p = hy * fx / (fx - fxy);    cross(p, hy, hx, p, 0.0);
-        p = hy * fzx / (fzx - fxyz); cross(p, hy, hx, p, hz);
-        p = hz * f / (f - fz);       cross(p, hz, 0.0, 0.0, p);
-        p = hz * fxy / (fxy - fxyz); cross(p, hz, hx, hy, p);
-        p = hz * fx / (fx - fzx);    cross(p, hz, hx, 0.0, p);
-        p = hz * fy / (fy - fzy);    cross(p, hz, 0.0, hy, p);
-        for (int l = 0; l < np; ++l) {
-            voxel(i, j, k, P[l][0], P[l][1], P[l][2]);
-            for (const Blend &b : kBlends) {
-                if (l < b.minl) continue;
-                double c[3];
-                for (int ax = 0; ax < 3; ++ax) {
-                    double acc = 0.0;
-                    for (int t = 0; t < b.n; ++t) {
-                        const int src_ax = (ax == 2 && t == b.zy) ? 1 : ax;
-                        const double term = b.w[t] * P[l - b.off[t]][src_ax];
-                        acc = (t == 0) ? term : acc + term;
-                    }
-                    c[ax] = acc / b.div;
-                }
-                voxel(i, j, k, c[0], c[1], c[2]);
-            }
-        }
     }
 };
 
@@ -237,6 +102,42 @@ void parallel_for(int lo, int hi, int nthreads, Fn fn)
 }
 
 }  // namespace
+
+namespace fold3d {
+
+// The tables of surface_planes: sin(x_i) (nx+2 values) and cos(y_j + x_i)
+// ((ny+2) rows of nx+2).
+void surface_tables(const fold3d_grid &g, double *sin_x, double *cos_yx, int nth)
+{
+    const int nx = g.nx, ny = g.ny;
+    const long long sy = nx + 2;
+    for (int i = 0; i < nx + 2; ++i) sin_x[i] = std::sin((i - 1) * g.dx + 0.);
+    parallel_for(0, ny + 2, nth, [&](int j) {
+        const double y = (j - 1) * g.dy + 0.;
+        for (int i = 0; i < nx + 2; ++i) cos_yx[(size_t)j * sy + i] = std::cos(y + ((i - 1) * g.dx + 0.));
+    });
+}
+
+// Implicit surface (Fold3dPMM.c:137-147) on node planes k0 <= k < k1, ghosts
+// included, into IF (plane k0 first).
+void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const double *sin_x, const double *cos_yx,
+                    int nth)
+{
+    const long long sy = g.nx + 2, sz = sy * (g.ny + 2);
+    parallel_for(k0, k1, nth, [&](int k) {
+        const double z = (k - 1) * g.dz + 0.;
+        for (int j = 0; j < g.ny + 2; ++j) {
+            const double y = (j - 1) * g.dy + 0.;
+            double *row = IF + sz * (k - k0) + sy * j;
+            for (int i = 0; i < g.nx + 2; ++i)
+                row[i] = surface_tab((i - 1) * g.dx + 0., y, z, sin_x[i], cos_yx[(size_t)j * sy + i]);
+        }
+    });
+}
+
+int init_threads() { return host_threads(); }
+
+}  // namespace fold3d
 
 extern "C" {
 
@@ -276,23 +177,13 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
     } catch (...) {
         return FOLD3D_ERR_NOMEM;
     }
-    for (int i = 0; i < nx + 2; ++i) sin_x[i] = std::sin((i - 1) * hx + 0.);
-    parallel_for(0, ny + 2, nth, [&](int j) {
-        const double y = (j - 1) * hy + 0.;
-        for (int i = 0; i < nx + 2; ++i) cos_yx[(size_t)j * sy + i] = std::cos(y + ((i - 1) * hx + 0.));
-    });
+    fold3d::surface_tables(*g, sin_x.data(), cos_yx.data(), nth);
+    fold3d::surface_planes(IF.data(), *g, 0, nz + 2, sin_x.data(), cos_yx.data(), nth);
     parallel_for(0, nz + 2, nth, [&](int k) {
-        const double z = (k - 1) * hz + 0.;
-        for (int j = 0; j < ny + 2; ++j) {
-            const double y = (j - 1) * hy + 0.;
-            for (int i = 0; i < nx + 2; ++i) {
-                const long long id = i + sy * j + sz * k;
-                IF[id] = surface_tab((i - 1) * hx + 0., y, z, sin_x[i], cos_yx[(size_t)j * sy + i]);
-                T[id] = (side(IF[id]) * 1.0) * kMaxT;
-            }
-        }
+        for (long long id = sz * k; id < sz * (k + 1); ++id) T[id] = (side(IF[id]) * 1.0) * kMaxT;
     });
-    Seeder s{T, sy, sz, m->F, {m->ax, m->ay, m->az}, {hx, hy, hz}};
+    HostNode node{T, sy, sz, m->F, {m->ax, m->ay, m->az}};
+    const double h[3] = {hx, hy, hz};
     // Voxels i = 1..nx-1 in slabs of >= 4 (the surface crosses every slab,
     // which balances the threads), even slabs then odd slabs: a voxel
     // min-updates nodes within 2 cells of it, so slabs of one phase never
@@ -307,7 +198,8 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
             const int i0 = 1 + slab * width, i1 = std::min(nx - 1, i0 + width - 1);
             for (int k = 1; k < nz; ++k)
                 for (int j = 1; j < ny; ++j)
-                    for (int i = i0; i <= i1; ++i) s.seed_voxel(IF.data(), i, j, k);
+                    for (int i = i0; i <= i1; ++i)
+                        fold3d_seed::seed_voxel(IF.data(), sy, sz, h, i, j, k, kSteps, kBlends, node);
         });
     }
     return FOLD3D_OK;

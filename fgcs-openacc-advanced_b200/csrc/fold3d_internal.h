@@ -90,6 +90,17 @@ struct WaveArgs {
     unsigned char *winners;      // elliptical medium: winner records, or NULL
     int dir;                     // direction of the pass (for the winner records)
 };
+// Host sampling of the implicit surface (fold3d_init.cpp).
+void surface_tables(const fold3d_grid &g, double *sin_x, double *cos_yx, int nth);
+void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const double *sin_x, const double *cos_yx,
+                    int nth);
+int init_threads();
+// ImplicitInitialiser into device field T (fold3d_init_dev.cu): IF_dev a
+// device scratch of one field, stage two pinned host buffers of stage_planes
+// node planes each.
+int init_implicit_device(const fold3d_grid &g, const fold3d_medium &m, double *T, double *IF_dev,
+                         double *stage[2], size_t stage_planes, cudaStream_t s);
+
 // Media of the local solver.
 enum Medium { kMediumDrift = 0, kMediumEllip = 1 };
 

@@ -36,7 +36,7 @@ EXPORTED = (
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
     "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
-    "fold3d_adjoint_batch",
+    "fold3d_adjoint_batch", "fold3d_init_implicit_device",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
@@ -124,6 +124,7 @@ def lib() -> C.CDLL:
     L.fold3d_solve_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
     L.fold3d_adjoint_batch.argtypes = [vp, i, P(AdjInstance), i, d, i, vp, P(Report)]
+    L.fold3d_init_implicit_device.argtypes = [vp, P(Grid), P(Medium), vp, vp]
     L.fold3d_solve_ellip_record.argtypes = [vp, P(Grid), P(Ellip), vp, vp, P(Opts), vp, P(Report)]
     L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
@@ -210,6 +211,14 @@ def init_implicit(nx, ny, nz, h, med: Medium | None = None) -> np.ndarray:
     _check(lib().fold3d_init_implicit(_host_ptr(T), C.byref(grid(nx, ny, nz, h)),
                                       C.byref(med or medium())))
     return T
+
+
+def init_implicit_device(ctx: "Context", T, h, med: Medium | None = None, stream=None):
+    """fold3d_init_implicit_device: the implicit-surface initialiser into the
+    device field T (float64 CUDA tensor, field layout)."""
+    nx, ny, nz = grid_of(T)
+    _check(lib().fold3d_init_implicit_device(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()),
+                                             _dev_ptr(T), C.c_void_p(stream) if stream else None))
 
 
 def init_point(nx, ny, nz, src) -> np.ndarray:

@@ -246,6 +246,15 @@ int fold3d_adjoint_batch(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance *
  * Uses all host cores. */
 int fold3d_init_implicit(double *T_host, const fold3d_grid *g, const fold3d_medium *m);
 
+/* ImplicitInitialiser into a device field T_dev (no counterpart in the
+ * reference, whose initialiser is host-only): the implicit surface is
+ * sampled on the host (the reference's libm, for the same bits) and streamed
+ * to the device in slabs; the crossings and node updates run on the GPU.
+ * The result equals fold3d_init_implicit's bit for bit.  Keeps one field of
+ * device scratch and two ~256 MB pinned host buffers in the context. */
+int fold3d_init_implicit_device(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_medium *m, double *T_dev,
+                                void *stream);
+
 /* Point source: T = +MAXT everywhere, T[si,sj,sk] = 0 (host field). */
 int fold3d_init_point(double *T_host, const fold3d_grid *g, int si, int sj, int sk);
 

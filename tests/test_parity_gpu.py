@@ -820,3 +820,23 @@ def test_batched_autograd_matches_per_source(cuda):
     loss.backward()
     for a, b in zip(Mb, Ms):
         assert cuda.allclose(a.grad, b.grad, rtol=1e-11, atol=1e-12 * float(b.grad.abs().max()))
+
+
+@pytest.mark.parametrize("dims,h,med", [((16, 16, 16), None, None),
+                                        ((20, 13, 17), (0.5, 0.8, 0.6), (1.3, (0.2, -0.5, 0.3))),
+                                        ((400, 400, 400), None, None)],
+                         ids=["16-golden", "20x13x17", "400-three-slabs"])
+def test_device_initialiser_matches_host(f3d, ctx, cuda, golden, dims, h, med):
+    """fold3d_init_implicit_device equals the host initialiser (and so the
+    reference's ImplicitInitialiser) bit for bit, ghosts included; at 400^3
+    the surface reaches the device in three slabs."""
+    n = dims[0]
+    if h is None:
+        h = (ref_spacing(n),) * 3
+    m = f3d.medium(*med) if med else f3d.medium()
+    ref = f3d.init_implicit(*dims, h, m)
+    if dims == (16, 16, 16):
+        assert_bitwise(ref, golden[16]["init"], "host init")
+    T = cuda.empty(ref.shape, dtype=cuda.float64, device="cuda")
+    f3d.init_implicit_device(ctx, T, h, m)
+    assert_bitwise(T.cpu().numpy(), ref, "device init")
