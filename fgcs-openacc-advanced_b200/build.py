@@ -31,7 +31,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math"
 
 CU_SOURCES = ["fold3d_kernels.cu", "fold3d_api.cu", "fold3d_noalloc.cu", "fold3d_wavefront.cu", "fold3d_adjoint.cu",
               "fold3d_init_dev.cu"]
-CXX_SOURCES = ["fold3d_init.cpp", "fold3d_tables.cpp"]
+CXX_SOURCES = ["fold3d_init.cpp", "fold3d_tables.cpp", "fold3d_io.cpp"]
 HEADERS = ["fold3d_internal.h", "fold3d_solver.cuh", "fold3d_fast.cuh", "fold3d_ellip.cuh", "fold3d_sync.cuh",
            "fold3d_seed.h"]
 

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <functional>
 #include <thread>
 #include <vector>
 
@@ -136,6 +137,11 @@ void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const doub
 }
 
 int init_threads() { return host_threads(); }
+
+void host_parallel_for(int lo, int hi, int nthreads, const std::function<void(int)> &fn)
+{
+    parallel_for(lo, hi, nthreads, fn);
+}
 
 }  // namespace fold3d
 

@@ -1,5 +1,7 @@
 // fold3d_internal.h -- shared declarations of the library's translation units.
 #pragma once
+
+#include <functional>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -95,6 +97,8 @@ void surface_tables(const fold3d_grid &g, double *sin_x, double *cos_yx, int nth
 void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const double *sin_x, const double *cos_yx,
                     int nth);
 int init_threads();
+// fn(i) for lo <= i < hi on up to nthreads host threads (contiguous ranges).
+void host_parallel_for(int lo, int hi, int nthreads, const std::function<void(int)> &fn);
 // ImplicitInitialiser into device field T (fold3d_init_dev.cu): IF_dev a
 // device scratch of one field, stage two pinned host buffers of stage_planes
 // node planes each.

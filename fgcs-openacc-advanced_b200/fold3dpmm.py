@@ -36,7 +36,8 @@ EXPORTED = (
     "fold3d_solve", "fold3d_solve_host", "fold3d_plane", "fold3d_init_implicit", "fold3d_init_point",
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
     "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
-    "fold3d_adjoint_batch", "fold3d_init_implicit_device",
+    "fold3d_adjoint_batch", "fold3d_init_implicit_device", "fold3d_write_text", "fold3d_write_vtk",
+    "fold3d_write_raw",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
@@ -125,6 +126,9 @@ def lib() -> C.CDLL:
     L.fold3d_solve_batch.argtypes = [vp, i, P(Instance), P(Opts), vp, P(Report)]
     L.fold3d_adjoint_batch.argtypes = [vp, i, P(AdjInstance), i, d, i, vp, P(Report)]
     L.fold3d_init_implicit_device.argtypes = [vp, P(Grid), P(Medium), vp, vp]
+    for name in ("fold3d_write_text", "fold3d_write_raw"):
+        getattr(L, name).argtypes = [C.c_char_p, vp, P(Grid)]
+    L.fold3d_write_vtk.argtypes = [C.c_char_p, vp, P(Grid), i]
     L.fold3d_solve_ellip_record.argtypes = [vp, P(Grid), P(Ellip), vp, vp, P(Opts), vp, P(Report)]
     L.fold3d_adjoint_ellip.argtypes = [vp, P(Grid), P(Ellip), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
     L.InitFoldFromPoint.argtypes = [d] * 7
@@ -219,6 +223,36 @@ def init_implicit_device(ctx: "Context", T, h, med: Medium | None = None, stream
     nx, ny, nz = grid_of(T)
     _check(lib().fold3d_init_implicit_device(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()),
                                              _dev_ptr(T), C.c_void_p(stream) if stream else None))
+
+
+def write_text(path, T: np.ndarray, h):
+    """fold3d_write_text: the reference's %f dump of a host field."""
+    nx, ny, nz = grid_of(T)
+    _check(lib().fold3d_write_text(os.fsencode(path), _host_ptr(T), C.byref(grid(nx, ny, nz, h))))
+
+
+def write_vtk(path, T: np.ndarray, h, ghosts=False):
+    """fold3d_write_vtk: legacy VTK structured points (binary)."""
+    nx, ny, nz = grid_of(T)
+    _check(lib().fold3d_write_vtk(os.fsencode(path), _host_ptr(T), C.byref(grid(nx, ny, nz, h)), int(bool(ghosts))))
+
+
+def write_raw(path, T: np.ndarray, h):
+    """fold3d_write_raw: 64-byte header and the whole field."""
+    nx, ny, nz = grid_of(T)
+    _check(lib().fold3d_write_raw(os.fsencode(path), _host_ptr(T), C.byref(grid(nx, ny, nz, h))))
+
+
+def read_raw(path):
+    """A file of fold3d_write_raw: (field, (dx, dy, dz))."""
+    with open(path, "rb") as f:
+        head = f.read(64)
+        if head[:8] != b"FOLD3DRW":
+            raise ValueError("not a fold3d raw file")
+        ver, nx, ny, nz = np.frombuffer(head[8:24], dtype="<i4")
+        h = tuple(float(v) for v in np.frombuffer(head[24:48], dtype="<f8"))
+        T = np.fromfile(f, dtype="<f8").reshape(nz + 2, ny + 2, nx + 2)
+    return T, h
 
 
 def init_point(nx, ny, nz, src) -> np.ndarray:

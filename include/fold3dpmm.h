@@ -255,6 +255,19 @@ int fold3d_init_implicit(double *T_host, const fold3d_grid *g, const fold3d_medi
 int fold3d_init_implicit_device(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_medium *m, double *T_dev,
                                 void *stream);
 
+/* Output of a host field.
+ * fold3d_write_text: the reference's error-checking dump
+ * (AN_ISO_1_OpenACC.c:1244-1260): "%f\n" per value, i outermost, k innermost,
+ * ghosts included -- the same bytes as the reference's file.
+ * fold3d_write_vtk: a legacy VTK STRUCTURED_POINTS file of the travel times
+ * (binary big-endian doubles, x fastest; ghosts = 0: the interior only), the
+ * file the reference's Write_VTK_Structured_Grid (:1098-1135) leaves empty.
+ * fold3d_write_raw: a 64-byte header ("FOLD3DRW", int32 version 1, nx, ny,
+ * nz, double dx, dy, dz) and the whole field, little-endian doubles. */
+int fold3d_write_text(const char *path, const double *T_host, const fold3d_grid *g);
+int fold3d_write_vtk(const char *path, const double *T_host, const fold3d_grid *g, int ghosts);
+int fold3d_write_raw(const char *path, const double *T_host, const fold3d_grid *g);
+
 /* Point source: T = +MAXT everywhere, T[si,sj,sk] = 0 (host field). */
 int fold3d_init_point(double *T_host, const fold3d_grid *g, int si, int sj, int sk);
 

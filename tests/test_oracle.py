@@ -277,3 +277,48 @@ def test_oracle_adjoint_matches_finite_differences():
         fd = (loss(up) - loss(dn)) / dv
         errs.append(abs(fd - G[comp][k, j, i]) / max(abs(fd), abs(G[comp][k, j, i])))
     assert np.median(errs) < 1e-6 and max(errs) < 1e-4, (np.median(errs), max(errs))
+
+
+# -- output files ------------------------------------------------------------
+
+def test_text_dump_matches_reference_program_128(f3d, orc, digests, tmp_path):
+    """fold3d_write_text gives the bytes of the reference program's own 128^3
+    output file (md5 from the reference's run)."""
+    n = 128
+    h = (ref_spacing(n),) * 3
+    T = orc.init_implicit(n, n, n, h)
+    orc.solve(T, h, 8)
+    p = tmp_path / "t.txt"
+    f3d.write_text(str(p), T, h[0])
+    assert hashlib.md5(p.read_bytes()).hexdigest() == digests["n128_s8_text_md5"]
+
+
+def test_vtk_and_raw_round_trip(f3d, tmp_path):
+    nx, ny, nz = 7, 5, 6
+    h = (0.5, 0.25, 0.75)
+    rng = np.random.default_rng(0)
+    T = rng.standard_normal((nz + 2, ny + 2, nx + 2))
+    for ghosts in (False, True):
+        p = tmp_path / ("t%d.vtk" % ghosts)
+        f3d.write_vtk(str(p), T, h, ghosts=ghosts)
+        raw = p.read_bytes()
+        head, _, data = raw.partition(b"LOOKUP_TABLE default\n")
+        lines = head.decode().splitlines()
+        e = 0 if ghosts else 1
+        dims = (nx + 2 - 2 * e, ny + 2 - 2 * e, nz + 2 - 2 * e)
+        assert lines[2] == "BINARY" and lines[3] == "DATASET STRUCTURED_POINTS"
+        assert lines[4] == "DIMENSIONS %d %d %d" % dims
+        assert [float(v) for v in lines[6].split()[1:]] == list(h)
+        vals = np.frombuffer(data[:8 * int(np.prod(dims))], dtype=">f8").reshape(dims[::-1])
+        inner = T[e:T.shape[0] - e, e:T.shape[1] - e, e:T.shape[2] - e]
+        assert np.array_equal(vals, inner)
+    p = tmp_path / "t.raw"
+    f3d.write_raw(str(p), T, h)
+    R, hr = f3d.read_raw(str(p))
+    assert hr == h and np.array_equal(R.view(np.uint64), T.view(np.uint64))
+
+
+def test_writers_reject_bad_paths(f3d, tmp_path):
+    T = np.zeros((5, 5, 5))
+    with pytest.raises(RuntimeError):
+        f3d.write_raw(str(tmp_path / "no" / "such" / "dir" / "t.raw"), T, 1.0)
