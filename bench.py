@@ -495,8 +495,10 @@ def run_adjoint(args):
                         device="cuda")
     rec = (1, ridx.view(-1, 1), ridx.view(1, -1))  # (k, j, i): top face
 
+    fdt = torch.float32 if args.adj_dtype == "f32" else torch.float64
+
     def t0_of(sp_):
-        t = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=torch.float64, device="cuda")
+        t = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=fdt, device="cuda")
         t[sp_[2], sp_[1], sp_[0]] = 0.0
         return t
 
@@ -526,13 +528,13 @@ def run_adjoint(args):
         if B > 1:  # B sources per batched forward solve and batched adjoint
             for c0 in range(0, len(srcs), B):
                 T = tomo.solve_batch(T0s[c0:c0 + B], h, Ml, tol=tol, adj_tol=args.adj_tol)
-                Ls = 0.5 * ((T[brec] - tobs_s[c0:c0 + B]) ** 2).sum()
+                Ls = 0.5 * ((T[brec].double() - tobs_s[c0:c0 + B].double()) ** 2).sum()
                 Ls.backward()
                 loss += Ls.detach()
         else:
             for sp_, to in zip(srcs, tobs):
                 T = tomo.solve(t0_of(sp_), h, Ml, tol=tol, adj_tol=args.adj_tol)
-                Ls = 0.5 * ((T[rec] - to) ** 2).sum()
+                Ls = 0.5 * ((T[rec].double() - to.double()) ** 2).sum()
                 Ls.backward()
                 loss += Ls.detach()
         torch.autograd.backward(Mg, [m.grad for m in Ml])
@@ -573,7 +575,7 @@ def run_adjoint(args):
     out = {
         "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": args.adj_dtype,
         "data": "synthetic: seeded heterogeneous TTI true medium (seed 2), smoothed starting medium",
         "config": {"workload": "tomography gradient %d^3 h=10 m, %d sources (jittered %dx%d, k=11), %d receivers "
                                "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
@@ -617,6 +619,8 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
+    ap.add_argument("--adj-dtype", choices=["f64", "f32"], default="f64",
+                    help="--medium adjoint: float64 or the float32 build (fields, solver, adjoint)")
     ap.add_argument("--adj-batch", type=int, default=64,
                     help="--medium adjoint: sources per batched forward solve and adjoint (1: one by one)")
     ap.add_argument("--adj-tol", type=float, default=1e-12,

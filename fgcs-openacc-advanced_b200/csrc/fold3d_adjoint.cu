@@ -44,24 +44,28 @@ namespace {
 __device__ __forceinline__ int fan_i(int p) { return p == 0 ? 0 : ell_ri(p - 1); }
 __device__ __forceinline__ int fan_j(int p) { return p == 0 ? 0 : ell_rj(p - 1); }
 
+template <class R> __device__ __forceinline__ R r_inf();
+template <> __device__ __forceinline__ double r_inf<double>() { return CUDART_INF; }
+template <> __device__ __forceinline__ float r_inf<float>() { return CUDART_INF_F; }
+
 // Candidate `id` without gates (same expressions as the forward solver):
 // returns its value or +inf, the footpoint's weights over fan points pt[],
 // and the footpoint-to-target vector c (spacing units) with its length n.
-__device__ double ell_cand(const EllipA &A, const double tv[9], int id, int pt[3], double w[3], int &np, double c[3],
-                           double &nlen)
+template <class R>
+__device__ R ell_cand(const EllipAT<R> &A, const R tv[9], int id, int pt[3], R w[3], int &np, R c[3], R &nlen)
 {
     np = 0;
     if (id <= 8) {
         const int i = fan_i(id), j = fan_j(id);
-        const double q = ell_bf(A, -i, -j, 1, -i, -j, 1);
-        if (!(q > 0.0)) return CUDART_INF;
+        const R q = ell_bf(A, -i, -j, 1, -i, -j, 1);
+        if (!(q > R(0))) return r_inf<R>();
         np = 1;
         pt[0] = id;
-        w[0] = 1.0;
-        c[0] = -i;
-        c[1] = -j;
-        c[2] = 1.0;
-        nlen = sqrt(q);
+        w[0] = R(1);
+        c[0] = (R)(-i);
+        c[1] = (R)(-j);
+        c[2] = R(1);
+        nlen = ell_sqrt(q);
         return tv[id] + nlen;
     }
     if (id <= 24) {
@@ -75,63 +79,63 @@ __device__ double ell_cand(const EllipA &A, const double tv[9], int id, int pt[3
         }
         const int pi = fan_i(P), pj = fan_j(P), qi = fan_i(Q), qj = fan_j(Q);
         const int ei = qi - pi, ej = qj - pj;
-        const double a = ell_bf(A, ei, ej, 0, ei, ej, 0);
-        const double b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
-        const double cc = ell_bf(A, -pi, -pj, 1, -pi, -pj, 1);
-        const double d = tv[Q] - tv[P];
-        const double den = a - d * d;
-        const double disc = a * cc - b * b;
-        if (!(den > 0.0 && disc > 0.0)) return CUDART_INF;
-        const double n = sqrt(disc / den);
-        const double lam = (b - d * n) / a;
-        if (!(lam > 0.0 && lam < 1.0)) return CUDART_INF;
+        const R a = ell_bf(A, ei, ej, 0, ei, ej, 0);
+        const R b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
+        const R cc = ell_bf(A, -pi, -pj, 1, -pi, -pj, 1);
+        const R d = tv[Q] - tv[P];
+        const R den = a - d * d;
+        const R disc = a * cc - b * b;
+        if (!(den > R(0) && disc > R(0))) return r_inf<R>();
+        const R n = ell_sqrt(disc / den);
+        const R lam = (b - d * n) / a;
+        if (!(lam > R(0) && lam < R(1))) return r_inf<R>();
         np = 2;
         pt[0] = P;
         pt[1] = Q;
-        w[0] = 1.0 - lam;
+        w[0] = R(1) - lam;
         w[1] = lam;
-        c[0] = -pi - lam * ei;
-        c[1] = -pj - lam * ej;
-        c[2] = 1.0;
+        c[0] = (R)(-pi) - lam * (R)ei;
+        c[1] = (R)(-pj) - lam * (R)ej;
+        c[2] = R(1);
         nlen = n;
         return tv[P] + lam * d + n;
     }
     const int r = id - 25, Pa = r + 1, Pb = (r + 1) % 8 + 1;
     const int ai = fan_i(Pa), aj = fan_j(Pa), bi = fan_i(Pb), bj = fan_j(Pb);
-    const double p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
-    const double p12 = ell_bf(A, ai, aj, 0, bi, bj, 0);
-    const double p22 = ell_bf(A, bi, bj, 0, bi, bj, 0);
-    const double q1 = ell_bf(A, ai, aj, 0, 0, 0, 1);
-    const double q2 = ell_bf(A, bi, bj, 0, 0, 0, 1);
-    const double cz = A.zz;
-    const double d1 = tv[Pa] - tv[0], d2 = tv[Pb] - tv[0];
-    const double det = p11 * p22 - p12 * p12;
-    if (!(det > 0.0)) return CUDART_INF;
-    const double u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
-    const double w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
-    const double s = (d1 * u1 + d2 * u2) / det;
-    const double rr = cz - (q1 * w1 + q2 * w2) / det;
-    if (!(s < 1.0 && rr > 0.0)) return CUDART_INF;
-    const double n = sqrt(rr / (1.0 - s));
-    const double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
-    if (!(l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0)) return CUDART_INF;
+    const R p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
+    const R p12 = ell_bf(A, ai, aj, 0, bi, bj, 0);
+    const R p22 = ell_bf(A, bi, bj, 0, bi, bj, 0);
+    const R q1 = ell_bf(A, ai, aj, 0, 0, 0, 1);
+    const R q2 = ell_bf(A, bi, bj, 0, 0, 0, 1);
+    const R cz = A.zz;
+    const R d1 = tv[Pa] - tv[0], d2 = tv[Pb] - tv[0];
+    const R det = p11 * p22 - p12 * p12;
+    if (!(det > R(0))) return r_inf<R>();
+    const R u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
+    const R w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
+    const R s = (d1 * u1 + d2 * u2) / det;
+    const R rr = cz - (q1 * w1 + q2 * w2) / det;
+    if (!(s < R(1) && rr > R(0))) return r_inf<R>();
+    const R n = ell_sqrt(rr / (R(1) - s));
+    const R l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
+    if (!(l1 > R(0) && l2 > R(0) && l1 + l2 < R(1))) return r_inf<R>();
     np = 3;
     pt[0] = 0;
     pt[1] = Pa;
     pt[2] = Pb;
-    w[0] = 1.0 - l1 - l2;
+    w[0] = R(1) - l1 - l2;
     w[1] = l1;
     w[2] = l2;
-    c[0] = -l1 * ai - l2 * bi;
-    c[1] = -l1 * aj - l2 * bj;
-    c[2] = 1.0;
+    c[0] = -l1 * (R)ai - l2 * (R)bi;
+    c[1] = -l1 * (R)aj - l2 * (R)bj;
+    c[2] = R(1);
     nlen = n;
     return tv[0] + (l1 * d1 + l2 * d2) + n;
 }
 
 // Fan times of the winner's direction for target x (source point first,
 // then the rim in order).
-__device__ __forceinline__ void fan_times(const double *T, long long x, const PlaneGeom &g, double tv[9])
+template <class R> __device__ __forceinline__ void fan_times(const R *T, long long x, const PlaneGeom &g, R tv[9])
 {
     const long long st = x - g.sn;
 #pragma unroll
@@ -152,8 +156,12 @@ constexpr int kAdjThreads = 32 * kWaveTV;
 // have work, push, publish.
 // Adds the largest pushed |amount| into dmax.  Returns false if a wait gave
 // up (the item is then left unpublished and the caller must leave).
+template <class R>
 __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam &ep, int item, double &dmax)
 {
+    const R *T = static_cast<const R *>(b.T);
+    R *lam = static_cast<R *>(b.lam);
+    R *pushed = static_cast<R *>(b.pushed);
     const WaveArgs &a = b.a;
     const PlaneGeom &g = a.pg;
     const int ntiles = a.ntu * a.ntv;
@@ -168,18 +176,19 @@ __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam 
     const int u = tu * 32 + lane + 1;
     const int v = tv * kWaveTV + warp + 1;
     long long x = -1, src[3] = {0, 0, 0};
-    double wt[3] = {0.0, 0.0, 0.0}, P = 0.0;
+    R wt[3] = {R(0), R(0), R(0)}, P = R(0);
     int np = 0;
     if (u <= g.nu && v <= g.nv) {
         const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
         const unsigned w = b.W[xc];
         if (w != kNoWinner && (int)(w / kEllipCands) == a.dir) {
             x = xc;
-            P = b.pushed[x];
-            double tv9[9], c[3], n;
+            P = pushed[x];
+            R tv9[9], c[3], n;
             int pt[3];
-            fan_times(b.T, x, g, tv9);
-            if (!(ell_cand(ell_local(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF))
+            fan_times(T, x, g, tv9);
+            if (!(ell_cand(ell_local<R>(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) <
+                  r_inf<R>()))
                 np = 0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
@@ -207,14 +216,14 @@ __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam 
     }
     if (__syncthreads_or(timed_out)) return false;
     if (x >= 0) {
-        const double L = __ldcg(b.lam + x);
-        const double D = L - P;
-        if (D != 0.0) {
-            b.pushed[x] = L;
+        const R L = __ldcg(lam + x);
+        const R D = L - P;
+        if (D != R(0)) {
+            pushed[x] = L;
 #pragma unroll
             for (int q = 0; q < 3; ++q)
-                if (q < np) atomicAdd(b.lam + src[q], wt[q] * D);
-            dmax = fmax(dmax, fabs(D));
+                if (q < np) atomicAdd(lam + src[q], wt[q] * D);
+            dmax = fmax(dmax, (double)fabs(D));
         }
     }
     // publish: the barrier makes every thread's atomics precede thread 0's
@@ -257,6 +266,7 @@ __device__ __forceinline__ void adj_flush(double d, unsigned long long *out)
 // The items are listed in ba.items (instance slot << 40 | item within the
 // instance's pass), tiles with work only, ordered step-major across the
 // instances: every item an item waits for comes earlier in the list.
+template <class R>
 __global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads) batch_adj_pass_kernel(BatchAdjArgs ba)
 {
     __shared__ long long s_next;
@@ -293,7 +303,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1024 / kAdjThreads) batch_adj_pas
             __syncthreads();
         }
         double dmax = 0.0;
-        if (!adj_item(s_inst.b, s_inst.ep, local, dmax)) break;
+        if (!adj_item<R>(s_inst.b, s_inst.ep, local, dmax)) break;
         adj_flush(dmax, s_inst.b.a.maxd);
     }
 }
@@ -360,10 +370,11 @@ __global__ void __launch_bounds__(kListThreads) adj_fill_kernel(const BatchAdjIn
 // field layout, accumulated in the order of the CPU statement.  Every cell is
 // written (ghosts and cells without a winner get 0), or, with accumulate,
 // added to.
-__global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict__ T, const double *__restrict__ lam,
+template <class R>
+__global__ void __launch_bounds__(256) adj_grad_kernel(const R *__restrict__ T, const R *__restrict__ lam,
                                                        const unsigned char *__restrict__ W,
                                                        const __grid_constant__ AdjGeom geo, EllipMedium med, int nx,
-                                                       int ny, int nz, double *dLdM, int accumulate)
+                                                       int ny, int nz, R *dLdM, int accumulate)
 {
     const long long sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
     const long long cells = sz * (nz + 2);
@@ -371,41 +382,49 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const double *__restrict_
          x += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(x % sy), j = (int)((x / sy) % (ny + 2)), k = (int)(x / sz);
         const bool interior = i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nz;
-        double dM[6] = {0, 0, 0, 0, 0, 0};
+        R dM[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
         const unsigned w = interior ? W[x] : kNoWinner;
         if (w < 6u * kEllipCands) {
             const int dir = (int)(w / kEllipCands);
             const EllipDir &D = geo.d[dir];
-            double tv[9];
+            R tv[9];
             fan_times(T, x, geo.pg[dir], tv);
             int pt[3], np;
-            double wt[3], c[3], n;
-            if (ell_cand(ell_local(med, D, x), tv, (int)(w % kEllipCands), pt, wt, np, c, n) < CUDART_INF) {
-                const double hh[3] = {D.hx, D.hy, D.hz};
+            R wt[3], c[3], n;
+            if (ell_cand(ell_local<R>(med, D, x), tv, (int)(w % kEllipCands), pt, wt, np, c, n) < r_inf<R>()) {
+                const R hh[3] = {(R)D.hx, (R)D.hy, (R)D.hz};
                 const int sxy[3][3] = {{1, D.sxy, D.sxz}, {D.sxy, 1, D.syz}, {D.sxz, D.syz, 1}};
                 const int comp[3][3] = {{D.ixx, D.ixy, D.ixz}, {D.ixy, D.iyy, D.iyz}, {D.ixz, D.iyz, D.izz}};
 #pragma unroll
                 for (int p = 0; p < 3; ++p)
 #pragma unroll
                     for (int r = p; r < 3; ++r) {
-                        const double dA = c[p] * c[r] / ((p == r ? 2.0 : 1.0) * n);
-                        dM[comp[p][r]] += dA * (double)sxy[p][r] * hh[p] * hh[r];
+                        const R dA = c[p] * c[r] / ((p == r ? R(2) : R(1)) * n);
+                        dM[comp[p][r]] += dA * (R)sxy[p][r] * hh[p] * hh[r];
                     }
             }
         }
-        const double L = interior ? lam[x] : 0.0;
+        const R L = interior ? lam[x] : R(0);
 #pragma unroll
         for (int m = 0; m < 6; ++m) {
-            double *o = dLdM + m * cells + x;
+            R *o = dLdM + m * cells + x;
             *o = accumulate ? *o + L * dM[m] : L * dM[m];
         }
     }
 }
 
-cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
-                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, int accumulate, cudaStream_t s)
+cudaError_t launch_adj_grad(const void *T, const void *lam, const unsigned char *W, const AdjGeom &geo,
+                            const EllipMedium &med, const fold3d_grid &g, void *dLdM, int accumulate, bool f32,
+                            cudaStream_t s)
 {
-    adj_grad_kernel<<<148 * 8, 256, 0, s>>>(T, lam, W, geo, med, g.nx, g.ny, g.nz, dLdM, accumulate);
+    if (f32)
+        adj_grad_kernel<float><<<148 * 8, 256, 0, s>>>(static_cast<const float *>(T), static_cast<const float *>(lam),
+                                                       W, geo, med, g.nx, g.ny, g.nz, static_cast<float *>(dLdM),
+                                                       accumulate);
+    else
+        adj_grad_kernel<double><<<148 * 8, 256, 0, s>>>(static_cast<const double *>(T),
+                                                        static_cast<const double *>(lam), W, geo, med, g.nx, g.ny,
+                                                        g.nz, static_cast<double *>(dLdM), accumulate);
     return cudaGetLastError();
 }
 
@@ -415,9 +434,10 @@ cudaError_t launch_adj_tiles(const unsigned char *W, const fold3d_grid &g, const
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, int grid, cudaStream_t s)
+cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, bool f32, int grid, cudaStream_t s)
 {
-    batch_adj_pass_kernel<<<grid, kAdjThreads, 0, s>>>(b);
+    if (f32) batch_adj_pass_kernel<float><<<grid, kAdjThreads, 0, s>>>(b);
+    else batch_adj_pass_kernel<double><<<grid, kAdjThreads, 0, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -430,11 +450,13 @@ cudaError_t launch_adj_list(const BatchAdjInst *inst, int k, int max_steps, int 
     return cudaGetLastError();
 }
 
-int batch_adj_blocks_per_sm()
+int batch_adj_blocks_per_sm(bool f32)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_adj_pass_kernel, kAdjThreads, 0) != cudaSuccess)
-        return 1;
+    const cudaError_t e =
+        f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_adj_pass_kernel<float>, kAdjThreads, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_adj_pass_kernel<double>, kAdjThreads, 0);
+    if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 

@@ -443,8 +443,9 @@ static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int d
     return p;
 }
 
+// T: double, or float when f32 (elliptical medium only).
 static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
-                           double *T, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep,
+                           void *T, bool f32, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep,
                            unsigned char *winners = nullptr)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
@@ -498,10 +499,10 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
             if ((e = cudaMemsetAsync(a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
                 return cuda_error(e, "cudaMemsetAsync");
             if (em) {
-                e = launch_wave_pass_ellip(T, a, ellip_param(g, *em, dir), grid, s);
+                e = launch_wave_pass_ellip(T, f32, a, ellip_param(g, *em, dir), grid, s);
             } else {
                 build_dir_table(make_frame(g, *fm, dir), tab);
-                e = launch_wave_pass(T, a, tab, grid, s);
+                e = launch_wave_pass(static_cast<double *>(T), a, tab, grid, s);
             }
             if (e != cudaSuccess) return cuda_error(e, "wavefront pass");
         }
@@ -599,8 +600,8 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
         c->wave_bps = wave_blocks_per_sm(kMediumDrift);
         c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
-    if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm();
-    if (!c->batch_adj_bps) c->batch_adj_bps = batch_adj_blocks_per_sm();
+    if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm(false);
+    if (!c->batch_adj_bps) c->batch_adj_bps = batch_adj_blocks_per_sm(false);
     c->bkey = key;
     return FOLD3D_OK;
 }
@@ -629,7 +630,24 @@ static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
     return s;
 }
 
-static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts &o, cudaStream_t s,
+// Instances of the batched drivers: fields of doubles, or of floats (f32).
+struct SolveInst {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    void *T;
+    unsigned char *winners;
+};
+struct AdjInst {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    const void *T;
+    const unsigned char *winners;
+    const void *dLdT;
+    void *lambda;
+    void *dLdM;
+};
+
+static int solve_batch(fold3d_ctx *c, int n, const SolveInst *in, bool f32, const fold3d_opts &o, cudaStream_t s,
                        fold3d_report *reps)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
@@ -731,7 +749,7 @@ static int solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
             const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_bps);
             if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
                 return cuda_error(e, "memset");
-            if (grid > 0 && (e = launch_batch_pass(args[dir], grid, s)) != cudaSuccess)
+            if (grid > 0 && (e = launch_batch_pass(args[dir], f32, grid, s)) != cudaSuccess)
                 return cuda_error(e, "batch pass");
         }
         ++sweep;
@@ -861,7 +879,7 @@ static int adj_list_scratch(fold3d_ctx *c, size_t items, size_t counts)
     return FOLD3D_OK;
 }
 
-static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,
+static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int max_sweeps, double tol,
                          int accumulate, cudaStream_t s, fold3d_report *reps)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(max_sweeps, 1 << 20) + 12u);
@@ -871,7 +889,8 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
     if ((rc = batch_scratch(c, grids))) return rc;
     std::vector<size_t> off(n + 1, 0);
     for (int i = 0; i < n; ++i) off[i + 1] = off[i] + field_cells(in[i].grid);
-    if ((rc = adj_scratch(c, off[n]))) return rc;
+    if ((rc = adj_scratch(c, off[n]))) return rc;  // doubles: room for floats too
+    const size_t esz = f32 ? sizeof(float) : sizeof(double);
     std::vector<size_t> hoff(n + 1, 0);
     for (int i = 0; i < n; ++i) hoff[i + 1] = hoff[i] + adj_tiles_bytes(in[i].grid);
     if ((rc = adj_has_scratch(c, hoff[n]))) return rc;
@@ -892,10 +911,10 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
     }
     cudaError_t e;
     for (int i = 0; i < n; ++i)
-        if ((e = cudaMemcpyAsync(in[i].lambda, in[i].dLdT, field_cells(in[i].grid) * sizeof(double),
-                                 cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(in[i].lambda, in[i].dLdT, field_cells(in[i].grid) * esz, cudaMemcpyDeviceToDevice,
+                                 s)) != cudaSuccess)
             return cuda_error(e, "adjoint setup");
-    if ((e = cudaMemsetAsync(c->adj_pushed, 0, off[n] * sizeof(double), s)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(c->adj_pushed, 0, off[n] * esz, s)) != cudaSuccess ||
         (e = cudaMemsetAsync(c->b_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess)
         return cuda_error(e, "adjoint setup");
     std::vector<char> active(n, 1);
@@ -938,7 +957,7 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
                 a.dir = dir;
                 bi.b.T = in[i].T;
                 bi.b.lam = in[i].lambda;
-                bi.b.pushed = c->adj_pushed + off[i];
+                bi.b.pushed = reinterpret_cast<char *>(c->adj_pushed) + off[i] * esz;
                 bi.b.W = in[i].winners;
                 bi.b.has = tiles[i].has[dir];
                 bi.ep = ellip_param(g, in[i].medium, dir);
@@ -985,7 +1004,7 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
             const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_adj_bps);
             if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
                 return cuda_error(e, "memset");
-            if (grid > 0 && (e = launch_batch_adj_pass(args[dir], grid, s)) != cudaSuccess)
+            if (grid > 0 && (e = launch_batch_adj_pass(args[dir], f32, grid, s)) != cudaSuccess)
                 return cuda_error(e, "batched adjoint pass");
         }
         ++sweep;
@@ -1020,7 +1039,7 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
                                in[i].medium.myy, in[i].medium.myz, in[i].medium.mzz};
         for (int k = 0; k < 6; ++k) med.m[k] = arr[k];
         if ((e = launch_adj_grad(in[i].T, in[i].lambda, in[i].winners, geo, med, in[i].grid, in[i].dLdM, accumulate,
-                                 s)) != cudaSuccess)
+                                 f32, s)) != cudaSuccess)
             return cuda_error(e, "gradient");
     }
     if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
@@ -1040,9 +1059,60 @@ static int adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
     return FOLD3D_OK;
 }
 
-extern "C" {
+static bool metric_ok(const fold3d_ellip *m)
+{
+    return m && m->mxx && m->mxy && m->mxz && m->myy && m->myz && m->mzz;
+}
 
-int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts *o, void *stream,
+static int ellip_opts_ok(const fold3d_opts *o)
+{
+    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "the elliptical medium runs on the wavefront engine, variant 0");
+    return FOLD3D_OK;
+}
+
+// fold3d_solve_ellip(_record)(_f32): W == NULL for no record.
+static int ellip_entry(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, void *T, bool f32,
+                       unsigned char *W, bool record, const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (record && !W) return set_error(FOLD3D_ERR_INVALID, "winner array is NULL");
+    if (!T || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (!metric_ok(m)) return set_error(FOLD3D_ERR_INVALID, "metric array is NULL");
+    int rc = check_grid(g);
+    if (rc || (rc = ellip_opts_ok(o))) return rc;
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    if (record) {
+        const cudaError_t e = cudaMemsetAsync(W, 0xff, field_cells(*g), s);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
+    }
+    return solve_wavefront(c, *g, nullptr, m, T, f32, *o, s, rep, record ? W : nullptr);
+}
+
+static int adjoint_entry(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int max_sweeps, double tol,
+                         int accumulate, void *stream, fold3d_report *reps)
+{
+    clear_error();
+    if (!c || !in) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    if (n < 1) return set_error(FOLD3D_ERR_INVALID, "n must be >= 1");
+    if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
+    if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
+    for (int i = 0; i < n; ++i) {
+        int rc = check_grid(&in[i].grid);
+        if (rc) return rc;
+        if (!in[i].T || !in[i].winners || !in[i].dLdT || !in[i].lambda || !in[i].dLdM || !metric_ok(&in[i].medium))
+            return set_error(FOLD3D_ERR_INVALID, n == 1 ? "NULL argument" : "instance with a NULL array");
+    }
+    DeviceGuard dg(c->device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    return adjoint_batch(c, n, in, f32, max_sweeps, tol, accumulate, s, reps);
+}
+
+static int batch_entry(fold3d_ctx *c, int n, const SolveInst *in, bool f32, const fold3d_opts *o, void *stream,
                        fold3d_report *reps)
 {
     clear_error();
@@ -1051,14 +1121,14 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
     for (int i = 0; i < n; ++i) {
         int rc = check_grid(&in[i].grid);
         if (rc) return rc;
-        const fold3d_ellip &m = in[i].medium;
-        if (!in[i].T || !m.mxx || !m.mxy || !m.mxz || !m.myy || !m.myz || !m.mzz)
-            return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
+        if (!in[i].T || !metric_ok(&in[i].medium)) return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
     }
-    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
-    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
-        return set_error(FOLD3D_ERR_UNSUPPORTED, "batched solves run on the wavefront engine, variant 0");
+    int rc = ellip_opts_ok(o);
+    if (rc) {
+        if (rc == FOLD3D_ERR_UNSUPPORTED)
+            return set_error(rc, "batched solves run on the wavefront engine, variant 0");
+        return rc;
+    }
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     for (int i = 0; i < n; ++i)
@@ -1066,7 +1136,27 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
             cudaError_t e = cudaMemsetAsync(in[i].winners, 0xff, field_cells(in[i].grid), s);
             if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
         }
-    return solve_batch(c, n, in, *o, s, reps);
+    return solve_batch(c, n, in, f32, *o, s, reps);
+}
+
+extern "C" {
+
+int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fold3d_opts *o, void *stream,
+                       fold3d_report *reps)
+{
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    std::vector<SolveInst> v(n);
+    for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+    return batch_entry(c, n, v.data(), false, o, stream, reps);
+}
+
+int fold3d_solve_batch_f32(fold3d_ctx *c, int n, const fold3d_instance_f32 *in, const fold3d_opts *o, void *stream,
+                           fold3d_report *reps)
+{
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    std::vector<SolveInst> v(n);
+    for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+    return batch_entry(c, n, v.data(), true, o, stream, reps);
 }
 
 int fold3d_init_implicit_device(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
@@ -1107,22 +1197,21 @@ int fold3d_init_implicit_device(fold3d_ctx *c, const fold3d_grid *g, const fold3
 int fold3d_adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,
                          int accumulate, void *stream, fold3d_report *reps)
 {
-    clear_error();
-    if (!c || !in) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    if (n < 1) return set_error(FOLD3D_ERR_INVALID, "n must be >= 1");
-    if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
-    if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    for (int i = 0; i < n; ++i) {
-        int rc = check_grid(&in[i].grid);
-        if (rc) return rc;
-        const fold3d_ellip &m = in[i].medium;
-        if (!in[i].T || !in[i].winners || !in[i].dLdT || !in[i].lambda || !in[i].dLdM || !m.mxx || !m.mxy ||
-            !m.mxz || !m.myy || !m.myz || !m.mzz)
-            return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
-    }
-    DeviceGuard dg(c->device);
-    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    return adjoint_batch(c, n, in, max_sweeps, tol, accumulate, s, reps);
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    std::vector<AdjInst> v(n);
+    for (int i = 0; i < n; ++i)
+        v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+    return adjoint_entry(c, n, v.data(), false, max_sweeps, tol, accumulate, stream, reps);
+}
+
+int fold3d_adjoint_batch_f32(fold3d_ctx *c, int n, const fold3d_adjoint_instance_f32 *in, int max_sweeps,
+                             double tol, int accumulate, void *stream, fold3d_report *reps)
+{
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    std::vector<AdjInst> v(n);
+    for (int i = 0; i < n; ++i)
+        v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+    return adjoint_entry(c, n, v.data(), true, max_sweeps, tol, accumulate, stream, reps);
 }
 
 int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
@@ -1151,7 +1240,7 @@ int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, do
     if (engine == FOLD3D_ENGINE_WAVEFRONT) {
         if (o->variant != kVariantFast)
             return set_error(FOLD3D_ERR_UNSUPPORTED, "the wavefront engine runs the default solver variant only");
-        return solve_wavefront(c, *g, m, nullptr, T, *o, s, rep);
+        return solve_wavefront(c, *g, m, nullptr, T, false, *o, s, rep);
     }
     return solve_planes(c, *g, *m, T, *o, s, rep);
 }
@@ -1231,59 +1320,43 @@ void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az,
 int fold3d_solve_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T, const fold3d_opts *o,
                        void *stream, fold3d_report *rep)
 {
-    clear_error();
-    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
-    if (!T || !m || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    if (!m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
-        return set_error(FOLD3D_ERR_INVALID, "metric array is NULL");
-    int rc = check_grid(g);
-    if (rc) return rc;
-    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
-    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
-        return set_error(FOLD3D_ERR_UNSUPPORTED, "the elliptical medium runs on the wavefront engine, variant 0");
-    DeviceGuard dg(c->device);
-    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    return solve_wavefront(c, *g, nullptr, m, T, *o, s, rep);
+    return ellip_entry(c, g, m, T, false, nullptr, false, o, stream, rep);
+}
+
+int fold3d_solve_ellip_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, float *T,
+                           const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    return ellip_entry(c, g, m, T, true, nullptr, false, o, stream, rep);
 }
 
 int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T,
                               unsigned char *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
-    clear_error();
-    if (!W) return set_error(FOLD3D_ERR_INVALID, "winner array is NULL");
-    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
-    int rc = check_grid(g);
-    if (rc) return rc;
-    DeviceGuard dg(c->device);
-    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    cudaError_t e = cudaMemsetAsync(W, 0xff, field_cells(*g), s);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync");
-    if (!T || !m || !o || !m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
-        return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
-    if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (o->engine == FOLD3D_ENGINE_PLANES || o->variant != kVariantFast)
-        return set_error(FOLD3D_ERR_UNSUPPORTED, "the elliptical medium runs on the wavefront engine, variant 0");
-    return solve_wavefront(c, *g, nullptr, m, T, *o, s, rep, W);
+    return ellip_entry(c, g, m, T, false, W, true, o, stream, rep);
+}
+
+int fold3d_solve_ellip_record_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, float *T,
+                                  unsigned char *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    return ellip_entry(c, g, m, T, true, W, true, o, stream, rep);
 }
 
 int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const double *T,
                          const unsigned char *W, const double *dLdT, double *lam, double *dLdM, int max_sweeps,
                          double tol, void *stream, fold3d_report *rep)
 {
-    clear_error();
-    if (!c || !g || !m || !T || !W || !dLdT || !lam || !dLdM) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    int rc = check_grid(g);
-    if (rc) return rc;
-    if (max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
-    if (!(tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
-    if (!m->mxx || !m->mxy || !m->mxz || !m->myy || !m->myz || !m->mzz)
-        return set_error(FOLD3D_ERR_INVALID, "NULL metric array");
-    DeviceGuard dg(c->device);
-    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    const fold3d_adjoint_instance one = {*g, *m, T, W, dLdT, lam, dLdM};
-    return adjoint_batch(c, 1, &one, max_sweeps, tol, 0, s, rep);
+    if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const AdjInst one = {*g, *m, T, W, dLdT, lam, dLdM};
+    return adjoint_entry(c, 1, &one, false, max_sweeps, tol, 0, stream, rep);
+}
+
+int fold3d_adjoint_ellip_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const float *T,
+                             const unsigned char *W, const float *dLdT, float *lam, float *dLdM, int max_sweeps,
+                             double tol, void *stream, fold3d_report *rep)
+{
+    if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const AdjInst one = {*g, *m, T, W, dLdT, lam, dLdM};
+    return adjoint_entry(c, 1, &one, true, max_sweeps, tol, 0, stream, rep);
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,

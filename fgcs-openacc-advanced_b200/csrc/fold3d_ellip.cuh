@@ -44,30 +44,40 @@ struct EllipParam {
 };
 
 #ifdef __CUDACC__
+// The solver is written once for the field's type R: double (the default
+// build) or float (the float32 build).  All arithmetic stays in R (literals
+// included), so the float build is float arithmetic throughout.
+
 // Local metric scaled by the spacings (Axx = M'xx hx hx, Axy = M'xy hx hy, ...).
-struct EllipA {
-    double xx, yy, zz, xy, xz, yz;
+template <class R> struct EllipAT {
+    R xx, yy, zz, xy, xz, yz;
 };
+using EllipA = EllipAT<double>;
+
+template <class R> __device__ __forceinline__ R ell_sqrt(R x);
+template <> __device__ __forceinline__ double ell_sqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float ell_sqrt<float>(float x) { return sqrtf(x); }
 
 // u^T M' v with u = (ui hx, uj hy, uk hz) and v likewise.
-__device__ __forceinline__ double ell_bf(const EllipA &A, int ui, int uj, int uk, int vi, int vj, int vk)
+template <class R>
+__device__ __forceinline__ R ell_bf(const EllipAT<R> &A, int ui, int uj, int uk, int vi, int vj, int vk)
 {
-    return (double)(ui * vi) * A.xx + (double)(uj * vj) * A.yy + (double)(uk * vk) * A.zz +
-           (double)(ui * vj + uj * vi) * A.xy + (double)(ui * vk + uk * vi) * A.xz +
-           (double)(uj * vk + uk * vj) * A.yz;
+    return (R)(ui * vi) * A.xx + (R)(uj * vj) * A.yy + (R)(uk * vk) * A.zz + (R)(ui * vj + uj * vi) * A.xy +
+           (R)(ui * vk + uk * vi) * A.xz + (R)(uj * vk + uk * vj) * A.yz;
 }
 
-__device__ __forceinline__ double ell_min(double a, double b) { return (a < b) ? a : b; }
+template <class R> __device__ __forceinline__ R ell_min(R a, R b) { return (a < b) ? a : b; }
 
 // Candidate ids (the adjoint's winner record): 0 vertex st, 1+r rim vertex r,
 // 9+r spoke st-rim[r], 17+r rim edge rim[r]-rim[r+1], 25+r triangle
 // (st, rim[r], rim[r+1]).  Each routine sets win when it lowers tn.
-__device__ __forceinline__ void ell_vertex(double &tn, int &win, int id, const EllipA &A, double tp, int i, int j)
+template <class R>
+__device__ __forceinline__ void ell_vertex(R &tn, int &win, int id, const EllipAT<R> &A, R tp, int i, int j)
 {
     if (!(tn > tp)) return;
-    const double c = ell_bf(A, -i, -j, 1, -i, -j, 1);
-    if (c > 0.0) {
-        const double cand = tp + sqrt(c);
+    const R c = ell_bf(A, -i, -j, 1, -i, -j, 1);
+    if (c > R(0)) {
+        const R cand = tp + ell_sqrt(c);
         if (cand < tn) {
             tn = cand;
             win = id;
@@ -75,22 +85,23 @@ __device__ __forceinline__ void ell_vertex(double &tn, int &win, int id, const E
     }
 }
 
-__device__ __forceinline__ void ell_edge(double &tn, int &win, int id, const EllipA &A, double tp, double tq, int pi,
-                                         int pj, int qi, int qj)
+template <class R>
+__device__ __forceinline__ void ell_edge(R &tn, int &win, int id, const EllipAT<R> &A, R tp, R tq, int pi, int pj,
+                                         int qi, int qj)
 {
     if (!(tn > ell_min(tp, tq))) return;
     const int ei = qi - pi, ej = qj - pj;
-    const double a = ell_bf(A, ei, ej, 0, ei, ej, 0);
-    const double b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
-    const double c = ell_bf(A, -pi, -pj, 1, -pi, -pj, 1);
-    const double d = tq - tp;
-    const double den = a - d * d;
-    const double disc = a * c - b * b;
-    if (den > 0.0 && disc > 0.0) {
-        const double n = sqrt(disc / den);
-        const double lam = (b - d * n) / a;
-        if (lam > 0.0 && lam < 1.0) {
-            const double cand = tp + lam * d + n;
+    const R a = ell_bf(A, ei, ej, 0, ei, ej, 0);
+    const R b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
+    const R c = ell_bf(A, -pi, -pj, 1, -pi, -pj, 1);
+    const R d = tq - tp;
+    const R den = a - d * d;
+    const R disc = a * c - b * b;
+    if (den > R(0) && disc > R(0)) {
+        const R n = ell_sqrt(disc / den);
+        const R lam = (b - d * n) / a;
+        if (lam > R(0) && lam < R(1)) {
+            const R cand = tp + lam * d + n;
             if (cand < tn) {
                 tn = cand;
                 win = id;
@@ -99,28 +110,29 @@ __device__ __forceinline__ void ell_edge(double &tn, int &win, int id, const Ell
     }
 }
 
-__device__ __forceinline__ void ell_tri(double &tn, int &win, int id, const EllipA &A, double t0, double ta, double tb,
-                                        int ai, int aj, int bi, int bj)
+template <class R>
+__device__ __forceinline__ void ell_tri(R &tn, int &win, int id, const EllipAT<R> &A, R t0, R ta, R tb, int ai,
+                                        int aj, int bi, int bj)
 {
     if (!(tn > ell_min(t0, ell_min(ta, tb)))) return;
-    const double p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
-    const double p12 = ell_bf(A, ai, aj, 0, bi, bj, 0);
-    const double p22 = ell_bf(A, bi, bj, 0, bi, bj, 0);
-    const double q1 = ell_bf(A, ai, aj, 0, 0, 0, 1);
-    const double q2 = ell_bf(A, bi, bj, 0, 0, 0, 1);
-    const double c = A.zz;
-    const double d1 = ta - t0, d2 = tb - t0;
-    const double det = p11 * p22 - p12 * p12;
-    if (!(det > 0.0)) return;
-    const double u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
-    const double w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
-    const double s = (d1 * u1 + d2 * u2) / det;
-    const double r = c - (q1 * w1 + q2 * w2) / det;
-    if (s < 1.0 && r > 0.0) {
-        const double n = sqrt(r / (1.0 - s));
-        const double l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
-        if (l1 > 0.0 && l2 > 0.0 && l1 + l2 < 1.0) {
-            const double cand = t0 + (l1 * d1 + l2 * d2) + n;
+    const R p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
+    const R p12 = ell_bf(A, ai, aj, 0, bi, bj, 0);
+    const R p22 = ell_bf(A, bi, bj, 0, bi, bj, 0);
+    const R q1 = ell_bf(A, ai, aj, 0, 0, 0, 1);
+    const R q2 = ell_bf(A, bi, bj, 0, 0, 0, 1);
+    const R c = A.zz;
+    const R d1 = ta - t0, d2 = tb - t0;
+    const R det = p11 * p22 - p12 * p12;
+    if (!(det > R(0))) return;
+    const R u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
+    const R w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
+    const R s = (d1 * u1 + d2 * u2) / det;
+    const R r = c - (q1 * w1 + q2 * w2) / det;
+    if (s < R(1) && r > R(0)) {
+        const R n = ell_sqrt(r / (R(1) - s));
+        const R l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
+        if (l1 > R(0) && l2 > R(0) && l1 + l2 < R(1)) {
+            const R cand = t0 + (l1 * d1 + l2 * d2) + n;
             if (cand < tn) {
                 tn = cand;
                 win = id;
@@ -135,27 +147,28 @@ __device__ __forceinline__ int ell_ri(int r) { return (r == 0 || r == 1 || r == 
 __device__ __forceinline__ int ell_rj(int r) { return (r >= 1 && r <= 3) ? 1 : (r >= 5) ? -1 : 0; }
 
 // Scaled local metric of the target at field index t.
-__device__ __forceinline__ EllipA ell_local(const EllipMedium &M, const EllipDir &D, long long t)
+template <class R> __device__ __forceinline__ EllipAT<R> ell_local(const EllipMedium &M, const EllipDir &D, long long t)
 {
-    EllipA A;
-    A.xx = (double)__ldg(M.m[D.ixx] + t) * D.hx * D.hx;
-    A.yy = (double)__ldg(M.m[D.iyy] + t) * D.hy * D.hy;
-    A.zz = (double)__ldg(M.m[D.izz] + t) * D.hz * D.hz;
-    A.xy = (double)D.sxy * (double)__ldg(M.m[D.ixy] + t) * D.hx * D.hy;
-    A.xz = (double)D.sxz * (double)__ldg(M.m[D.ixz] + t) * D.hx * D.hz;
-    A.yz = (double)D.syz * (double)__ldg(M.m[D.iyz] + t) * D.hy * D.hz;
+    const R hx = (R)D.hx, hy = (R)D.hy, hz = (R)D.hz;
+    EllipAT<R> A;
+    A.xx = (R)__ldg(M.m[D.ixx] + t) * hx * hx;
+    A.yy = (R)__ldg(M.m[D.iyy] + t) * hy * hy;
+    A.zz = (R)__ldg(M.m[D.izz] + t) * hz * hz;
+    A.xy = (R)D.sxy * (R)__ldg(M.m[D.ixy] + t) * hx * hy;
+    A.xz = (R)D.sxz * (R)__ldg(M.m[D.ixz] + t) * hx * hz;
+    A.yz = (R)D.syz * (R)__ldg(M.m[D.iyz] + t) * hy * hz;
     return A;
 }
 
 // New signed value of a target from st and its rim values (rim order above);
 // win: id of the candidate that set it, -1 if none did.
-__device__ __forceinline__ double point_update_ellip(double told, double st, const double nb[8], const EllipA &A,
-                                                     int &win)
+template <class R>
+__device__ __forceinline__ R point_update_ellip(R told, R st, const R nb[8], const EllipAT<R> &A, int &win)
 {
-    double tn = fabs(told);
+    R tn = fabs(told);
     win = -1;
     ell_vertex(tn, win, 0, A, st, 0, 0);
-    double m = st;
+    R m = st;
 #pragma unroll
     for (int r = 0; r < 8; ++r) m = ell_min(m, nb[r]);
     if (tn > m) {
@@ -174,7 +187,7 @@ __device__ __forceinline__ double point_update_ellip(double told, double st, con
             ell_tri(tn, win, 25 + r, A, st, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
     }
-    return ((told > 0) ? 1.0 : -1.0) * tn;
+    return ((told > R(0)) ? R(1) : R(-1)) * tn;
 }
 #endif  // __CUDACC__
 

@@ -118,8 +118,9 @@ struct EllipDir;     // fold3d_ellip.cuh
 struct EllipParam;   // below, once EllipDir is complete
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s);
-cudaError_t launch_wave_pass_ellip(double *T, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s);
-int wave_blocks_per_sm(int medium);
+// The elliptical medium's field is double, or float when f32.
+cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s);
+int wave_blocks_per_sm(int medium, bool f32 = false);
 
 }  // namespace fold3d
 #include "fold3d_ellip.cuh"
@@ -130,7 +131,7 @@ namespace fold3d {
 struct BatchInst {
     WaveArgs a;
     EllipParam p;
-    double *T;
+    void *T;  // double, or float in a float32 batch
 };
 static_assert(sizeof(BatchInst) % 4 == 0, "BatchInst is copied in words");
 
@@ -147,8 +148,8 @@ struct BatchArgs {
     unsigned *work, *status;
     unsigned epoch, skip_from;  // pass number and first pass that may skip
 };
-cudaError_t launch_batch_pass(const BatchArgs &b, int grid, cudaStream_t s);
-int batch_blocks_per_sm();
+cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int grid, cudaStream_t s);
+int batch_blocks_per_sm(bool f32);
 
 // Adjoint of the elliptical solver (fold3d_adjoint.cu).
 struct AdjGeom {
@@ -160,8 +161,8 @@ struct AdjGeom {
 // receives max |pushed amount|, a.epoch numbers the pass like a forward pass.
 struct AdjWaveArgs {
     WaveArgs a;
-    const double *T;
-    double *lam, *pushed;
+    const void *T;           // double, or float in a float32 adjoint (as lam and pushed)
+    void *lam, *pushed;
     const unsigned char *W;
     const unsigned char *has;  // [plane][tile] of this pass's orientation: 1 if a cell's winner is a.dir
 };
@@ -191,15 +192,16 @@ struct BatchAdjArgs {
     unsigned *work, *status;
     unsigned epoch;
 };
-cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, int grid, cudaStream_t s);
+cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, bool f32, int grid, cudaStream_t s);
 // Item list of a backward pass over k instance slots: with off == NULL,
 // cnt[p * k + q] <- tiles with work at step p of slot q; else items[] <- the
 // list, off[p * k + q] being the exclusive prefix of cnt in that order.
 cudaError_t launch_adj_list(const BatchAdjInst *inst, int k, int max_steps, int *cnt, const long long *off,
                             unsigned long long *items, cudaStream_t s);
-int batch_adj_blocks_per_sm();
-cudaError_t launch_adj_grad(const double *T, const double *lam, const unsigned char *W, const AdjGeom &geo,
-                            const EllipMedium &med, const fold3d_grid &g, double *dLdM, int accumulate, cudaStream_t s);
+int batch_adj_blocks_per_sm(bool f32);
+cudaError_t launch_adj_grad(const void *T, const void *lam, const unsigned char *W, const AdjGeom &geo,
+                            const EllipMedium &med, const fold3d_grid &g, void *dLdM, int accumulate, bool f32,
+                            cudaStream_t s);
 
 // Kernel launchers (fold3d_kernels.cu).  tab is required for kVariantFast.
 cudaError_t launch_plane(double *T, const PlaneGeom &pg, const LocalFrameH &L, const DirTable *tab,

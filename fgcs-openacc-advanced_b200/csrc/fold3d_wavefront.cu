@@ -48,6 +48,11 @@ namespace fold3d {
 namespace {
 
 __device__ __forceinline__ double ld_cg(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ float ld_cg(const float *p) { return __ldcg(p); }
+
+// Whether a stored value changes (bit patterns, so -0 vs +0 counts).
+__device__ __forceinline__ bool bits_differ(double a, double b) { return __double_as_longlong(a) != __double_as_longlong(b); }
+__device__ __forceinline__ bool bits_differ(float a, float b) { return __float_as_int(a) != __float_as_int(b); }
 
 }  // namespace
 
@@ -68,8 +73,8 @@ template <> struct WaveMedium<kMediumEllip> {
 // publish its flag.  Adds each changed point's |dT| into dmax and the
 // evaluated points into evaluated.  Returns false if a wait gave up (the
 // item is then left unpublished and the caller must leave).
-template <int MED>
-__device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs &a,
+template <int MED, class R>
+__device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
                                           const typename WaveMedium<MED>::type &tab, int item, double &dmax,
                                           unsigned long long &evaluated)
 {
@@ -120,30 +125,31 @@ __device__ __forceinline__ bool wave_item(double *__restrict__ T, const WaveArgs
         if (u <= g.nu && v <= g.nv) {
             const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
             const long long d = s + g.sn;
-            const double st = fabs(ld_cg(T + s));
-            const double xt = fabs(ld_cg(T + s + g.sx));
-            const double yt = fabs(ld_cg(T + s + g.sy));
-            const double xnt = fabs(ld_cg(T + s - g.sx));
-            const double ynt = fabs(ld_cg(T + s - g.sy));
-            const double txm = fabs(ld_cg(T + s + g.sx - g.sy));
-            const double txy = fabs(ld_cg(T + s + g.sx + g.sy));
-            const double tym = fabs(ld_cg(T + s - g.sx + g.sy));
-            const double txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
-            const double told = ld_cg(T + d);
-            double tnew;
+            const R st = fabs(ld_cg(T + s));
+            const R xt = fabs(ld_cg(T + s + g.sx));
+            const R yt = fabs(ld_cg(T + s + g.sy));
+            const R xnt = fabs(ld_cg(T + s - g.sx));
+            const R ynt = fabs(ld_cg(T + s - g.sy));
+            const R txm = fabs(ld_cg(T + s + g.sx - g.sy));
+            const R txy = fabs(ld_cg(T + s + g.sx + g.sy));
+            const R tym = fabs(ld_cg(T + s - g.sx + g.sy));
+            const R txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
+            const R told = ld_cg(T + d);
+            R tnew;
             if constexpr (MED == kMediumDrift) {
+                static_assert(sizeof(R) == 8, "the drift medium is solved in double");
                 tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
             } else {
-                const double nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
+                const R nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
                 int win;
-                tnew = point_update_ellip(told, st, nb, ell_local(tab.med, tab.dir, d), win);
-                if (a.winners && __double_as_longlong(tnew) != __double_as_longlong(told))
+                tnew = point_update_ellip(told, st, nb, ell_local<R>(tab.med, tab.dir, d), win);
+                if (a.winners && bits_differ(tnew, told))
                     a.winners[d] = (win < 0) ? (unsigned char)kNoWinner : (unsigned char)(a.dir * kEllipCands + win);
             }
-            if (__double_as_longlong(tnew) != __double_as_longlong(told)) {
+            if (bits_differ(tnew, told)) {
                 T[d] = tnew;
                 changed = 1;
-                dmax = fmax(dmax, fabs(tnew - told));
+                dmax = fmax(dmax, (double)fabs(tnew - told));
                 // mark the point's tile in the two other orientations
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
@@ -191,9 +197,9 @@ __device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsig
     __syncthreads();
 }
 
-template <int MED>
+template <int MED, class R>
 __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
-    wave_pass_kernel(double *__restrict__ T, WaveArgs a, const __grid_constant__ typename WaveMedium<MED>::type tab)
+    wave_pass_kernel(R *__restrict__ T, WaveArgs a, const __grid_constant__ typename WaveMedium<MED>::type tab)
 {
     __shared__ int s_next;
     const long long total = (long long)a.steps * a.ntu * a.ntv;
@@ -216,7 +222,7 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
             }
             s_next = it;
         }
-        if (!wave_item<MED>(T, a, tab, item, dmax, evaluated)) break;
+        if (!wave_item<MED, R>(T, a, tab, item, dmax, evaluated)) break;
     }
     wave_flush(dmax, evaluated, a.maxd, a.evaluated);
 }
@@ -230,6 +236,7 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
 // same instance) come earlier in that order, and the launch's claimed items
 // spread over many instances at once.
 // ---------------------------------------------------------------------------
+template <class R>
 __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads) batch_pass_kernel(BatchArgs b)
 {
     __shared__ int s_next;
@@ -267,45 +274,54 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads) batch_pass_
         __syncthreads();
         double dmax = 0.0;
         unsigned long long evaluated = 0;
-        if (!wave_item<kMediumEllip>(s_inst.T, s_inst.a, s_inst.p, s_loc[1], dmax, evaluated)) break;
+        if (!wave_item<kMediumEllip, R>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[1], dmax, evaluated))
+            break;
         wave_flush(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
     }
 }
 
-cudaError_t launch_batch_pass(const BatchArgs &b, int grid, cudaStream_t s)
+cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int grid, cudaStream_t s)
 {
-    batch_pass_kernel<<<grid, kWaveThreads, 0, s>>>(b);
+    if (f32) batch_pass_kernel<float><<<grid, kWaveThreads, 0, s>>>(b);
+    else batch_pass_kernel<double><<<grid, kWaveThreads, 0, s>>>(b);
     return cudaGetLastError();
 }
 
-int batch_blocks_per_sm()
+int batch_blocks_per_sm(bool f32)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel, kWaveThreads, 0) != cudaSuccess)
-        return 1;
+    const cudaError_t e =
+        f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<float>, kWaveThreads, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<double>, kWaveThreads, 0);
+    if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)
 {
-    wave_pass_kernel<kMediumDrift><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
+    wave_pass_kernel<kMediumDrift, double><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_pass_ellip(double *T, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s)
+cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s)
 {
-    wave_pass_kernel<kMediumEllip><<<grid, kWaveThreads, 0, s>>>(T, a, p);
+    if (f32) wave_pass_kernel<kMediumEllip, float><<<grid, kWaveThreads, 0, s>>>(static_cast<float *>(T), a, p);
+    else wave_pass_kernel<kMediumEllip, double><<<grid, kWaveThreads, 0, s>>>(static_cast<double *>(T), a, p);
     return cudaGetLastError();
 }
 
-int wave_blocks_per_sm(int medium)
+int wave_blocks_per_sm(int medium, bool f32)
 {
     int n = 0;
-    cudaError_t e = (medium == kMediumEllip)
-                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip>,
-                                                                        kWaveThreads, 0)
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumDrift>,
-                                                                        kWaveThreads, 0);
+    cudaError_t e;
+    if (medium == kMediumEllip)
+        e = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip, float>,
+                                                                kWaveThreads, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip, double>,
+                                                                kWaveThreads, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumDrift, double>, kWaveThreads,
+                                                          0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }

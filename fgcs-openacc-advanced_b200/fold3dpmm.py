@@ -37,7 +37,8 @@ EXPORTED = (
     "fold3d_exact_time", "fold3d_compat_set_grid", "fold3d_solve_noalloc", "fold3d_compat_plane",
     "fold3d_selftest_wait_timeout", "fold3d_ellip_metric", "fold3d_solve_ellip", "fold3d_solve_batch",
     "fold3d_adjoint_batch", "fold3d_init_implicit_device", "fold3d_write_text", "fold3d_write_vtk",
-    "fold3d_write_raw",
+    "fold3d_write_raw", "fold3d_solve_ellip_f32", "fold3d_solve_ellip_record_f32", "fold3d_adjoint_ellip_f32",
+    "fold3d_solve_batch_f32", "fold3d_adjoint_batch_f32",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
@@ -144,6 +145,12 @@ def lib() -> C.CDLL:
     L.acc_free.argtypes = [vp]
     L.acc_memcpy_to_device.argtypes = [vp, vp, C.c_size_t]
     L.acc_memcpy_from_device.argtypes = [vp, vp, C.c_size_t]
+    # the float32 build takes the same arguments (float fields)
+    L.fold3d_solve_ellip_f32.argtypes = list(L.fold3d_solve_ellip.argtypes)
+    L.fold3d_solve_ellip_record_f32.argtypes = list(L.fold3d_solve_ellip_record.argtypes)
+    L.fold3d_adjoint_ellip_f32.argtypes = list(L.fold3d_adjoint_ellip.argtypes)
+    L.fold3d_solve_batch_f32.argtypes = list(L.fold3d_solve_batch.argtypes)
+    L.fold3d_adjoint_batch_f32.argtypes = list(L.fold3d_adjoint_batch.argtypes)
     _lib = L
     return L
 
@@ -344,24 +351,42 @@ def solve_noalloc(T, h, med: Medium | None = None, o: Opts | None = None, stream
     return rep
 
 
+def _field_ptr(t):
+    """A float64 or float32 device field: (pointer, float32?)."""
+    import torch
+
+    if t.dtype not in (torch.float64, torch.float32) or not t.is_contiguous() or not t.is_cuda:
+        raise ValueError("device field must be a contiguous float64 or float32 CUDA tensor")
+    return C.c_void_p(t.data_ptr()), t.dtype == torch.float32
+
+
+def _entry(name, f32):
+    return getattr(lib(), name + ("_f32" if f32 else ""))
+
+
 def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> Report:
-    """Solve in place on a float64 CUDA tensor with an elliptical medium M
-    (six float32 CUDA tensors in the field layout)."""
+    """Solve in place on a float64 (or float32: the float32 build) CUDA
+    tensor with an elliptical medium M (six float32 CUDA tensors in the field
+    layout)."""
     nx, ny, nz = grid_of(T)
     rep = Report()
     e = ellip(M)
-    _check(lib().fold3d_solve_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), _dev_ptr(T),
-                                    C.byref(o or opts()), C.c_void_p(stream) if stream else None, C.byref(rep)))
+    ptr, f32 = _field_ptr(T)
+    _check(_entry("fold3d_solve_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr,
+                                             C.byref(o or opts()), C.c_void_p(stream) if stream else None,
+                                             C.byref(rep)))
     return rep
 
 
-def _check_like(name, X, T, itemsize, lead=()):
+def _check_like(name, X, T, itemsize=None, lead=()):
     """X must be a contiguous CUDA tensor of shape lead + T.shape with
-    itemsize-byte elements (the library writes that many bytes)."""
-    if not (X.is_cuda and X.is_contiguous() and X.element_size() == itemsize
-            and tuple(X.shape) == tuple(lead) + tuple(T.shape)):
-        raise ValueError("%s: need a contiguous CUDA tensor of shape %s with %d-byte elements"
-                         % (name, tuple(lead) + tuple(T.shape), itemsize))
+    itemsize-byte elements (the library writes that many bytes); itemsize
+    None: of T's dtype (a field-typed array)."""
+    ok = X.is_cuda and X.is_contiguous() and tuple(X.shape) == tuple(lead) + tuple(T.shape)
+    ok = ok and (X.dtype == T.dtype if itemsize is None else X.element_size() == itemsize)
+    if not ok:
+        raise ValueError("%s: need a contiguous CUDA tensor of shape %s and %s" % (
+            name, tuple(lead) + tuple(T.shape), T.dtype if itemsize is None else "%d-byte elements" % itemsize))
 
 
 def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream=None) -> Report:
@@ -371,27 +396,31 @@ def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream
     _check_like("W", W, T, 1)
     nx, ny, nz = grid_of(T)
     rep = Report()
-    _check(lib().fold3d_solve_ellip_record(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
+    ptr, f32 = _field_ptr(T)
+    _check(_entry("fold3d_solve_ellip_record", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), ptr,
                                            C.c_void_p(W.data_ptr()), C.byref(o or opts()),
                                            C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 
 def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, tol=0.0, stream=None) -> Report:
-    """fold3d_adjoint_ellip: lam <- dL/dT (total), dLdM (shape (6,)+T.shape,
-    float64) <- dL/dM, from the converged T, its winner record W and dLdT.
-    Backward sweeps stop once one pushes at most tol times the first sweep's
-    largest push (tol 0: once one pushes nothing)."""
+    """fold3d_adjoint_ellip(_f32): lam <- dL/dT (total), dLdM (shape
+    (6,)+T.shape) <- dL/dM, from the converged T, its winner record W and
+    dLdT (all of T's dtype).  Backward sweeps stop once one pushes at most
+    tol times the first sweep's largest push (tol 0: once one pushes
+    nothing)."""
     _check_like("W", W, T, 1)
-    _check_like("dLdT", dLdT, T, 8)
-    _check_like("lam", lam, T, 8)
-    _check_like("dLdM", dLdM, T, 8, lead=(6,))
+    _check_like("dLdT", dLdT, T)
+    _check_like("lam", lam, T)
+    _check_like("dLdM", dLdM, T, lead=(6,))
     nx, ny, nz = grid_of(T)
     rep = Report()
-    _check(lib().fold3d_adjoint_ellip(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), _dev_ptr(T),
-                                      C.c_void_p(W.data_ptr()), _dev_ptr(dLdT), _dev_ptr(lam),
-                                      C.c_void_p(dLdM.data_ptr()), int(max_sweeps), float(tol),
-                                      C.c_void_p(stream) if stream else None, C.byref(rep)))
+    ptr, f32 = _field_ptr(T)
+    _check(_entry("fold3d_adjoint_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), ptr,
+                                               C.c_void_p(W.data_ptr()), C.c_void_p(dLdT.data_ptr()),
+                                               C.c_void_p(lam.data_ptr()), C.c_void_p(dLdM.data_ptr()),
+                                               int(max_sweeps), float(tol), C.c_void_p(stream) if stream else None,
+                                               C.byref(rep)))
     return rep
 
 
@@ -402,17 +431,21 @@ def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream
     reports."""
     n = len(fields)
     arr = (Instance * n)()
+    kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
         arr[i].medium = ellip(M)
-        arr[i].T = _dev_ptr(T)
+        arr[i].T, f32 = _field_ptr(T)
+        kinds.add(f32)
         if winners is not None and winners[i] is not None:
             _check_like("winners[%d]" % i, winners[i], T, 1)
             arr[i].winners = winners[i].data_ptr()
+    if len(kinds) > 1:
+        raise ValueError("a batch is all float64 or all float32")
     reps = (Report * n)()
-    _check(lib().fold3d_solve_batch(ctx._h, n, arr, C.byref(o or opts()), C.c_void_p(stream) if stream else None,
-                                    reps))
+    _check(_entry("fold3d_solve_batch", kinds.pop())(ctx._h, n, arr, C.byref(o or opts()),
+                                                     C.c_void_p(stream) if stream else None, reps))
     return list(reps)
 
 
@@ -424,22 +457,27 @@ def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, m
     Returns the per-instance reports."""
     n = len(fields)
     arr = (AdjInstance * n)()
+    kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
         _check_like("winners[%d]" % i, winners[i], T, 1)
-        _check_like("dLdT[%d]" % i, dLdT[i], T, 8)
-        _check_like("lam[%d]" % i, lam[i], T, 8)
-        _check_like("dLdM[%d]" % i, dLdM[i], T, 8, lead=(6,))
+        _check_like("dLdT[%d]" % i, dLdT[i], T)
+        _check_like("lam[%d]" % i, lam[i], T)
+        _check_like("dLdM[%d]" % i, dLdM[i], T, lead=(6,))
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
         arr[i].medium = ellip(M)
-        arr[i].T = _dev_ptr(T)
+        arr[i].T, f32 = _field_ptr(T)
+        kinds.add(f32)
         arr[i].winners = winners[i].data_ptr()
-        arr[i].dLdT = _dev_ptr(dLdT[i])
-        arr[i].lambda_ = _dev_ptr(lam[i])
+        arr[i].dLdT = dLdT[i].data_ptr()
+        arr[i].lambda_ = lam[i].data_ptr()
         arr[i].dLdM = dLdM[i].data_ptr()
+    if len(kinds) > 1:
+        raise ValueError("a batch is all float64 or all float32")
     reps = (Report * n)()
-    _check(lib().fold3d_adjoint_batch(ctx._h, n, arr, int(max_sweeps), float(tol), int(bool(accumulate)),
-                                      C.c_void_p(stream) if stream else None, reps))
+    _check(_entry("fold3d_adjoint_batch", kinds.pop())(ctx._h, n, arr, int(max_sweeps), float(tol),
+                                                       int(bool(accumulate)), C.c_void_p(stream) if stream else None,
+                                                       reps))
     return list(reps)
 
 

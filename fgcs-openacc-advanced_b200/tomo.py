@@ -4,9 +4,9 @@ and its adjoint run in libfold3dpmm (fold3d_solve_ellip_record,
 fold3d_adjoint_ellip).
 
 EllipSolve.apply(T0, h, max_sweeps, tol, adj_tol, *M) returns the converged
-field for the initial field T0 (a point source) and a float64 metric M (six
-CUDA tensors, xx xy xz yy yz zz, field layout; the solver stores it as
-float32).  tol stops the forward sweeps (max |dT| <= tol), adj_tol the
+field for the initial field T0 (a point source; float64, or float32 for the
+float32 build) and a metric M (six CUDA tensors, xx xy xz yy yz zz, field
+layout; the solver stores it as float32).  tol stops the forward sweeps (max |dT| <= tol), adj_tol the
 backward ones (fold3d_adjoint_ellip's tol).
 Its backward pass returns dL/dM in float64, so torch carries the gradient on
 to whatever produced M (slowness, epsilon and axis through
@@ -49,6 +49,7 @@ class EllipSolve(torch.autograd.Function):
         M32 = [m.detach().to(torch.float32).contiguous() for m in M]
         T = T0.detach().clone()
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
+        ctx.mdtypes = [m.dtype for m in M]
         rep = _note("forward", f3d.solve_ellip_record(context(), T, h, M32, W,
                                                       f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol)))
         ctx.save_for_backward(T, W, *M32)
@@ -61,10 +62,10 @@ class EllipSolve(torch.autograd.Function):
     def backward(ctx, gT):
         T, W, *M32 = ctx.saved_tensors
         lam = torch.empty_like(T)
-        dLdM = torch.empty((6,) + tuple(T.shape), dtype=torch.float64, device=T.device)
-        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.contiguous(), lam, dLdM,
+        dLdM = torch.empty((6,) + tuple(T.shape), dtype=T.dtype, device=T.device)
+        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.to(T.dtype).contiguous(), lam, dLdM,
                                            tol=ctx.adj_tol))
-        return (None, None, None, None, None) + tuple(dLdM[m] for m in range(6))
+        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(6))
 
 
 def solve(T0, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):
@@ -83,6 +84,7 @@ class EllipSolveBatch(torch.autograd.Function):
         T = T0s.detach().clone().contiguous()
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         S = T.shape[0]
+        ctx.mdtypes = [m.dtype for m in M]
         reps = f3d.solve_batch(context(), [T[s] for s in range(S)], [h] * S, [M32] * S,
                                f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol),
                                winners=[W[s] for s in range(S)])
@@ -97,15 +99,15 @@ class EllipSolveBatch(torch.autograd.Function):
     def backward(ctx, gT):
         T, W, *M32 = ctx.saved_tensors
         S = T.shape[0]
-        gT = gT.contiguous()
+        gT = gT.to(T.dtype).contiguous()
         lam = torch.empty_like(T)
-        dLdM = torch.zeros((6,) + tuple(T.shape[1:]), dtype=torch.float64, device=T.device)
+        dLdM = torch.zeros((6,) + tuple(T.shape[1:]), dtype=T.dtype, device=T.device)
         reps = f3d.adjoint_batch(context(), [T[s] for s in range(S)], [ctx.h] * S, [M32] * S,
                                  [W[s] for s in range(S)], [gT[s] for s in range(S)], [lam[s] for s in range(S)],
                                  [dLdM] * S, tol=ctx.adj_tol, accumulate=True)
         for r in reps:
             _note("adjoint_batch", r)
-        return (None, None, None, None, None) + tuple(dLdM[m] for m in range(6))
+        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(6))
 
 
 def solve_batch(T0s, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):

@@ -241,6 +241,40 @@ typedef struct {
 int fold3d_adjoint_batch(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance *inst, int max_sweeps, double tol,
                          int accumulate, void *stream, fold3d_report *reps);
 
+/* Float32 build of the elliptical medium (no counterpart in the reference):
+ * the entry points above with float fields.  The local solver, the winner
+ * records and the adjoint compute in float arithmetic throughout (the metric
+ * arrays are float in both builds); dLdM is float too. */
+typedef struct {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    float *T;
+    unsigned char *winners;
+} fold3d_instance_f32;
+
+typedef struct {
+    fold3d_grid grid;
+    fold3d_ellip medium;
+    const float *T;
+    const unsigned char *winners;
+    const float *dLdT;
+    float *lambda;
+    float *dLdM;
+} fold3d_adjoint_instance_f32;
+
+int fold3d_solve_ellip_f32(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, float *T_dev,
+                           const fold3d_opts *o, void *stream, fold3d_report *rep);
+int fold3d_solve_ellip_record_f32(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, float *T_dev,
+                                  unsigned char *winners_dev, const fold3d_opts *o, void *stream,
+                                  fold3d_report *rep);
+int fold3d_adjoint_ellip_f32(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_ellip *m, const float *T_dev,
+                             const unsigned char *winners_dev, const float *dLdT_dev, float *lambda_dev,
+                             float *dLdM_dev, int max_sweeps, double tol, void *stream, fold3d_report *rep);
+int fold3d_solve_batch_f32(fold3d_ctx *ctx, int n, const fold3d_instance_f32 *inst, const fold3d_opts *o,
+                           void *stream, fold3d_report *reps);
+int fold3d_adjoint_batch_f32(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance_f32 *inst, int max_sweeps,
+                             double tol, int accumulate, void *stream, fold3d_report *reps);
+
 /* Implicit-surface source initialisation of a host field (the reference's
  * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).
  * Uses all host cores. */

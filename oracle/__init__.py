@@ -84,6 +84,8 @@ class Oracle:
         L.orc_ell_solve_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _int,
                                         _dbl, C.POINTER(_dbl)]
         L.orc_ell_solve_rec.restype = _int
+        L.orc_ellf_solve_rec.argtypes = list(L.orc_ell_solve_rec.argtypes)
+        L.orc_ellf_solve_rec.restype = _int
         L.orc_ell_adjoint_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _ptr,
                                           _ptr, _ptr]
         L.orc_ell_adjoint_rec.restype = C.c_long
@@ -144,6 +146,18 @@ class Oracle:
         d = _dbl(0.0)
         s = self.L.orc_ell_solve_rec(_p(T), ptrs, W.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2], nsweeps,
                                      tol, C.byref(d))
+        return s, d.value, W
+
+    def ellf_solve_rec(self, T, M, h, nsweeps, tol=-1.0):
+        """The float32 build (T: float32 field, in place): (sweeps, last
+        change, winner record)."""
+        if T.dtype != np.float32 or not T.flags.c_contiguous:
+            raise ValueError("need a contiguous float32 field")
+        arrs, ptrs = self._metric(M)
+        W = np.full(T.shape, 0xFF, dtype=np.uint8)
+        d = _dbl(0.0)
+        s = self.L.orc_ellf_solve_rec(T.ctypes.data_as(_ptr), ptrs, W.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1],
+                                      h[2], nsweeps, tol, C.byref(d))
         return s, d.value, W
 
     def ell_adjoint(self, T, M, h, W, r):

@@ -765,6 +765,177 @@ int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, doub
 }
 
 /* ------------------------------------------------------------------------ */
+/* The float32 build of the elliptical solver: the same computation with     */
+/* float fields and float arithmetic throughout (spacings rounded to float   */
+/* first, float literals, sqrtf), as the GPU's float instantiation.  x86-64  */
+/* evaluates float expressions in float (FLT_EVAL_METHOD 0).                 */
+/* ------------------------------------------------------------------------ */
+typedef struct { float xx, yy, zz, xy, xz, yz; } orc_aqf;
+
+static float orc_bff(const orc_aqf *A, int ui, int uj, int uk, int vi, int vj, int vk)
+{
+    return (float)(ui * vi) * A->xx + (float)(uj * vj) * A->yy + (float)(uk * vk) * A->zz +
+           (float)(ui * vj + uj * vi) * A->xy + (float)(ui * vk + uk * vi) * A->xz +
+           (float)(uj * vk + uk * vj) * A->yz;
+}
+
+static float ominf(float a, float b) { return (a < b) ? a : b; }
+
+static void orc_ellf_vertex(float *tn, int *win, int id, const orc_aqf *A, float tp, int i, int j)
+{
+    if (!(*tn > tp)) return;
+    const float c = orc_bff(A, -i, -j, 1, -i, -j, 1);
+    if (c > 0.0f) {
+        const float cand = tp + sqrtf(c);
+        if (cand < *tn) { *tn = cand; *win = id; }
+    }
+}
+
+static void orc_ellf_edge(float *tn, int *win, int id, const orc_aqf *A, float tp, float tq, int pi, int pj, int qi,
+                          int qj)
+{
+    if (!(*tn > ominf(tp, tq))) return;
+    const int ei = qi - pi, ej = qj - pj;
+    const float a = orc_bff(A, ei, ej, 0, ei, ej, 0);
+    const float b = orc_bff(A, ei, ej, 0, -pi, -pj, 1);
+    const float c = orc_bff(A, -pi, -pj, 1, -pi, -pj, 1);
+    const float d = tq - tp;
+    const float den = a - d * d;
+    const float disc = a * c - b * b;
+    if (den > 0.0f && disc > 0.0f) {
+        const float n = sqrtf(disc / den);
+        const float lam = (b - d * n) / a;
+        if (lam > 0.0f && lam < 1.0f) {
+            const float cand = tp + lam * d + n;
+            if (cand < *tn) { *tn = cand; *win = id; }
+        }
+    }
+}
+
+static void orc_ellf_tri(float *tn, int *win, int id, const orc_aqf *A, float t0, float ta, float tb, int ai, int aj,
+                         int bi, int bj)
+{
+    if (!(*tn > ominf(t0, ominf(ta, tb)))) return;
+    const float p11 = orc_bff(A, ai, aj, 0, ai, aj, 0);
+    const float p12 = orc_bff(A, ai, aj, 0, bi, bj, 0);
+    const float p22 = orc_bff(A, bi, bj, 0, bi, bj, 0);
+    const float q1 = orc_bff(A, ai, aj, 0, 0, 0, 1);
+    const float q2 = orc_bff(A, bi, bj, 0, 0, 0, 1);
+    const float c = A->zz;
+    const float d1 = ta - t0, d2 = tb - t0;
+    const float det = p11 * p22 - p12 * p12;
+    if (!(det > 0.0f)) return;
+    const float u1 = p22 * d1 - p12 * d2, u2 = p11 * d2 - p12 * d1;
+    const float w1 = p22 * q1 - p12 * q2, w2 = p11 * q2 - p12 * q1;
+    const float s = (d1 * u1 + d2 * u2) / det;
+    const float r = c - (q1 * w1 + q2 * w2) / det;
+    if (s < 1.0f && r > 0.0f) {
+        const float n = sqrtf(r / (1.0f - s));
+        const float l1 = (w1 - n * u1) / det, l2 = (w2 - n * u2) / det;
+        if (l1 > 0.0f && l2 > 0.0f && l1 + l2 < 1.0f) {
+            const float cand = t0 + (l1 * d1 + l2 * d2) + n;
+            if (cand < *tn) { *tn = cand; *win = id; }
+        }
+    }
+}
+
+static float orc_ellf_point(float told, float st, const float nb[8], const orc_aqf *A, int *win)
+{
+    float tn = fabsf(told);
+    *win = -1;
+    orc_ellf_vertex(&tn, win, 0, A, st, 0, 0);
+    float m = st;
+    for (int r = 0; r < 8; ++r) m = ominf(m, nb[r]);
+    if (tn > m) {
+        for (int r = 0; r < 8; ++r) orc_ellf_vertex(&tn, win, 1 + r, A, nb[r], ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) orc_ellf_edge(&tn, win, 9 + r, A, st, nb[r], 0, 0, ORC_RIM[r][0], ORC_RIM[r][1]);
+        for (int r = 0; r < 8; ++r) {
+            const int s = (r + 1) & 7;
+            orc_ellf_edge(&tn, win, 17 + r, A, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0],
+                          ORC_RIM[s][1]);
+        }
+        for (int r = 0; r < 8; ++r) {
+            const int s = (r + 1) & 7;
+            orc_ellf_tri(&tn, win, 25 + r, A, st, nb[r], nb[s], ORC_RIM[r][0], ORC_RIM[r][1], ORC_RIM[s][0],
+                         ORC_RIM[s][1]);
+        }
+    }
+    return ((told > 0.0f) ? 1.0f : -1.0f) * tn;
+}
+
+void orc_ellf_plane_rec(float *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                        double dy, double dz, int dir, int src)
+{
+    const orc_grid g = orc_make_grid(nx, ny, nz);
+    const orc_dir d = ORC_DIRS[dir];
+    const double h[3] = {dx, dy, dz};
+    const float hz = (float)h[d.nrm], hx = (float)h[d.xa], hy = (float)h[d.ya];
+    const int ax[3] = {d.xa, d.ya, d.nrm};
+    const int sgn[3] = {d.xs, d.ys, d.sg};
+    const int64_t sn = g.stride[d.nrm];
+    const int64_t sx = d.xs * g.stride[d.xa], sy = d.ys * g.stride[d.ya];
+    int u = (d.nrm == 0) ? 1 : 0;
+    int v = (d.nrm == 2) ? 1 : 2;
+    const int nu = g.n[u], nv = g.n[v];
+    const int64_t su = g.stride[u], sv = g.stride[v];
+#pragma omp parallel for schedule(static)
+    for (int b = 1; b <= nv; ++b)
+        for (int c = 1; c <= nu; ++c) {
+            const int64_t s = (int64_t)src * sn + (int64_t)c * su + (int64_t)b * sv;
+            const int64_t t = s + d.sg * sn;
+            orc_aqf A;
+            A.xx = M[orc_mi(ax[0], ax[0])][t] * hx * hx;
+            A.yy = M[orc_mi(ax[1], ax[1])][t] * hy * hy;
+            A.zz = M[orc_mi(ax[2], ax[2])][t] * hz * hz;
+            A.xy = (float)(sgn[0] * sgn[1]) * M[orc_mi(ax[0], ax[1])][t] * hx * hy;
+            A.xz = (float)(sgn[0] * sgn[2]) * M[orc_mi(ax[0], ax[2])][t] * hx * hz;
+            A.yz = (float)(sgn[1] * sgn[2]) * M[orc_mi(ax[1], ax[2])][t] * hy * hz;
+            float nb[8];
+            for (int r = 0; r < 8; ++r) nb[r] = fabsf(T[s + ORC_RIM[r][0] * sx + ORC_RIM[r][1] * sy]);
+            int win;
+            const float nvv = orc_ellf_point(T[t], fabsf(T[s]), nb, &A, &win);
+            if (W && memcmp(&nvv, &T[t], sizeof nvv) != 0)
+                W[t] = (win < 0) ? ORC_NOWIN : (unsigned char)(dir * ORC_NCAND + win);
+            T[t] = nvv;
+        }
+}
+
+/* Sweeps of the float32 build; semantics as orc_ell_solve_rec (the change
+ * of a sweep measured in float, reported as double). */
+int orc_ellf_solve_rec(float *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                       double dy, double dz, int nsweeps, double tol, double *last_delta)
+{
+    const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+    const int n[3] = {nx, ny, nz};
+    float *prev = (float *)malloc(cells * sizeof(float));
+    if (!prev) return -1;
+    int s = 0;
+    double delta = 0.0;
+    for (s = 0; s < nsweeps;) {
+        memcpy(prev, T, cells * sizeof(float));
+        for (int dir = 0; dir < 6; ++dir) {
+            const orc_dir d = ORC_DIRS[dir];
+            const int nn = n[d.nrm];
+            if (d.sg > 0)
+                for (int p = 1; p < nn; ++p) orc_ellf_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
+            else
+                for (int p = nn; p > 1; --p) orc_ellf_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
+        }
+        ++s;
+        delta = 0.0;
+        for (size_t c = 0; c < cells; ++c) {
+            const float df = T[c] - prev[c];
+            const double e = fabs((double)df);
+            if (e > delta) delta = e;
+        }
+        if (tol >= 0.0 && delta <= tol) break;
+    }
+    free(prev);
+    if (last_delta) *last_delta = delta;
+    return s;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Adjoint of the elliptical solver                                          */
 /* ------------------------------------------------------------------------ */
 /*

@@ -840,3 +840,95 @@ def test_device_initialiser_matches_host(f3d, ctx, cuda, golden, dims, h, med):
     T = cuda.empty(ref.shape, dtype=cuda.float64, device="cuda")
     f3d.init_implicit_device(ctx, T, h, m)
     assert_bitwise(T.cpu().numpy(), ref, "device init")
+
+
+# -- float32 build of the elliptical solver -----------------------------------
+
+@pytest.mark.parametrize("kind,dims,src", [("homog", (40, 40, 40), (21, 21, 21)),
+                                           ("tti", (37, 29, 33), (5, 20, 9))])
+def test_ellip_f32_matches_float_oracle(f3d, orc, ctx, cuda, kind, dims, src):
+    """The float32 build on the GPU equals the oracle's float statement bit
+    for bit (fields and winner records), after 3 fixed sweeps and when run
+    until nothing changes."""
+    h = (10.0, 10.0, 10.0)
+    M = _ell_case(kind, dims, h[0])
+    Md = [m.cuda() for m in M]
+    Mh = [m.numpy() for m in M]
+    T0 = orc.init_point(*dims, src).astype(np.float32)
+    for fixed, sweeps, tol in ((True, 3, 0.0), (False, 300, 0.0)):
+        ref = T0.copy()
+        s_ref, d_ref, W_ref = orc.ellf_solve_rec(ref, Mh, h, sweeps, tol=(-1.0 if fixed else tol))
+        d = cuda.from_numpy(T0.copy()).cuda()
+        W = cuda.empty(d.shape, dtype=cuda.uint8, device="cuda")
+        rep = f3d.solve_ellip_record(ctx, d, h, Md, W, f3d.opts(max_sweeps=sweeps, fixed=fixed, tol=tol))
+        assert rep.sweeps == s_ref
+        out = d.cpu().numpy()
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), \
+            "%d cells differ" % int((out.view(np.uint32) != ref.view(np.uint32)).sum())
+        assert np.array_equal(W.cpu().numpy(), W_ref)
+
+
+def test_adjoint_f32_matches_cpu_adjoint(f3d, orc, ctx, cuda):
+    """The float32 adjoint against the FP64 CPU adjoint of the same (float)
+    field and winner record, within float rounding."""
+    M, T0, rec = _adj_case(cuda)
+    Md = [m.cuda() for m in M]
+    T = T0.float().clone()
+    W = cuda.empty(T.shape, dtype=cuda.uint8, device="cuda")
+    f3d.solve_ellip_record(ctx, T, 10.0, Md, W, f3d.opts(max_sweeps=300, tol=0.0))
+    r = cuda.zeros_like(T)
+    r[rec] = T[rec] * 0.01 + 1.0
+    lam = cuda.empty_like(T)
+    g = cuda.empty((6,) + tuple(T.shape), dtype=cuda.float32, device="cuda")
+    rep = f3d.adjoint_ellip(ctx, T, 10.0, Md, W, r, lam, g)
+    assert rep.max_delta == 0.0
+    lr, gr, nc = orc.ell_adjoint(T.double().cpu().numpy(), [m.numpy() for m in M], (10.0,) * 3,
+                                 W.cpu().numpy(), r.double().cpu().numpy())
+    assert nc == 0
+    lam_h, g_h = lam.double().cpu().numpy(), g.double().cpu().numpy()
+    assert np.abs(lam_h - lr).max() <= 1e-4 * np.abs(lr).max()
+    assert np.linalg.norm(g_h - gr) <= 1e-4 * np.linalg.norm(gr)
+
+
+def test_batch_f32_equals_one_by_one(f3d, ctx, cuda):
+    import media
+
+    cases = [((30, 22, 26), (7, 9, 4), 41), ((19, 33, 24), (15, 3, 20), 42)]
+    Ms, Ts = [], []
+    for dims, src, seed in cases:
+        Ms.append([m.cuda() for m in media.heterogeneous_tti(*dims, 10.0, seed=seed)])
+        nx, ny, nz = dims
+        T = cuda.full((nz + 2, ny + 2, nx + 2), MAXT, dtype=cuda.float32, device="cuda")
+        T[src[2], src[1], src[0]] = 0.0
+        Ts.append(T)
+    o = f3d.opts(max_sweeps=300, tol=0.0)
+    Tb = [t.clone() for t in Ts]
+    f3d.solve_batch(ctx, Tb, [10.0] * 2, Ms, o)
+    for T, M, Tbat in zip(Ts, Ms, Tb):
+        T1 = T.clone()
+        f3d.solve_ellip(ctx, T1, 10.0, M, o)
+        assert cuda.equal(Tbat.view(cuda.int32), T1.view(cuda.int32))
+
+
+def test_batched_autograd_f32_close_to_f64(cuda):
+    """The float32 build through tomo.solve_batch: fields within float
+    rounding of the float64 build, gradients close (winners can differ where
+    candidates tie within float rounding)."""
+    import tomo
+
+    dims = (26, 22, 24)
+    srcs = [(4, 5, 3), (20, 17, 3)]
+    M, T0 = _batch_sources(cuda, dims, srcs, seed=51)
+    rec = (slice(None), 1, slice(1, -1, 2), slice(1, -1, 2))
+    out = {}
+    for dt in (cuda.float64, cuda.float32):
+        Mx = [m.double().requires_grad_(True) for m in M]
+        T = tomo.solve_batch(T0.to(dt), 10.0, Mx)
+        (0.5 * (T[rec].double() * 0.03) ** 2).sum().backward()
+        out[dt] = (T.detach().double(), [m.grad for m in Mx])
+    (T64, g64), (T32, g32) = out[cuda.float64], out[cuda.float32]
+    I = (slice(None), slice(1, -1), slice(1, -1), slice(1, -1))
+    assert float(((T32 - T64)[I]).abs().max() / T64[I].abs().max()) < 1e-6
+    num = sum(float((a - b).norm()) ** 2 for a, b in zip(g32, g64)) ** 0.5
+    den = sum(float(b.norm()) ** 2 for b in g64) ** 0.5
+    assert num <= 2e-2 * den, num / den
