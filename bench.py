@@ -259,7 +259,8 @@ def run_tti(args):
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     src = (n // 2 + 1, n // 2 + 1, n // 8 + 1)  # (i, j, k): centre column, depth index n/8
-    T0 = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=torch.float64, device="cuda")
+    fdt = torch.float32 if args.field_dtype == "f32" else torch.float64
+    T0 = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=fdt, device="cuda")
     T0[src[2], src[1], src[0]] = 0.0
     T = torch.empty_like(T0)
     ctx = f3d.Context(local)
@@ -304,13 +305,14 @@ def run_tti(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        nb_in = hT0.numel() * 8 + sum(m.numel() * 4 for m in hM)
+        nb_in = hT0.numel() * hT0.element_size() + sum(m.numel() * 4 for m in hM)
         e2e = {"value": world * upd * args.steps / (ems / 1e3) / 1e9, "unit": "Gcell-updates/s",
-               "h2d_bytes_per_step": nb_in, "d2h_bytes_per_step": hT0.numel() * 8,
+               "h2d_bytes_per_step": nb_in, "d2h_bytes_per_step": hT0.numel() * hT0.element_size(),
                "ms_per_step": ems / args.steps}
     peak, peak_kind = load_peaks()
     per_ms = solve_ms / args.steps
-    achieved = 40.0 * upd / (per_ms / 1e3) / 1e9
+    bpu = 40.0 if fdt == torch.float64 else 32.0  # field read + write, six float32 metric words
+    achieved = bpu * upd / (per_ms / 1e3) / 1e9
     launches = rep.sweeps * 6
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -328,22 +330,26 @@ def run_tti(args):
             while time.perf_counter() - t1 < args.cpu_seconds and planes < n - 1:
                 for d in range(6):
                     first, step = (1, 1) if d in (0, 2, 5) else (n, -1)
-                    orc.L.orc_ell_plane(Th.ctypes.data_as(C.c_void_p), ptrs, n, n, n, h, h, h, d,
-                                        first + step * planes)
+                    if fdt == torch.float32:
+                        orc.L.orc_ellf_plane_rec(Th.ctypes.data_as(C.c_void_p), ptrs, None, n, n, n, h, h, h, d,
+                                                 first + step * planes)
+                    else:
+                        orc.L.orc_ell_plane(Th.ctypes.data_as(C.c_void_p), ptrs, n, n, n, h, h, h, d,
+                                            first + step * planes)
                 planes += 1
                 upd_cpu += 6 * n * n
             dt = time.perf_counter() - t1
             cpu = {"value": upd_cpu / dt / 1e9, "unit": "Gcell-updates/s", "cores": host_threads(), "kind": "port",
                    "sample": "%d planes of each of the 6 passes of sweep 1 at %d^3 (%d updates), this "
-                             "repository's FP64 CPU statement of the elliptical solver (no reference "
-                             "implementation exists), OpenMP" % (planes, n, upd_cpu)}
+                             "repository's %s CPU statement of the elliptical solver (no reference "
+                             "implementation exists), OpenMP" % (planes, n, upd_cpu, args.field_dtype.upper())}
         except Exception as e:
             cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "port",
                    "sample": "unavailable: %s" % str(e).splitlines()[0]}
     out = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None, "dtype": args.field_dtype,
         "data": "synthetic: seeded heterogeneous tilted-elliptical medium (seed 0), point source",
         "config": {"workload": "TTI %d^3 h=10 m heterogeneous (seed 0), source (i,j,k)=%s, run to max|dT|<=1e-10"
                                % (n, src), "grid": n, "sweeps": rep.sweeps, "engine": "wavefront",
@@ -352,7 +358,7 @@ def run_tti(args):
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "kernel": "wave_pass_kernel<ellip>",
-                     "alg_bytes_per_update": 40, "note": "FP64-ALU bound"},
+                     "alg_bytes_per_update": bpu, "note": "ALU bound"},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary(),
         "solve_ms": per_ms, "evaluated_updates_per_step": rep.evaluated_updates, "medium_gen_s": gen_s,
     }
@@ -495,7 +501,7 @@ def run_adjoint(args):
                         device="cuda")
     rec = (1, ridx.view(-1, 1), ridx.view(1, -1))  # (k, j, i): top face
 
-    fdt = torch.float32 if args.adj_dtype == "f32" else torch.float64
+    fdt = torch.float32 if args.field_dtype == "f32" else torch.float64
 
     def t0_of(sp_):
         t = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=fdt, device="cuda")
@@ -575,7 +581,7 @@ def run_adjoint(args):
     out = {
         "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.adj_dtype,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.field_dtype,
         "data": "synthetic: seeded heterogeneous TTI true medium (seed 2), smoothed starting medium",
         "config": {"workload": "tomography gradient %d^3 h=10 m, %d sources (jittered %dx%d, k=11), %d receivers "
                                "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
@@ -619,8 +625,9 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
-    ap.add_argument("--adj-dtype", choices=["f64", "f32"], default="f64",
-                    help="--medium adjoint: float64 or the float32 build (fields, solver, adjoint)")
+    ap.add_argument("--field-dtype", choices=["f64", "f32"], default="f64",
+                    help="--medium tti/batch/adjoint: float64 fields, or the float32 build of the elliptical "
+                         "solver (and adjoint)")
     ap.add_argument("--adj-batch", type=int, default=64,
                     help="--medium adjoint: sources per batched forward solve and adjoint (1: one by one)")
     ap.add_argument("--adj-tol", type=float, default=1e-12,

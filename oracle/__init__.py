@@ -86,6 +86,8 @@ class Oracle:
         L.orc_ell_solve_rec.restype = _int
         L.orc_ellf_solve_rec.argtypes = list(L.orc_ell_solve_rec.argtypes)
         L.orc_ellf_solve_rec.restype = _int
+        L.orc_ellf_plane_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _int,
+                                         _int]
         L.orc_ell_adjoint_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _ptr,
                                           _ptr, _ptr]
         L.orc_ell_adjoint_rec.restype = C.c_long
