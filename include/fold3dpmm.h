@@ -49,7 +49,7 @@ extern "C" {
 #define FOLD3D_ERR_NOMEM 2       /* host or device allocation failed       */
 #define FOLD3D_ERR_CUDA 3        /* a CUDA runtime call failed             */
 #define FOLD3D_ERR_TIMEOUT 4     /* a bounded device-side wait gave up      */
-#define FOLD3D_ERR_UNSUPPORTED 5 /* valid request this build cannot serve  */
+#define FOLD3D_ERR_UNSUPPORTED 5 /* valid request the library cannot serve */
 
 /* Unreached time, Fold3dPMM.h:6 (MAXT). */
 #define FOLD3D_MAXT (10e15 * 1.0)

@@ -2,8 +2,8 @@
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its
 ``cpu_baseline`` leg and ``--impl reference``) may import this package, and
-only as the checker or the timed CPU baseline; the product library never
-does.
+only to check results or as the timed CPU baseline; the product library
+never does.
 
 Two oracles live here:
 

@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
  * calls this file; only tests/, __graft_entry__.smoke() and bench.py's
- * cpu_baseline leg use it, and only as the checker.
+ * cpu_baseline leg use it, to check results or to time the CPU path.
  *
  * It is a plain-C restatement of the reference's single-device path
  * (ezhilmathik/FGCS-OpenACC-Advanced, Stencil-OpenACC/AN_ISO_1_OpenACC.c and
