@@ -253,12 +253,19 @@ def run_tti(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
     dist = init_ranks(local)
-    n, h = args.size, 10.0
+    n, h = args.size, args.spacing
+    # grids above 768^3 are built in float32 (float64 temporaries would not fit)
+    gen_dtype = torch.float64 if n <= 768 else torch.float32
     t0 = time.perf_counter()
-    M = media.heterogeneous_tti(n, n, n, h, seed=0, device="cuda")
+    M = media.heterogeneous_tti(n, n, n, h, seed=0, device="cuda", dtype=gen_dtype)
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
-    src = (n // 2 + 1, n // 2 + 1, n // 8 + 1)  # (i, j, k): centre column, depth index n/8
+    gen_peak_gb = torch.cuda.max_memory_allocated() / 1e9
+    torch.cuda.empty_cache()
+    if args.source == "top":
+        src = (n // 2 + 1, n // 2 + 1, 1)  # (i, j, k): top-face centre
+    else:
+        src = (n // 2 + 1, n // 2 + 1, n // 8 + 1)  # centre column, depth index n/8
     fdt = torch.float32 if args.field_dtype == "f32" else torch.float64
     T0 = torch.full((n + 2,) * 3, 10e15 * 1.0, dtype=fdt, device="cuda")
     T0[src[2], src[1], src[0]] = 0.0
@@ -351,8 +358,9 @@ def run_tti(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.field_dtype,
         "data": "synthetic: seeded heterogeneous tilted-elliptical medium (seed 0), point source",
-        "config": {"workload": "TTI %d^3 h=10 m heterogeneous (seed 0), source (i,j,k)=%s, run to max|dT|<=1e-10"
-                               % (n, src), "grid": n, "sweeps": rep.sweeps, "engine": "wavefront",
+        "config": {"workload": "TTI %d^3 h=%g m heterogeneous (seed 0), source (i,j,k)=%s, run to max|dT|<=1e-10"
+                               % (n, h, src), "grid": n, "sweeps": rep.sweeps, "engine": "wavefront",
+                   "medium_construction": str(gen_dtype).replace("torch.", ""),
                    "skip": bool(args.skip), "medium": "6 float32 metric words per cell",
                    "l2": "field + medium %.1f GB > 126 MB L2" % ((n + 2) ** 3 * 32 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single"},
@@ -361,6 +369,7 @@ def run_tti(args):
                      "alg_bytes_per_update": bpu, "note": "ALU bound"},
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary(),
         "solve_ms": per_ms, "evaluated_updates_per_step": rep.evaluated_updates, "medium_gen_s": gen_s,
+        "medium_gen_peak_gb": gen_peak_gb,
     }
     if rank == 0:
         print(json.dumps(out))
@@ -627,6 +636,10 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
+    ap.add_argument("--spacing", type=float, default=10.0, help="--medium tti: grid spacing h (m)")
+    ap.add_argument("--source", choices=["depth", "top"], default="depth",
+                    help="--medium tti: point source in the centre column at depth index n/8, or at the "
+                         "top-face centre")
     ap.add_argument("--field-dtype", choices=["f64", "f32"], default="f64",
                     help="--medium tti/batch/adjoint: float64 fields, or the float32 build of the elliptical "
                          "solver (and adjoint)")

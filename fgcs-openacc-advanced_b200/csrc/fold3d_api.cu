@@ -152,7 +152,8 @@ struct fold3d_ctx {
     unsigned *w_counters = nullptr;          // [0] work, [1] status
     unsigned long long *w_evaluated = nullptr;
     unsigned epoch = 0;                      // passes run so far on this context (never decreases)
-    int sms = 0, wave_bps = 0, wave_bps_ell = 0, batch_bps = 0, batch_adj_bps = 0;
+    int sms = 0, batch_bps = 0, batch_adj_bps = 0;
+    int wave_bps[2][2][2] = {};              // [ellip][f32][large plane] resident CTAs per SM
     // batched solves: per-instance scratch and per-direction staging
     std::vector<int> bkey;                   // dims of the instances the scratch is sized for
     unsigned *b_scratch = nullptr;           // flags and change maps of all instances
@@ -411,8 +412,6 @@ static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
-        c->wave_bps = wave_blocks_per_sm(kMediumDrift);
-        c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
     c->key_wg = g;  // fresh flags and maps are zero, below every pass number to come
     return FOLD3D_OK;
@@ -494,15 +493,17 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
             a.dir = dir;
             a.winners = winners;
             const long long items = (long long)a.steps * a.ntu * a.ntv;
-            const int bps = em ? c->wave_bps_ell : c->wave_bps;
+            const bool large = (long long)a.ntu * a.ntv >= kLargePlaneTiles;
+            int &bps = c->wave_bps[em ? 1 : 0][f32 ? 1 : 0][large ? 1 : 0];
+            if (!bps) bps = wave_blocks_per_sm(em ? kMediumEllip : kMediumDrift, f32, large);
             const int grid = (int)std::min<long long>(items, (long long)c->sms * bps);
             if ((e = cudaMemsetAsync(a.work, 0, sizeof(unsigned), s)) != cudaSuccess)
                 return cuda_error(e, "cudaMemsetAsync");
             if (em) {
-                e = launch_wave_pass_ellip(T, f32, a, ellip_param(g, *em, dir), grid, s);
+                e = launch_wave_pass_ellip(T, f32, a, ellip_param(g, *em, dir), grid, s, large);
             } else {
                 build_dir_table(make_frame(g, *fm, dir), tab);
-                e = launch_wave_pass(static_cast<double *>(T), a, tab, grid, s);
+                e = launch_wave_pass(static_cast<double *>(T), a, tab, grid, s, large);
             }
             if (e != cudaSuccess) return cuda_error(e, "wavefront pass");
         }
@@ -597,8 +598,6 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
-        c->wave_bps = wave_blocks_per_sm(kMediumDrift);
-        c->wave_bps_ell = wave_blocks_per_sm(kMediumEllip);
     }
     if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm(false);
     if (!c->batch_adj_bps) c->batch_adj_bps = batch_adj_blocks_per_sm(false);

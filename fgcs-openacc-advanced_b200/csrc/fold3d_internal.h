@@ -71,6 +71,32 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #define FOLD3D_WAVE_TV 4
 #endif
 constexpr int kWaveTV = FOLD3D_WAVE_TV;
+
+// Resident CTAs per SM the forward dataflow kernels are compiled for (their
+// register budget is 65536 / (32 * kWaveTV * this)); build options.  Passes
+// over planes of fewer than kLargePlaneTiles tiles run best with fewer,
+// register-rich CTAs (no spills); passes over larger planes and batched
+// solves (many small instances) with more of them.  Measured with 32 x 4
+// tiles at 512^3 and 1280^3.
+#ifndef FOLD3D_WAVE_MINB_DRIFT
+#define FOLD3D_WAVE_MINB_DRIFT 7
+#endif
+#ifndef FOLD3D_WAVE_MINB_ELLIP
+#define FOLD3D_WAVE_MINB_ELLIP 6
+#endif
+#ifndef FOLD3D_WAVE_MINB_ELLIP_F32
+#define FOLD3D_WAVE_MINB_ELLIP_F32 8
+#endif
+#ifndef FOLD3D_WAVE_MINB_BATCH
+#define FOLD3D_WAVE_MINB_BATCH 8
+#endif
+#ifndef FOLD3D_WAVE_MINB_LARGE
+#define FOLD3D_WAVE_MINB_LARGE 8
+#endif
+#ifndef FOLD3D_WAVE_LARGE_TILES
+#define FOLD3D_WAVE_LARGE_TILES 8192
+#endif
+constexpr int kLargePlaneTiles = FOLD3D_WAVE_LARGE_TILES;
 static_assert(kWaveTV == 1 || kWaveTV == 2 || kWaveTV == 4 || kWaveTV == 8, "tile rows");
 
 // Arguments of one WAVEFRONT pass (fold3d_wavefront.cu).
@@ -117,10 +143,13 @@ constexpr unsigned kNoWinner = 0xffu;
 struct EllipDir;     // fold3d_ellip.cuh
 struct EllipParam;   // below, once EllipDir is complete
 
-cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s);
+// large: the variant compiled for passes over large planes (kLargePlaneTiles).
+cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s,
+                             bool large = false);
 // The elliptical medium's field is double, or float when f32.
-cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s);
-int wave_blocks_per_sm(int medium, bool f32 = false);
+cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s,
+                                   bool large = false);
+int wave_blocks_per_sm(int medium, bool f32 = false, bool large = false);
 
 }  // namespace fold3d
 #include "fold3d_ellip.cuh"

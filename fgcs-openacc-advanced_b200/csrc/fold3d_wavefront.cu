@@ -58,6 +58,13 @@ __device__ __forceinline__ bool bits_differ(float a, float b) { return __float_a
 
 constexpr int kWaveThreads = 32 * kWaveTV;
 
+template <int MED, class R, bool LARGE> constexpr int wave_min_blocks()
+{
+    return LARGE ? FOLD3D_WAVE_MINB_LARGE
+                 : MED == kMediumDrift ? FOLD3D_WAVE_MINB_DRIFT
+                                       : (sizeof(R) == 8 ? FOLD3D_WAVE_MINB_ELLIP : FOLD3D_WAVE_MINB_ELLIP_F32);
+}
+
 // Medium-dependent launch parameters: the drift medium's constant table, or
 // the elliptical medium's direction constants and metric arrays.
 template <int MED> struct WaveMedium;
@@ -197,8 +204,8 @@ __device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsig
     __syncthreads();
 }
 
-template <int MED, class R>
-__global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
+template <int MED, class R, bool LARGE>
+__global__ void __launch_bounds__(kWaveThreads, (wave_min_blocks<MED, R, LARGE>()))
     wave_pass_kernel(R *__restrict__ T, WaveArgs a, const __grid_constant__ typename WaveMedium<MED>::type tab)
 {
     __shared__ int s_next;
@@ -237,7 +244,7 @@ __global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads)
 // spread over many instances at once.
 // ---------------------------------------------------------------------------
 template <class R>
-__global__ void __launch_bounds__(kWaveThreads, 1024 / kWaveThreads) batch_pass_kernel(BatchArgs b)
+__global__ void __launch_bounds__(kWaveThreads, FOLD3D_WAVE_MINB_BATCH) batch_pass_kernel(BatchArgs b)
 {
     __shared__ int s_next;
     __shared__ int s_loc[2];
@@ -297,33 +304,45 @@ int batch_blocks_per_sm(bool f32)
     return n > 0 ? n : 1;
 }
 
-cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s)
+cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s, bool large)
 {
-    wave_pass_kernel<kMediumDrift, double><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
+    if (large) wave_pass_kernel<kMediumDrift, double, true><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
+    else wave_pass_kernel<kMediumDrift, double, false><<<grid, kWaveThreads, 0, s>>>(T, a, tab);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s)
+cudaError_t launch_wave_pass_ellip(void *T, bool f32, const WaveArgs &a, const EllipParam &p, int grid, cudaStream_t s,
+                                   bool large)
 {
-    if (f32) wave_pass_kernel<kMediumEllip, float><<<grid, kWaveThreads, 0, s>>>(static_cast<float *>(T), a, p);
-    else wave_pass_kernel<kMediumEllip, double><<<grid, kWaveThreads, 0, s>>>(static_cast<double *>(T), a, p);
+    float *tf = static_cast<float *>(T);
+    double *td = static_cast<double *>(T);
+    if (f32) {
+        if (large) wave_pass_kernel<kMediumEllip, float, true><<<grid, kWaveThreads, 0, s>>>(tf, a, p);
+        else wave_pass_kernel<kMediumEllip, float, false><<<grid, kWaveThreads, 0, s>>>(tf, a, p);
+    } else {
+        if (large) wave_pass_kernel<kMediumEllip, double, true><<<grid, kWaveThreads, 0, s>>>(td, a, p);
+        else wave_pass_kernel<kMediumEllip, double, false><<<grid, kWaveThreads, 0, s>>>(td, a, p);
+    }
     return cudaGetLastError();
 }
 
-int wave_blocks_per_sm(int medium, bool f32)
+template <class K> static int occupancy(K kernel)
 {
     int n = 0;
-    cudaError_t e;
-    if (medium == kMediumEllip)
-        e = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip, float>,
-                                                                kWaveThreads, 0)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumEllip, double>,
-                                                                kWaveThreads, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_pass_kernel<kMediumDrift, double>, kWaveThreads,
-                                                          0);
-    if (e != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kWaveThreads, 0) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+int wave_blocks_per_sm(int medium, bool f32, bool large)
+{
+    if (medium != kMediumEllip)
+        return large ? occupancy(wave_pass_kernel<kMediumDrift, double, true>)
+                     : occupancy(wave_pass_kernel<kMediumDrift, double, false>);
+    if (f32)
+        return large ? occupancy(wave_pass_kernel<kMediumEllip, float, true>)
+                     : occupancy(wave_pass_kernel<kMediumEllip, float, false>);
+    return large ? occupancy(wave_pass_kernel<kMediumEllip, double, true>)
+                 : occupancy(wave_pass_kernel<kMediumEllip, double, false>);
 }
 
 }  // namespace fold3d

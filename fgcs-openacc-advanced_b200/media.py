@@ -49,56 +49,91 @@ def homogeneous_ellip(nx, ny, nz, vz, eps, tilt_deg, azimuth_deg, device="cpu"):
 
 
 def _smooth(x, sigma):
-    """Periodic Gaussian smoothing of a float64 (nz, ny, nx) tensor."""
+    """Periodic Gaussian smoothing of a (nz, ny, nx) tensor (float64 or
+    float32; the result has its type).  The kernel is built from broadcast
+    1-D frequency axes and applied in place, to keep the temporaries to the
+    spectrum and one kernel array."""
     if sigma <= 0:
         return x
     spec = torch.fft.rfftn(x)
-    k = [torch.fft.fftfreq(n, device=x.device, dtype=torch.float64) for n in x.shape[:2]]
-    k.append(torch.fft.rfftfreq(x.shape[2], device=x.device, dtype=torch.float64))
-    kz, ky, kx = torch.meshgrid(*k, indexing="ij")
-    g = torch.exp(-2.0 * (math.pi * sigma) ** 2 * (kx * kx + ky * ky + kz * kz))
-    return torch.fft.irfftn(spec * g, s=x.shape)
+    ft = x.dtype
+    k = [torch.fft.fftfreq(n, device=x.device, dtype=ft) for n in x.shape[:2]]
+    k.append(torch.fft.rfftfreq(x.shape[2], device=x.device, dtype=ft))
+    kz, ky, kx = k[0].view(-1, 1, 1), k[1].view(1, -1, 1), k[2].view(1, 1, -1)
+    g = kx * kx + ky * ky + kz * kz
+    g.mul_(-2.0 * (math.pi * sigma) ** 2).exp_()
+    spec.mul_(g)
+    del g
+    return torch.fft.irfftn(spec, s=x.shape)
 
 
-def heterogeneous_tti(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
-    """Six float32 metric arrays of the seeded heterogeneous TTI medium."""
-    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies)
-    return [_pad(m) for m in metric_from(vz, eps, axis)]
+def heterogeneous_tti(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, dtype=torch.float64):
+    """Six float32 metric arrays of the seeded heterogeneous TTI medium.
+    dtype: working precision of the construction (float32 for grids too large
+    for float64 temporaries, e.g. 1280^3 on one GPU)."""
+    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=dtype)
+    M = metric_slabs(vz, eps, axis)
+    del vz, eps, axis
+    for k in range(6):
+        M[k] = _pad(M[k])
+    return M
 
 
-def tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, pad=False):
-    """The parameters of heterogeneous_tti(): float64 (vz, eps, (ax, ay, az))
-    on the interior (nz, ny, nx), or in the field layout with pad=True."""
+def tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, pad=False, dtype=torch.float64):
+    """The parameters of heterogeneous_tti(): (vz, eps, (ax, ay, az)) on the
+    interior (nz, ny, nx), or in the field layout with pad=True.  dtype is the
+    working precision: float64 (the default) or float32 for grids too large
+    for float64 temporaries (the random numbers are drawn in float64 either
+    way, from the same seeded stream).  Anomalies are accumulated from
+    broadcast 1-D coordinates and arrays are freed as soon as they are used,
+    so the peak is about twelve arrays of the grid's size."""
     gen = torch.Generator(device="cpu").manual_seed(seed)
     scale = max(nx, ny, nz) / 512.0
     shape = (nz, ny, nx)
     dev = torch.device(device)
-    k = torch.arange(nz, dtype=torch.float64, device=dev)
-    depth = (k * h).view(nz, 1, 1)
-    vz = (1500.0 + 0.8 * depth).expand(shape).clone()
-    zz, yy, xx = torch.meshgrid(*(torch.arange(n, dtype=torch.float64, device=dev) for n in shape), indexing="ij")
-    pert = torch.zeros(shape, dtype=torch.float64, device=dev)
+    kz = torch.arange(nz, dtype=dtype, device=dev).view(nz, 1, 1)
+    ky = torch.arange(ny, dtype=dtype, device=dev).view(1, ny, 1)
+    kx = torch.arange(nx, dtype=dtype, device=dev).view(1, 1, nx)
+    vz = (1500.0 + 0.8 * (kz * h)).expand(shape).clone()
+    pert = torch.zeros(shape, dtype=dtype, device=dev)
     for _ in range(anomalies):
         c = torch.rand(3, generator=gen, dtype=torch.float64) * torch.tensor([nz, ny, nx], dtype=torch.float64)
         sig = (20.0 + 40.0 * torch.rand(1, generator=gen, dtype=torch.float64).item()) * scale
         amp = 0.15 if torch.rand(1, generator=gen).item() < 0.5 else -0.15
-        r2 = (zz - c[0].item()) ** 2 + (yy - c[1].item()) ** 2 + (xx - c[2].item()) ** 2
-        pert += amp * torch.exp(-r2 / (2.0 * sig * sig))
-    del zz, yy, xx
-    vz = vz * (1.0 + pert)
+        r2 = (kz - c[0].item()) ** 2 + (ky - c[1].item()) ** 2 + (kx - c[2].item()) ** 2
+        r2.neg_().div_(2.0 * sig * sig).exp_().mul_(amp)
+        pert.add_(r2)
+        del r2
+    pert.add_(1.0)
+    vz.mul_(pert)
     del pert
     sig = 8.0 * scale
-    eps = _smooth((0.25 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev), sig)
-    th = torch.deg2rad(45.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev)
-    ph = torch.deg2rad(360.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev)
-    ax = _smooth(torch.sin(th) * torch.cos(ph), sig)
-    ay = _smooth(torch.sin(th) * torch.sin(ph), sig)
-    az = _smooth(torch.cos(th), sig)
+    eps = _smooth((0.25 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev, dtype), sig)
+    th = torch.deg2rad(45.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev, dtype)
+    ph = torch.deg2rad(360.0 * torch.rand(shape, generator=gen, dtype=torch.float64)).to(dev, dtype)
+    st = torch.sin(th)
+    ax = st * torch.cos(ph)
+    ay = st * torch.sin(ph)
+    del st
+    az = torch.cos(th)
     del th, ph
-    eps = eps.clamp(0.0, 0.25)
+    ax, ay, az = _smooth(ax, sig), _smooth(ay, sig), _smooth(az, sig)
+    eps = eps.clamp_(0.0, 0.25)
     if pad:
         return _pad(vz), _pad(eps), (_pad(ax), _pad(ay), _pad(az))
     return vz, eps, (ax, ay, az)
+
+
+def metric_slabs(vz, eps, n_axis, planes=64):
+    """metric_from() one block of z-planes at a time (the same values; the
+    temporaries are a block's, not the volume's)."""
+    nz = vz.shape[0]
+    out = [torch.empty(vz.shape, dtype=torch.float32, device=vz.device) for _ in range(6)]
+    for k0 in range(0, nz, planes):
+        sl = slice(k0, min(nz, k0 + planes))
+        for o, m in zip(out, metric_from(vz[sl], eps[sl], tuple(a[sl] for a in n_axis))):
+            o[sl] = m
+    return out
 
 
 def _smooth_edges(x, sigma):

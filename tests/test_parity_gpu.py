@@ -932,3 +932,48 @@ def test_batched_autograd_f32_close_to_f64(cuda):
     num = sum(float((a - b).norm()) ** 2 for a, b in zip(g32, g64)) ** 0.5
     den = sum(float(b.norm()) ** 2 for b in g64) ** 0.5
     assert num <= 2e-2 * den, num / den
+
+
+# -- the variants compiled for large planes -----------------------------------
+
+def test_large_plane_variant_drift_matches_planes(f3d, ctx, cuda):
+    """Planes of >= 8192 tiles (here the k-planes of 1024 x 1040) run the
+    kernel variant compiled for large planes; 8 sweeps equal the PLANES
+    engine bit for bit."""
+    dims = (1024, 1040, 5)
+    h = (0.01, 0.011, 0.012)
+    T0 = f3d.init_point(*dims, (500, 600, 3))
+    out = {}
+    for eng in ("planes", "wavefront"):
+        d = cuda.from_numpy(T0.copy()).cuda()
+        e = f3d.ENGINE_PLANES if eng == "planes" else f3d.ENGINE_WAVEFRONT
+        ctx.solve(d, h, None, f3d.opts(max_sweeps=8, fixed=True, engine=e))
+        out[eng] = d.cpu().numpy()
+    assert_bitwise(out["wavefront"], out["planes"], "large-plane variant")
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_large_plane_variant_ellip_matches_oracle(f3d, orc, ctx, cuda, dtype):
+    """The elliptical solver's large-plane variants (float64 and float32)
+    against the CPU statements, 3 sweeps.  The medium is built on the GPU:
+    torch's CPU irfftn crashes on such flat shapes (4 or 6 planes of
+    1040 x 1024)."""
+    import media
+
+    dims = (1024, 1040, 4)
+    h = (10.0, 10.0, 10.0)
+    Md = media.heterogeneous_tti(*dims, 10.0, seed=61, device="cuda")
+    Mh = [m.cpu().numpy() for m in Md]
+    T0 = orc.init_point(*dims, (300, 700, 2))
+    if dtype == "f32":
+        T0 = T0.astype(np.float32)
+        ref = T0.copy()
+        orc.ellf_solve_rec(ref, Mh, h, 3, tol=-1.0)
+    else:
+        ref = T0.copy()
+        orc.ell_solve(ref, Mh, h, 3, tol=-1.0)
+    d = cuda.from_numpy(T0.copy()).cuda()
+    f3d.solve_ellip(ctx, d, h, Md, f3d.opts(max_sweeps=3, fixed=True))
+    out = d.cpu().numpy()
+    w = np.uint32 if dtype == "f32" else np.uint64
+    assert np.array_equal(out.view(w), ref.view(w)), int((out.view(w) != ref.view(w)).sum())
