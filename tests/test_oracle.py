@@ -322,3 +322,19 @@ def test_writers_reject_bad_paths(f3d, tmp_path):
     T = np.zeros((5, 5, 5))
     with pytest.raises(RuntimeError):
         f3d.write_raw(str(tmp_path / "no" / "such" / "dir" / "t.raw"), T, 1.0)
+
+
+def test_heterogeneous_tti_float32_construction_close_to_float64():
+    """The float32 construction (used for grids too large for float64
+    temporaries) gives a positive-definite metric within float rounding of
+    the float64 construction."""
+    import media
+    import torch
+
+    a = media.heterogeneous_tti(30, 26, 34, 5.0, seed=3)
+    b = media.heterogeneous_tti(30, 26, 34, 5.0, seed=3, dtype=torch.float32)
+    for x, y in zip(a, b):
+        assert float((x.double() - y.double()).abs().max()) <= 1e-5 * float(x.double().abs().max())
+    xx, xy, xz, yy, yz, zz = (m.double() for m in b)
+    det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * xz) + xz * (xy * yz - yy * xz)
+    assert bool((xx > 0).all()) and bool((xx * yy - xy * xy > 0).all()) and bool((det > 0).all())
