@@ -122,3 +122,76 @@ def test_dropin_program_links_to_library():
         assert sym.get(s) == "U", s
     ldd = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
     assert "libfold3dpmm.so" in ldd and "libgomp" not in ldd
+
+
+def _prototypes():
+    """{name: number of parameters} of every function declared in
+    include/fold3dpmm.h."""
+    src = open(os.path.join(ROOT, "include", "fold3dpmm.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = "\n".join(ln for ln in src.splitlines() if not ln.lstrip().startswith("#"))
+    out = {}
+    for m in re.finditer(r"\b(\w+)\s*\(([^;{}]*?)\)\s*;", src):
+        name, params = m.group(1), m.group(2).strip()
+        if name in ("defined", "if", "sizeof"):
+            continue
+        depth, n = 0, (0 if params in ("", "void") else 1)
+        for ch in params:
+            depth += ch in "(["
+            depth -= ch in ")]"
+            n += ch == "," and depth == 0
+        out[name] = n
+    return out
+
+
+def test_binding_argument_counts_match_header(f3d):
+    """Every function the ctypes binding gives argtypes takes, in the header,
+    exactly that many parameters."""
+    protos = _prototypes()
+    L = f3d.lib()
+    checked = 0
+    for name, n in protos.items():
+        at = getattr(L, name).argtypes
+        if at is None:
+            continue
+        assert len(at) == n, "%s: header %d parameters, binding %d" % (name, n, len(at))
+        checked += 1
+    assert checked >= 25
+
+
+def test_struct_layouts_match_header(f3d, tmp_path):
+    """sizeof and field offsets of the header's structs, from a C program,
+    against the ctypes structures of the binding (the float32 instance
+    structs share the binding's double ones: every field is a pointer)."""
+    layouts = {
+        "fold3d_grid": (f3d.Grid, ["nx", "ny", "nz", "dx", "dy", "dz"]),
+        "fold3d_medium": (f3d.Medium, ["F", "ax", "ay", "az"]),
+        "fold3d_ellip": (f3d.Ellip, ["mxx", "mxy", "mxz", "myy", "myz", "mzz"]),
+        "fold3d_opts": (f3d.Opts, ["max_sweeps", "fixed", "tol", "engine", "skip", "variant"]),
+        "fold3d_report": (f3d.Report, ["sweeps", "max_delta", "elapsed_ms", "nominal_updates",
+                                       "evaluated_updates", "engine"]),
+        "fold3d_instance": (f3d.Instance, ["grid", "medium", "T", "winners"]),
+        "fold3d_instance_f32": (f3d.Instance, ["grid", "medium", "T", "winners"]),
+        "fold3d_adjoint_instance": (f3d.AdjInstance, ["grid", "medium", "T", "winners", "dLdT", "lambda",
+                                                      "dLdM"]),
+        "fold3d_adjoint_instance_f32": (f3d.AdjInstance, ["grid", "medium", "T", "winners", "dLdT", "lambda",
+                                                          "dLdM"]),
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fold3dpmm.h"', 'int main(void) {']
+    for cname, (_, fields) in layouts.items():
+        lines.append('printf("%s %%zu", sizeof(%s));' % (cname, cname))
+        for f in fields:
+            lines.append('printf(" %%zu", offsetof(%s, %s));' % (cname, f))
+        lines.append('printf("\\n");')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        name, *vals = ln.split()
+        got[name] = [int(v) for v in vals]
+    for cname, (S, fields) in layouts.items():
+        py = [C.sizeof(S)] + [getattr(S, f if f != "lambda" else "lambda_").offset for f in fields]
+        assert got[cname] == py, "%s: C %s, ctypes %s" % (cname, got[cname], py)
