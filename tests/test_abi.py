@@ -195,3 +195,16 @@ def test_struct_layouts_match_header(f3d, tmp_path):
     for cname, (S, fields) in layouts.items():
         py = [C.sizeof(S)] + [getattr(S, f if f != "lambda" else "lambda_").offset for f in fields]
         assert got[cname] == py, "%s: C %s, ctypes %s" % (cname, got[cname], py)
+
+
+def test_integration_c_example_compiles_and_links(f3d, tmp_path):
+    """The C caller shown in INTEGRATION.md compiles against the header and
+    links against the library as written."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    sec = doc[doc.index("## A C caller"):]
+    code = sec[sec.index("```c") + 4:sec.index("```", sec.index("```c") + 4)]
+    src = tmp_path / "caller.c"
+    src.write_text(code)
+    libdir = os.path.dirname(f3d.LIB_PATH)
+    subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                    str(tmp_path / "caller"), "-L", libdir, "-lfold3dpmm", "-Wl,-rpath," + libdir], check=True)
