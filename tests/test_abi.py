@@ -208,3 +208,15 @@ def test_integration_c_example_compiles_and_links(f3d, tmp_path):
     libdir = os.path.dirname(f3d.LIB_PATH)
     subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
                     str(tmp_path / "caller"), "-L", libdir, "-lfold3dpmm", "-Wl,-rpath," + libdir], check=True)
+
+
+def test_integration_adjoint_example_compiles(tmp_path):
+    """The elliptical/adjoint C example of INTEGRATION.md compiles as written."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    sec = doc[doc.index("## Elliptical medium, batches and the adjoint from C"):]
+    code = sec[sec.index("```c") + 4:sec.index("```", sec.index("```c") + 4)]
+    src = tmp_path / "gradient.c"
+    src.write_text(code)
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    subprocess.run(["gcc", "-Wall", "-Werror", "-c", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src),
+                    "-o", str(tmp_path / "gradient.o")], check=True)
