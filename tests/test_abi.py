@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -220,3 +221,39 @@ def test_integration_adjoint_example_compiles(tmp_path):
     cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
     subprocess.run(["gcc", "-Wall", "-Werror", "-c", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src),
                     "-o", str(tmp_path / "gradient.o")], check=True)
+
+
+def test_newer_entry_points_reject_null_context(f3d, tmp_path):
+    """Every entry point that takes a context rejects a NULL one (and NULL or
+    empty instance arrays) with FOLD3D_ERR_INVALID before touching a GPU."""
+    L = f3d.lib()
+    g = f3d.grid(8, 8, 8, 1.0)
+    e = f3d.Ellip()
+    for k in ("mxx", "mxy", "mxz", "myy", "myz", "mzz"):
+        setattr(e, k, 16)
+    o = f3d.opts()
+    rep = f3d.Report()
+    p = C.c_void_p(16)  # never dereferenced: the context is checked first
+    inst = (f3d.Instance * 1)()
+    adj = (f3d.AdjInstance * 1)()
+    calls = {
+        "fold3d_solve_ellip": lambda L, s: getattr(L, s)(None, C.byref(g), C.byref(e), p, C.byref(o), None,
+                                                          C.byref(rep)),
+        "fold3d_solve_ellip_record": lambda L, s: getattr(L, s)(None, C.byref(g), C.byref(e), p, p, C.byref(o),
+                                                                 None, C.byref(rep)),
+        "fold3d_adjoint_ellip": lambda L, s: getattr(L, s)(None, C.byref(g), C.byref(e), p, p, p, p, p, 10, 0.0,
+                                                            None, C.byref(rep)),
+        "fold3d_solve_batch": lambda L, s: getattr(L, s)(None, 1, inst, C.byref(o), None, None),
+        "fold3d_adjoint_batch": lambda L, s: getattr(L, s)(None, 1, adj, 10, 0.0, 0, None, None),
+    }
+    for name, call in calls.items():
+        for suffix in ("", "_f32"):
+            assert call(L, name + suffix) == f3d.ERR_INVALID, name + suffix
+    assert L.fold3d_solve_batch(None, 0, inst, C.byref(o), None, None) == f3d.ERR_INVALID
+    assert L.fold3d_solve_batch(None, 1, None, C.byref(o), None, None) == f3d.ERR_INVALID
+    assert L.fold3d_adjoint_batch(None, 0, adj, 10, 0.0, 0, None, None) == f3d.ERR_INVALID
+    assert L.fold3d_init_implicit_device(None, C.byref(g), C.byref(f3d.medium()), p, None) == f3d.ERR_INVALID
+    T = np.zeros((10, 10, 10))
+    for w in ("fold3d_write_text", "fold3d_write_raw"):
+        assert getattr(L, w)(None, T.ctypes.data_as(C.c_void_p), C.byref(g)) == f3d.ERR_INVALID
+    assert L.fold3d_write_vtk(None, T.ctypes.data_as(C.c_void_p), C.byref(g), 0) == f3d.ERR_INVALID
