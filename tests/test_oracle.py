@@ -338,3 +338,25 @@ def test_heterogeneous_tti_float32_construction_close_to_float64():
     xx, xy, xz, yy, yz, zz = (m.double() for m in b)
     det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * xz) + xz * (xy * yz - yy * xz)
     assert bool((xx > 0).all()) and bool((xx * yy - xy * xy > 0).all()) and bool((det > 0).all())
+
+
+def test_oracle_float_statement_close_to_double():
+    """The oracle's float32 statement of the elliptical solver (the float32
+    build's checker) converges and agrees with the FP64 statement to float
+    precision; its winner codes are valid."""
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    dims = (20, 18, 22)
+    M = [m.numpy() for m in media.heterogeneous_tti(*dims, 10.0, seed=3)]
+    T0 = o.init_point(*dims, (10, 9, 5))
+    Tf, Td = T0.astype(np.float32), T0.copy()
+    sf, df, Wf = o.ellf_solve_rec(Tf, M, (10.0,) * 3, 300, tol=0.0)
+    sd, dd, Wd = o.ell_solve_rec(Td, M, (10.0,) * 3, 300, tol=0.0)
+    assert df == 0.0 and dd == 0.0
+    I = (slice(1, -1),) * 3
+    assert np.abs(Tf[I] - Td[I]).max() <= 4e-7 * np.abs(Td[I]).max()
+    inner = Wf[I]
+    assert (inner == 0xFF).sum() == 1 and int(inner[inner != 0xFF].max()) < 6 * 33
+    assert (Wf[I] != Wd[I]).mean() < 0.05  # winners differ only where candidates tie within float rounding
