@@ -23,6 +23,8 @@
 #include <cstdint>
 #include <cstdlib>
 #include <functional>
+#include <memory>
+#include <new>
 #include <thread>
 #include <vector>
 
@@ -167,12 +169,10 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const long long sy = nx + 2, sz = (long long)(nx + 2) * (ny + 2);
     const size_t cells = (size_t)sz * (nz + 2);
-    std::vector<double> IF;
-    try {
-        IF.resize(cells);
-    } catch (...) {
-        return FOLD3D_ERR_NOMEM;
-    }
+    // not zero-filled: the parallel sampling pass writes (and first touches) every element
+    std::unique_ptr<double[]> IF_buf(new (std::nothrow) double[cells]);
+    if (!IF_buf) return FOLD3D_ERR_NOMEM;
+    double *const IF = IF_buf.get();
     const int nth = host_threads();
     const double hx = g->dx, hy = g->dy, hz = g->dz;
     // :137-147, node coordinates from x/y/z (:115-126)
@@ -184,7 +184,7 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
         return FOLD3D_ERR_NOMEM;
     }
     fold3d::surface_tables(*g, sin_x.data(), cos_yx.data(), nth);
-    fold3d::surface_planes(IF.data(), *g, 0, nz + 2, sin_x.data(), cos_yx.data(), nth);
+    fold3d::surface_planes(IF, *g, 0, nz + 2, sin_x.data(), cos_yx.data(), nth);
     parallel_for(0, nz + 2, nth, [&](int k) {
         for (long long id = sz * k; id < sz * (k + 1); ++id) T[id] = (side(IF[id]) * 1.0) * kMaxT;
     });
@@ -205,7 +205,7 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
             for (int k = 1; k < nz; ++k)
                 for (int j = 1; j < ny; ++j)
                     for (int i = i0; i <= i1; ++i)
-                        fold3d_seed::seed_voxel(IF.data(), sy, sz, h, i, j, k, kSteps, kBlends, node);
+                        fold3d_seed::seed_voxel(IF, sy, sz, h, i, j, k, kSteps, kBlends, node);
         });
     }
     return FOLD3D_OK;
