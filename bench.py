@@ -237,6 +237,45 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+# Directions in the solve's order (x_down, x_up, k_up, k_down, y_up, y_down):
+# normal axis (0 x, 1 y, 2 z) and step sign.
+_DIR_NRM = (0, 0, 2, 2, 1, 1)
+_DIR_SG = (1, -1, 1, -1, -1, 1)
+
+
+def oracle_ellip_sample(fields, media_h, hs, seconds, f32=False):
+    """The oracle's CPU statement of the elliptical solver (OpenMP) timed on a
+    bounded sample: the six passes of a first sweep of each instance in turn
+    (host fields, float64 or float32, and float32 metrics), until `seconds`
+    have passed.  Returns (cell updates per second, instances done,
+    updates)."""
+    import ctypes as C
+
+    from oracle import Oracle
+
+    orc = Oracle()
+    upd, done = 0, 0
+    t1 = time.perf_counter()
+    for T, M, h in zip(fields, media_h, hs):
+        nz, ny, nx = (int(v) - 2 for v in T.shape)
+        n = (nx, ny, nz)
+        arrs, ptrs = orc._metric(M)
+        Tp = T.ctypes.data_as(C.c_void_p)
+        for d in range(6):
+            nn = n[_DIR_NRM[d]]
+            planes = range(1, nn) if _DIR_SG[d] > 0 else range(nn, 1, -1)
+            for p in planes:
+                if f32:
+                    orc.L.orc_ellf_plane_rec(Tp, ptrs, None, nx, ny, nz, h, h, h, d, p)
+                else:
+                    orc.L.orc_ell_plane(Tp, ptrs, nx, ny, nz, h, h, h, d, p)
+            upd += (nn - 1) * (nx * ny * nz // nn)
+        done += 1
+        if time.perf_counter() - t1 >= seconds:
+            break
+    return upd / (time.perf_counter() - t1), done, upd
+
+
 def run_tti(args):
     """--medium tti: the 512^3 heterogeneous tilted-elliptical configuration
     (seeded medium, point source at depth index 64 of the centre column), each
@@ -452,6 +491,21 @@ def run_batch(args):
     cells = sum((d[0] + 2) * (d[1] + 2) * (d[2] + 2) for d in dims)
     peak, peak_kind = load_peaks()
     achieved = 40.0 * nominal / (batch_ms / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu:  # the first 16 instances, a first sweep each, within --cpu-seconds
+        try:
+            k = min(16, args.batch)
+            f32 = args.field_dtype == "f32"
+            rate, done, upd_cpu = oracle_ellip_sample([t.cpu().numpy() for t in T0[:k]],
+                                                      [[m.cpu().numpy() for m in Mi] for Mi in M[:k]],
+                                                      hs[:k], args.cpu_seconds, f32=f32)
+            cpu = {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": host_threads(), "kind": "port",
+                   "sample": "first sweep of %d of the first %d instances (%d updates), this repository's %s CPU "
+                             "statement of the elliptical solver (no reference implementation exists), OpenMP"
+                             % (done, k, upd_cpu, "F32" if f32 else "F64")}
+        except Exception as e:
+            cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "port",
+                   "sample": "unavailable: %s" % str(e).splitlines()[0]}
     out = {
         "metric": "Gcell-updates/s", "value": nominal / (batch_ms / 1e3) / 1e9, "unit": "Gcell-updates/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms,
@@ -466,6 +520,7 @@ def run_batch(args):
                      "traffic": None, "peak_kind": peak_kind, "kernel": "batch_pass_kernel",
                      "alg_bytes_per_update": 40},
         "evaluated_updates_per_step": evald, "clocks": clk.summary(), "medium_gen_s": gen_s,
+        "cpu_baseline": cpu,
         "gpu_launches": 6 * max(r.sweeps for r in reps) * args.steps,
     }
     print(json.dumps(out))

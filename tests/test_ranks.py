@@ -54,3 +54,27 @@ def test_reference_arm_runs_on_rank_0_only():
                        capture_output=True, text=True, timeout=300)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_oracle_sample_times_the_elliptical_statement():
+    """bench.py's CPU sample of the elliptical statement: runs the first
+    sweep of small instances (float64 and float32) and counts their updates."""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "fgcs-openacc-advanced_b200"))
+    import numpy as np
+
+    import bench
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    dims = [(9, 7, 8), (6, 10, 5)]
+    for f32 in (False, True):
+        fields = [o.init_point(*d, (2, 3, 2)) for d in dims]
+        if f32:
+            fields = [f.astype(np.float32) for f in fields]
+        Ms = [[m.numpy() for m in media.heterogeneous_tti(*d, 10.0, seed=1)] for d in dims]
+        rate, done, upd = bench.oracle_ellip_sample(fields, Ms, [10.0, 10.0], 60.0, f32=f32)
+        assert done == 2 and rate > 0
+        assert upd == sum(2 * ((nx - 1) * ny * nz + (ny - 1) * nx * nz + (nz - 1) * nx * ny) for nx, ny, nz in dims)
+        assert all(np.isfinite(f[1:-1, 1:-1, 1:-1]).all() and (f[1:-1, 1:-1, 1:-1] < 1e15).any() for f in fields)
