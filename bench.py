@@ -276,6 +276,26 @@ def oracle_ellip_sample(fields, media_h, hs, seconds, f32=False):
     return upd / (time.perf_counter() - t1), done, upd
 
 
+def oracle_adjoint_sample(T0, T, M, h, W, r, fwd_sweeps):
+    """The oracle's CPU statement of one source's gradient, timed in two
+    parts: one recording forward sweep (six passes, OpenMP) from the initial
+    field T0, and the whole FP64 adjoint (winner weights, cells by decreasing
+    time, dL/dM) from the converged field T, its winner record W and
+    r = dL/dT.  Host arrays; M as six float32 metric arrays.  Returns
+    (seconds per source-gradient = sweep time x fwd_sweeps + adjoint time,
+    sweep seconds, adjoint seconds)."""
+    from oracle import Oracle
+
+    orc = Oracle()
+    t1 = time.perf_counter()
+    orc.ell_solve_rec(T0.copy(), M, (h,) * 3, 1, tol=0.0)
+    sweep_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    orc.ell_adjoint(T, M, (h,) * 3, W, r)
+    adj_s = time.perf_counter() - t1
+    return sweep_s * fwd_sweeps + adj_s, sweep_s, adj_s
+
+
 def run_tti(args):
     """--medium tti: the 512^3 heterogeneous tilted-elliptical configuration
     (seeded medium, point source at depth index 64 of the centre column), each
@@ -644,6 +664,31 @@ def run_adjoint(args):
         adj = sum(r.elapsed_ms for r in ar) / len(ar)
         # one launch per direction pass (forward and backward), plus the gradient
         launches = sum(6 * r.sweeps for r in fr) + sum(6 * r.sweeps + 1 for r in ar)
+    cpu = {"value": None, "unit": "source-gradients/s", "cores": 0, "kind": "port",
+           "sample": "skipped: grids above 320^3 (the CPU adjoint's per-cell records need ~110 B a cell)"}
+    if not args.no_cpu and (n + 2) ** 3 <= 322 ** 3:
+        # source 0 in the starting medium, its field and winner record from one more (untimed) solve
+        try:
+            import fold3dpmm as f3d
+
+            M32 = [m.double().float().contiguous() for m in media.metric_from(1.0 / (1.0 / vz0), eps0, ax0)]
+            Tc = t0_of(srcs[0]).double()
+            T0h = Tc.cpu().numpy()
+            Wc = torch.empty(Tc.shape, dtype=torch.uint8, device="cuda")
+            f3d.solve_ellip_record(tomo.context(), Tc, h, M32, Wc, f3d.opts(max_sweeps=1000, fixed=False, tol=tol))
+            rh = torch.zeros_like(Tc)
+            rh[rec] = Tc[rec] - tobs[0].double()
+            Th, Wh, rh = Tc.cpu().numpy(), Wc.cpu().numpy(), rh.cpu().numpy()
+            Mh = [m.cpu().numpy() for m in M32]
+            del Tc, Wc, M32
+            sw = sum(r.sweeps for r in fr) / len(fr)
+            per_src, sweep_s, adj_s = oracle_adjoint_sample(T0h, Th, Mh, h, Wh, rh, sw)
+            cpu = {"value": 1.0 / per_src, "unit": "source-gradients/s", "cores": host_threads(), "kind": "port",
+                   "sample": "source 0: one recording forward sweep (%.2f s) x the GPU's mean %.1f forward sweeps "
+                             "+ the whole FP64 adjoint from its winner record (%.2f s); this repository's CPU "
+                             "statement (no reference implementation exists), OpenMP" % (sweep_s, sw, adj_s)}
+        except Exception as e:
+            cpu["sample"] = "unavailable: %s" % str(e).splitlines()[0]
     out = {
         "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -660,7 +705,7 @@ def run_adjoint(args):
         "adjoint_sweeps": [min(r.sweeps for r in ar), max(r.sweeps for r in ar)],
         "harness_ms_per_source": ms / nsrc - fwd - adj, "loss": loss,
         "grad_norms": {"slowness": float(gs.norm()), "eps": float(ge.norm())},
-        "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": launches,
+        "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": launches, "cpu_baseline": cpu,
     }
     print(json.dumps(out))
 

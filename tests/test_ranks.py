@@ -78,3 +78,31 @@ def test_oracle_sample_times_the_elliptical_statement():
         assert done == 2 and rate > 0
         assert upd == sum(2 * ((nx - 1) * ny * nz + (ny - 1) * nx * nz + (nz - 1) * nx * ny) for nx, ny, nz in dims)
         assert all(np.isfinite(f[1:-1, 1:-1, 1:-1]).all() and (f[1:-1, 1:-1, 1:-1] < 1e15).any() for f in fields)
+
+
+def test_oracle_adjoint_sample_times_forward_and_adjoint():
+    """bench.py's CPU sample of one source's gradient: one recording forward
+    sweep from the initial field (left untouched) plus the whole FP64 adjoint
+    from the converged field's winner record; the estimate adds the sweep
+    time times the forward sweep count to the adjoint time."""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "fgcs-openacc-advanced_b200"))
+    import numpy as np
+
+    import bench
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    d = (9, 7, 8)
+    T0 = o.init_point(*d, (2, 3, 2))
+    M = [m.numpy() for m in media.heterogeneous_tti(*d, 10.0, seed=1)]
+    T = T0.copy()
+    s, _, W = o.ell_solve_rec(T, M, (10.0,) * 3, 100, tol=0.0)
+    r = np.zeros_like(T)
+    r[1, 1:-1, 1:-1] = 1.0
+    before = T0.copy()
+    per_src, sweep_s, adj_s = bench.oracle_adjoint_sample(T0, T, M, 10.0, W, r, s)
+    assert np.array_equal(T0.view(np.uint64), before.view(np.uint64))
+    assert sweep_s > 0 and adj_s > 0
+    assert per_src == sweep_s * s + adj_s
