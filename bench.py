@@ -154,6 +154,19 @@ def max_over_ranks(ms, dist, device="cuda"):
     return float(t.item())
 
 
+def over_ranks(vals, dist, op, device="cuda"):
+    """Element-wise "sum" | "min" | "max" of every rank's list of numbers
+    (float64, exact for integers below 2^53); the list itself for a single
+    process."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op={"sum": dist.ReduceOp.SUM, "min": dist.ReduceOp.MIN, "max": dist.ReduceOp.MAX}[op])
+    return t.tolist()
+
+
 def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None):
     """Time the reference's own sweep functions (oracle/_ref, OpenMP
     transform on `threads` cores) on the first planes of each of the six
@@ -444,22 +457,34 @@ def run_batch(args):
     (seed 1000 + i) and a uniformly placed point source, each run to
     max|dT| <= 1e-10.  One step = one batched solve of all instances.  The
     same fields are also solved one after the other (fold3d_solve_ellip) to
-    give the batched launch's speed-up over sequential solves."""
+    give the batched launch's speed-up over sequential solves.  Under
+    torchrun the instances are split over the ranks, greedily by cell count
+    (shard.partition); each rank solves its part in one batch, with no
+    exchange, and the step time is the slowest rank's."""
     import numpy as np
     import torch
 
     import fold3dpmm as f3d
     import media
+    import shard
 
+    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.batch < world:
+        raise SystemExit("--batch %d is smaller than the %d ranks" % (args.batch, world))
     torch.cuda.set_device(local)
+    dist = init_ranks(local)
     rng = np.random.default_rng(1)
     lo, hi = args.batch_dims
     dims = [tuple(int(v) for v in rng.integers(lo, hi + 1, 3)) for _ in range(args.batch)]
     srcs = [tuple(int(rng.integers(1, d + 1)) for d in dd) for dd in dims]
+    parts = shard.partition([(d[0] + 2) * (d[1] + 2) * (d[2] + 2) for d in dims], world)
+    mine = parts[rank]
     t0 = time.perf_counter()
     M, T0 = [], []
-    for i, (dd, sp_) in enumerate(zip(dims, srcs)):
+    for i in mine:
+        dd, sp_ = dims[i], srcs[i]
         M.append(media.heterogeneous_tti(*dd, 10.0, seed=1000 + i, device="cuda"))
         nx, ny, nz = dd
         t = torch.full((nz + 2, ny + 2, nx + 2), 10e15 * 1.0,
@@ -473,11 +498,17 @@ def run_batch(args):
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     o = f3d.opts(max_sweeps=2000, fixed=False, tol=1e-10, skip=bool(args.skip))
-    hs = [10.0] * args.batch
+    hs = [10.0] * len(mine)
 
     def restore():
         for a, b in zip(T, T0):
             a.copy_(b)
+
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
 
     reps = None
     for _ in range(args.warmup):
@@ -488,31 +519,37 @@ def run_batch(args):
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             restore()
+            sync_all()
             ev0.record(stream)
             reps = f3d.solve_batch(ctx, T, hs, M, o, stream=sp)
             ev1.record(stream)
-            torch.cuda.synchronize()
+            sync_all()
             batch_ms += ev0.elapsed_time(ev1)
-    batch_ms /= args.steps
+    batch_ms = max_over_ranks(batch_ms / args.steps, dist)
     batched = [t.clone() for t in T]
     # the same solves one after the other
     restore()
     seq_reps = []
+    sync_all()
     ev0.record(stream)
-    for i in range(args.batch):
-        seq_reps.append(f3d.solve_ellip(ctx, T[i], 10.0, M[i], o, stream=sp))
+    for q in range(len(mine)):
+        seq_reps.append(f3d.solve_ellip(ctx, T[q], 10.0, M[q], o, stream=sp))
     ev1.record(stream)
-    torch.cuda.synchronize()
-    seq_ms = ev0.elapsed_time(ev1)
+    sync_all()
+    seq_ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     ibits = lambda t: t.view(torch.int64 if t.element_size() == 8 else torch.int32)
     same = all(torch.equal(ibits(a), ibits(b)) for a, b in zip(batched, T))
-    nominal = sum(r.nominal_updates for r in reps)
-    evald = sum(r.evaluated_updates for r in reps)
+    nominal, evald, nsame, launches = over_ranks(
+        [sum(r.nominal_updates for r in reps), sum(r.evaluated_updates for r in reps), int(same),
+         6 * max(r.sweeps for r in reps) * args.steps], dist, "sum")
+    smin, = over_ranks([min(r.sweeps for r in reps)], dist, "min")
+    smax, = over_ranks([max(r.sweeps for r in reps)], dist, "max")
     cells = sum((d[0] + 2) * (d[1] + 2) * (d[2] + 2) for d in dims)
     peak, peak_kind = load_peaks()
-    achieved = 40.0 * nominal / (batch_ms / 1e3) / 1e9
+    # per GPU: each rank's kernels move 40 B per update of its own instances
+    achieved = 40.0 * nominal / world / (batch_ms / 1e3) / 1e9
     cpu = None
-    if not args.no_cpu:  # the first 16 instances, a first sweep each, within --cpu-seconds
+    if rank == 0 and world == 1 and not args.no_cpu:  # the first 16 instances, a first sweep each, within --cpu-seconds
         try:
             k = min(16, args.batch)
             f32 = args.field_dtype == "f32"
@@ -528,23 +565,30 @@ def run_batch(args):
                    "sample": "unavailable: %s" % str(e).splitlines()[0]}
     out = {
         "metric": "Gcell-updates/s", "value": nominal / (batch_ms / 1e3) / 1e9, "unit": "Gcell-updates/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.field_dtype,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": args.field_dtype,
         "data": "synthetic: %d seeded heterogeneous TTI media and point sources" % args.batch,
         "config": {"workload": "batch of %d solves, dims per axis U[%d,%d] (seed 1), h=10 m, each run to "
                                "max|dT|<=1e-10" % (args.batch, lo, hi), "cells": cells,
-                   "sweeps_min_max": [min(r.sweeps for r in reps), max(r.sweeps for r in reps)],
-                   "engine": "wavefront batch", "skip": bool(args.skip)},
-        "sequential_ms": seq_ms, "speedup_vs_sequential": seq_ms / batch_ms, "batched_equals_sequential": same,
+                   "sweeps_min_max": [int(smin), int(smax)],
+                   "engine": "wavefront batch", "skip": bool(args.skip),
+                   "parallelism": "instances split over %d ranks by cells, no exchange" % world
+                   if world > 1 else "single",
+                   "instances_per_rank": [len(q) for q in parts]},
+        "sequential_ms": seq_ms, "speedup_vs_sequential": seq_ms / batch_ms,
+        "batched_equals_sequential": nsame == world,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "kernel": "batch_pass_kernel",
                      "alg_bytes_per_update": 40},
         "evaluated_updates_per_step": evald, "clocks": clk.summary(), "medium_gen_s": gen_s,
         "cpu_baseline": cpu,
-        "gpu_launches": 6 * max(r.sweeps for r in reps) * args.steps,
+        "gpu_launches": int(launches),
     }
-    print(json.dumps(out))
+    if rank == 0:
+        print(json.dumps(out))
     ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_adjoint(args):
@@ -559,15 +603,23 @@ def run_adjoint(args):
     (to max|dT| <= 1e-10) and the adjoint, through tomo.EllipSolve (torch
     autograd over the C-ABI), then torch's chain rule from the metric to
     slowness and eps.  The forward and adjoint library calls are also timed
-    on their own (CUDA events inside the library)."""
+    on their own (CUDA events inside the library).  Under torchrun the
+    sources are split over the ranks (shard.partition); each rank solves its
+    own sources in the whole medium, and the step ends with one sum over the
+    ranks of the loss and of the two gradient fields (NCCL all-reduce), so
+    every rank holds the survey's full gradient."""
     import numpy as np
     import torch
 
     import media
+    import shard
     import tomo
 
+    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
+    dist = init_ranks(local)
     n, h = args.adj_size, 10.0
     nsrc_side, nrec_side = 8, 64
     t0 = time.perf_counter()
@@ -583,6 +635,11 @@ def run_adjoint(args):
             i = int((a + 0.5) * cell + rng.uniform(-cell / 4, cell / 4)) + 1
             j = int((b + 0.5) * cell + rng.uniform(-cell / 4, cell / 4)) + 1
             srcs.append((min(max(i, 1), n), min(max(j, 1), n), 11))
+    nsrc = len(srcs)
+    if nsrc < world:
+        raise SystemExit("%d sources for %d ranks" % (nsrc, world))
+    parts = shard.partition([1] * nsrc, world)
+    srcs = [srcs[q] for q in parts[rank]]  # this rank's sources
     ridx = torch.tensor([1 + (n // nrec_side) // 2 + (n // nrec_side) * q for q in range(nrec_side)],
                         device="cuda")
     rec = (1, ridx.view(-1, 1), ridx.view(1, -1))  # (k, j, i): top face
@@ -616,7 +673,7 @@ def run_adjoint(args):
         e = eps0.clone().requires_grad_(True)
         Mg = [m.double() for m in media.metric_from(1.0 / s, e, ax0)]
         Ml = [m.detach().requires_grad_(True) for m in Mg]
-        loss = torch.zeros((), dtype=torch.float64, device="cuda")
+        loss = torch.zeros((1,), dtype=torch.float64, device="cuda")
         if B > 1:  # B sources per batched forward solve and batched adjoint
             for c0 in range(0, len(srcs), B):
                 T = tomo.solve_batch(T0s[c0:c0 + B], h, Ml, tol=tol, adj_tol=args.adj_tol)
@@ -630,23 +687,29 @@ def run_adjoint(args):
                 Ls.backward()
                 loss += Ls.detach()
         torch.autograd.backward(Mg, [m.grad for m in Ml])
+        shard.sum_over_ranks_([loss, s.grad, e.grad], dist)  # the survey's loss and gradient on every rank
         return float(loss), s.grad, e.grad
+
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
 
     for _ in range(args.warmup):
         step()
     reps.clear()
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
+    sync_all()
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             loss, gs, ge = step()
         ev1.record(stream)
-        torch.cuda.synchronize()
+        sync_all()
     tomo.collect_reports(None)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    nsrc = len(srcs)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist)
     if B > 1:
         fr = [r for k, r in reps if k == "forward_batch"]
         ar = [r for k, r in reps if k == "adjoint_batch"]
@@ -664,9 +727,12 @@ def run_adjoint(args):
         adj = sum(r.elapsed_ms for r in ar) / len(ar)
         # one launch per direction pass (forward and backward), plus the gradient
         launches = sum(6 * r.sweeps for r in fr) + sum(6 * r.sweeps + 1 for r in ar)
-    cpu = {"value": None, "unit": "source-gradients/s", "cores": 0, "kind": "port",
-           "sample": "skipped: grids above 320^3 (the CPU adjoint's per-cell records need ~110 B a cell)"}
-    if not args.no_cpu and (n + 2) ** 3 <= 322 ** 3:
+    launches = int(over_ranks([launches], dist, "sum")[0])
+    cpu = None  # timed on a single process only
+    if world == 1 and not args.no_cpu and (n + 2) ** 3 > 322 ** 3:
+        cpu = {"value": None, "unit": "source-gradients/s", "cores": 0, "kind": "port",
+               "sample": "skipped: grids above 320^3 (the CPU adjoint's per-cell records need ~110 B a cell)"}
+    elif world == 1 and not args.no_cpu:
         # source 0 in the starting medium, its field and winner record from one more (untimed) solve
         try:
             import fold3dpmm as f3d
@@ -688,18 +754,22 @@ def run_adjoint(args):
                              "+ the whole FP64 adjoint from its winner record (%.2f s); this repository's CPU "
                              "statement (no reference implementation exists), OpenMP" % (sweep_s, sw, adj_s)}
         except Exception as e:
-            cpu["sample"] = "unavailable: %s" % str(e).splitlines()[0]
+            cpu = {"value": None, "unit": "source-gradients/s", "cores": 0, "kind": "port",
+                   "sample": "unavailable: %s" % str(e).splitlines()[0]}
     out = {
         "metric": "source-gradients/s", "value": nsrc / (ms / 1e3), "unit": "source-gradients/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.field_dtype,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": args.field_dtype,
         "data": "synthetic: seeded heterogeneous TTI true medium (seed 2), smoothed starting medium",
         "config": {"workload": "tomography gradient %d^3 h=10 m, %d sources (jittered %dx%d, k=11), %d receivers "
                                "(%dx%d, k=1), loss 1/2 sum (t-t_obs)^2, solves to max|dT|<=1e-10"
                                % (n, nsrc, nsrc_side, nsrc_side, nrec_side ** 2, nrec_side, nrec_side),
                    "grid": n, "sources": nsrc, "receivers": nrec_side ** 2,
                    "gradient": "slowness and eps (torch autograd over the C-ABI)", "adjoint_tol": args.adj_tol,
-                   "sources_per_batch": B},
+                   "sources_per_batch": B,
+                   "parallelism": "sources split over %d ranks, gradient summed by all-reduce" % world
+                   if world > 1 else "single",
+                   "sources_per_rank": [len(q) for q in parts]},
         "forward_ms_per_source": fwd, "adjoint_ms_per_source": adj, "adjoint_over_forward": adj / fwd,
         "forward_sweeps": [min(r.sweeps for r in fr), max(r.sweeps for r in fr)],
         "adjoint_sweeps": [min(r.sweeps for r in ar), max(r.sweeps for r in ar)],
@@ -707,7 +777,10 @@ def run_adjoint(args):
         "grad_norms": {"slowness": float(gs.norm()), "eps": float(ge.norm())},
         "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": launches, "cpu_baseline": cpu,
     }
-    print(json.dumps(out))
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def workload_config(args):
