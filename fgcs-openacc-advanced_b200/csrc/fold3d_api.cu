@@ -98,8 +98,15 @@ static int check_grid(const fold3d_grid *g)
     if (!(g->dx > 0 && g->dy > 0 && g->dz > 0) || !std::isfinite(g->dx) ||
         !std::isfinite(g->dy) || !std::isfinite(g->dz))
         return set_error(FOLD3D_ERR_INVALID, "grid spacings must be finite and > 0");
-    const double cells = (double)(g->nx + 2) * (g->ny + 2) * (g->nz + 2);
+    const double n3[3] = {(double)g->nx, (double)g->ny, (double)g->nz};
+    const double cells = (n3[0] + 2) * (n3[1] + 2) * (n3[2] + 2);
     if (cells > 4.0e18 / 8) return set_error(FOLD3D_ERR_INVALID, "grid too large");
+    // The (plane, tile) items of one pass are counted in int.  Tiles hold at
+    // least 4 x 4 points in either orientation, so this bound is safe; it only
+    // rejects grids whose FP64 field alone exceeds 270 GB.
+    for (int a = 0; a < 3; ++a)
+        if (n3[a] * std::ceil(n3[(a + 1) % 3] / 4) * std::ceil(n3[(a + 2) % 3] / 4) > 2147483647.0)
+            return set_error(FOLD3D_ERR_INVALID, "grid too large");
     return FOLD3D_OK;
 }
 

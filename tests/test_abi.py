@@ -55,7 +55,10 @@ def test_null_arguments_rejected(f3d):
 
 
 @pytest.mark.parametrize("g,msg", [((1, 8, 8, 1.0), "sizes"), ((8, 8, 8, 0.0), "spacing"),
-                                   ((8, 8, 8, float("nan")), "spacing")])
+                                   ((8, 8, 8, float("nan")), "spacing"),
+                                   ((2 ** 31 - 1, 8, 8, 1.0), "too large"),
+                                   ((8, 2 ** 31 - 2, 2 ** 31 - 2, 1.0), "too large"),
+                                   ((70000, 70000, 70000, 1.0), "too large")])
 def test_bad_grid_rejected_before_any_launch(f3d, g, msg):
     L = f3d.lib()
     gr = f3d.Grid(g[0], g[1], g[2], g[3], g[3], g[3])
