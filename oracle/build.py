@@ -128,7 +128,7 @@ def build_ref(n: int, with_program: bool = False, force: bool = False) -> str:
     need_prog = with_program and (force or not _newer(prog, acc, init, __file__))
     if not (need_lib or need_prog):
         return outdir
-    with tempfile.TemporaryDirectory(prefix="fold3d_ref_") as tmp:
+    with tempfile.TemporaryDirectory(prefix="gen_", dir=outdir) as tmp:  # generated sources stay in _ref
         hdr = _gen_header(n, tmp)
         common = [*CFLAGS, "-w", "-include", hdr]
         if need_lib:
@@ -171,7 +171,7 @@ def build_dropin(n: int = 128, force: bool = False) -> str:
     if not os.path.exists(lib):
         raise RuntimeError("libfold3dpmm.so must be built first")
     os.makedirs(os.path.dirname(out), exist_ok=True)
-    with tempfile.TemporaryDirectory(prefix="fold3d_dropin_") as tmp:
+    with tempfile.TemporaryDirectory(prefix="gen_", dir=os.path.dirname(out)) as tmp:
         hdr = _gen_header(n, tmp)
         obj = os.path.join(tmp, "an_iso_1.o")
         _run(["gcc", *CFLAGS, "-w", "-fPIC", "-fno-inline", "-include", hdr, "-c", acc, "-o", obj])

@@ -14,8 +14,12 @@ for p in (ROOT, PKG):
         sys.path.insert(0, p)
 
 
+@pytest.hookimpl(tryfirst=True)
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (runs on the B200 box)")
+    # temporary files of the tests stay inside the checkout (git-ignored)
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, ".pytest_tmp")
 
 
 def bits(a):

@@ -66,7 +66,7 @@ def main():
         f["point_s8"] = P
         np.savez_compressed(os.path.join(HERE, "ref_n%d.npz" % n), **f)
     dig = {}
-    for n in (32, 64):
+    for n in (32, 37, 64, 99):  # 37 and 99: sizes that leave partial tiles on every axis
         build.build_ref(n)
         r = RefLib(n)
         T = r.init_implicit()
@@ -78,7 +78,7 @@ def main():
         dig["n%d_point_s8" % n] = sha(P)
     if "--dump128" in sys.argv:
         d = build.build_ref(128, with_program=True)
-        with tempfile.TemporaryDirectory() as tmp:
+        with tempfile.TemporaryDirectory(prefix="run_", dir=d) as tmp:
             subprocess.run([os.path.join(d, "an_iso_1_ref")], cwd=tmp, check=True,
                            stdout=subprocess.DEVNULL)
             with open(os.path.join(tmp, "an_iso_1_openacc.txt"), "rb") as fh:

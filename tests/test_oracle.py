@@ -44,7 +44,7 @@ def test_oracle_point_source_matches_reference(orc, golden, n):
     assert_bitwise(T, golden[n]["point_s8"], "point source")
 
 
-@pytest.mark.parametrize("n", [32, 64])
+@pytest.mark.parametrize("n", [32, 37, 64, 99])
 def test_oracle_digests_match_reference(orc, digests, n):
     h = (ref_spacing(n),) * 3
     T = orc.init_implicit(n, n, n, h)
@@ -105,10 +105,10 @@ def test_product_init_matches_reference(f3d, golden, n):
     assert_bitwise(T, golden[n]["init"], "product init n=%d" % n)
 
 
-def test_product_init_digest_64(f3d, digests):
-    n = 64
+@pytest.mark.parametrize("n", [37, 64, 99])
+def test_product_init_digest(f3d, digests, n):
     T = f3d.init_implicit(n, n, n, ref_spacing(n))
-    assert sha(T) == digests["n64_init"]
+    assert sha(T) == digests["n%d_init" % n]
 
 
 @pytest.mark.parametrize("dims,h", [((9, 6, 7), (0.7, 0.9, 1.1)), ((20, 13, 17), (0.5, 0.8, 0.6))])
