@@ -35,6 +35,7 @@
 // slot loop may visit the calls in any order; it keeps the reference's order.
 #pragma once
 #include <cstdint>
+#include <cstring>
 
 namespace fold3d {
 
@@ -86,12 +87,26 @@ constexpr unsigned kDivExpLo = 1023 - 400;
 constexpr unsigned kDivExpSpan = 800;
 
 #ifdef __CUDACC__
+// The functions below also compile for the host (IEEE double, fma, sqrt and
+// division correctly rounded on both sides, no contraction), where a test
+// runs them against the CPU statement of the reference.
+__host__ __device__ __forceinline__ unsigned hi_word(double x)
+{
+#ifdef __CUDA_ARCH__
+    return (unsigned)__double2hiint(x);
+#else
+    uint64_t b;
+    std::memcpy(&b, &x, sizeof b);
+    return (unsigned)(b >> 32);
+#endif
+}
+
 // Correctly rounded x / c for a constant c given r = RN(1/c) (r == 0: use
 // the IEEE division); see above.  Operands outside the safe range, zero
 // included, also take the IEEE division.
-__device__ __forceinline__ double div_by_const(double x, double c, double r)
+__host__ __device__ __forceinline__ double div_by_const(double x, double c, double r)
 {
-    const unsigned ex = ((unsigned)__double2hiint(x) >> 20) & 0x7ffu;
+    const unsigned ex = (hi_word(x) >> 20) & 0x7ffu;
     if (ex - kDivExpLo > kDivExpSpan || r == 0.0) return x / c;
     double q = x * r;
     double e = fma(-q, c, x);
@@ -100,9 +115,9 @@ __device__ __forceinline__ double div_by_const(double x, double c, double r)
     return fma(e, r, q);
 }
 
-__device__ __forceinline__ double kmin(double a, double b) { return (a < b) ? a : b; }
+__host__ __device__ __forceinline__ double kmin(double a, double b) { return (a < b) ? a : b; }
 
-__device__ __forceinline__ void edge_k(double &tn, double s0, double s1, const EdgeK &k, double F)
+__host__ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1, const EdgeK &k, double F)
 {
     if (tn < kmin(s1, s0) || (k.early && s1 > s0)) return;
     const double d = div_by_const(s1 - s0, k.hx, k.rhx);
@@ -120,8 +135,8 @@ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1, const E
     if (tn > s1 && k.fb_ok) tn = kmin(tn, s1 + k.K);
 }
 
-__device__ __forceinline__ void surf_k(double &tn, double s0, double s1, double s2, const SurfK &k,
-                                       const SideTable &t)
+__host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1, double s2, const SurfK &k,
+                                                const SideTable &t)
 {
     if (tn < kmin(s0, kmin(s1, s2)) || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
     const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
@@ -145,9 +160,9 @@ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1, double 
 
 // New signed value of a target whose stored value is `told`, from the nine
 // previous-plane magnitudes (named as in the reference, :195-204).
-__device__ __forceinline__ double point_update_fast(double told, double st, double xt, double yt,
-                                                    double xnt, double ynt, double txy, double txm,
-                                                    double tym, double txnyn, const DirTable *tab)
+__host__ __device__ __forceinline__ double point_update_fast(double told, double st, double xt, double yt,
+                                                             double xnt, double ynt, double txy, double txm,
+                                                             double tym, double txnyn, const DirTable *tab)
 {
     double tn = fabs(told);
     const SideTable &t = tab->side[told < 0 ? 1 : 0];

@@ -1,0 +1,85 @@
+"""The kernels' arithmetic core without a GPU: the library's point update
+(csrc/fold3d_fast.cuh) and direction tables (csrc/fold3d_tables.cpp), built
+for the host by tests/fast_solver_host.cu, swept over whole fields and
+compared bit for bit with the oracle's statement of the reference
+(Stencil-OpenACC/AN_ISO_1_OpenACC.c:59-326).  Both IEEE double builds round
+every operation on its own, so equal bits here are the bits the kernels
+compute: the folded constants, the division by constants without a divide
+instruction and the slot loops, over media and spacings the GPU tests do
+not reach, drifts close to F among them."""
+import ctypes as C
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, assert_bitwise
+from oracle import REF_A, REF_F, ref_spacing
+
+_dbl, _int, _ptr = C.c_double, C.c_int, C.c_void_p
+
+
+@pytest.fixture(scope="module")
+def host(tmp_path_factory):
+    import build as pkg_build  # fgcs-openacc-advanced_b200/build.py
+
+    out = str(tmp_path_factory.mktemp("fast_host") / "libfast_host.so")
+    cmd = [pkg_build.NVCC, "-O2", "-std=c++17", *pkg_build.ARCH, "--fmad=false", "-shared",
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", pkg_build.INCLUDE, "-I", pkg_build.CSRC,
+           os.path.join(ROOT, "tests", "fast_solver_host.cu"), os.path.join(pkg_build.CSRC, "fold3d_tables.cpp"),
+           "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    L = C.CDLL(out)
+    L.fast_host_sweeps.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int]
+    L.fast_host_sweeps.restype = _int
+    return L
+
+
+def _host_sweeps(host, T, h, F, a, sweeps):
+    nz, ny, nx = (s - 2 for s in T.shape)
+    host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps)
+
+
+# (dims, spacings, F, drift, source): the reference's medium and others, with
+# drifts from zero to 0.95 F
+CASES = [
+    ((37, 37, 37), None, REF_F, REF_A, "implicit"),
+    ((29, 21, 25), (0.7, 0.9, 1.1), REF_F, REF_A, "implicit"),
+    ((24, 17, 30), (0.41, 0.33, 0.5), 1.0, (0.0, 0.0, 0.0), "point"),
+    ((33, 35, 18), (1.0, 0.6, 0.8), 1.3, (0.2, -0.5, 0.3), "point"),
+    ((26, 26, 26), (0.5, 0.5, 0.5), 1.0, (0.55, -0.55, 0.55), "point"),
+    ((20, 31, 22), (0.3, 0.45, 0.4), 2.0, (-1.1, 0.6, -1.2), "implicit"),
+    ((21, 19, 23), (0.5, 0.5, 0.5), 1.0, (0.6, 0.5, 0.6), "point"),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[0])) + c[4])
+def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
+    dims, h, F, a, src = case
+    nx, ny, nz = dims
+    if h is None:
+        h = (ref_spacing(nx),) * 3
+    if src == "implicit":
+        T0 = orc.init_implicit(nx, ny, nz, h, F=F, a=a)
+    else:
+        T0 = orc.init_point(nx, ny, nz, (nx // 3 + 1, ny // 2 + 1, nz - 2))
+    ref = T0.copy()
+    orc.solve(ref, h, 8, F=F, a=a)
+    T = T0.copy()
+    _host_sweeps(host, T, h, F, a, 8)
+    assert_bitwise(T, ref, "host build of the point update")
+
+
+def test_host_build_matches_reference_digest_99(host, digests):
+    """The reference's own 8-sweep result at 99^3 (partial tiles on every
+    axis), through the host build."""
+    from oracle import Oracle
+
+    n = 99
+    h = (ref_spacing(n),) * 3
+    T = Oracle().init_implicit(n, n, n, h)
+    _host_sweeps(host, T, h, REF_F, REF_A, 8)
+    assert hashlib.sha256(np.ascontiguousarray(T).tobytes()).hexdigest() == digests["n99_s8"]
