@@ -33,6 +33,22 @@
 // current time, and every gate that depends on the current time only skips
 // calls that could not lower it, the update is min(T_old, candidates), so the
 // slot loop may visit the calls in any order; it keeps the reference's order.
+//
+// 3. One more such gate skips a FoldSurf3Points body (its nested edge still
+//    runs) when the current time is at most min(s0, s1, s2) + Bs.  The body
+//    solves the drift medium's eikonal F|p| + a.p = 1 for the plane wave
+//    through the three base values and takes the root whose ray, of
+//    direction F p/|p| + a, points from the base plane to the target (:152);
+//    it accepts the candidate only if that ray leaves the base triangle at a
+//    point inside it (:158-163).  The time there, interpolated linearly, is
+//    at least the smallest base value, and the ray then crosses the slab of
+//    width dzz between base and target, which takes at least dzz / (F + az):
+//    one time unit after leaving a point, the front is the sphere
+//    |x - a| = F.  Bs is that bound less a relative 1e-4, far above the
+//    body's rounding (below 1e-6 relative where F^2 >= 1.1 |a|^2, through
+//    the square root of a cancelled difference), and 0 for stronger drifts.
+//    FoldEdge2Points gets no such gate: its footpoint test (:88,92) does not
+//    follow its own ray, and its accepted candidates can lie below the bound.
 #pragma once
 #include <cstdint>
 #include <cstring>
@@ -67,6 +83,7 @@ struct SideTable {
     double F, az, hz;
     double g, rg;       // F*F - az*az, RN(1/g)          (:147)
     double K1;          // 1-D candidate increment dzz*dzz/q (:225)
+    double Bs;          // surf bodies skipped when the time is <= min(s0, s1, s2) + Bs (3. above)
     int d1_ok;          // 1-D candidate defined (:219, :223)
     // the per-call flags below as bit masks, bit k for call k
     unsigned m_e1, m_e2, m_nblock;  // surf[k].e1, .e2, .nblock
@@ -138,21 +155,24 @@ __host__ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1
 __host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1, double s2, const SurfK &k,
                                                 const SideTable &t)
 {
-    if (tn < kmin(s0, kmin(s1, s2)) || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
-    const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
-    const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
-    double dd = dx * dx + dy * dy;
-    double al = 1.0 - k.ax * dx - k.ay * dy;
-    double q = al * al - dd * t.g;
-    if (q > 0.0) {
-        al = div_by_const(-t.az * al + t.F * sqrt(q), t.g, t.rg);
-        const double g = s0 + t.hz * al;
-        if (g < tn && g > kmin(kmin(s0, s1), s2)) {
-            q = sqrt(dd + al * al);
-            dd = -t.hz / (t.F * al + t.az * q);
-            const double xe = dd * (t.F * dx + k.ax * q);
-            const double ye = dd * (t.F * dy + k.ay * q);
-            if (0.0 <= kmin(xe, ye) && ye * k.hx <= xe * k.hy && xe <= k.hx) tn = g;
+    const double mn = kmin(s0, kmin(s1, s2));
+    if (tn < mn || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
+    if (!(tn <= mn + t.Bs)) {  // 3. above
+        const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
+        const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
+        double dd = dx * dx + dy * dy;
+        double al = 1.0 - k.ax * dx - k.ay * dy;
+        double q = al * al - dd * t.g;
+        if (q > 0.0) {
+            al = div_by_const(-t.az * al + t.F * sqrt(q), t.g, t.rg);
+            const double g = s0 + t.hz * al;
+            if (g < tn && g > mn) {
+                q = sqrt(dd + al * al);
+                dd = -t.hz / (t.F * al + t.az * q);
+                const double xe = dd * (t.F * dx + k.ax * q);
+                const double ye = dd * (t.F * dy + k.ay * q);
+                if (0.0 <= kmin(xe, ye) && ye * k.hx <= xe * k.hy && xe <= k.hx) tn = g;
+            }
         }
     }
     if (tn > kmin(s1, s2) && !(k.nblock && s1 > s2)) edge_k(tn, s1, s2, k.nest, t.F);

@@ -25,6 +25,17 @@ double safe_recip(double c)
     return 1.0 / c;
 }
 
+// Skip bound of the FoldSurf3Points bodies of one side (fold3d_fast.cuh,
+// 3.): dzz / (F + az) less a relative 1e-4, or 0 (no skipping beyond the
+// reference's own gates) unless F^2 >= 1.1 |a|^2.
+double surf_skip_bound(double F, double ax, double ay, double az, double dzz)
+{
+    const double a2 = ax * ax + ay * ay + az * az;
+    if (!(F > 0.0 && dzz > 0.0 && F * F >= 1.1 * a2)) return 0.0;
+    const double B = dzz / (F + az) * (1.0 - 1e-4);
+    return (std::isfinite(B) && B > 0.0) ? B : 0.0;
+}
+
 // FoldEdge2Points call with arguments (F, ax, ay, az, dxx=hx, dzz=hz),
 // AN_ISO_1_OpenACC.c:59-114.
 EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double hz)
@@ -91,6 +102,7 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
     t.F = F;
     t.az = az;
     t.hz = hz;
+    t.Bs = surf_skip_bound(F, ax, ay, az, hz);
     t.g = F * F - az * az;  // :147
     t.rg = safe_recip(t.g);
     // 1-D normal candidate, :214-228, up to the final addition

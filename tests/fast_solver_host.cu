@@ -47,15 +47,19 @@ LocalFrameH host_frame(int dir, const double h[3], double F, const double a[3])
 
 }  // namespace
 
-// Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).
+// Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  With
+// surf_skip == 0 the tables' FoldSurf3Points skip bounds are cleared first.
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
-                                double a0, double a1, double a2, int sweeps)
+                                double a0, double a1, double a2, int sweeps, int surf_skip)
 {
     const int n[3] = {nx, ny, nz};
     const int64_t stride[3] = {1, (int64_t)nx + 2, ((int64_t)nx + 2) * (ny + 2)};
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
     DirTable tabs[6];
-    for (int dir = 0; dir < 6; ++dir) build_dir_table(host_frame(dir, h, F, a), tabs[dir]);
+    for (int dir = 0; dir < 6; ++dir) {
+        build_dir_table(host_frame(dir, h, F, a), tabs[dir]);
+        if (!surf_skip) tabs[dir].side[0].Bs = tabs[dir].side[1].Bs = 0.0;
+    }
     for (int s = 0; s < sweeps; ++s)
         for (int dir = 0; dir < 6; ++dir) {
             const HostDir &d = kHostDirs[dir];
@@ -77,4 +81,17 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
             }
         }
     return 0;
+}
+
+// The FoldSurf3Points skip bound of every direction and side, out[2 dir + side].
+extern "C" void fast_host_surf_bounds(double dx, double dy, double dz, double F, double a0, double a1, double a2,
+                                      double *out)
+{
+    const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
+    for (int dir = 0; dir < 6; ++dir) {
+        DirTable t;
+        build_dir_table(host_frame(dir, h, F, a), t);
+        out[2 * dir] = t.side[0].Bs;
+        out[2 * dir + 1] = t.side[1].Bs;
+    }
 }

@@ -5,8 +5,9 @@ compared bit for bit with the oracle's statement of the reference
 (Stencil-OpenACC/AN_ISO_1_OpenACC.c:59-326).  Both IEEE double builds round
 every operation on its own, so equal bits here are the bits the kernels
 compute: the folded constants, the division by constants without a divide
-instruction and the slot loops, over media and spacings the GPU tests do
-not reach, drifts close to F among them."""
+instruction, the slot loops and the skip of FoldSurf3Points bodies that
+cannot lower the time (csrc/fold3d_fast.cuh, 3.), over media and spacings
+the GPU tests do not reach, drifts close to F among them."""
 import ctypes as C
 import hashlib
 import os
@@ -33,18 +34,20 @@ def host(tmp_path_factory):
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     L = C.CDLL(out)
-    L.fast_host_sweeps.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int]
+    L.fast_host_sweeps.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int, _int]
     L.fast_host_sweeps.restype = _int
+    L.fast_host_surf_bounds.argtypes = [_dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _ptr]
+    L.fast_host_surf_bounds.restype = None
     return L
 
 
-def _host_sweeps(host, T, h, F, a, sweeps):
+def _host_sweeps(host, T, h, F, a, sweeps, surf_skip=True):
     nz, ny, nx = (s - 2 for s in T.shape)
-    host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps)
+    host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps, int(surf_skip))
 
 
 # (dims, spacings, F, drift, source): the reference's medium and others, with
-# drifts from zero to 0.95 F
+# drifts from zero to 0.98 F (the skip is off above 0.95 F)
 CASES = [
     ((37, 37, 37), None, REF_F, REF_A, "implicit"),
     ((29, 21, 25), (0.7, 0.9, 1.1), REF_F, REF_A, "implicit"),
@@ -53,6 +56,8 @@ CASES = [
     ((26, 26, 26), (0.5, 0.5, 0.5), 1.0, (0.55, -0.55, 0.55), "point"),
     ((20, 31, 22), (0.3, 0.45, 0.4), 2.0, (-1.1, 0.6, -1.2), "implicit"),
     ((21, 19, 23), (0.5, 0.5, 0.5), 1.0, (0.6, 0.5, 0.6), "point"),
+    ((40, 30, 50), (0.2, 0.05, 0.3), 1.0, (0.0, 0.0, 0.0), "point"),
+    ((24, 28, 20), (0.25, 0.3, 0.2), 1.5, (1.3, -0.3, 0.4), "implicit"),
 ]
 
 
@@ -68,9 +73,10 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
         T0 = orc.init_point(nx, ny, nz, (nx // 3 + 1, ny // 2 + 1, nz - 2))
     ref = T0.copy()
     orc.solve(ref, h, 8, F=F, a=a)
-    T = T0.copy()
-    _host_sweeps(host, T, h, F, a, 8)
-    assert_bitwise(T, ref, "host build of the point update")
+    for skip in (True, False):
+        T = T0.copy()
+        _host_sweeps(host, T, h, F, a, 8, skip)
+        assert_bitwise(T, ref, "host build of the point update, surf skip %s" % skip)
 
 
 def test_host_build_matches_reference_digest_99(host, digests):
@@ -83,3 +89,19 @@ def test_host_build_matches_reference_digest_99(host, digests):
     T = Oracle().init_implicit(n, n, n, h)
     _host_sweeps(host, T, h, REF_F, REF_A, 8)
     assert hashlib.sha256(np.ascontiguousarray(T).tobytes()).hexdigest() == digests["n99_s8"]
+
+
+def test_surf_skip_bounds_follow_the_closed_form(host):
+    """Each side's bound is dzz / (F + az) (1 - 1e-4), az the drift along the
+    normal towards the target (negated on the negative side), where
+    F^2 >= 1.1 |a|^2; 0 for stronger drifts."""
+    h = (0.7, 0.9, 1.1)
+    out = np.zeros(12)
+    host.fast_host_surf_bounds(*h, REF_F, *REF_A, out.ctypes.data)
+    dirs = [(0, +1), (0, -1), (2, +1), (2, -1), (1, -1), (1, +1)]  # normal axis, sign (x_down ... y_down)
+    for d, (nrm, sg) in enumerate(dirs):
+        for side in (0, 1):
+            az = sg * REF_A[nrm] * (-1 if side else 1)
+            assert out[2 * d + side] == pytest.approx(h[nrm] / (REF_F + az) * (1 - 1e-4), rel=1e-14)
+    host.fast_host_surf_bounds(*h, 1.0, 0.6, 0.5, 0.6, out.ctypes.data)  # |a| = 0.98 F
+    assert not out.any()
