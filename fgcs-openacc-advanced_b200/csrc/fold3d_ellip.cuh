@@ -19,6 +19,18 @@
 // time, so, like the drift solver, the update is min(T_old, candidates): the
 // WAVEFRONT engine's tile skipping holds unchanged.
 //
+// Each candidate is t(p) + ||X - p||_M at a point p of its vertex, edge or
+// triangle (the closed forms are the exact stationary values), and t(p) is
+// at least the smallest time it is built from.  ||X - p||_M is at least
+// B = min over the whole source plane of ||X - p||_M, which in the scaled
+// local frame (X = (0, 0, 1)) is the square root of the Schur complement
+// Azz - [Axz Ayz] [[Axx Axy] [Axy Ayy]]^-1 [Axz Ayz]^T.  So a candidate is
+// only computed while the running time is above its smallest input plus
+// B (1 - 1e-3): a candidate skipped that way could not have lowered it.  The
+// margin 1e-3 is far above the rounding of the closed forms near that bound
+// (their square roots are well conditioned there), in float as in double;
+// with B = 0 (a rounded Schur complement <= 0) the gates are the plain ones.
+//
 // oracle/fold3d_oracle.c (orc_ell_*) states the same computation on the
 // CPU; this file follows it operation by operation (no FMA contraction), so
 // the two agree bit for bit.
@@ -46,7 +58,8 @@ struct EllipParam {
 #ifdef __CUDACC__
 // The solver is written once for the field's type R: double (the default
 // build) or float (the float32 build).  All arithmetic stays in R (literals
-// included), so the float build is float arithmetic throughout.
+// included), so the float build is float arithmetic throughout.  It also
+// compiles for the host, where a test runs it against the CPU statement.
 
 // Local metric scaled by the spacings (Axx = M'xx hx hx, Axy = M'xy hx hy, ...).
 template <class R> struct EllipAT {
@@ -54,27 +67,49 @@ template <class R> struct EllipAT {
 };
 using EllipA = EllipAT<double>;
 
-template <class R> __device__ __forceinline__ R ell_sqrt(R x);
-template <> __device__ __forceinline__ double ell_sqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float ell_sqrt<float>(float x) { return sqrtf(x); }
+template <class R> __host__ __device__ __forceinline__ R ell_sqrt(R x);
+template <> __host__ __device__ __forceinline__ double ell_sqrt<double>(double x) { return sqrt(x); }
+template <> __host__ __device__ __forceinline__ float ell_sqrt<float>(float x) { return sqrtf(x); }
+
+// A read-only metric word (through the read-only data cache on the device).
+__host__ __device__ __forceinline__ float ell_ld(const float *p)
+{
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
 
 // u^T M' v with u = (ui hx, uj hy, uk hz) and v likewise.
 template <class R>
-__device__ __forceinline__ R ell_bf(const EllipAT<R> &A, int ui, int uj, int uk, int vi, int vj, int vk)
+__host__ __device__ __forceinline__ R ell_bf(const EllipAT<R> &A, int ui, int uj, int uk, int vi, int vj, int vk)
 {
     return (R)(ui * vi) * A.xx + (R)(uj * vj) * A.yy + (R)(uk * vk) * A.zz + (R)(ui * vj + uj * vi) * A.xy +
            (R)(ui * vk + uk * vi) * A.xz + (R)(uj * vk + uk * vj) * A.yz;
 }
 
-template <class R> __device__ __forceinline__ R ell_min(R a, R b) { return (a < b) ? a : b; }
+template <class R> __host__ __device__ __forceinline__ R ell_min(R a, R b) { return (a < b) ? a : b; }
+
+// B (1 - 1e-3), B the smallest ||X - p||_M over the source plane (header
+// comment), or 0 when the rounded Schur complement is not positive.
+template <class R> __host__ __device__ __forceinline__ R ell_skip_bound(const EllipAT<R> &A)
+{
+    const R cof = A.xx * A.yy - A.xy * A.xy;
+    if (!(cof > R(0))) return R(0);
+    const R sch = A.zz - (A.xz * (A.xz * A.yy - A.yz * A.xy) + A.yz * (A.yz * A.xx - A.xz * A.xy)) / cof;
+    return (sch > R(0)) ? ell_sqrt(sch) * R(0.999) : R(0);
+}
 
 // Candidate ids (the adjoint's winner record): 0 vertex st, 1+r rim vertex r,
 // 9+r spoke st-rim[r], 17+r rim edge rim[r]-rim[r+1], 25+r triangle
-// (st, rim[r], rim[r+1]).  Each routine sets win when it lowers tn.
+// (st, rim[r], rim[r+1]).  Each routine sets win when it lowers tn, and runs
+// only while tn is above its smallest input time plus gate (ell_skip_bound).
 template <class R>
-__device__ __forceinline__ void ell_vertex(R &tn, int &win, int id, const EllipAT<R> &A, R tp, int i, int j)
+__host__ __device__ __forceinline__ void ell_vertex(R &tn, int &win, int id, const EllipAT<R> &A, R gate, R tp, int i,
+                                                    int j)
 {
-    if (!(tn > tp)) return;
+    if (!(tn > tp + gate)) return;
     const R c = ell_bf(A, -i, -j, 1, -i, -j, 1);
     if (c > R(0)) {
         const R cand = tp + ell_sqrt(c);
@@ -86,10 +121,10 @@ __device__ __forceinline__ void ell_vertex(R &tn, int &win, int id, const EllipA
 }
 
 template <class R>
-__device__ __forceinline__ void ell_edge(R &tn, int &win, int id, const EllipAT<R> &A, R tp, R tq, int pi, int pj,
-                                         int qi, int qj)
+__host__ __device__ __forceinline__ void ell_edge(R &tn, int &win, int id, const EllipAT<R> &A, R gate, R tp, R tq,
+                                                  int pi, int pj, int qi, int qj)
 {
-    if (!(tn > ell_min(tp, tq))) return;
+    if (!(tn > ell_min(tp, tq) + gate)) return;
     const int ei = qi - pi, ej = qj - pj;
     const R a = ell_bf(A, ei, ej, 0, ei, ej, 0);
     const R b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
@@ -111,10 +146,10 @@ __device__ __forceinline__ void ell_edge(R &tn, int &win, int id, const EllipAT<
 }
 
 template <class R>
-__device__ __forceinline__ void ell_tri(R &tn, int &win, int id, const EllipAT<R> &A, R t0, R ta, R tb, int ai,
-                                        int aj, int bi, int bj)
+__host__ __device__ __forceinline__ void ell_tri(R &tn, int &win, int id, const EllipAT<R> &A, R gate, R t0, R ta,
+                                                 R tb, int ai, int aj, int bi, int bj)
 {
-    if (!(tn > ell_min(t0, ell_min(ta, tb)))) return;
+    if (!(tn > ell_min(t0, ell_min(ta, tb)) + gate)) return;
     const R p11 = ell_bf(A, ai, aj, 0, ai, aj, 0);
     const R p12 = ell_bf(A, ai, aj, 0, bi, bj, 0);
     const R p22 = ell_bf(A, bi, bj, 0, bi, bj, 0);
@@ -143,48 +178,53 @@ __device__ __forceinline__ void ell_tri(R &tn, int &win, int id, const EllipAT<R
 
 // Rim of the fan in order: (1,0) xt, (1,1) txy, (0,1) yt, (-1,1) tym,
 // (-1,0) xnt, (-1,-1) txnyn, (0,-1) ynt, (1,-1) txm.
-__device__ __forceinline__ int ell_ri(int r) { return (r == 0 || r == 1 || r == 7) ? 1 : (r >= 3 && r <= 5) ? -1 : 0; }
-__device__ __forceinline__ int ell_rj(int r) { return (r >= 1 && r <= 3) ? 1 : (r >= 5) ? -1 : 0; }
+__host__ __device__ __forceinline__ int ell_ri(int r)
+{
+    return (r == 0 || r == 1 || r == 7) ? 1 : (r >= 3 && r <= 5) ? -1 : 0;
+}
+__host__ __device__ __forceinline__ int ell_rj(int r) { return (r >= 1 && r <= 3) ? 1 : (r >= 5) ? -1 : 0; }
 
 // Scaled local metric of the target at field index t.
-template <class R> __device__ __forceinline__ EllipAT<R> ell_local(const EllipMedium &M, const EllipDir &D, long long t)
+template <class R>
+__host__ __device__ __forceinline__ EllipAT<R> ell_local(const EllipMedium &M, const EllipDir &D, long long t)
 {
     const R hx = (R)D.hx, hy = (R)D.hy, hz = (R)D.hz;
     EllipAT<R> A;
-    A.xx = (R)__ldg(M.m[D.ixx] + t) * hx * hx;
-    A.yy = (R)__ldg(M.m[D.iyy] + t) * hy * hy;
-    A.zz = (R)__ldg(M.m[D.izz] + t) * hz * hz;
-    A.xy = (R)D.sxy * (R)__ldg(M.m[D.ixy] + t) * hx * hy;
-    A.xz = (R)D.sxz * (R)__ldg(M.m[D.ixz] + t) * hx * hz;
-    A.yz = (R)D.syz * (R)__ldg(M.m[D.iyz] + t) * hy * hz;
+    A.xx = (R)ell_ld(M.m[D.ixx] + t) * hx * hx;
+    A.yy = (R)ell_ld(M.m[D.iyy] + t) * hy * hy;
+    A.zz = (R)ell_ld(M.m[D.izz] + t) * hz * hz;
+    A.xy = (R)D.sxy * (R)ell_ld(M.m[D.ixy] + t) * hx * hy;
+    A.xz = (R)D.sxz * (R)ell_ld(M.m[D.ixz] + t) * hx * hz;
+    A.yz = (R)D.syz * (R)ell_ld(M.m[D.iyz] + t) * hy * hz;
     return A;
 }
 
 // New signed value of a target from st and its rim values (rim order above);
 // win: id of the candidate that set it, -1 if none did.
 template <class R>
-__device__ __forceinline__ R point_update_ellip(R told, R st, const R nb[8], const EllipAT<R> &A, int &win)
+__host__ __device__ __forceinline__ R point_update_ellip(R told, R st, const R nb[8], const EllipAT<R> &A, int &win)
 {
     R tn = fabs(told);
     win = -1;
-    ell_vertex(tn, win, 0, A, st, 0, 0);
+    const R gate = ell_skip_bound(A);
+    ell_vertex(tn, win, 0, A, gate, st, 0, 0);
     R m = st;
 #pragma unroll
     for (int r = 0; r < 8; ++r) m = ell_min(m, nb[r]);
-    if (tn > m) {
+    if (tn > m + gate) {  // otherwise every routine below would return at its gate
 #pragma unroll
-        for (int r = 0; r < 8; ++r) ell_vertex(tn, win, 1 + r, A, nb[r], ell_ri(r), ell_rj(r));
+        for (int r = 0; r < 8; ++r) ell_vertex(tn, win, 1 + r, A, gate, nb[r], ell_ri(r), ell_rj(r));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) ell_edge(tn, win, 9 + r, A, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
+        for (int r = 0; r < 8; ++r) ell_edge(tn, win, 9 + r, A, gate, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            ell_edge(tn, win, 17 + r, A, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
+            ell_edge(tn, win, 17 + r, A, gate, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            ell_tri(tn, win, 25 + r, A, st, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
+            ell_tri(tn, win, 25 + r, A, gate, st, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
     }
     return ((told > R(0)) ? R(1) : R(-1)) * tn;

@@ -10,6 +10,7 @@ cannot lower the time (csrc/fold3d_fast.cuh, 3.), over media and spacings
 the GPU tests do not reach, drifts close to F among them."""
 import ctypes as C
 import hashlib
+import math
 import os
 import subprocess
 
@@ -105,3 +106,77 @@ def test_surf_skip_bounds_follow_the_closed_form(host):
             assert out[2 * d + side] == pytest.approx(h[nrm] / (REF_F + az) * (1 - 1e-4), rel=1e-14)
     host.fast_host_surf_bounds(*h, 1.0, 0.6, 0.5, 0.6, out.ctypes.data)  # |a| = 0.98 F
     assert not out.any()
+
+
+@pytest.fixture(scope="module")
+def ellip_host(tmp_path_factory):
+    import build as pkg_build  # fgcs-openacc-advanced_b200/build.py
+
+    out = str(tmp_path_factory.mktemp("ellip_host") / "libellip_host.so")
+    cmd = [pkg_build.NVCC, "-O2", "-std=c++17", *pkg_build.ARCH, "--fmad=false", "-shared",
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", pkg_build.INCLUDE, "-I", pkg_build.CSRC,
+           os.path.join(ROOT, "tests", "ellip_solver_host.cu"), "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    L = C.CDLL(out)
+    L.ellip_host_sweeps.argtypes = [_ptr, _ptr, _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _int, _int]
+    L.ellip_host_sweeps.restype = _int
+    L.ellip_host_bound.argtypes = [_dbl] * 6
+    L.ellip_host_bound.restype = _dbl
+    return L
+
+
+def _tti(kind, dims):
+    import media
+
+    nx, ny, nz = dims
+    if kind == "c1":  # the tilted ellipse of the 128^3 configuration: Vz 2000, Vx=Vy 2400, tilt 30, azimuth 45
+        M = media.homogeneous_ellip(nx, ny, nz, 2000.0, 0.22, 30.0, 45.0)
+    elif kind == "strong":  # eps 0.25 with the axis tilted 70 degrees
+        M = media.homogeneous_ellip(nx, ny, nz, 1800.0, 0.25, 70.0, 200.0)
+    else:
+        M = media.heterogeneous_tti(nx, ny, nz, 10.0, seed=int(kind[-1]))
+    return [np.ascontiguousarray(m.numpy(), dtype=np.float32) for m in M]
+
+
+# (medium, dims, spacings, source)
+ELLIP_CASES = [
+    ("c1", (24, 24, 24), (10.0, 10.0, 10.0), (13, 13, 13)),
+    ("strong", (21, 26, 19), (8.0, 12.0, 10.0), (4, 20, 10)),
+    ("seed0", (30, 22, 27), (10.0, 10.0, 10.0), (15, 11, 4)),
+    ("seed1", (25, 31, 20), (6.0, 9.0, 14.0), (20, 5, 18)),
+]
+
+
+@pytest.mark.parametrize("f32", [False, True], ids=["f64", "f32"])
+@pytest.mark.parametrize("case", ELLIP_CASES, ids=lambda c: c[0])
+def test_host_build_of_the_elliptical_update_matches_oracle(orc, ellip_host, case, f32):
+    """Fields and winner records after 6 sweeps, bit for bit, against
+    orc_ell_solve_rec / orc_ellf_solve_rec (which skip nothing)."""
+    kind, dims, h, src = case
+    nx, ny, nz = dims
+    M = _tti(kind, dims)
+    dt = np.float32 if f32 else np.float64
+    T0 = np.full((nz + 2, ny + 2, nx + 2), 1e16, dtype=dt)
+    T0[src[2], src[1], src[0]] = 0.0
+    ref = T0.copy()
+    _, _, Wref = (orc.ellf_solve_rec if f32 else orc.ell_solve_rec)(ref, M, h, 6, tol=-1.0)
+    T = T0.copy()
+    W = np.full(T.shape, 0xFF, dtype=np.uint8)
+    ptrs = (C.c_void_p * 6)(*(m.ctypes.data for m in M))
+    ellip_host.ellip_host_sweeps(T.ctypes.data, W.ctypes.data, ptrs, nx, ny, nz, *h, 6, int(f32))
+    assert np.array_equal(T.view(np.uint32 if f32 else np.uint64), ref.view(np.uint32 if f32 else np.uint64))
+    assert np.array_equal(W, Wref)
+    assert (np.abs(T[1:-1, 1:-1, 1:-1]) < 1e15).all()  # every interior cell reached
+
+
+def test_elliptical_skip_bound_is_the_plane_distance(ellip_host):
+    """ell_skip_bound = 0.999 min over the source plane of ||X - p||_M, i.e.
+    0.999 / sqrt((A^-1)_zz) for the scaled local metric A, X = (0, 0, 1)."""
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        G = rng.normal(size=(3, 3))
+        A = G @ G.T + 0.05 * np.eye(3)
+        got = ellip_host.ellip_host_bound(A[0, 0], A[1, 1], A[2, 2], A[0, 1], A[0, 2], A[1, 2])
+        assert got == pytest.approx(0.999 / math.sqrt(np.linalg.inv(A)[2, 2]), rel=1e-9)
+    assert ellip_host.ellip_host_bound(1.0, 1.0, 1.0, 1.0, 0.0, 0.0) == 0.0  # singular in-plane block
