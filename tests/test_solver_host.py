@@ -134,6 +134,8 @@ def _tti(kind, dims):
         M = media.homogeneous_ellip(nx, ny, nz, 2000.0, 0.22, 30.0, 45.0)
     elif kind == "strong":  # eps 0.25 with the axis tilted 70 degrees
         M = media.homogeneous_ellip(nx, ny, nz, 1800.0, 0.25, 70.0, 200.0)
+    elif kind == "extreme":  # eps 2 (speeds differ by sqrt(5)), axis tilted 45 degrees
+        M = media.homogeneous_ellip(nx, ny, nz, 1500.0, 2.0, 45.0, 30.0)
     else:
         M = media.heterogeneous_tti(nx, ny, nz, 10.0, seed=int(kind[-1]))
     return [np.ascontiguousarray(m.numpy(), dtype=np.float32) for m in M]
@@ -145,6 +147,7 @@ ELLIP_CASES = [
     ("strong", (21, 26, 19), (8.0, 12.0, 10.0), (4, 20, 10)),
     ("seed0", (30, 22, 27), (10.0, 10.0, 10.0), (15, 11, 4)),
     ("seed1", (25, 31, 20), (6.0, 9.0, 14.0), (20, 5, 18)),
+    ("extreme", (23, 20, 25), (12.0, 5.0, 8.0), (2, 19, 24)),
 ]
 
 
