@@ -44,11 +44,25 @@
 //    at least the smallest base value, and the ray then crosses the slab of
 //    width dzz between base and target, which takes at least dzz / (F + az):
 //    one time unit after leaving a point, the front is the sphere
-//    |x - a| = F.  Bs is that bound less a relative 1e-4, far above the
+//    |x - a| = F.  Bs is that bound less a relative 1e-3, far above the
 //    body's rounding (below 1e-6 relative where F^2 >= 1.1 |a|^2, through
 //    the square root of a cancelled difference), and 0 for stronger drifts.
-//    FoldEdge2Points gets no such gate: its footpoint test (:88,92) does not
-//    follow its own ray, and its accepted candidates can lie below the bound.
+//
+// 4. FoldEdge2Points bodies get a weaker gate of the same kind, B in EdgeK.
+//    Its footpoint test (:88,92) does not follow the ray of its own root: it
+//    uses the direction w = (F'/F) p/|p| + a2 (F' = sqrt(F^2 - ay^2),
+//    a2 = (ax, az), p = (d, c) the plane wave's slowness, which satisfies
+//    F'|p| + a2.p = 1), where the ray is F' p/|p| + a2.  So the candidate
+//    exceeds the linear time at the test's footpoint (at least min(s0, s1))
+//    by dzz (p.w) / w_z, with p.w = 1 - F'|p| (1 - 1/F).  When
+//      - ga > 0 and |ax| < sqrt(ga) (then c0 = 1 - d ax > 0 wherever the
+//        root exists, and the root is the upper one of F'|p| + a2.p = 1,
+//        whose ray points towards the target),
+//      - F' > |a2| (so |p| <= 1 / (F' - |a2|)), and
+//      - F >= 1 with az >= 0, or F <= 1 with az <= 0 (then w_z > 0 too),
+//    p.w >= 1 - F'(1 - 1/F) / (F' - |a2|) for F >= 1 (>= 1 for F <= 1) and
+//    w_z <= F'/F + az, which gives B (less the same relative 1e-3 margin);
+//    elsewhere B = 0.  The fall-back candidate from s1 alone is not gated.
 #pragma once
 #include <cstdint>
 #include <cstring>
@@ -63,6 +77,7 @@ struct EdgeK {
     double g, rg;       // F*F - ay*ay and RN(1/g)
     double ga, rga;     // g - az*az and RN(1/ga)
     double K;           // fall-back increment g'/c' of :99-113 (when fb_ok)
+    double B;           // body skipped when the time is <= min(s0, s1) + B (4. above)
     int early;          // ax > 0: return when s1 > s0 (:71)
     int fb_ok;          // fall-back defined: its q > 0 and c > 0
 };
@@ -136,17 +151,20 @@ __host__ __device__ __forceinline__ double kmin(double a, double b) { return (a 
 
 __host__ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1, const EdgeK &k, double F)
 {
-    if (tn < kmin(s1, s0) || (k.early && s1 > s0)) return;
-    const double d = div_by_const(s1 - s0, k.hx, k.rhx);
-    double c = (1.0 - d * k.ax);
-    double q = k.g * (c * c - d * d * k.ga);
-    if (0.0 < q) {
-        c = div_by_const(-k.az * c + sqrt(q), k.ga, k.rga);
-        q = s0 + k.hz * c;
-        if (q < tn && q > kmin(s0, s1)) {
-            const double g = sqrt(div_by_const((d * d + c * c) * F * F, k.g, k.rg));
-            const double xe = -k.hz * (d + k.ax * g) / (c + k.az * g);
-            if (0.0 < xe && xe < k.hx) tn = q;
+    const double mn = kmin(s1, s0);
+    if (tn < mn || (k.early && s1 > s0)) return;
+    if (!(tn <= mn + k.B)) {  // 4. above
+        const double d = div_by_const(s1 - s0, k.hx, k.rhx);
+        double c = (1.0 - d * k.ax);
+        double q = k.g * (c * c - d * d * k.ga);
+        if (0.0 < q) {
+            c = div_by_const(-k.az * c + sqrt(q), k.ga, k.rga);
+            q = s0 + k.hz * c;
+            if (q < tn && q > mn) {
+                const double g = sqrt(div_by_const((d * d + c * c) * F * F, k.g, k.rg));
+                const double xe = -k.hz * (d + k.ax * g) / (c + k.az * g);
+                if (0.0 < xe && xe < k.hx) tn = q;
+            }
         }
     }
     if (tn > s1 && k.fb_ok) tn = kmin(tn, s1 + k.K);

@@ -26,13 +26,32 @@ double safe_recip(double c)
 }
 
 // Skip bound of the FoldSurf3Points bodies of one side (fold3d_fast.cuh,
-// 3.): dzz / (F + az) less a relative 1e-4, or 0 (no skipping beyond the
+// 3.): dzz / (F + az) less a relative 1e-3, or 0 (no skipping beyond the
 // reference's own gates) unless F^2 >= 1.1 |a|^2.
 double surf_skip_bound(double F, double ax, double ay, double az, double dzz)
 {
     const double a2 = ax * ax + ay * ay + az * az;
     if (!(F > 0.0 && dzz > 0.0 && F * F >= 1.1 * a2)) return 0.0;
-    const double B = dzz / (F + az) * (1.0 - 1e-4);
+    const double B = dzz / (F + az) * (1.0 - 1e-3);
+    return (std::isfinite(B) && B > 0.0) ? B : 0.0;
+}
+
+// Skip bound of a FoldEdge2Points body with arguments (F, ax, ay, az, dxx,
+// dzz) (fold3d_fast.cuh, 4.): dzz P / W less a relative 1e-3, with
+// P = 1 - F'(1 - 1/F) / (F' - |a2|) (1 for F <= 1) and W = F'/F + az, where
+// F' = sqrt(F^2 - ay^2) and a2 = (ax, az); 0 unless the conditions of 4. hold
+// with some room: F^2 >= 1.1 |a|^2, |ax| < sqrt(ga) and F' > |a2| by 5%.
+double edge_skip_bound(double F, double ax, double ay, double az, double dzz)
+{
+    const double Fp2 = F * F - ay * ay, ga = Fp2 - az * az;
+    if (!(F > 0.0 && dzz > 0.0 && F * F >= 1.1 * (ax * ax + ay * ay + az * az) && ga > 0.0)) return 0.0;
+    const double Fp = std::sqrt(Fp2), a2 = std::sqrt(ax * ax + az * az);
+    if (!(std::fabs(ax) < 0.95 * std::sqrt(ga) && a2 < 0.95 * Fp)) return 0.0;
+    if (!((F >= 1.0 && az >= 0.0) || (F <= 1.0 && az <= 0.0))) return 0.0;
+    const double P = (F >= 1.0) ? 1.0 - Fp * (1.0 - 1.0 / F) / (Fp - a2) : 1.0;
+    const double W = Fp / F + az;
+    if (!(P > 0.0 && W > 0.0)) return 0.0;
+    const double B = dzz * P / W * (1.0 - 1e-3);
     return (std::isfinite(B) && B > 0.0) ? B : 0.0;
 }
 
@@ -53,6 +72,7 @@ EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double h
     k.ga = k.g - az * az;      // :80, :83
     k.rga = safe_recip(k.ga);
     k.early = (ax > 0.0);      // :71
+    k.B = edge_skip_bound(F, ax, ay, az, hz);
     // fall-back candidate from xt alone, :99-113, up to the final addition
     double c = (-hx * ax + hz * az);
     const double g = hx * hx + hz * hz;

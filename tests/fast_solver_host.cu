@@ -45,12 +45,21 @@ LocalFrameH host_frame(int dir, const double h[3], double F, const double a[3])
     return L;
 }
 
+void clear_bounds(SideTable &t)
+{
+    t.Bs = 0.0;
+    for (int k = 0; k < 8; ++k) {
+        t.edge[k].B = 0.0;
+        t.surf[k].nest.B = 0.0;
+    }
+}
+
 }  // namespace
 
 // Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  With
-// surf_skip == 0 the tables' FoldSurf3Points skip bounds are cleared first.
+// skip == 0 the tables' body-skip bounds are cleared first.
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
-                                double a0, double a1, double a2, int sweeps, int surf_skip)
+                                double a0, double a1, double a2, int sweeps, int skip)
 {
     const int n[3] = {nx, ny, nz};
     const int64_t stride[3] = {1, (int64_t)nx + 2, ((int64_t)nx + 2) * (ny + 2)};
@@ -58,7 +67,10 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
     DirTable tabs[6];
     for (int dir = 0; dir < 6; ++dir) {
         build_dir_table(host_frame(dir, h, F, a), tabs[dir]);
-        if (!surf_skip) tabs[dir].side[0].Bs = tabs[dir].side[1].Bs = 0.0;
+        if (!skip) {
+            clear_bounds(tabs[dir].side[0]);
+            clear_bounds(tabs[dir].side[1]);
+        }
     }
     for (int s = 0; s < sweeps; ++s)
         for (int dir = 0; dir < 6; ++dir) {
@@ -83,15 +95,23 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
     return 0;
 }
 
-// The FoldSurf3Points skip bound of every direction and side, out[2 dir + side].
-extern "C" void fast_host_surf_bounds(double dx, double dy, double dz, double F, double a0, double a1, double a2,
-                                      double *out)
+// The skip bounds of every direction and side: 17 values at
+// out[17 (2 dir + side)]: Bs, the eight edge calls' B, the eight nested
+// edges' B.
+extern "C" void fast_host_bounds(double dx, double dy, double dz, double F, double a0, double a1, double a2,
+                                 double *out)
 {
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
     for (int dir = 0; dir < 6; ++dir) {
         DirTable t;
         build_dir_table(host_frame(dir, h, F, a), t);
-        out[2 * dir] = t.side[0].Bs;
-        out[2 * dir + 1] = t.side[1].Bs;
+        for (int sd = 0; sd < 2; ++sd) {
+            double *o = out + 17 * (2 * dir + sd);
+            o[0] = t.side[sd].Bs;
+            for (int k = 0; k < 8; ++k) {
+                o[1 + k] = t.side[sd].edge[k].B;
+                o[9 + k] = t.side[sd].surf[k].nest.B;
+            }
+        }
     }
 }

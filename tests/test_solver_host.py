@@ -5,8 +5,8 @@ compared bit for bit with the oracle's statement of the reference
 (Stencil-OpenACC/AN_ISO_1_OpenACC.c:59-326).  Both IEEE double builds round
 every operation on its own, so equal bits here are the bits the kernels
 compute: the folded constants, the division by constants without a divide
-instruction, the slot loops and the skip of FoldSurf3Points bodies that
-cannot lower the time (csrc/fold3d_fast.cuh, 3.), over media and spacings
+instruction, the slot loops and the skipping of solver bodies that cannot
+lower the time (csrc/fold3d_fast.cuh, 3. and 4.), over media and spacings
 the GPU tests do not reach, drifts close to F among them."""
 import ctypes as C
 import hashlib
@@ -37,14 +37,14 @@ def host(tmp_path_factory):
     L = C.CDLL(out)
     L.fast_host_sweeps.argtypes = [_ptr, _int, _int, _int, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _int, _int]
     L.fast_host_sweeps.restype = _int
-    L.fast_host_surf_bounds.argtypes = [_dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _ptr]
-    L.fast_host_surf_bounds.restype = None
+    L.fast_host_bounds.argtypes = [_dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _ptr]
+    L.fast_host_bounds.restype = None
     return L
 
 
-def _host_sweeps(host, T, h, F, a, sweeps, surf_skip=True):
+def _host_sweeps(host, T, h, F, a, sweeps, skip=True):
     nz, ny, nx = (s - 2 for s in T.shape)
-    host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps, int(surf_skip))
+    host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps, int(skip))
 
 
 # (dims, spacings, F, drift, source): the reference's medium and others, with
@@ -77,7 +77,7 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
     for skip in (True, False):
         T = T0.copy()
         _host_sweeps(host, T, h, F, a, 8, skip)
-        assert_bitwise(T, ref, "host build of the point update, surf skip %s" % skip)
+        assert_bitwise(T, ref, "host build of the point update, skip %s" % skip)
 
 
 def test_host_build_matches_reference_digest_99(host, digests):
@@ -92,20 +92,59 @@ def test_host_build_matches_reference_digest_99(host, digests):
     assert hashlib.sha256(np.ascontiguousarray(T).tobytes()).hexdigest() == digests["n99_s8"]
 
 
-def test_surf_skip_bounds_follow_the_closed_form(host):
-    """Each side's bound is dzz / (F + az) (1 - 1e-4), az the drift along the
-    normal towards the target (negated on the negative side), where
-    F^2 >= 1.1 |a|^2; 0 for stronger drifts."""
+# the reference's direction table (AN_ISO_1_OpenACC.c:1195-1236): normal axis,
+# sign, local x axis and sign, local y axis and sign
+_DIRS = [(0, +1, 2, +1, 1, +1), (0, -1, 2, -1, 1, -1), (2, +1, 1, +1, 0, +1),
+         (2, -1, 1, -1, 0, -1), (1, -1, 0, -1, 2, -1), (1, +1, 0, +1, 2, +1)]
+
+
+def _edge_bound(F, ax, ay, az, dzz):
+    """fold3d_fast.cuh 4., restated: the FoldEdge2Points skip bound."""
+    Fp2 = F * F - ay * ay
+    ga = Fp2 - az * az
+    if not (F * F >= 1.1 * (ax * ax + ay * ay + az * az) and ga > 0):
+        return 0.0
+    Fp, a2 = math.sqrt(Fp2), math.hypot(ax, az)
+    if not (abs(ax) < 0.95 * math.sqrt(ga) and a2 < 0.95 * Fp):
+        return 0.0
+    if not ((F >= 1 and az >= 0) or (F <= 1 and az <= 0)):
+        return 0.0
+    P = 1 - Fp * (1 - 1 / F) / (Fp - a2) if F >= 1 else 1.0
+    W = Fp / F + az
+    return dzz * P / W * (1 - 1e-3) if P > 0 and W > 0 else 0.0
+
+
+@pytest.mark.parametrize("F,a", [(REF_F, REF_A), (0.8, (0.3, -0.2, -0.4)), (1.0, (0.6, 0.5, 0.6))])
+def test_skip_bounds_follow_the_closed_forms(host, F, a):
+    """Bs = dzz / (F + az) (1 - 1e-3) where F^2 >= 1.1 |a|^2 (0 otherwise),
+    az the drift along the normal towards the target (negated on the negative
+    side); every edge call's B, the nested ones included, follows 4. of
+    fold3d_fast.cuh with that call's own arguments (AN_ISO_1_OpenACC.c:242-253,
+    :172-173)."""
     h = (0.7, 0.9, 1.1)
-    out = np.zeros(12)
-    host.fast_host_surf_bounds(*h, REF_F, *REF_A, out.ctypes.data)
-    dirs = [(0, +1), (0, -1), (2, +1), (2, -1), (1, -1), (1, +1)]  # normal axis, sign (x_down ... y_down)
-    for d, (nrm, sg) in enumerate(dirs):
+    out = np.zeros(6 * 2 * 17)
+    host.fast_host_bounds(*h, F, *a, out.ctypes.data)
+    out = out.reshape(6, 2, 17)
+    strong = F * F < 1.1 * sum(x * x for x in a)
+    for d, (nrm, sg, xa, xs, ya, ys) in enumerate(_DIRS):
         for side in (0, 1):
-            az = sg * REF_A[nrm] * (-1 if side else 1)
-            assert out[2 * d + side] == pytest.approx(h[nrm] / (REF_F + az) * (1 - 1e-4), rel=1e-14)
-    host.fast_host_surf_bounds(*h, 1.0, 0.6, 0.5, 0.6, out.ctypes.data)  # |a| = 0.98 F
-    assert not out.any()
+            s = -1 if side else 1
+            ax, ay, az = s * xs * a[xa], s * ys * a[ya], s * sg * a[nrm]
+            hx, hy, hz = h[xa], h[ya], h[nrm]
+            hxy, hxz, hyz = math.hypot(hx, hy), math.hypot(hx, hz), math.hypot(hy, hz)
+            assert out[d, side, 0] == (0.0 if strong else pytest.approx(hz / (F + az) * (1 - 1e-3), rel=1e-14))
+            edges = [(ax, ay, az, hz), ((ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hz),
+                     (ay, ax, az, hz), (-(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hz),
+                     (-ax, ay, az, hz), (-(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hz),
+                     (-ay, ax, az, hz), ((ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hz)]
+            surfs = [(ax, ay, hx, hxz), (ax, -ay, hx, hxz), (-ax, -ay, hx, hxz), (-ax, ay, hx, hxz),
+                     (-ay, -ax, hy, hyz), (-ay, ax, hy, hyz), (ay, ax, hy, hyz), (ay, -ax, hy, hyz)]
+            nests = [(say, (sax * hz + az * shx) / shxz, (-sax * shx + az * hz) / shxz, shxz)
+                     for sax, say, shx, shxz in surfs]
+            for k, (cax, cay, caz, dzz) in enumerate(edges + nests):
+                assert out[d, side, 1 + k] == pytest.approx(_edge_bound(F, cax, cay, caz, dzz), rel=1e-12, abs=0)
+    if not strong:
+        assert (out[:, :, 0] > 0).all() and (out[:, :, 1:] > 0).any()
 
 
 @pytest.fixture(scope="module")
