@@ -6,8 +6,11 @@
 // the side the table is for, in IEEE double with no FMA contraction
 // (-ffp-contract=off), so the kernel obtains exactly the bits the reference
 // computes point by point.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <queue>
+#include <vector>
 
 #include "fold3d_fast.cuh"
 #include "fold3d_internal.h"
@@ -55,6 +58,104 @@ double edge_skip_bound(double F, double ax, double ay, double az, double dzz)
     return (std::isfinite(B) && B > 0.0) ? B : 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// A proved lower bound on the accepted increment of one FoldEdge2Points call
+// site, by interval branch and bound.  With d = (s1 - s0)/dxx the body
+// computes c0 = 1 - d ax, Q = g (c0^2 - d^2 ga), c = (-az c0 + sqrt Q)/ga
+// and accepts q = s0 + dzz c when Q > 0, q > min(s0, s1) and the footpoint
+// xe = -dzz (d + ax G)/(c + az G), G = sqrt((d^2 + c^2) F^2 / g), lies in
+// (0, dxx) (:71-95).  Its increment over min(s0, s1),
+// D(d) = dzz c + max(0, -d dxx), depends on d alone, and d ranges over the
+// bounded interval where Q > 0 when |ax| < sqrt(ga).  The search encloses D
+// and the acceptance tests on sub-intervals of d in interval arithmetic
+// rounded outwards, drops sub-intervals where no d can be accepted (Q <= 0,
+// D <= 0, num * den >= 0 or dzz |num| >= dxx |den| for xe = -dzz num/den,
+// the last also near the pole den = 0), splits the one with the smallest
+// enclosure of D, and returns the smallest lower end left.  The constants are
+// the table's own doubles; the kernel's rounding is covered by the caller's
+// relative margin.
+// ---------------------------------------------------------------------------
+struct Iv {
+    double lo, hi;
+};
+inline double rdn(double x) { return std::nextafter(x, -HUGE_VAL); }
+inline double rup(double x) { return std::nextafter(x, HUGE_VAL); }
+inline Iv ivp(double x) { return {x, x}; }
+inline Iv iadd(Iv a, Iv b) { return {rdn(a.lo + b.lo), rup(a.hi + b.hi)}; }
+inline Iv isub(Iv a, Iv b) { return {rdn(a.lo - b.hi), rup(a.hi - b.lo)}; }
+inline Iv imul(Iv a, Iv b)
+{
+    const double p0 = a.lo * b.lo, p1 = a.lo * b.hi, p2 = a.hi * b.lo, p3 = a.hi * b.hi;
+    return {rdn(std::min(std::min(p0, p1), std::min(p2, p3))), rup(std::max(std::max(p0, p1), std::max(p2, p3)))};
+}
+inline Iv isqr(Iv a)
+{
+    if (a.lo >= 0.0) return {rdn(a.lo * a.lo), rup(a.hi * a.hi)};
+    if (a.hi <= 0.0) return {rdn(a.hi * a.hi), rup(a.lo * a.lo)};
+    return {0.0, rup(std::max(a.lo * a.lo, a.hi * a.hi))};
+}
+inline Iv idivp(Iv a, double b) { return {rdn(a.lo / b), rup(a.hi / b)}; }  // b > 0
+inline Iv isqrt(Iv a) { return {a.lo > 0.0 ? rdn(std::sqrt(a.lo)) : 0.0, a.hi > 0.0 ? rup(std::sqrt(a.hi)) : 0.0}; }
+inline Iv iabs(Iv a)
+{
+    if (a.lo >= 0.0) return a;
+    if (a.hi <= 0.0) return {-a.hi, -a.lo};
+    return {0.0, std::max(-a.lo, a.hi)};
+}
+
+// Encloses D over the d in `d` when some of them may be accepted; false when
+// none can be.
+bool edge_increment(const EdgeK &k, double F, Iv d, Iv &D)
+{
+    const Iv c0 = isub(ivp(1.0), imul(d, ivp(k.ax)));
+    const Iv Q = imul(ivp(k.g), isub(isqr(c0), imul(isqr(d), ivp(k.ga))));
+    if (!(Q.hi > 0.0)) return false;
+    const Iv c = idivp(iadd(imul(ivp(-k.az), c0), isqrt(Q)), k.ga);
+    const Iv m = imul(d, ivp(-k.hx));
+    D = iadd(imul(ivp(k.hz), c), Iv{std::max(0.0, m.lo), std::max(0.0, m.hi)});
+    if (!(D.hi > 0.0)) return false;
+    const Iv G = isqrt(idivp(imul(imul(iadd(isqr(d), isqr(c)), ivp(F)), ivp(F)), k.g));
+    const Iv num = iadd(d, imul(ivp(k.ax), G)), den = iadd(c, imul(ivp(k.az), G));
+    if (!(imul(num, den).lo < 0.0)) return false;  // xe > 0 needs num * den < 0
+    return imul(ivp(k.hz), iabs(num)).lo < imul(ivp(k.hx), iabs(den)).hi;  // |xe| < dxx
+}
+
+// The proved lower bound (0 when the search does not apply).
+double edge_bb_bound(const EdgeK &k, double F)
+{
+    if (!(k.g > 0.0 && k.ga > 0.0 && k.hx > 0.0 && k.hz > 0.0 && F > 0.0)) return 0.0;
+    const double sga = std::sqrt(k.ga);
+    if (!(std::fabs(k.ax) < 0.99 * sga)) return 0.0;
+    // Q > 0 between the roots 1/(ax - sqrt ga) < 0 < 1/(ax + sqrt ga), widened
+    double lo = 1.0 / (k.ax - sga) * (1.0 + 1e-9), hi = 1.0 / (k.ax + sga) * (1.0 + 1e-9);
+    if (k.early) hi = 0.0;  // ax > 0: the body returns when s1 > s0, i.e. d > 0 (:71)
+    if (!(lo < hi) || !std::isfinite(lo) || !std::isfinite(hi)) return 0.0;
+    using Item = std::pair<double, Iv>;
+    auto cmp = [](const Item &a, const Item &b) { return a.first > b.first; };
+    std::priority_queue<Item, std::vector<Item>, decltype(cmp)> heap(cmp);
+    Iv D;
+    if (edge_increment(k, F, Iv{lo, hi}, D)) heap.push({D.lo, Iv{lo, hi}});
+    const double min_width = (hi - lo) * 1e-12;
+    double frozen = HUGE_VAL;  // sub-intervals too narrow to split
+    for (int it = 0; it < 600 && !heap.empty(); ++it) {
+        const Item top = heap.top();
+        heap.pop();
+        const Iv x = top.second;
+        const double mid = 0.5 * (x.lo + x.hi);
+        if (!(x.hi - x.lo > min_width) || !(mid > x.lo && mid < x.hi)) {
+            frozen = std::min(frozen, top.first);
+            continue;
+        }
+        const Iv halves[2] = {{x.lo, mid}, {mid, x.hi}};
+        for (const Iv &h : halves)
+            if (edge_increment(k, F, h, D)) heap.push({D.lo, h});
+    }
+    double b = frozen;
+    if (!heap.empty()) b = std::min(b, heap.top().first);
+    if (b == HUGE_VAL) return 0.0;  // nothing can be accepted; 0 keeps the plain gates
+    return std::max(b, 0.0);
+}
+
 // FoldEdge2Points call with arguments (F, ax, ay, az, dxx=hx, dzz=hz),
 // AN_ISO_1_OpenACC.c:59-114.
 EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double hz)
@@ -72,7 +173,12 @@ EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double h
     k.ga = k.g - az * az;      // :80, :83
     k.rga = safe_recip(k.ga);
     k.early = (ax > 0.0);      // :71
+    // the larger of two proved lower bounds, less the relative margin
     k.B = edge_skip_bound(F, ax, ay, az, hz);
+    if (F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
+        const double bb = edge_bb_bound(k, F) * (1.0 - 1e-3);
+        if (std::isfinite(bb) && bb > k.B) k.B = bb;
+    }
     // fall-back candidate from xt alone, :99-113, up to the final addition
     double c = (-hx * ax + hz * az);
     const double g = hx * hx + hz * hz;
@@ -168,8 +274,28 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
 
 void build_dir_table(const LocalFrameH &L, DirTable &out)
 {
+    // The edge bounds take a search per call site; a solve asks for the same
+    // six frames every sweep, so each thread keeps its last twelve tables.
+    struct Entry {
+        LocalFrameH key;
+        DirTable tab;
+        bool used;
+    };
+    constexpr int kEntries = 12;
+    thread_local std::vector<Entry> memo(kEntries);
+    thread_local int next = 0;
+    for (const Entry &e : memo)
+        if (e.used && std::memcmp(&e.key, &L, sizeof L) == 0) {
+            out = e.tab;
+            return;
+        }
     side_table(L, false, out.side[0]);
     side_table(L, true, out.side[1]);
+    Entry &e = memo[next];
+    next = (next + 1) % kEntries;
+    e.key = L;
+    e.tab = out;
+    e.used = true;
 }
 
 }  // namespace fold3d

@@ -114,18 +114,48 @@ def _edge_bound(F, ax, ay, az, dzz):
     return dzz * P / W * (1 - 1e-3) if P > 0 and W > 0 else 0.0
 
 
-@pytest.mark.parametrize("F,a", [(REF_F, REF_A), (0.8, (0.3, -0.2, -0.4)), (1.0, (0.6, 0.5, 0.6))])
-def test_skip_bounds_follow_the_closed_forms(host, F, a):
+def _edge_sampled_inf(F, ax, ay, az, hx, hz, n=200001):
+    """Smallest increment over min(s0, s1) that a FoldEdge2Points call with
+    these arguments accepts (AN_ISO_1_OpenACC.c:71-95), over n values of
+    d = (s1 - s0)/dxx spanning the interval where its square root is real;
+    an upper estimate of the true infimum.  None when that interval is not
+    bounded, inf when no sample is accepted."""
+    g = F * F - ay * ay
+    ga = g - az * az
+    if not (ga > 0 and abs(ax) < math.sqrt(ga)):
+        return None
+    lo, hi = 1 / (ax - math.sqrt(ga)), 1 / (ax + math.sqrt(ga))
+    if ax > 0:
+        hi = 0.0
+    d = np.linspace(lo, hi, n)[1:-1]
+    c0 = 1 - d * ax
+    Q = g * (c0 * c0 - d * d * ga)
+    ok = Q > 0
+    c = (-az * c0 + np.sqrt(np.where(ok, Q, 0))) / ga
+    mn = np.minimum(0, d * hx)
+    G = np.sqrt((d * d + c * c) * F * F / g)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        xe = -hz * (d + ax * G) / (c + az * G)
+    acc = ok & (hz * c > mn) & (xe > 0) & (xe < hx)
+    return float((hz * c - mn)[acc].min()) if acc.any() else math.inf
+
+
+@pytest.mark.parametrize("F,a,h", [(REF_F, REF_A, (0.7, 0.9, 1.1)), (REF_F, REF_A, (1.0, 1.0, 1.0)),
+                                   (1.3, (0.2, -0.5, 0.3), (1.0, 0.6, 0.8)), (0.8, (0.3, -0.2, -0.4), (0.5, 0.5, 0.5)),
+                                   (1.0, (0.6, 0.5, 0.6), (0.5, 0.5, 0.5))])
+def test_skip_bounds_are_proved_lower_bounds(host, F, a, h):
     """Bs = dzz / (F + az) (1 - 1e-3) where F^2 >= 1.1 |a|^2 (0 otherwise),
     az the drift along the normal towards the target (negated on the negative
-    side); every edge call's B, the nested ones included, follows 4. of
-    fold3d_fast.cuh with that call's own arguments (AN_ISO_1_OpenACC.c:242-253,
-    :172-173)."""
-    h = (0.7, 0.9, 1.1)
+    side).  Every edge call's B (AN_ISO_1_OpenACC.c:242-253, and the nested
+    calls :172-173, with each call's own arguments) is at least the analytic
+    bound of fold3d_fast.cuh 4. and at most the smallest accepted increment
+    found by dense sampling; in the reference's medium the branch-and-bound
+    search brings it within 2% of that."""
     out = np.zeros(6 * 2 * 17)
     host.fast_host_bounds(*h, F, *a, out.ctypes.data)
     out = out.reshape(6, 2, 17)
     strong = F * F < 1.1 * sum(x * x for x in a)
+    tight = []
     for d, (nrm, sg, xa, xs, ya, ys) in enumerate(_DIRS):
         for side in (0, 1):
             s = -1 if side else 1
@@ -133,16 +163,28 @@ def test_skip_bounds_follow_the_closed_forms(host, F, a):
             hx, hy, hz = h[xa], h[ya], h[nrm]
             hxy, hxz, hyz = math.hypot(hx, hy), math.hypot(hx, hz), math.hypot(hy, hz)
             assert out[d, side, 0] == (0.0 if strong else pytest.approx(hz / (F + az) * (1 - 1e-3), rel=1e-14))
-            edges = [(ax, ay, az, hz), ((ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hz),
-                     (ay, ax, az, hz), (-(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hz),
-                     (-ax, ay, az, hz), (-(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hz),
-                     (-ay, ax, az, hz), ((ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hz)]
-            surfs = [(ax, ay, hx, hxz), (ax, -ay, hx, hxz), (-ax, -ay, hx, hxz), (-ax, ay, hx, hxz),
-                     (-ay, -ax, hy, hyz), (-ay, ax, hy, hyz), (ay, ax, hy, hyz), (ay, -ax, hy, hyz)]
-            nests = [(say, (sax * hz + az * shx) / shxz, (-sax * shx + az * hz) / shxz, shxz)
-                     for sax, say, shx, shxz in surfs]
-            for k, (cax, cay, caz, dzz) in enumerate(edges + nests):
-                assert out[d, side, 1 + k] == pytest.approx(_edge_bound(F, cax, cay, caz, dzz), rel=1e-12, abs=0)
+            edges = [(ax, ay, az, hx, hz), ((ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz),
+                     (ay, ax, az, hy, hz), (-(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz),
+                     (-ax, ay, az, hx, hz), (-(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz),
+                     (-ay, ax, az, hy, hz), ((ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz)]
+            surfs = [(ax, ay, hx, hy, hxz), (ax, -ay, hx, hy, hxz), (-ax, -ay, hx, hy, hxz), (-ax, ay, hx, hy, hxz),
+                     (-ay, -ax, hy, hx, hyz), (-ay, ax, hy, hx, hyz), (ay, ax, hy, hx, hyz), (ay, -ax, hy, hx, hyz)]
+            nests = [(say, (sax * hz + az * shx) / shxz, (-sax * shx + az * hz) / shxz, shy, shxz)
+                     for sax, say, shx, shy, shxz in surfs]
+            for k, (cax, cay, caz, chx, chz) in enumerate(edges + nests):
+                B = out[d, side, 1 + k]
+                if strong:
+                    assert B == 0.0
+                    continue
+                assert B >= _edge_bound(F, cax, cay, caz, chz) * (1 - 1e-12)
+                inf = _edge_sampled_inf(F, cax, cay, caz, chx, chz)
+                if inf is None:
+                    assert B == _edge_bound(F, cax, cay, caz, chz)
+                elif inf < math.inf:
+                    assert B <= inf
+                    tight.append(B / inf)
+    if F == REF_F:
+        assert min(tight) > 0.98
     if not strong:
         assert (out[:, :, 0] > 0).all() and (out[:, :, 1:] > 0).any()
 
