@@ -35,7 +35,7 @@
 // slot loop may visit the calls in any order; it keeps the reference's order.
 //
 // 3. One more such gate skips a FoldSurf3Points body (its nested edge still
-//    runs) when the current time is at most min(s0, s1, s2) + Bs.  The body
+//    runs) when the current time is at most min(s0, s1, s2) + B.  The body
 //    solves the drift medium's eikonal F|p| + a.p = 1 for the plane wave
 //    through the three base values and takes the root whose ray, of
 //    direction F p/|p| + a, points from the base plane to the target (:152);
@@ -44,9 +44,11 @@
 //    at least the smallest base value, and the ray then crosses the slab of
 //    width dzz between base and target, which takes at least dzz / (F + az):
 //    one time unit after leaving a point, the front is the sphere
-//    |x - a| = F.  Bs is that bound less a relative 1e-3, far above the
-//    body's rounding (below 1e-6 relative where F^2 >= 1.1 |a|^2, through
-//    the square root of a cancelled difference), and 0 for stronger drifts.
+//    |x - a| = F.  B is the larger of that bound and one proved per call
+//    site by a search over the body's two gradients (fold3d_tables.cpp),
+//    less a relative 1e-3, far above the body's rounding (below 1e-6
+//    relative where F^2 >= 1.1 |a|^2, through the square root of a cancelled
+//    difference); 0 for stronger drifts.
 //
 // 4. FoldEdge2Points bodies get a weaker gate of the same kind, B in EdgeK.
 //    Its footpoint test (:88,92) does not follow the ray of its own root: it
@@ -90,6 +92,7 @@ struct SurfK {
     int e1, e2;         // ax > 0, ay > 0 (early returns of :132)
     int nblock;         // ax*dzz + az*dxx > 0: nested edge skipped when s1 > s2 (:170)
     int pad_;
+    double B;           // body skipped when the time is <= min(s0, s1, s2) + B (3. above)
     EdgeK nest;         // the nested FoldEdge2Points call (:172-173)
 };
 
@@ -98,7 +101,6 @@ struct SideTable {
     double F, az, hz;
     double g, rg;       // F*F - az*az, RN(1/g)          (:147)
     double K1;          // 1-D candidate increment dzz*dzz/q (:225)
-    double Bs;          // surf bodies skipped when the time is <= min(s0, s1, s2) + Bs (3. above)
     int d1_ok;          // 1-D candidate defined (:219, :223)
     // the per-call flags below as bit masks, bit k for call k
     unsigned m_e1, m_e2, m_nblock;  // surf[k].e1, .e2, .nblock
@@ -175,7 +177,7 @@ __host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1
 {
     const double mn = kmin(s0, kmin(s1, s2));
     if (tn < mn || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
-    if (!(tn <= mn + t.Bs)) {  // 3. above
+    if (!(tn <= mn + k.B)) {  // 3. above
         const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
         const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
         double dd = dx * dx + dy * dy;

@@ -82,7 +82,7 @@ extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m
 
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t s = (cudaStream_t)stream;
-    DirTable tab;  // one direction's constants at a time (4.5 KiB of host stack)
+    DirTable tab;  // one direction's constants at a time (4.6 KiB of host stack)
     int sweeps = 0;
     unsigned long long bits = 0;
     while (sweeps < o->max_sweeps) {

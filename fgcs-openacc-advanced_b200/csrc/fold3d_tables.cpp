@@ -120,6 +120,18 @@ bool edge_increment(const EdgeK &k, double F, Iv d, Iv &D)
     return imul(ivp(k.hz), iabs(num)).lo < imul(ivp(k.hx), iabs(den)).hi;  // |xe| < dxx
 }
 
+// The increment the body accepts at one d, or +inf (double arithmetic; only
+// used to stop the search once its bound is within 1% of it).
+double edge_point(const EdgeK &k, double F, double d)
+{
+    const double c0 = 1.0 - d * k.ax, Q = k.g * (c0 * c0 - d * d * k.ga);
+    if (!(Q > 0.0)) return HUGE_VAL;
+    const double c = (-k.az * c0 + std::sqrt(Q)) / k.ga, D = k.hz * c - std::min(0.0, d * k.hx);
+    if (!(D > 0.0)) return HUGE_VAL;
+    const double G = std::sqrt((d * d + c * c) * F * F / k.g), xe = -k.hz * (d + k.ax * G) / (c + k.az * G);
+    return (0.0 < xe && xe < k.hx) ? D : HUGE_VAL;
+}
+
 // The proved lower bound (0 when the search does not apply).
 double edge_bb_bound(const EdgeK &k, double F)
 {
@@ -137,11 +149,14 @@ double edge_bb_bound(const EdgeK &k, double F)
     if (edge_increment(k, F, Iv{lo, hi}, D)) heap.push({D.lo, Iv{lo, hi}});
     const double min_width = (hi - lo) * 1e-12;
     double frozen = HUGE_VAL;  // sub-intervals too narrow to split
-    for (int it = 0; it < 600 && !heap.empty(); ++it) {
+    double seen = HUGE_VAL;    // smallest increment accepted at a sampled point
+    for (int it = 0; it < 2000 && !heap.empty(); ++it) {
         const Item top = heap.top();
+        if (top.first >= 0.99 * seen) break;  // within 1%: the bound is tight enough
         heap.pop();
         const Iv x = top.second;
         const double mid = 0.5 * (x.lo + x.hi);
+        seen = std::min(seen, edge_point(k, F, mid));
         if (!(x.hi - x.lo > min_width) || !(mid > x.lo && mid < x.hi)) {
             frozen = std::min(frozen, top.first);
             continue;
@@ -154,6 +169,107 @@ double edge_bb_bound(const EdgeK &k, double F)
     if (!heap.empty()) b = std::min(b, heap.top().first);
     if (b == HUGE_VAL) return 0.0;  // nothing can be accepted; 0 keeps the plain gates
     return std::max(b, 0.0);
+}
+
+// The same search for a FoldSurf3Points call site (drift arguments ax, ay;
+// the side's F, az, dzz; spacings dxx, dyy), over the two gradients
+// dx = (s1 - s0)/dxx, dy = (s2 - s1)/dyy.  The body (:131-165) computes
+// al = 1 - ax dx - ay dy, q = al^2 - (dx^2 + dy^2) g with g = F^2 - az^2,
+// al' = (-az al + F sqrt q)/g and accepts s0 + dzz al' when q > 0, it lies
+// above min(s0, s1, s2) and its footpoint xe = -dzz nx/den,
+// ye = -dzz ny/den (nx = F dx + ax r, ny = F dy + ay r, den = F al' + az r,
+// r = sqrt(dx^2 + dy^2 + al'^2)) satisfies 0 <= min(xe, ye),
+// ye dxx <= xe dyy and xe <= dxx.  Its increment over min(s0, s1, s2) is
+// D = dzz al' - min(0, dx dxx, dx dxx + dy dyy).  The gradients range over
+// the disc where q > 0, of radius 1/(sqrt g - |(ax, ay)|), and the early
+// returns (:132) keep dx <= 0 when ax > 0 and dy <= 0 when ay > 0.
+struct Box {
+    Iv x, y;
+};
+
+bool surf_increment(double F, double az, double hz, double g, double ax, double ay, double hx, double hy, const Box &b,
+                    Iv &D)
+{
+    const Iv dd = iadd(isqr(b.x), isqr(b.y));
+    const Iv al = isub(isub(ivp(1.0), imul(ivp(ax), b.x)), imul(ivp(ay), b.y));
+    const Iv q = isub(isqr(al), imul(dd, ivp(g)));
+    if (!(q.hi > 0.0)) return false;
+    const Iv al2 = idivp(iadd(imul(ivp(-az), al), imul(ivp(F), isqrt(q))), g);
+    const Iv ux = imul(b.x, ivp(hx)), uxy = iadd(ux, imul(b.y, ivp(hy)));
+    const Iv mn = {std::min(0.0, std::min(ux.lo, uxy.lo)), std::min(0.0, std::min(ux.hi, uxy.hi))};
+    D = isub(imul(ivp(hz), al2), mn);
+    if (!(D.hi > 0.0)) return false;
+    const Iv r = isqrt(iadd(dd, isqr(al2)));
+    const Iv den = iadd(imul(ivp(F), al2), imul(ivp(az), r));
+    const Iv nx = iadd(imul(ivp(F), b.x), imul(ivp(ax), r)), ny = iadd(imul(ivp(F), b.y), imul(ivp(ay), r));
+    if (imul(nx, den).lo > 0.0 || imul(ny, den).lo > 0.0) return false;  // xe >= 0 and ye >= 0 need <= 0
+    const Iv ad = iabs(den);
+    if (imul(ivp(hz), iabs(nx)).lo > imul(ivp(hx), ad).hi) return false;  // |xe| <= dxx
+    if (imul(ivp(hz), iabs(ny)).lo > imul(ivp(hy), ad).hi) return false;  // |ye| <= dyy (implied by the two tests)
+    // ye dxx <= xe dyy:  -dzz (ny dxx - nx dyy) / den <= 0, i.e. den (ny dxx - nx dyy) >= 0
+    if (imul(den, isub(imul(ny, ivp(hx)), imul(nx, ivp(hy)))).hi < 0.0) return false;
+    return true;
+}
+
+// The increment the body accepts at one (dx, dy), or +inf (double
+// arithmetic; only used to stop the search).
+double surf_point(double F, double az, double hz, double g, double ax, double ay, double hx, double hy, double dx,
+                  double dy)
+{
+    const double dd = dx * dx + dy * dy, al = 1.0 - ax * dx - ay * dy, q = al * al - dd * g;
+    if (!(q > 0.0)) return HUGE_VAL;
+    const double al2 = (-az * al + F * std::sqrt(q)) / g;
+    const double D = hz * al2 - std::min(0.0, std::min(dx * hx, dx * hx + dy * hy));
+    if (!(D > 0.0)) return HUGE_VAL;
+    const double r = std::sqrt(dd + al2 * al2), m = -hz / (F * al2 + az * r);
+    const double xe = m * (F * dx + ax * r), ye = m * (F * dy + ay * r);
+    return (0.0 <= std::min(xe, ye) && ye * hx <= xe * hy && xe <= hx) ? D : HUGE_VAL;
+}
+
+double surf_bb_bound(double F, double az, double hz, double ax, double ay, double hx, double hy)
+{
+    const double g = F * F - az * az;
+    if (!(g > 0.0 && hx > 0.0 && hy > 0.0 && hz > 0.0 && F > 0.0)) return 0.0;
+    const double ain = std::sqrt(ax * ax + ay * ay), sg = std::sqrt(g);
+    if (!(ain < 0.99 * sg)) return 0.0;
+    const double R = 1.0 / (sg - ain) * (1.0 + 1e-9);
+    Box root{{-R, ax > 0.0 ? 0.0 : R}, {-R, ay > 0.0 ? 0.0 : R}};
+    using Item = std::pair<double, Box>;
+    auto cmp = [](const Item &a, const Item &b) { return a.first > b.first; };
+    std::priority_queue<Item, std::vector<Item>, decltype(cmp)> heap(cmp);
+    Iv D;
+    if (surf_increment(F, az, hz, g, ax, ay, hx, hy, root, D)) heap.push({D.lo, root});
+    const double min_width = R * 1e-12;
+    double frozen = HUGE_VAL;
+    double seen = HUGE_VAL;
+    for (int it = 0; it < 6000 && !heap.empty(); ++it) {
+        const Item top = heap.top();
+        if (top.first >= 0.99 * seen) break;
+        heap.pop();
+        const Box b = top.second;
+        seen = std::min(seen, surf_point(F, az, hz, g, ax, ay, hx, hy, 0.5 * (b.x.lo + b.x.hi), 0.5 * (b.y.lo + b.y.hi)));
+        const bool along_x = (b.x.hi - b.x.lo) >= (b.y.hi - b.y.lo);
+        const Iv w = along_x ? b.x : b.y;
+        const double mid = 0.5 * (w.lo + w.hi);
+        if (!(w.hi - w.lo > min_width) || !(mid > w.lo && mid < w.hi)) {
+            frozen = std::min(frozen, top.first);
+            continue;
+        }
+        Box h0 = b, h1 = b;
+        if (along_x) {
+            h0.x.hi = mid;
+            h1.x.lo = mid;
+        } else {
+            h0.y.hi = mid;
+            h1.y.lo = mid;
+        }
+        for (const Box &h : {h0, h1})
+            if (surf_increment(F, az, hz, g, ax, ay, hx, hy, h, D)) heap.push({D.lo, h});
+    }
+    double bound = frozen;
+    if (!heap.empty()) bound = std::min(bound, heap.top().first);
+    if (bound == HUGE_VAL) return 0.0;
+    return std::max(bound, 0.0);
 }
 
 // FoldEdge2Points call with arguments (F, ax, ay, az, dxx=hx, dzz=hz),
@@ -211,6 +327,13 @@ SurfK surf_consts(double F, double ax, double ay, double az, double hx, double h
     k.e2 = (ay > 0.0);
     k.nblock = (ax * hz + az * hx > 0.0);  // :170
     k.nest = edge_consts(F, ay, (ax * hz + az * hx) / hxz, (-ax * hx + az * hz) / hxz, hy, hxz);  // :172-173
+    // body-skip bound (fold3d_fast.cuh, 3.): the larger of the physical bound
+    // and the searched one, less the relative margin
+    k.B = surf_skip_bound(F, ax, ay, az, hz);
+    if (F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
+        const double bb = surf_bb_bound(F, az, hz, ax, ay, hx, hy) * (1.0 - 1e-3);
+        if (std::isfinite(bb) && bb > k.B) k.B = bb;
+    }
     return k;
 }
 
@@ -228,7 +351,6 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
     t.F = F;
     t.az = az;
     t.hz = hz;
-    t.Bs = surf_skip_bound(F, ax, ay, az, hz);
     t.g = F * F - az * az;  // :147
     t.rg = safe_recip(t.g);
     // 1-D normal candidate, :214-228, up to the final addition

@@ -47,8 +47,8 @@ LocalFrameH host_frame(int dir, const double h[3], double F, const double a[3])
 
 void clear_bounds(SideTable &t)
 {
-    t.Bs = 0.0;
     for (int k = 0; k < 8; ++k) {
+        t.surf[k].B = 0.0;
         t.edge[k].B = 0.0;
         t.surf[k].nest.B = 0.0;
     }
@@ -95,9 +95,9 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
     return 0;
 }
 
-// The skip bounds of every direction and side: 17 values at
-// out[17 (2 dir + side)]: Bs, the eight edge calls' B, the eight nested
-// edges' B.
+// The skip bounds of every direction and side: 24 values at
+// out[24 (2 dir + side)]: the eight FoldSurf3Points calls' B, the eight
+// FoldEdge2Points calls' B, the eight nested edges' B.
 extern "C" void fast_host_bounds(double dx, double dy, double dz, double F, double a0, double a1, double a2,
                                  double *out)
 {
@@ -106,11 +106,11 @@ extern "C" void fast_host_bounds(double dx, double dy, double dz, double F, doub
         DirTable t;
         build_dir_table(host_frame(dir, h, F, a), t);
         for (int sd = 0; sd < 2; ++sd) {
-            double *o = out + 17 * (2 * dir + sd);
-            o[0] = t.side[sd].Bs;
+            double *o = out + 24 * (2 * dir + sd);
             for (int k = 0; k < 8; ++k) {
-                o[1 + k] = t.side[sd].edge[k].B;
-                o[9 + k] = t.side[sd].surf[k].nest.B;
+                o[k] = t.side[sd].surf[k].B;
+                o[8 + k] = t.side[sd].edge[k].B;
+                o[16 + k] = t.side[sd].surf[k].nest.B;
             }
         }
     }

@@ -140,29 +140,59 @@ def _edge_sampled_inf(F, ax, ay, az, hx, hz, n=200001):
     return float((hz * c - mn)[acc].min()) if acc.any() else math.inf
 
 
+def _surf_sampled_inf(F, ax, ay, az, hx, hy, hz, n=601):
+    """Smallest increment over min(s0, s1, s2) that a FoldSurf3Points call
+    with these arguments accepts (AN_ISO_1_OpenACC.c:131-165), over an n x n
+    grid of the gradients (dx, dy) covering the disc where its square root
+    is real; an upper estimate of the true infimum (inf when no sample is
+    accepted, None when the disc is not bounded)."""
+    g = F * F - az * az
+    ain = math.hypot(ax, ay)
+    if not (g > 0 and ain < math.sqrt(g)):
+        return None
+    R = 1 / (math.sqrt(g) - ain)
+    xs = np.linspace(-R, 0.0 if ax > 0 else R, n)
+    ys = np.linspace(-R, 0.0 if ay > 0 else R, n)
+    dx, dy = np.meshgrid(xs, ys)
+    dd = dx * dx + dy * dy
+    al = 1 - ax * dx - ay * dy
+    q = al * al - dd * g
+    ok = q > 0
+    al2 = (-az * al + F * np.sqrt(np.where(ok, q, 0))) / g
+    mn = np.minimum(0, np.minimum(dx * hx, dx * hx + dy * hy))
+    inc = hz * al2 - mn
+    r = np.sqrt(dd + al2 * al2)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d2 = -hz / (F * al2 + az * r)
+        xe, ye = d2 * (F * dx + ax * r), d2 * (F * dy + ay * r)
+        acc = ok & (inc > 0) & (np.minimum(xe, ye) >= 0) & (ye * hx <= xe * hy) & (xe <= hx)
+    return float(inc[acc].min()) if acc.any() else math.inf
+
+
 @pytest.mark.parametrize("F,a,h", [(REF_F, REF_A, (0.7, 0.9, 1.1)), (REF_F, REF_A, (1.0, 1.0, 1.0)),
                                    (1.3, (0.2, -0.5, 0.3), (1.0, 0.6, 0.8)), (0.8, (0.3, -0.2, -0.4), (0.5, 0.5, 0.5)),
                                    (1.0, (0.6, 0.5, 0.6), (0.5, 0.5, 0.5))])
 def test_skip_bounds_are_proved_lower_bounds(host, F, a, h):
-    """Bs = dzz / (F + az) (1 - 1e-3) where F^2 >= 1.1 |a|^2 (0 otherwise),
-    az the drift along the normal towards the target (negated on the negative
-    side).  Every edge call's B (AN_ISO_1_OpenACC.c:242-253, and the nested
-    calls :172-173, with each call's own arguments) is at least the analytic
-    bound of fold3d_fast.cuh 4. and at most the smallest accepted increment
-    found by dense sampling; in the reference's medium the branch-and-bound
-    search brings it within 2% of that."""
-    out = np.zeros(6 * 2 * 17)
+    """Every FoldSurf3Points call's B (AN_ISO_1_OpenACC.c:233-240) is at
+    least the physical bound dzz / (F + az) (1 - 1e-3), az the drift along
+    the normal towards the target (negated on the negative side); every
+    FoldEdge2Points call's B (:242-253, and the nested calls :172-173, with
+    each call's own arguments) is at least the analytic bound of
+    fold3d_fast.cuh 4.  Each is at most the smallest accepted increment found
+    by dense sampling, and all are 0 where F^2 < 1.1 |a|^2.  In the
+    reference's medium the searches bring the edge bounds within 2% of the
+    sampled infimum and the triangle bounds within 10%."""
+    out = np.zeros(6 * 2 * 24)
     host.fast_host_bounds(*h, F, *a, out.ctypes.data)
-    out = out.reshape(6, 2, 17)
+    out = out.reshape(6, 2, 24)
     strong = F * F < 1.1 * sum(x * x for x in a)
-    tight = []
+    tight, tight_s = [], []
     for d, (nrm, sg, xa, xs, ya, ys) in enumerate(_DIRS):
         for side in (0, 1):
             s = -1 if side else 1
             ax, ay, az = s * xs * a[xa], s * ys * a[ya], s * sg * a[nrm]
             hx, hy, hz = h[xa], h[ya], h[nrm]
             hxy, hxz, hyz = math.hypot(hx, hy), math.hypot(hx, hz), math.hypot(hy, hz)
-            assert out[d, side, 0] == (0.0 if strong else pytest.approx(hz / (F + az) * (1 - 1e-3), rel=1e-14))
             edges = [(ax, ay, az, hx, hz), ((ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz),
                      (ay, ax, az, hy, hz), (-(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz),
                      (-ax, ay, az, hx, hz), (-(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz),
@@ -171,8 +201,18 @@ def test_skip_bounds_are_proved_lower_bounds(host, F, a, h):
                      (-ay, -ax, hy, hx, hyz), (-ay, ax, hy, hx, hyz), (ay, ax, hy, hx, hyz), (ay, -ax, hy, hx, hyz)]
             nests = [(say, (sax * hz + az * shx) / shxz, (-sax * shx + az * hz) / shxz, shy, shxz)
                      for sax, say, shx, shy, shxz in surfs]
+            for k, (sax, say, shx, shy, _) in enumerate(surfs):
+                B = out[d, side, k]
+                if strong:
+                    assert B == 0.0
+                    continue
+                assert B >= hz / (F + az) * (1 - 1e-3) * (1 - 1e-12)
+                inf = _surf_sampled_inf(F, sax, say, az, shx, shy, hz)
+                if inf is not None and inf < math.inf:
+                    assert B <= inf
+                    tight_s.append(B / inf)
             for k, (cax, cay, caz, chx, chz) in enumerate(edges + nests):
-                B = out[d, side, 1 + k]
+                B = out[d, side, 8 + k]
                 if strong:
                     assert B == 0.0
                     continue
@@ -184,9 +224,9 @@ def test_skip_bounds_are_proved_lower_bounds(host, F, a, h):
                     assert B <= inf
                     tight.append(B / inf)
     if F == REF_F:
-        assert min(tight) > 0.98
+        assert min(tight) > 0.98 and min(tight_s) > 0.9
     if not strong:
-        assert (out[:, :, 0] > 0).all() and (out[:, :, 1:] > 0).any()
+        assert (out[:, :, :8] > 0).all() and (out[:, :, 8:] > 0).any()
 
 
 @pytest.fixture(scope="module")
