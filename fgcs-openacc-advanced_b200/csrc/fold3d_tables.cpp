@@ -9,6 +9,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <new>
 #include <queue>
 #include <vector>
 
@@ -133,7 +135,7 @@ double edge_point(const EdgeK &k, double F, double d)
 }
 
 // The proved lower bound (0 when the search does not apply).
-double edge_bb_bound(const EdgeK &k, double F)
+double edge_bb_search(const EdgeK &k, double F)
 {
     if (!(k.g > 0.0 && k.ga > 0.0 && k.hx > 0.0 && k.hz > 0.0 && F > 0.0)) return 0.0;
     const double sga = std::sqrt(k.ga);
@@ -226,7 +228,7 @@ double surf_point(double F, double az, double hz, double g, double ax, double ay
     return (0.0 <= std::min(xe, ye) && ye * hx <= xe * hy && xe <= hx) ? D : HUGE_VAL;
 }
 
-double surf_bb_bound(double F, double az, double hz, double ax, double ay, double hx, double hy)
+double surf_bb_search(double F, double az, double hz, double ax, double ay, double hx, double hy)
 {
     const double g = F * F - az * az;
     if (!(g > 0.0 && hx > 0.0 && hy > 0.0 && hz > 0.0 && F > 0.0)) return 0.0;
@@ -270,6 +272,26 @@ double surf_bb_bound(double F, double az, double hz, double ax, double ay, doubl
     if (!heap.empty()) bound = std::min(bound, heap.top().first);
     if (bound == HUGE_VAL) return 0.0;
     return std::max(bound, 0.0);
+}
+
+// The searches run inside the C entry points: an allocation failure there
+// gives the bound 0, which skips nothing and is always valid.
+double edge_bb_bound(const EdgeK &k, double F)
+{
+    try {
+        return edge_bb_search(k, F);
+    } catch (...) {
+        return 0.0;
+    }
+}
+
+double surf_bb_bound(double F, double az, double hz, double ax, double ay, double hx, double hy)
+{
+    try {
+        return surf_bb_search(F, az, hz, ax, ay, hx, hy);
+    } catch (...) {
+        return 0.0;
+    }
 }
 
 // FoldEdge2Points call with arguments (F, ax, ay, az, dxx=hx, dzz=hz),
@@ -404,15 +426,18 @@ void build_dir_table(const LocalFrameH &L, DirTable &out)
         bool used;
     };
     constexpr int kEntries = 12;
-    thread_local std::vector<Entry> memo(kEntries);
+    thread_local std::unique_ptr<Entry[]> memo;
     thread_local int next = 0;
-    for (const Entry &e : memo)
-        if (e.used && std::memcmp(&e.key, &L, sizeof L) == 0) {
-            out = e.tab;
-            return;
-        }
+    if (!memo) memo.reset(new (std::nothrow) Entry[kEntries]());  // stays empty if that fails
+    if (memo)
+        for (int i = 0; i < kEntries; ++i)
+            if (memo[i].used && std::memcmp(&memo[i].key, &L, sizeof L) == 0) {
+                out = memo[i].tab;
+                return;
+            }
     side_table(L, false, out.side[0]);
     side_table(L, true, out.side[1]);
+    if (!memo) return;
     Entry &e = memo[next];
     next = (next + 1) % kEntries;
     e.key = L;
