@@ -50,7 +50,7 @@
 //    relative where F^2 >= 1.1 |a|^2, through the square root of a cancelled
 //    difference); 0 for stronger drifts.
 //
-// 4. FoldEdge2Points bodies get a weaker gate of the same kind, B in EdgeK.
+// 4. FoldEdge2Points bodies get a gate of the same kind, B in EdgeK.
 //    Its footpoint test (:88,92) does not follow the ray of its own root: it
 //    uses the direction w = (F'/F) p/|p| + a2 (F' = sqrt(F^2 - ay^2),
 //    a2 = (ax, az), p = (d, c) the plane wave's slowness, which satisfies
@@ -63,8 +63,11 @@
 //      - F' > |a2| (so |p| <= 1 / (F' - |a2|)), and
 //      - F >= 1 with az >= 0, or F <= 1 with az <= 0 (then w_z > 0 too),
 //    p.w >= 1 - F'(1 - 1/F) / (F' - |a2|) for F >= 1 (>= 1 for F <= 1) and
-//    w_z <= F'/F + az, which gives B (less the same relative 1e-3 margin);
-//    elsewhere B = 0.  The fall-back candidate from s1 alone is not gated.
+//    w_z <= F'/F + az, which gives one bound; elsewhere it is 0.  B is the
+//    larger of that and one proved per call site by an interval search over
+//    the body's single gradient d (fold3d_tables.cpp), less the same
+//    relative 1e-3 margin.  The fall-back candidate from s1 alone is not
+//    gated.
 #pragma once
 #include <cstdint>
 #include <cstring>
