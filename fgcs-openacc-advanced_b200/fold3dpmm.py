@@ -277,7 +277,8 @@ class Context:
 
     def __init__(self, device: int = 0):
         self._h = C.c_void_p()
-        _check(lib().fold3d_create(C.byref(self._h), int(device)))
+        self.device = int(device)
+        _check(lib().fold3d_create(C.byref(self._h), self.device))
 
     def close(self):
         if self._h:
@@ -327,14 +328,34 @@ def ellip_metric(vz, eps, axis):
     return list(out)
 
 
-def ellip(M):
-    """fold3d_ellip from six contiguous float32 CUDA tensors (xx xy xz yy yz zz)."""
+def ellip(M, like=None):
+    """fold3d_ellip from six contiguous float32 CUDA tensors (xx xy xz yy yz
+    zz).  like: the field they go with; every array must then have its shape
+    and device, since the kernels read the metric at the field's indices and
+    the library cannot check the size behind a pointer."""
     import torch
 
+    if len(M) != 6:
+        raise ValueError("a metric is six arrays (xx xy xz yy yz zz), got %d" % len(M))
     for m in M:
+        if like is not None and (tuple(m.shape) != tuple(like.shape) or m.device != like.device):
+            raise ValueError("metric arrays must have the field's shape %s and device %s, got %s on %s"
+                             % (tuple(like.shape), like.device, tuple(m.shape), m.device))
         if m.dtype != torch.float32 or not m.is_cuda or not m.is_contiguous():
             raise ValueError("metric arrays must be contiguous float32 CUDA tensors")
     return Ellip(*(C.c_void_p(m.data_ptr()) for m in M))
+
+
+def _on_context(ctx, T, name="field"):
+    """T must live on the context's device."""
+    if getattr(T, "is_cuda", False) and T.device.index != ctx.device:
+        raise ValueError("%s is on %s but the context is on cuda:%d" % (name, T.device, ctx.device))
+
+
+def _same_length(**lists):
+    n = {k: len(v) for k, v in lists.items()}
+    if len(set(n.values())) > 1:
+        raise ValueError("batch lists differ in length: %s" % n)
 
 
 NOALLOC_MAX_SWEEPS = 4096
@@ -370,8 +391,9 @@ def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> 
     layout)."""
     nx, ny, nz = grid_of(T)
     rep = Report()
-    e = ellip(M)
+    e = ellip(M, T)
     ptr, f32 = _field_ptr(T)
+    _on_context(ctx, T)
     _check(_entry("fold3d_solve_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr,
                                              C.byref(o or opts()), C.c_void_p(stream) if stream else None,
                                              C.byref(rep)))
@@ -397,7 +419,8 @@ def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream
     nx, ny, nz = grid_of(T)
     rep = Report()
     ptr, f32 = _field_ptr(T)
-    _check(_entry("fold3d_solve_ellip_record", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), ptr,
+    _on_context(ctx, T)
+    _check(_entry("fold3d_solve_ellip_record", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M, T)), ptr,
                                            C.c_void_p(W.data_ptr()), C.byref(o or opts()),
                                            C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
@@ -416,7 +439,8 @@ def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, 
     nx, ny, nz = grid_of(T)
     rep = Report()
     ptr, f32 = _field_ptr(T)
-    _check(_entry("fold3d_adjoint_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M)), ptr,
+    _on_context(ctx, T)
+    _check(_entry("fold3d_adjoint_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M, T)), ptr,
                                                C.c_void_p(W.data_ptr()), C.c_void_p(dLdT.data_ptr()),
                                                C.c_void_p(lam.data_ptr()), C.c_void_p(dLdM.data_ptr()),
                                                int(max_sweeps), float(tol), C.c_void_p(stream) if stream else None,
@@ -430,13 +454,15 @@ def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream
     uint8 winner records shaped like fields[i].  Returns the per-instance
     reports."""
     n = len(fields)
+    _same_length(fields=fields, hs=hs, media=media, **({} if winners is None else {"winners": winners}))
     arr = (Instance * n)()
     kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
-        arr[i].medium = ellip(M)
+        arr[i].medium = ellip(M, T)
         arr[i].T, f32 = _field_ptr(T)
+        _on_context(ctx, T, "fields[%d]" % i)
         kinds.add(f32)
         if winners is not None and winners[i] is not None:
             _check_like("winners[%d]" % i, winners[i], T, 1)
@@ -456,6 +482,7 @@ def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, m
     accumulate: dLdM[i] += the gradient (instances may share one dLdM).
     Returns the per-instance reports."""
     n = len(fields)
+    _same_length(fields=fields, hs=hs, media=media, winners=winners, dLdT=dLdT, lam=lam, dLdM=dLdM)
     arr = (AdjInstance * n)()
     kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
@@ -465,8 +492,9 @@ def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, m
         _check_like("dLdM[%d]" % i, dLdM[i], T, lead=(6,))
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
-        arr[i].medium = ellip(M)
+        arr[i].medium = ellip(M, T)
         arr[i].T, f32 = _field_ptr(T)
+        _on_context(ctx, T, "fields[%d]" % i)
         kinds.add(f32)
         arr[i].winners = winners[i].data_ptr()
         arr[i].dLdT = dLdT[i].data_ptr()

@@ -260,3 +260,25 @@ def test_newer_entry_points_reject_null_context(f3d, tmp_path):
     for w in ("fold3d_write_text", "fold3d_write_raw"):
         assert getattr(L, w)(None, T.ctypes.data_as(C.c_void_p), C.byref(g)) == f3d.ERR_INVALID
     assert L.fold3d_write_vtk(None, T.ctypes.data_as(C.c_void_p), C.byref(g), 0) == f3d.ERR_INVALID
+
+
+def test_binding_rejects_metric_and_batch_mismatches(f3d):
+    """The Python binding checks what the C ABI cannot see behind a pointer
+    before any call: a metric is six arrays with the field's shape and
+    device, and a batch's lists have one entry per instance."""
+    import torch
+
+    T = torch.zeros(6, 7, 8, dtype=torch.float64)
+    M = [torch.zeros(6, 7, 8, dtype=torch.float32) for _ in range(6)]
+    with pytest.raises(ValueError, match="six arrays"):
+        f3d.ellip(M[:5], T)
+    small = [torch.zeros(4, 5, 6, dtype=torch.float32) for _ in range(6)]  # interior only: would be read past its end
+    with pytest.raises(ValueError, match="field's shape"):
+        f3d.ellip(small, T)
+    with pytest.raises(ValueError, match="differ in length"):
+        f3d.solve_batch(None, [T, T], [1.0, 1.0], [M])
+    with pytest.raises(ValueError, match="differ in length"):
+        f3d.solve_batch(None, [T], [1.0], [M], winners=[])
+    W = torch.zeros(6, 7, 8, dtype=torch.uint8)
+    with pytest.raises(ValueError, match="differ in length"):
+        f3d.adjoint_batch(None, [T, T], [1.0, 1.0], [M, M], [W, W], [T, T], [T], [T, T])
