@@ -311,10 +311,13 @@ class Context:
         s = C.c_void_p(stream) if stream else None
         if isinstance(T, np.ndarray) or not T.is_cuda:
             src = _any_host_ptr(T)
+            if out is not None and tuple(out.shape) != tuple(T.shape):  # the library writes a whole field
+                raise ValueError("out must have the field's shape %s, got %s" % (tuple(T.shape), tuple(out.shape)))
             dst = _any_host_ptr(out) if out is not None else src
             _check(lib().fold3d_solve_host(self._h, C.byref(g), C.byref(med), src, dst, C.byref(o), s,
                                            C.byref(rep)))
         else:
+            _on_context(self, T)
             _check(lib().fold3d_solve(self._h, C.byref(g), C.byref(med), _dev_ptr(T), C.byref(o), s,
                                       C.byref(rep)))
         return rep

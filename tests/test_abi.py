@@ -282,3 +282,16 @@ def test_binding_rejects_metric_and_batch_mismatches(f3d):
     W = torch.zeros(6, 7, 8, dtype=torch.uint8)
     with pytest.raises(ValueError, match="differ in length"):
         f3d.adjoint_batch(None, [T, T], [1.0, 1.0], [M, M], [W, W], [T, T], [T], [T, T])
+
+
+def test_host_solve_rejects_a_short_output(f3d):
+    """Context.solve's host path writes a whole field into `out`: a smaller
+    array is refused before the library is called."""
+    import numpy as np
+
+    ctx = object.__new__(f3d.Context)  # no device needed: the check comes first
+    ctx._h, ctx.device = None, 0
+    T = np.zeros((6, 7, 8))
+    with pytest.raises(ValueError, match="field's shape"):
+        f3d.Context.solve(ctx, T, 1.0, out=np.zeros((6, 7, 7)))
+    ctx._h = C.c_void_p()  # keep __del__ from closing anything
