@@ -228,6 +228,7 @@ def init_implicit_device(ctx: "Context", T, h, med: Medium | None = None, stream
     """fold3d_init_implicit_device: the implicit-surface initialiser into the
     device field T (float64 CUDA tensor, field layout)."""
     nx, ny, nz = grid_of(T)
+    _on_context(ctx, T)
     _check(lib().fold3d_init_implicit_device(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(med or medium()),
                                              _dev_ptr(T), C.c_void_p(stream) if stream else None))
 
