@@ -37,6 +37,8 @@ def _note(kind, rep):
 
 
 def context(device=None) -> f3d.Context:
+    """The library context of a device (default: the current one), created
+    once per process."""
     dev = torch.cuda.current_device() if device is None else device
     if dev not in _ctx:
         _ctx[dev] = f3d.Context(dev)
@@ -50,7 +52,7 @@ class EllipSolve(torch.autograd.Function):
         T = T0.detach().clone()
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         ctx.mdtypes = [m.dtype for m in M]
-        rep = _note("forward", f3d.solve_ellip_record(context(), T, h, M32, W,
+        rep = _note("forward", f3d.solve_ellip_record(context(T.device.index), T, h, M32, W,
                                                       f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol)))
         ctx.save_for_backward(T, W, *M32)
         ctx.h = h
@@ -63,8 +65,8 @@ class EllipSolve(torch.autograd.Function):
         T, W, *M32 = ctx.saved_tensors
         lam = torch.empty_like(T)
         dLdM = torch.empty((6,) + tuple(T.shape), dtype=T.dtype, device=T.device)
-        _note("adjoint", f3d.adjoint_ellip(context(), T, ctx.h, M32, W, gT.to(T.dtype).contiguous(), lam, dLdM,
-                                           tol=ctx.adj_tol))
+        _note("adjoint", f3d.adjoint_ellip(context(T.device.index), T, ctx.h, M32, W, gT.to(T.dtype).contiguous(),
+                                           lam, dLdM, tol=ctx.adj_tol))
         return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(6))
 
 
@@ -85,7 +87,7 @@ class EllipSolveBatch(torch.autograd.Function):
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         S = T.shape[0]
         ctx.mdtypes = [m.dtype for m in M]
-        reps = f3d.solve_batch(context(), [T[s] for s in range(S)], [h] * S, [M32] * S,
+        reps = f3d.solve_batch(context(T.device.index), [T[s] for s in range(S)], [h] * S, [M32] * S,
                                f3d.opts(max_sweeps=max_sweeps, fixed=False, tol=tol),
                                winners=[W[s] for s in range(S)])
         for r in reps:
@@ -102,7 +104,7 @@ class EllipSolveBatch(torch.autograd.Function):
         gT = gT.to(T.dtype).contiguous()
         lam = torch.empty_like(T)
         dLdM = torch.zeros((6,) + tuple(T.shape[1:]), dtype=T.dtype, device=T.device)
-        reps = f3d.adjoint_batch(context(), [T[s] for s in range(S)], [ctx.h] * S, [M32] * S,
+        reps = f3d.adjoint_batch(context(T.device.index), [T[s] for s in range(S)], [ctx.h] * S, [M32] * S,
                                  [W[s] for s in range(S)], [gT[s] for s in range(S)], [lam[s] for s in range(S)],
                                  [dLdM] * S, tol=ctx.adj_tol, accumulate=True)
         for r in reps:
