@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <functional>
 #include <memory>
 #include <new>
@@ -45,11 +46,11 @@ double surface(double x, double y, double z)
            (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
 }
 
-// surface() with sin(x) and cos(y + x) given (the same values, computed once
-// per node column and row of the grid).
-inline double surface_tab(double x, double y, double z, double sin_x, double cos_yx)
+// surface() with sin(x), cos(y + x) and sin(x + y + z) given (the same
+// values, computed once per node column, row or distinct argument).
+inline double surface_tab(double x, double y, double z, double sin_x, double cos_yx, double sin_xyz)
 {
-    return 5.0 + (sin_x + cos_yx + std::sin(x + y + z)) * 0.4 - z + (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
+    return 5.0 + (sin_x + cos_yx + sin_xyz) * 0.4 - z + (x - 5.0) * (y - 5.0) * (z - 5) / 55.0;
 }
 
 constexpr fold3d_seed::NodeStep kSteps[fold3d_seed::kNodeSteps] = FOLD3D_SEED_STEPS;
@@ -108,32 +109,76 @@ void parallel_for(int lo, int hi, int nthreads, Fn fn)
 
 namespace fold3d {
 
-// The tables of surface_planes: sin(x_i) (nx+2 values) and cos(y_j + x_i)
-// ((ny+2) rows of nx+2).
-void surface_tables(const fold3d_grid &g, double *sin_x, double *cos_yx, int nth)
+bool surface_tables(const fold3d_grid &g, SurfaceTables &t, int nth)
 {
     const int nx = g.nx, ny = g.ny;
-    const long long sy = nx + 2;
-    for (int i = 0; i < nx + 2; ++i) sin_x[i] = std::sin((i - 1) * g.dx + 0.);
+    const size_t sy = (size_t)nx + 2, pairs = sy * (ny + 2);
+    try {
+        t.sin_x.resize(sy);
+        t.cos_yx.resize(pairs);
+        t.sums.clear();
+        t.sum_of.clear();
+    } catch (...) {
+        return false;
+    }
+    for (int i = 0; i < nx + 2; ++i) t.sin_x[i] = std::sin((i - 1) * g.dx + 0.);
     parallel_for(0, ny + 2, nth, [&](int j) {
         const double y = (j - 1) * g.dy + 0.;
-        for (int i = 0; i < nx + 2; ++i) cos_yx[(size_t)j * sy + i] = std::cos(y + ((i - 1) * g.dx + 0.));
+        for (int i = 0; i < nx + 2; ++i) t.cos_yx[(size_t)j * sy + i] = std::cos(y + ((i - 1) * g.dx + 0.));
     });
+    // the distinct rounded sums x_i + y_j (compared as bits); kept only when
+    // they are at most half of the pairs
+    try {
+        std::vector<uint64_t> bits(pairs);
+        for (int j = 0; j < ny + 2; ++j) {
+            const double y = (j - 1) * g.dy + 0.;
+            for (int i = 0; i < nx + 2; ++i) {
+                const double u = ((i - 1) * g.dx + 0.) + y;
+                std::memcpy(&bits[(size_t)j * sy + i], &u, sizeof u);
+            }
+        }
+        std::vector<uint64_t> uniq(bits);
+        std::sort(uniq.begin(), uniq.end());
+        uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+        if (uniq.size() * 2 > pairs) return true;
+        t.sums.resize(uniq.size());
+        for (size_t d = 0; d < uniq.size(); ++d) std::memcpy(&t.sums[d], &uniq[d], sizeof(double));
+        t.sum_of.resize(pairs);
+        for (size_t q = 0; q < pairs; ++q)
+            t.sum_of[q] = (int)(std::lower_bound(uniq.begin(), uniq.end(), bits[q]) - uniq.begin());
+    } catch (...) {
+        t.sums.clear();  // evaluate every node directly instead
+        t.sum_of.clear();
+    }
+    return true;
 }
 
 // Implicit surface (Fold3dPMM.c:137-147) on node planes k0 <= k < k1, ghosts
 // included, into IF (plane k0 first).
-void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const double *sin_x, const double *cos_yx,
-                    int nth)
+void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const SurfaceTables &t, int nth)
 {
     const long long sy = g.nx + 2, sz = sy * (g.ny + 2);
     parallel_for(k0, k1, nth, [&](int k) {
         const double z = (k - 1) * g.dz + 0.;
+        std::vector<double> sin_u;  // sin(sum + z) for each distinct sum of the tables
+        if (!t.sums.empty()) {
+            try {
+                sin_u.resize(t.sums.size());
+                for (size_t d = 0; d < t.sums.size(); ++d) sin_u[d] = std::sin(t.sums[d] + z);
+            } catch (...) {
+                sin_u.clear();
+            }
+        }
         for (int j = 0; j < g.ny + 2; ++j) {
             const double y = (j - 1) * g.dy + 0.;
             double *row = IF + sz * (k - k0) + sy * j;
-            for (int i = 0; i < g.nx + 2; ++i)
-                row[i] = surface_tab((i - 1) * g.dx + 0., y, z, sin_x[i], cos_yx[(size_t)j * sy + i]);
+            const size_t r = (size_t)j * sy;
+            for (int i = 0; i < g.nx + 2; ++i) {
+                const double x = (i - 1) * g.dx + 0.;
+                // x + y + z rounds as (x + y) + z: the tabulated sum plus z
+                const double sxyz = sin_u.empty() ? std::sin(x + y + z) : sin_u[t.sum_of[r + i]];
+                row[i] = surface_tab(x, y, z, t.sin_x[i], t.cos_yx[r + i], sxyz);
+            }
         }
     });
 }
@@ -176,15 +221,9 @@ int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m
     const int nth = host_threads();
     const double hx = g->dx, hy = g->dy, hz = g->dz;
     // :137-147, node coordinates from x/y/z (:115-126)
-    std::vector<double> sin_x, cos_yx;
-    try {
-        sin_x.resize(nx + 2);
-        cos_yx.resize((size_t)sy * (ny + 2));
-    } catch (...) {
-        return FOLD3D_ERR_NOMEM;
-    }
-    fold3d::surface_tables(*g, sin_x.data(), cos_yx.data(), nth);
-    fold3d::surface_planes(IF, *g, 0, nz + 2, sin_x.data(), cos_yx.data(), nth);
+    fold3d::SurfaceTables tabs;
+    if (!fold3d::surface_tables(*g, tabs, nth)) return FOLD3D_ERR_NOMEM;
+    fold3d::surface_planes(IF, *g, 0, nz + 2, tabs, nth);
     parallel_for(0, nz + 2, nth, [&](int k) {
         for (long long id = sz * k; id < sz * (k + 1); ++id) T[id] = (side(IF[id]) * 1.0) * kMaxT;
     });

@@ -84,8 +84,8 @@ int init_implicit_device(const fold3d_grid &g, const fold3d_medium &m, double *T
 {
     const long long sy = g.nx + 2, sz = sy * (g.ny + 2), cells = sz * (g.nz + 2);
     const int nth = init_threads();
-    std::vector<double> sin_x(g.nx + 2), cos_yx((size_t)sz);
-    surface_tables(g, sin_x.data(), cos_yx.data(), nth);
+    SurfaceTables tabs;
+    if (!surface_tables(g, tabs, nth)) return set_error(FOLD3D_ERR_NOMEM, "surface tables");
     cudaEvent_t done[2];
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2; ++b)
@@ -96,7 +96,7 @@ int init_implicit_device(const fold3d_grid &g, const fold3d_medium &m, double *T
     for (int k0 = 0; k0 < g.nz + 2 && e == cudaSuccess; k0 += (int)stage_planes, b ^= 1) {
         const int k1 = std::min(g.nz + 2, k0 + (int)stage_planes);
         if (used[b] && (e = cudaEventSynchronize(done[b])) != cudaSuccess) break;  // its last copy is done
-        surface_planes(stage[b], g, k0, k1, sin_x.data(), cos_yx.data(), nth);
+        surface_planes(stage[b], g, k0, k1, tabs, nth);
         if ((e = cudaMemcpyAsync(IF_dev + sz * k0, stage[b], (size_t)sz * (k1 - k0) * sizeof(double),
                                  cudaMemcpyHostToDevice, s)) != cudaSuccess ||
             (e = cudaEventRecord(done[b], s)) != cudaSuccess)

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "fold3dpmm.h"
 
@@ -118,10 +119,20 @@ struct WaveArgs {
     unsigned char *winners;      // elliptical medium: winner records, or NULL
     int dir;                     // direction of the pass (for the winner records)
 };
-// Host sampling of the implicit surface (fold3d_init.cpp).
-void surface_tables(const fold3d_grid &g, double *sin_x, double *cos_yx, int nth);
-void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const double *sin_x, const double *cos_yx,
-                    int nth);
+// Host sampling of the implicit surface (fold3d_init.cpp).  The tables hold
+// the factors of Fold3dPMM.c:29-33 that do not depend on every coordinate:
+// sin(x_i), cos(y_j + x_i) and, when the rounded sums x_i + y_j take few
+// distinct values (equal or commensurate spacings), those values and each
+// (i, j)'s index among them, so that each plane evaluates sin(x + y + z) once
+// per distinct sum (the same arguments, so the same bits).
+struct SurfaceTables {
+    std::vector<double> sin_x;   // nx + 2 values
+    std::vector<double> cos_yx;  // (ny + 2) rows of nx + 2
+    std::vector<double> sums;    // distinct x_i + y_j, or empty
+    std::vector<int> sum_of;     // index into sums of each (i, j), row-major like cos_yx
+};
+bool surface_tables(const fold3d_grid &g, SurfaceTables &t, int nth);  // false: out of memory
+void surface_planes(double *IF, const fold3d_grid &g, int k0, int k1, const SurfaceTables &t, int nth);
 int init_threads();
 // fn(i) for lo <= i < hi on up to nthreads host threads (contiguous ranges).
 void host_parallel_for(int lo, int hi, int nthreads, const std::function<void(int)> &fn);

@@ -111,7 +111,8 @@ def test_product_init_digest(f3d, digests, n):
     assert sha(T) == digests["n%d_init" % n]
 
 
-@pytest.mark.parametrize("dims,h", [((9, 6, 7), (0.7, 0.9, 1.1)), ((20, 13, 17), (0.5, 0.8, 0.6))])
+@pytest.mark.parametrize("dims,h", [((9, 6, 7), (0.7, 0.9, 1.1)), ((20, 13, 17), (0.5, 0.8, 0.6)),
+                                    ((24, 17, 19), (0.5, 0.25, 0.75))])  # the last: few distinct x + y
 def test_product_init_noncubic_matches_oracle(f3d, orc, dims, h):
     med = f3d.medium(1.3, (0.2, -0.5, 0.3))
     T = f3d.init_implicit(*dims, h, med)
