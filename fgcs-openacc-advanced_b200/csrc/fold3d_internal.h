@@ -51,7 +51,10 @@ void clear_error();
 struct DirTable;  // fold3d_fast.cuh
 
 // Per-direction solver constants, evaluated on the host (fold3d_tables.cpp).
-void build_dir_table(const LocalFrameH &L, DirTable &out);
+// The direction table of a frame.  search: prove the tight skip bounds (a
+// host search, memoised per thread); false: closed-form bounds only, with
+// no memory allocated (fold3d_solve_noalloc).
+void build_dir_table(const LocalFrameH &L, DirTable &out, bool search = true);
 
 // Solver variants of the plane kernel.
 enum Variant {

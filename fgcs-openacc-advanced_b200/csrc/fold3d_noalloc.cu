@@ -91,7 +91,7 @@ extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m
         for (int d = 0; d < 6; ++d) {
             const PlaneGeom pg = make_geom(*g, d);
             const LocalFrameH L = make_frame(*g, *m, d);
-            build_dir_table(L, tab);
+            build_dir_table(L, tab, false);  // no search: it would allocate
             int src = pass_first(pg, d);
             for (int p = 0; p < pass_count(pg); ++p, src += kDirs[d].sg)
                 if ((e = launch_plane(T, pg, L, &tab, o->variant, src, slot, s)) != cudaSuccess)

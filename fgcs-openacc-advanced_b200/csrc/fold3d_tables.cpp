@@ -296,7 +296,7 @@ double surf_bb_bound(double F, double az, double hz, double ax, double ay, doubl
 
 // FoldEdge2Points call with arguments (F, ax, ay, az, dxx=hx, dzz=hz),
 // AN_ISO_1_OpenACC.c:59-114.
-EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double hz)
+EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double hz, bool search)
 {
     EdgeK k;
     std::memset(&k, 0, sizeof k);
@@ -313,7 +313,7 @@ EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double h
     k.early = (ax > 0.0);      // :71
     // the larger of two proved lower bounds, less the relative margin
     k.B = edge_skip_bound(F, ax, ay, az, hz);
-    if (F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
+    if (search && F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
         const double bb = edge_bb_bound(k, F) * (1.0 - 1e-3);
         if (std::isfinite(bb) && bb > k.B) k.B = bb;
     }
@@ -335,7 +335,8 @@ EdgeK edge_consts(double F, double ax, double ay, double az, double hx, double h
 
 // FoldSurf3Points call with drift arguments (ax, ay) and spacings
 // (dxx=hx, dyy=hy, dxz=hxz); F, az, dzz are the direction's.  :119-175.
-SurfK surf_consts(double F, double ax, double ay, double az, double hx, double hy, double hz, double hxz)
+SurfK surf_consts(double F, double ax, double ay, double az, double hx, double hy, double hz, double hxz,
+                  bool search)
 {
     SurfK k;
     std::memset(&k, 0, sizeof k);
@@ -348,18 +349,18 @@ SurfK surf_consts(double F, double ax, double ay, double az, double hx, double h
     k.e1 = (ax > 0.0);
     k.e2 = (ay > 0.0);
     k.nblock = (ax * hz + az * hx > 0.0);  // :170
-    k.nest = edge_consts(F, ay, (ax * hz + az * hx) / hxz, (-ax * hx + az * hz) / hxz, hy, hxz);  // :172-173
+    k.nest = edge_consts(F, ay, (ax * hz + az * hx) / hxz, (-ax * hx + az * hz) / hxz, hy, hxz, search);  // :172-173
     // body-skip bound (fold3d_fast.cuh, 3.): the larger of the physical bound
     // and the searched one, less the relative margin
     k.B = surf_skip_bound(F, ax, ay, az, hz);
-    if (F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
+    if (search && F * F >= 1.1 * (ax * ax + ay * ay + az * az)) {
         const double bb = surf_bb_bound(F, az, hz, ax, ay, hx, hy) * (1.0 - 1e-3);
         if (std::isfinite(bb) && bb > k.B) k.B = bb;
     }
     return k;
 }
 
-void side_table(const LocalFrameH &L, bool negative, SideTable &t)
+void side_table(const LocalFrameH &L, bool negative, bool search, SideTable &t)
 {
     std::memset(&t, 0, sizeof t);
     const double F = L.F, hz = L.hz, hx = L.hx, hy = L.hy;
@@ -387,23 +388,23 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
         }
     }
     // the eight FoldSurf3Points calls, :233-240
-    t.surf[0] = surf_consts(F, ax, ay, az, hx, hy, hz, hxz);
-    t.surf[1] = surf_consts(F, ax, -ay, az, hx, hy, hz, hxz);
-    t.surf[2] = surf_consts(F, -ax, -ay, az, hx, hy, hz, hxz);
-    t.surf[3] = surf_consts(F, -ax, ay, az, hx, hy, hz, hxz);
-    t.surf[4] = surf_consts(F, -ay, -ax, az, hy, hx, hz, hyz);
-    t.surf[5] = surf_consts(F, -ay, ax, az, hy, hx, hz, hyz);
-    t.surf[6] = surf_consts(F, ay, ax, az, hy, hx, hz, hyz);
-    t.surf[7] = surf_consts(F, ay, -ax, az, hy, hx, hz, hyz);
+    t.surf[0] = surf_consts(F, ax, ay, az, hx, hy, hz, hxz, search);
+    t.surf[1] = surf_consts(F, ax, -ay, az, hx, hy, hz, hxz, search);
+    t.surf[2] = surf_consts(F, -ax, -ay, az, hx, hy, hz, hxz, search);
+    t.surf[3] = surf_consts(F, -ax, ay, az, hx, hy, hz, hxz, search);
+    t.surf[4] = surf_consts(F, -ay, -ax, az, hy, hx, hz, hyz, search);
+    t.surf[5] = surf_consts(F, -ay, ax, az, hy, hx, hz, hyz, search);
+    t.surf[6] = surf_consts(F, ay, ax, az, hy, hx, hz, hyz, search);
+    t.surf[7] = surf_consts(F, ay, -ax, az, hy, hx, hz, hyz, search);
     // the eight FoldEdge2Points calls, :242-253
-    t.edge[0] = edge_consts(F, ax, ay, az, hx, hz);
-    t.edge[1] = edge_consts(F, (ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz);
-    t.edge[2] = edge_consts(F, ay, ax, az, hy, hz);
-    t.edge[3] = edge_consts(F, -(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz);
-    t.edge[4] = edge_consts(F, -ax, ay, az, hx, hz);
-    t.edge[5] = edge_consts(F, -(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz);
-    t.edge[6] = edge_consts(F, -ay, ax, az, hy, hz);
-    t.edge[7] = edge_consts(F, (ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz);
+    t.edge[0] = edge_consts(F, ax, ay, az, hx, hz, search);
+    t.edge[1] = edge_consts(F, (ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz, search);
+    t.edge[2] = edge_consts(F, ay, ax, az, hy, hz, search);
+    t.edge[3] = edge_consts(F, -(ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz, search);
+    t.edge[4] = edge_consts(F, -ax, ay, az, hx, hz, search);
+    t.edge[5] = edge_consts(F, -(ax * hx + ay * hy) / hxy, (-ax * hy + ay * hx) / hxy, az, hxy, hz, search);
+    t.edge[6] = edge_consts(F, -ay, ax, az, hy, hz, search);
+    t.edge[7] = edge_consts(F, (ax * hx - ay * hy) / hxy, (ax * hy + ay * hx) / hxy, az, hxy, hz, search);
     t.m_e1 = t.m_e2 = t.m_nblock = t.m_nest_early = t.m_edge_early = 0;
     for (int k = 0; k < 8; ++k) {
         t.m_e1 |= (unsigned)(t.surf[k].e1 != 0) << k;
@@ -416,9 +417,14 @@ void side_table(const LocalFrameH &L, bool negative, SideTable &t)
 
 }  // namespace
 
-void build_dir_table(const LocalFrameH &L, DirTable &out)
+void build_dir_table(const LocalFrameH &L, DirTable &out, bool search)
 {
-    // The edge bounds take a search per call site; a solve asks for the same
+    if (!search) {  // closed-form bounds only: nothing allocated
+        side_table(L, false, false, out.side[0]);
+        side_table(L, true, false, out.side[1]);
+        return;
+    }
+    // The skip bounds take a search per call site; a solve asks for the same
     // six frames every sweep, so each thread keeps its last twelve tables.
     struct Entry {
         LocalFrameH key;
@@ -435,8 +441,8 @@ void build_dir_table(const LocalFrameH &L, DirTable &out)
                 out = memo[i].tab;
                 return;
             }
-    side_table(L, false, out.side[0]);
-    side_table(L, true, out.side[1]);
+    side_table(L, false, true, out.side[0]);
+    side_table(L, true, true, out.side[1]);
     if (!memo) return;
     Entry &e = memo[next];
     next = (next + 1) % kEntries;

@@ -56,8 +56,9 @@ void clear_bounds(SideTable &t)
 
 }  // namespace
 
-// Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  With
-// skip == 0 the tables' body-skip bounds are cleared first.
+// Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  skip:
+// 1 the tables as solves build them (searched bounds), 2 the closed-form
+// bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all.
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
                                 double a0, double a1, double a2, int sweeps, int skip)
 {
@@ -66,7 +67,7 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
     DirTable tabs[6];
     for (int dir = 0; dir < 6; ++dir) {
-        build_dir_table(host_frame(dir, h, F, a), tabs[dir]);
+        build_dir_table(host_frame(dir, h, F, a), tabs[dir], skip != 2);
         if (!skip) {
             clear_bounds(tabs[dir].side[0]);
             clear_bounds(tabs[dir].side[1]);

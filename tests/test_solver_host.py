@@ -42,7 +42,7 @@ def host(tmp_path_factory):
     return L
 
 
-def _host_sweeps(host, T, h, F, a, sweeps, skip=True):
+def _host_sweeps(host, T, h, F, a, sweeps, skip=1):
     nz, ny, nx = (s - 2 for s in T.shape)
     host.fast_host_sweeps(T.ctypes.data, nx, ny, nz, *h, F, *a, sweeps, int(skip))
 
@@ -74,10 +74,10 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
         T0 = orc.init_point(nx, ny, nz, (nx // 3 + 1, ny // 2 + 1, nz - 2))
     ref = T0.copy()
     orc.solve(ref, h, 8, F=F, a=a)
-    for skip in (True, False):
+    for skip in (1, 2, 0):  # searched bounds, closed-form bounds (the no-alloc solve's), none
         T = T0.copy()
         _host_sweeps(host, T, h, F, a, 8, skip)
-        assert_bitwise(T, ref, "host build of the point update, skip %s" % skip)
+        assert_bitwise(T, ref, "host build of the point update, skip mode %d" % skip)
 
 
 def test_host_build_matches_reference_digest_99(host, digests):
