@@ -3,7 +3,7 @@
 // swept over a field in the reference driver's direction order
 // (Stencil-OpenACC/AN_ISO_1_OpenACC.c:1195-1236) with the winner record the
 // kernels keep.  The solver uses IEEE +, -, *, / and sqrt only, in double or
-// in float, with no contraction on either side, so this build computes the
+// in float, with no contraction on either side, so the host build computes the
 // bits the kernels compute; tests/test_solver_host.py runs it against the
 // oracle's CPU statements.  Test code only: the library has no host solver.
 #include <cmath>

@@ -2,7 +2,7 @@
 // direction tables (csrc/fold3d_tables.cpp), swept over a field in the
 // reference driver's order (Stencil-OpenACC/AN_ISO_1_OpenACC.c:1195-1236).
 // Every operation of the update is an IEEE double +, -, *, /, sqrt or fma
-// with no contraction on either side, so this build computes the bits the
+// with no contraction on either side, so the host build computes the bits the
 // kernels compute; tests/test_solver_host.py runs it against the oracle.
 // Test code only: the library has no host solver.
 #include <cmath>

@@ -155,7 +155,7 @@ def _oracle_source_grad(src, n, M):
     return 0.5 * float((T[1, 1:-1, 1:-1] ** 2).sum()), g
 
 
-_SURVEY = dict(n=10, srcs=[(2, 3, 2), (8, 8, 2), (5, 2, 3), (3, 9, 2), (7, 4, 2)])
+_SHOTS = dict(n=10, srcs=[(2, 3, 2), (8, 8, 2), (5, 2, 3), (3, 9, 2), (7, 4, 2)])
 
 
 def _survey_rank_main(rank, world, port, out_dir):
@@ -171,7 +171,7 @@ def _survey_rank_main(rank, world, port, out_dir):
     import shard
 
     dist = bench.init_ranks(rank, backend="gloo")
-    n, srcs = _SURVEY["n"], _SURVEY["srcs"]
+    n, srcs = _SHOTS["n"], _SHOTS["srcs"]
     M = [m.numpy() for m in media.heterogeneous_tti(n, n, n, 10.0, seed=1)]
     mine = shard.partition([1] * len(srcs), world)[rank]
     loss = torch.zeros(1, dtype=torch.float64)
@@ -207,7 +207,7 @@ def test_survey_gradient_split_over_two_ranks(tmp_path):
     import media
 
     mp.start_processes(_survey_rank_main, args=(2, _free_port(), str(tmp_path)), nprocs=2, start_method="spawn")
-    n, srcs = _SURVEY["n"], _SURVEY["srcs"]
+    n, srcs = _SHOTS["n"], _SHOTS["srcs"]
     M = [m.numpy() for m in media.heterogeneous_tti(n, n, n, 10.0, seed=1)]
     loss1, G1 = 0.0, np.zeros((6,) + (n + 2,) * 3)
     for sp_ in srcs:
