@@ -969,7 +969,9 @@ def main():
                 "kernel": "plane_kernel" if rep.engine == f3d.ENGINE_PLANES else "wavefront_kernel",
                 "alg_bytes_per_launch": alg_bytes / launches_per_step,
                 "avg_launch_us": solve_ms * 1e3 / launches_per_step,
-                "note": "FP64-ALU bound: ~100 FLOP per 16 B"}
+                "note": "FP64-ALU bound: ~100 FLOP per 16 B",
+                "traffic_note": "one pass's DRAM bytes from an ncu capture of the kernel before it skipped "
+                                "solver bodies; every point still loads the same ten values" if traffic else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
