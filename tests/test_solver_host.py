@@ -304,3 +304,35 @@ def test_elliptical_skip_bound_is_the_plane_distance(ellip_host):
         got = ellip_host.ellip_host_bound(A[0, 0], A[1, 1], A[2, 2], A[0, 1], A[0, 2], A[1, 2])
         assert got == pytest.approx(0.999 / math.sqrt(np.linalg.inv(A)[2, 2]), rel=1e-9)
     assert ellip_host.ellip_host_bound(1.0, 1.0, 1.0, 1.0, 0.0, 0.0) == 0.0  # singular in-plane block
+
+
+def test_tables_are_the_same_from_concurrent_threads(host):
+    """build_dir_table keeps a per-thread memo and its searches use only local
+    state: tables built for several media from four threads at once (ctypes
+    releases the GIL) equal the ones built one after the other."""
+    import threading
+
+    media_ = [(REF_F, REF_A, (0.7, 0.9, 1.1)), (1.3, (0.2, -0.5, 0.3), (1.0, 0.6, 0.8)),
+              (0.8, (0.1, -0.2, -0.3), (0.5, 0.5, 0.5)), (1.1, (0.3, 0.3, -0.5), (1.0, 1.0, 1.0))]
+
+    def bounds(F, a, h):
+        out = np.zeros(288)
+        host.fast_host_bounds(*h, F, *a, out.ctypes.data)
+        return out
+
+    want = [bounds(*m) for m in media_]
+    got = [[None] * len(media_) for _ in range(4)]
+
+    def work(t):
+        for q in range(len(media_)):
+            m = media_[(q + t) % len(media_)]
+            got[t][(q + t) % len(media_)] = bounds(*m)
+
+    threads = [threading.Thread(target=work, args=(t,)) for t in range(4)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    for t in range(4):
+        for q in range(len(media_)):
+            assert np.array_equal(got[t][q], want[q])
