@@ -120,15 +120,29 @@ __host__ __device__ __forceinline__ void ell_vertex(R &tn, int &win, int id, con
     }
 }
 
-template <class R>
+template <bool kOwnBound, class R>
 __host__ __device__ __forceinline__ void ell_edge(R &tn, int &win, int id, const EllipAT<R> &A, R gate, R tp, R tq,
                                                   int pi, int pj, int qi, int qj)
 {
-    if (!(tn > ell_min(tp, tq) + gate)) return;
+    const R mn = ell_min(tp, tq);
+    if (!(tn > mn + gate)) return;
     const int ei = qi - pi, ej = qj - pj;
     const R a = ell_bf(A, ei, ej, 0, ei, ej, 0);
     const R b = ell_bf(A, ei, ej, 0, -pi, -pj, 1);
     const R c = ell_bf(A, -pi, -pj, 1, -pi, -pj, 1);
+    // kOwnBound (the rim edges, away from the foot of X): the edge's own
+    // distance bound.  The candidate is at least mn plus the smallest
+    // ||X - p|| over the segment, whose square is c (b <= 0), c - 2b + a
+    // (b >= a) or (ac - b^2)/a; skip while tn - mn is at most 0.999 of it,
+    // compared in squares (ac - b^2 = ac sin^2 of the angle between the edge
+    // and X - P, far from 0 for an edge of the source plane).
+    if (kOwnBound && a > R(0)) {
+        const R e2 = (tn - mn) * (tn - mn);
+        const bool skip = !(b > R(0))  ? e2 <= R(0.998) * c
+                          : !(b < a)   ? e2 <= R(0.998) * (c - R(2) * b + a)
+                                       : e2 * a <= R(0.998) * (a * c - b * b);
+        if (skip) return;
+    }
     const R d = tq - tp;
     const R den = a - d * d;
     const R disc = a * c - b * b;
@@ -215,11 +229,11 @@ __host__ __device__ __forceinline__ R point_update_ellip(R told, R st, const R n
 #pragma unroll
         for (int r = 0; r < 8; ++r) ell_vertex(tn, win, 1 + r, A, gate, nb[r], ell_ri(r), ell_rj(r));
 #pragma unroll
-        for (int r = 0; r < 8; ++r) ell_edge(tn, win, 9 + r, A, gate, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
+        for (int r = 0; r < 8; ++r) ell_edge<false>(tn, win, 9 + r, A, gate, st, nb[r], 0, 0, ell_ri(r), ell_rj(r));
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
             const int s = (r + 1) & 7;
-            ell_edge(tn, win, 17 + r, A, gate, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
+            ell_edge<true>(tn, win, 17 + r, A, gate, nb[r], nb[s], ell_ri(r), ell_rj(r), ell_ri(s), ell_rj(s));
         }
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
