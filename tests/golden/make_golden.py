@@ -37,11 +37,19 @@ sys.path.insert(0, ROOT)
 from oracle import MAXT, RefLib, build  # noqa: E402
 
 
-def point_field(n):
+def point_field(n, src=None):
+    """MAXT everywhere, 0 at src = (i, j, k) (1-based; default the centre)."""
     T = np.full((n + 2,) * 3, MAXT)
-    c = n // 2 + 1
-    T[c, c, c] = 0.0
+    i, j, k = src if src is not None else (n // 2 + 1,) * 3
+    T[k, j, i] = 0.0
     return T
+
+
+# off-centre point sources (1-based i, j, k) for the digests of n = 37 and 99
+OFF_CENTRE = {
+    "corner_point": lambda n: (2, 1, 2),
+    "face_point": lambda n: (n, n // 3 + 1, 2 * n // 3 + 1),
+}
 
 
 def sha(a: np.ndarray) -> str:
@@ -76,6 +84,11 @@ def main():
         P = point_field(n)
         r.sweeps(P, 8)
         dig["n%d_point_s8" % n] = sha(P)
+        if n in (37, 99):  # sources next to a corner and on a face
+            for name, src in OFF_CENTRE.items():
+                P = point_field(n, src(n))
+                r.sweeps(P, 8)
+                dig["n%d_%s_s8" % (n, name)] = sha(P)
     if "--dump128" in sys.argv:
         d = build.build_ref(128, with_program=True)
         with tempfile.TemporaryDirectory(prefix="run_", dir=d) as tmp:

@@ -57,6 +57,18 @@ def test_oracle_digests_match_reference(orc, digests, n):
     assert sha(P) == digests["n%d_point_s8" % n]
 
 
+@pytest.mark.parametrize("n", [37, 99])
+@pytest.mark.parametrize("name,src", [("corner_point", lambda n: (2, 1, 2)),
+                                      ("face_point", lambda n: (n, n // 3 + 1, 2 * n // 3 + 1))])
+def test_oracle_off_centre_point_sources_match_reference(orc, digests, n, name, src):
+    """Point sources next to a corner and on a face (the reference's own
+    sweeps from the same field, tests/golden/make_golden.py), 8 sweeps."""
+    h = (ref_spacing(n),) * 3
+    P = orc.init_point(n, n, n, src(n))
+    orc.solve(P, h, 8)
+    assert sha(P) == digests["n%d_%s_s8" % (n, name)]
+
+
 def test_oracle_reproduces_reference_text_dump_128(orc, digests):
     """The reference program's own output file at 128^3 after 8 sweeps
     (AN_ISO_1_OpenACC.c:1244-1260: '%f' per value, i outermost, k innermost)."""

@@ -80,6 +80,18 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
         assert_bitwise(T, ref, "host build of the point update, skip mode %d" % skip)
 
 
+@pytest.mark.parametrize("n", [37, 99])
+@pytest.mark.parametrize("name,src", [("corner_point", lambda n: (2, 1, 2)),
+                                      ("face_point", lambda n: (n, n // 3 + 1, 2 * n // 3 + 1))])
+def test_host_build_matches_reference_off_centre_sources(orc, host, digests, n, name, src):
+    """The reference's own 8-sweep results for point sources next to a
+    corner and on a face, through the host build of the kernels' code."""
+    h = (ref_spacing(n),) * 3
+    P = orc.init_point(n, n, n, src(n))
+    _host_sweeps(host, P, h, REF_F, REF_A, 8)
+    assert hashlib.sha256(np.ascontiguousarray(P).tobytes()).hexdigest() == digests["n%d_%s_s8" % (n, name)]
+
+
 def test_host_build_matches_reference_digest_99(host, digests):
     """The reference's own 8-sweep result at 99^3 (partial tiles on every
     axis), through the host build."""
