@@ -74,6 +74,19 @@ def test_digests_64(f3d, ctx, cuda, digests, engine):
     assert sha(out) == digests["n64_point_s8"]
 
 
+@pytest.mark.parametrize("engine", ["wavefront", "planes"])
+@pytest.mark.parametrize("n", [37, 99])
+@pytest.mark.parametrize("name,src", [("corner_point", lambda n: (2, 1, 2)),
+                                      ("face_point", lambda n: (n, n // 3 + 1, 2 * n // 3 + 1))])
+def test_digests_off_centre_point_sources(f3d, ctx, cuda, digests, n, name, src, engine):
+    """The reference's own 8-sweep results for point sources next to a
+    corner and on a face, at sizes that leave partial tiles on every axis."""
+    h = (ref_spacing(n),) * 3
+    P = f3d.init_point(n, n, n, src(n))
+    out, _ = gpu_solve(f3d, ctx, cuda, P, h, 8, engine=engine)
+    assert sha(out) == digests["n%d_%s_s8" % (n, name)]
+
+
 CASES = [
     # dims, spacing, F, drift, source
     ((13, 9, 11), (0.7, 0.9, 1.1), 1.3, (0.2, -0.5, 0.3), "implicit"),
