@@ -10,6 +10,7 @@
 #include <numeric>
 #include <vector>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "fold3d_acc.h"
@@ -32,12 +33,32 @@ static thread_local std::string t_err;
 
 int set_error(int code, const std::string &msg)
 {
-    t_err = msg;
+    try {
+        t_err = msg;
+    } catch (...) {  // no memory for the message: keep the code
+    }
     return code;
 }
 int cuda_error(cudaError_t e, const char *what)
 {
-    return set_error(FOLD3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    try {
+        return set_error(FOLD3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    } catch (...) {
+        return FOLD3D_ERR_CUDA;
+    }
+}
+
+// Runs an entry point's body: a host exception (an allocation that failed,
+// say) becomes a status code instead of crossing the C boundary.
+template <class Fn> static int host_guard(Fn &&fn)
+{
+    try {
+        return fn();
+    } catch (const std::bad_alloc &) {
+        return set_error(FOLD3D_ERR_NOMEM, "out of host memory");
+    } catch (...) {
+        return set_error(FOLD3D_ERR_INVALID, "unexpected host error");
+    }
 }
 void clear_error() { t_err.clear(); }
 
@@ -1151,18 +1172,22 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
                        fold3d_report *reps)
 {
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
-    std::vector<SolveInst> v(n);
-    for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
-    return batch_entry(c, n, v.data(), false, o, stream, reps);
+    return host_guard([&] {
+        std::vector<SolveInst> v(n);
+        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+        return batch_entry(c, n, v.data(), false, o, stream, reps);
+    });
 }
 
 int fold3d_solve_batch_f32(fold3d_ctx *c, int n, const fold3d_instance_f32 *in, const fold3d_opts *o, void *stream,
                            fold3d_report *reps)
 {
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
-    std::vector<SolveInst> v(n);
-    for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
-    return batch_entry(c, n, v.data(), true, o, stream, reps);
+    return host_guard([&] {
+        std::vector<SolveInst> v(n);
+        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+        return batch_entry(c, n, v.data(), true, o, stream, reps);
+    });
 }
 
 int fold3d_init_implicit_device(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,
@@ -1197,27 +1222,31 @@ int fold3d_init_implicit_device(fold3d_ctx *c, const fold3d_grid *g, const fold3
                 return set_error(FOLD3D_ERR_NOMEM, "device initialiser staging");
         c->i_stage_bytes = bytes;
     }
-    return init_implicit_device(*g, *m, T, c->i_if, c->i_stage, c->i_stage_bytes / plane, s);
+    return host_guard([&] { return init_implicit_device(*g, *m, T, c->i_if, c->i_stage, c->i_stage_bytes / plane, s); });
 }
 
 int fold3d_adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in, int max_sweeps, double tol,
                          int accumulate, void *stream, fold3d_report *reps)
 {
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
-    std::vector<AdjInst> v(n);
-    for (int i = 0; i < n; ++i)
-        v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
-    return adjoint_entry(c, n, v.data(), false, max_sweeps, tol, accumulate, stream, reps);
+    return host_guard([&] {
+        std::vector<AdjInst> v(n);
+        for (int i = 0; i < n; ++i)
+            v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+        return adjoint_entry(c, n, v.data(), false, max_sweeps, tol, accumulate, stream, reps);
+    });
 }
 
 int fold3d_adjoint_batch_f32(fold3d_ctx *c, int n, const fold3d_adjoint_instance_f32 *in, int max_sweeps,
                              double tol, int accumulate, void *stream, fold3d_report *reps)
 {
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
-    std::vector<AdjInst> v(n);
-    for (int i = 0; i < n; ++i)
-        v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
-    return adjoint_entry(c, n, v.data(), true, max_sweeps, tol, accumulate, stream, reps);
+    return host_guard([&] {
+        std::vector<AdjInst> v(n);
+        for (int i = 0; i < n; ++i)
+            v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+        return adjoint_entry(c, n, v.data(), true, max_sweeps, tol, accumulate, stream, reps);
+    });
 }
 
 int fold3d_solve(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, double *T,

@@ -207,7 +207,20 @@ double fold3d_exact_time(const fold3d_medium *m, double x, double y, double z)
     return exact_time(m->F, m->ax, m->ay, m->az, x, y, z);
 }
 
+static int init_implicit_host(double *T, const fold3d_grid *g, const fold3d_medium *m);
+
 int fold3d_init_implicit(double *T, const fold3d_grid *g, const fold3d_medium *m)
+{
+    try {  // host threads and tables: an exception becomes a status code, not a crash
+        return init_implicit_host(T, g, m);
+    } catch (const std::bad_alloc &) {
+        return FOLD3D_ERR_NOMEM;
+    } catch (...) {
+        return FOLD3D_ERR_INVALID;
+    }
+}
+
+static int init_implicit_host(double *T, const fold3d_grid *g, const fold3d_medium *m)
 {
     if (!T || !g || !m) return FOLD3D_ERR_INVALID;
     if (g->nx < 2 || g->ny < 2 || g->nz < 2) return FOLD3D_ERR_INVALID;
