@@ -94,14 +94,19 @@ void parallel_for(int lo, int hi, int nthreads, Fn fn)
         for (int i = lo; i < hi; ++i) fn(i);
         return;
     }
+    auto range = [=](int t) {
+        const int a = lo + (int)((long long)n * t / nthreads);
+        const int b = lo + (int)((long long)n * (t + 1) / nthreads);
+        for (int i = a; i < b; ++i) fn(i);
+    };
     std::vector<std::thread> th;
-    th.reserve(nthreads);
-    for (int t = 0; t < nthreads; ++t)
-        th.emplace_back([=]() {
-            const int a = lo + (int)((long long)n * t / nthreads);
-            const int b = lo + (int)((long long)n * (t + 1) / nthreads);
-            for (int i = a; i < b; ++i) fn(i);
-        });
+    int started = 0;
+    try {
+        th.reserve(nthreads);
+        for (; started < nthreads; ++started) th.emplace_back(range, started);
+    } catch (...) {  // no more threads: this thread runs the ranges left
+    }
+    for (int t = started; t < nthreads; ++t) range(t);
     for (auto &x : th) x.join();
 }
 

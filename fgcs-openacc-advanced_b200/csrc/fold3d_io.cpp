@@ -15,9 +15,11 @@
 // ny, nz as int32, dx, dy, dz as double, padding) and then the whole field
 // as little-endian doubles in the field layout.
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -41,7 +43,34 @@ bool put(FILE *f, const void *p, size_t n) { return std::fwrite(p, 1, n, f) == n
 
 extern "C" {
 
+static int write_text(const char *path, const double *T, const fold3d_grid *g);
+static int write_vtk(const char *path, const double *T, const fold3d_grid *g, int ghosts);
+
+// Host exceptions (memory for the formatted lines, the row buffer, threads)
+// become status codes instead of crossing the C boundary.
 int fold3d_write_text(const char *path, const double *T, const fold3d_grid *g)
+{
+    try {
+        return write_text(path, T, g);
+    } catch (const std::bad_alloc &) {
+        return FOLD3D_ERR_NOMEM;
+    } catch (...) {
+        return FOLD3D_ERR_INVALID;
+    }
+}
+
+int fold3d_write_vtk(const char *path, const double *T, const fold3d_grid *g, int ghosts)
+{
+    try {
+        return write_vtk(path, T, g, ghosts);
+    } catch (const std::bad_alloc &) {
+        return FOLD3D_ERR_NOMEM;
+    } catch (...) {
+        return FOLD3D_ERR_INVALID;
+    }
+}
+
+static int write_text(const char *path, const double *T, const fold3d_grid *g)
 {
     if (!path || !T || !g || g->nx < 1 || g->ny < 1 || g->nz < 1) return FOLD3D_ERR_INVALID;
     const int px = g->nx + 2, py = g->ny + 2, pz = g->nz + 2;
@@ -52,25 +81,31 @@ int fold3d_write_text(const char *path, const double *T, const fold3d_grid *g)
     // one i-plane (all j, k) per task, formatted by nth threads, written in order
     const int batch = std::max(1, nth);
     std::vector<std::string> text(batch);
+    std::atomic<bool> failed(false);  // a worker that ran out of memory (it must not throw)
     for (int i0 = 0; i0 < px; i0 += batch) {
         const int i1 = std::min(px, i0 + batch);
         fold3d::host_parallel_for(i0, i1, nth, [&](int i) {
-            std::string &s = text[i - i0];
-            s.clear();
-            char buf[512];
-            for (int j = 0; j < py; ++j)
-                for (int k = 0; k < pz; ++k) {
-                    const int n = std::snprintf(buf, sizeof buf, "%f\n", T[i + sy * j + sz * k]);
-                    s.append(buf, (size_t)n);
-                }
+            try {
+                std::string &s = text[i - i0];
+                s.clear();
+                char buf[512];
+                for (int j = 0; j < py; ++j)
+                    for (int k = 0; k < pz; ++k) {
+                        const int n = std::snprintf(buf, sizeof buf, "%f\n", T[i + sy * j + sz * k]);
+                        s.append(buf, (size_t)n);
+                    }
+            } catch (...) {
+                failed = true;
+            }
         });
+        if (failed) return FOLD3D_ERR_NOMEM;
         for (int i = i0; i < i1; ++i)
             if (!put(out.f, text[i - i0].data(), text[i - i0].size())) return FOLD3D_ERR_INVALID;
     }
     return FOLD3D_OK;
 }
 
-int fold3d_write_vtk(const char *path, const double *T, const fold3d_grid *g, int ghosts)
+static int write_vtk(const char *path, const double *T, const fold3d_grid *g, int ghosts)
 {
     if (!path || !T || !g || g->nx < 1 || g->ny < 1 || g->nz < 1) return FOLD3D_ERR_INVALID;
     const int px = g->nx + 2, py = g->ny + 2;
