@@ -1556,8 +1556,14 @@ void *acc_malloc(size_t bytes)
         set_error(FOLD3D_ERR_NOMEM, "acc_malloc: cudaMalloc failed");
         return nullptr;
     }
-    std::lock_guard<std::mutex> lk(g_compat_mu);
-    g_acc_allocs[(uintptr_t)p] = bytes;
+    try {
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        g_acc_allocs[(uintptr_t)p] = bytes;
+    } catch (...) {  // no host memory for the record: give the device block back
+        cudaFree(p);
+        set_error(FOLD3D_ERR_NOMEM, "acc_malloc: out of host memory");
+        return nullptr;
+    }
     return p;
 }
 
