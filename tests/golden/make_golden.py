@@ -12,9 +12,13 @@ Outputs:
       s1, s2, s8      after 1, 2 and 8 sweeps (implicit-surface source)
       point_s8        point source at the centre (+MAXT elsewhere), 8 sweeps
   digests.json      sha256 of the raw float64 bytes of larger reference
-                    results (the fields themselves would be too big), plus
-                    the md5 of the reference program's own text dump at 128^3
-                    (an_iso_1_openacc.txt, written by its unmodified main).
+                    results (the fields themselves would be too big): at 32,
+                    37, 64 and 99 the initial field, 8 sweeps from it and 8
+                    sweeps from a centred point source; at 37 and 99 also 8
+                    sweeps from point sources next to a corner and on a face.
+                    Plus the md5 of the reference program's own text dump at
+                    128^3 (an_iso_1_openacc.txt, written by its unmodified
+                    main).
 
     python tests/golden/make_golden.py            # everything but 128^3 dump
     python tests/golden/make_golden.py --dump128  # also run the 128^3 program (~30 s)
