@@ -3,6 +3,7 @@
 // reference driver calls.
 #include <cmath>
 #include <cstdio>
+#include <cstdarg>
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
@@ -29,38 +30,29 @@ const DirSpec kDirs[6] = {
     {1, +1, 0, +1, 2, +1},  // y_down  :636
 };
 
-static thread_local std::string t_err;
+// The last error message of this host thread.  A fixed buffer: recording an
+// error allocates nothing, so no error path can throw.
+static thread_local char t_err[512];
 
-int set_error(int code, const std::string &msg)
+int set_error(int code, const char *msg)
 {
-    try {
-        t_err = msg;
-    } catch (...) {  // no memory for the message: keep the code
-    }
+    snprintf(t_err, sizeof t_err, "%s", msg ? msg : "");
+    return code;
+}
+int set_errorf(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_err, sizeof t_err, fmt, ap);
+    va_end(ap);
     return code;
 }
 int cuda_error(cudaError_t e, const char *what)
 {
-    try {
-        return set_error(FOLD3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-    } catch (...) {
-        return FOLD3D_ERR_CUDA;
-    }
+    return set_errorf(FOLD3D_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// Runs an entry point's body: a host exception (an allocation that failed,
-// say) becomes a status code instead of crossing the C boundary.
-template <class Fn> static int host_guard(Fn &&fn)
-{
-    try {
-        return fn();
-    } catch (const std::bad_alloc &) {
-        return set_error(FOLD3D_ERR_NOMEM, "out of host memory");
-    } catch (...) {
-        return set_error(FOLD3D_ERR_INVALID, "unexpected host error");
-    }
-}
-void clear_error() { t_err.clear(); }
+void clear_error() { t_err[0] = 0; }
 
 static void strides(const fold3d_grid &g, long long st[3])
 {
@@ -111,7 +103,7 @@ LocalFrameH make_frame(const fold3d_grid &g, const fold3d_medium &m, int dir)
     return L;
 }
 
-static int check_grid(const fold3d_grid *g)
+int check_grid(const fold3d_grid *g)
 {
     if (!g) return set_error(FOLD3D_ERR_INVALID, "grid is NULL");
     if (g->nx < 2 || g->ny < 2 || g->nz < 2)
@@ -131,7 +123,7 @@ static int check_grid(const fold3d_grid *g)
     return FOLD3D_OK;
 }
 
-static int check_medium(const fold3d_medium *m)
+int check_medium(const fold3d_medium *m)
 {
     if (!m) return set_error(FOLD3D_ERR_INVALID, "medium is NULL");
     if (!(m->F > 0) || !std::isfinite(m->F) || !std::isfinite(m->ax) || !std::isfinite(m->ay) ||
@@ -223,7 +215,7 @@ struct DeviceGuard {
 
 extern "C" {
 
-const char *fold3d_last_error(void) { return t_err.c_str(); }
+const char *fold3d_last_error(void) { return t_err; }
 
 const char *fold3d_version(void) { return "fold3dpmm-b200 0.1 (sm_100a)"; }
 
@@ -426,15 +418,15 @@ static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
         const size_t words = (size_t)(n[b] + 2) * ntu * ntv;
         if ((e = cudaMalloc(&c->w_mod[b], words * 4)) != cudaSuccess ||
             (e = cudaMemset(c->w_mod[b], 0, words * 4)) != cudaSuccess)
-            return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+            return set_errorf(FOLD3D_ERR_NOMEM, "wavefront scratch: %s", cudaGetErrorString(e));
     }
     if ((e = cudaMalloc(&c->w_flags, flag_words * 4)) != cudaSuccess ||
         (e = cudaMemset(c->w_flags, 0, flag_words * 4)) != cudaSuccess)
-        return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+        return set_errorf(FOLD3D_ERR_NOMEM, "wavefront scratch: %s", cudaGetErrorString(e));
     if (!c->w_counters) {
         if ((e = cudaMalloc(&c->w_counters, 2 * sizeof(unsigned))) != cudaSuccess ||
             (e = cudaMalloc(&c->w_evaluated, sizeof(unsigned long long))) != cudaSuccess)
-            return set_error(FOLD3D_ERR_NOMEM, std::string("wavefront scratch: ") + cudaGetErrorString(e));
+            return set_errorf(FOLD3D_ERR_NOMEM, "wavefront scratch: %s", cudaGetErrorString(e));
     }
     if (!c->sms) {
         int dev = 0;
@@ -612,16 +604,16 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
     if ((e = cudaMalloc(&c->b_scratch, words * 4)) != cudaSuccess ||
         (e = cudaMemset(c->b_scratch, 0, words * 4)) != cudaSuccess ||
         (e = cudaMalloc(&c->b_slots, 2 * (size_t)n * 8)) != cudaSuccess)
-        return set_error(FOLD3D_ERR_NOMEM, std::string("batch scratch: ") + cudaGetErrorString(e));
+        return set_errorf(FOLD3D_ERR_NOMEM, "batch scratch: %s", cudaGetErrorString(e));
     if (!c->b_counters && (e = cudaMalloc(&c->b_counters, 2 * sizeof(unsigned))) != cudaSuccess)
-        return set_error(FOLD3D_ERR_NOMEM, std::string("batch scratch: ") + cudaGetErrorString(e));
+        return set_errorf(FOLD3D_ERR_NOMEM, "batch scratch: %s", cudaGetErrorString(e));
     // per direction: inst[n], step_off[max_steps+1], step_k[max_steps], tile_pre[n+1]
     const size_t per = align_up((size_t)n * kStageInst, 256) + align_up((max_steps + 1) * 8, 256) +
                        align_up((size_t)max_steps * 4, 256) + align_up(((size_t)n + 1) * 8, 256);
     c->b_stage_bytes = per;
     if ((e = cudaMalloc(&c->b_stage_d, 6 * per)) != cudaSuccess ||
         (e = cudaMallocHost(&c->b_stage_h, 6 * per)) != cudaSuccess)
-        return set_error(FOLD3D_ERR_NOMEM, std::string("batch staging: ") + cudaGetErrorString(e));
+        return set_errorf(FOLD3D_ERR_NOMEM, "batch staging: %s", cudaGetErrorString(e));
     if (!c->sms) {
         int dev = 0;
         cudaGetDevice(&dev);
@@ -1411,7 +1403,7 @@ int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *
         c->d_field_cells = 0;
         if (c->sweep_exec && c->key_T) c->key_T = nullptr;  // force a re-capture
         if ((e = cudaMalloc(&c->d_field, cells * sizeof(double))) != cudaSuccess)
-            return set_error(FOLD3D_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            return set_errorf(FOLD3D_ERR_NOMEM, "cudaMalloc: %s", cudaGetErrorString(e));
         c->d_field_cells = cells;
     }
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
@@ -1457,38 +1449,54 @@ std::map<uintptr_t, size_t> g_acc_allocs;  // base -> bytes, from acc_malloc
 int g_compat_n[3] = {0, 0, 0};
 
 // Grid of a compat call: the size set by fold3d_compat_set_grid, else the
-// cube whose field fills the acc_malloc allocation T points into.
-bool compat_grid(const double *T, fold3d_grid &g)
+// cube whose field fills the acc_malloc allocation that starts at T.  When T
+// lies inside an acc_malloc allocation, the field must also fit between T
+// and the allocation's end.  NULL, or the reason the call is rejected.
+const char *compat_grid(const double *T, fold3d_grid &g)
 {
     std::lock_guard<std::mutex> lk(g_compat_mu);
+    // the acc_malloc allocation T points into, if any
+    auto it = g_acc_allocs.upper_bound((uintptr_t)T);
+    bool inside = false;
+    if (it != g_acc_allocs.begin()) {
+        --it;
+        inside = (uintptr_t)T < it->first + it->second;
+    }
     if (g_compat_n[0] > 0) {
         g.nx = g_compat_n[0];
         g.ny = g_compat_n[1];
         g.nz = g_compat_n[2];
+        if (inside) {
+            const double need = ((double)g.nx + 2) * ((double)g.ny + 2) * ((double)g.nz + 2) * sizeof(double);
+            if (need > (double)(it->first + it->second - (uintptr_t)T))
+                return "function_*: the field of the grid set by fold3d_compat_set_grid does not fit in the "
+                       "acc_malloc allocation from T on";
+        }
     } else {
-        auto it = g_acc_allocs.upper_bound((uintptr_t)T);
-        if (it == g_acc_allocs.begin()) return false;
-        --it;
-        if ((uintptr_t)T >= it->first + it->second) return false;
+        if (!inside)
+            return "function_*: grid size unknown (call fold3d_compat_set_grid or allocate with acc_malloc)";
+        if ((uintptr_t)T != it->first)
+            return "function_*: T points inside an acc_malloc allocation, not at its start; call "
+                   "fold3d_compat_set_grid to give the grid size";
         const size_t cells = it->second / sizeof(double);
         long long p = (long long)std::llround(std::cbrt((double)cells));
         while (p * p * p > (long long)cells) --p;
         while ((p + 1) * (p + 1) * (p + 1) <= (long long)cells) ++p;
-        if (p * p * p != (long long)cells || p < 4) return false;
+        if (p * p * p != (long long)cells || p < 4)
+            return "function_*: the acc_malloc allocation at T is not a cubic field; call fold3d_compat_set_grid";
         g.nx = g.ny = g.nz = (int)(p - 2);
     }
     g.dx = g.dy = g.dz = 1.0;  // geometry only; spacings come from the call
-    return true;
+    return nullptr;
 }
 
-void compat_plane(int dir, double *T, int src, double dzz, double dxx, double dyy, double dxy, double dxz,
-                  double dyz, double F, double ay, double ax, double az)
+void compat_plane_body(int dir, double *T, int src, double dzz, double dxx, double dyy, double dxy, double dxz,
+                       double dyz, double F, double ay, double ax, double az)
 {
-    clear_error();
     fold3d_grid g;
-    if (!T || !compat_grid(T, g)) {
-        set_error(FOLD3D_ERR_INVALID,
-                  "function_*: grid size unknown (call fold3d_compat_set_grid or allocate with acc_malloc)");
+    const char *why = T ? compat_grid(T, g) : "function_*: T is NULL";
+    if (why) {
+        set_error(FOLD3D_ERR_INVALID, why);
         return;
     }
     const PlaneGeom pg = make_geom(g, dir);
@@ -1506,6 +1514,56 @@ void compat_plane(int dir, double *T, int src, double dzz, double dxx, double dy
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) cuda_error(e, "function_*");
 }
+
+int g_host_n[3] = {0, 0, 0};  // grid of the last ImplicitInitialiser call
+}  // namespace
+
+void fold3d::compat_note_host_grid(int nx, int ny, int nz)
+{
+    host_guard([&] {
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        g_host_n[0] = nx;
+        g_host_n[1] = ny;
+        g_host_n[2] = nz;
+        return FOLD3D_OK;
+    });
+}
+
+bool fold3d::compat_host_pitch(long long &sy, long long &sz)
+{
+    int n[3] = {0, 0, 0};
+    const int rc = host_guard([&] {
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        const int *src = (g_compat_n[0] > 0) ? g_compat_n : g_host_n;
+        n[0] = src[0];
+        n[1] = src[1];
+        n[2] = src[2];
+        return FOLD3D_OK;
+    });
+    if (rc) return false;
+    if (n[0] < 2 || n[1] < 2) {
+        set_error(FOLD3D_ERR_INVALID, "InitNode/updateVoxel: grid size unknown (call fold3d_compat_set_grid or "
+                                      "ImplicitInitialiser first)");
+        return false;
+    }
+    clear_error();
+    sy = (long long)n[0] + 2;
+    sz = sy * ((long long)n[1] + 2);
+    return true;
+}
+
+namespace {
+// The reference's sweep functions return nothing; errors are left in
+// fold3d_last_error, and no host exception leaves the library.
+void compat_plane(int dir, double *T, int src, double dzz, double dxx, double dyy, double dxy, double dxz,
+                  double dyz, double F, double ay, double ax, double az)
+{
+    clear_error();
+    host_guard([&] {
+        compat_plane_body(dir, T, src, dzz, dxx, dyy, dxy, dxz, dyz, F, ay, ax, az);
+        return FOLD3D_OK;
+    });
+}
 }  // namespace
 
 extern "C" {
@@ -1515,11 +1573,13 @@ int fold3d_compat_set_grid(int nx, int ny, int nz)
     clear_error();
     if ((nx | ny | nz) != 0 && (nx < 2 || ny < 2 || nz < 2))
         return set_error(FOLD3D_ERR_INVALID, "grid sizes must be >= 2 (or all 0 to unset)");
-    std::lock_guard<std::mutex> lk(g_compat_mu);
-    g_compat_n[0] = nx;
-    g_compat_n[1] = ny;
-    g_compat_n[2] = nz;
-    return FOLD3D_OK;
+    return host_guard([&] {
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        g_compat_n[0] = nx;
+        g_compat_n[1] = ny;
+        g_compat_n[2] = nz;
+        return FOLD3D_OK;
+    });
 }
 
 void fold3d_compat_plane(int dir, double *T, int p, double dzz, double dxx, double dyy, double dxy, double dxz,
@@ -1570,10 +1630,11 @@ void *acc_malloc(size_t bytes)
 void acc_free(void *p)
 {
     if (!p) return;
-    {
+    host_guard([&] {
         std::lock_guard<std::mutex> lk(g_compat_mu);
         g_acc_allocs.erase((uintptr_t)p);
-    }
+        return FOLD3D_OK;
+    });
     cudaFree(p);
 }
 

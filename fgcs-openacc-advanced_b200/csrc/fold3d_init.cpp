@@ -279,12 +279,46 @@ int fold3d_init_point(double *T, const fold3d_grid *g, int si, int sj, int sk)
 }
 
 // Reference signature (Fold3dPMM.h:81-85): the reference medium constants
-// (:49-52) and pitch nx+2.
+// (:49-52) and pitch nx+2.  The grid is remembered as the pitch of InitNode
+// and updateVoxel, whose reference signatures carry no size.
 void ImplicitInitialiser(double *T, int nx, int ny, int nz, double dxx, double dyy, double dzz)
 {
     const fold3d_grid g = {nx, ny, nz, dxx, dyy, dzz};
     const fold3d_medium m = {1.1, -0.35, 0.4, 0.7};
+    fold3d::compat_note_host_grid(nx, ny, nz);
     fold3d_init_implicit(T, &g, &m);
 }
+
+// InitNode (Fold3dPMM.h:64, Fold3dPMM.c:35-54): min-update of node (i, j, k)
+// with the reference medium's exact time from a point at (x, y, z) relative
+// to the node, keeping the node's sign.  The reference indexes T with its
+// compile-time HEIGHT; here the pitch is the host grid (see
+// fold3d::compat_host_pitch).  Without one, nothing is written and
+// fold3d_last_error says why.
+void InitNode(double x, double y, double z, int i, int j, int k, double *T)
+{
+    long long sy, sz;
+    if (!T || !fold3d::compat_host_pitch(sy, sz)) return;
+    const HostNode node{T, sy, sz, 1.1, {-0.35, 0.4, 0.7}};
+    node(x, y, z, i, j, k);
+}
+
+// updateVoxel (Fold3dPMM.h:67-70, Fold3dPMM.c:56-112): the 44 node updates of
+// one seeding point, in the reference's order and with its index slips (the
+// same table the initialisers use).
+void updateVoxel(double *T, int i, int j, int k, double xp, double yp, double zp, double dxx, double dyy, double dzz)
+{
+    long long sy, sz;
+    if (!T || !fold3d::compat_host_pitch(sy, sz)) return;
+    HostNode node{T, sy, sz, 1.1, {-0.35, 0.4, 0.7}};
+    const double h[3] = {dxx, dyy, dzz};
+    fold3d_seed::seed_point(kSteps, h, i, j, k, xp, yp, zp, node);
+}
+
+// Node coordinates (Fold3dPMM.h:72-76, Fold3dPMM.c:115-126): the reference's
+// domain starts at 0 on every axis (_xmin, _ymin, _zmin).
+double x(int i, double DX) { return (i - 1) * DX + 0.; }
+double y(int j, double dy) { return (j - 1) * dy + 0.; }
+double z(int k, double dz) { return (k - 1) * dz + 0.; }
 
 }  // extern "C"

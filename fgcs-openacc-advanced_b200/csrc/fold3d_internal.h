@@ -2,6 +2,7 @@
 #pragma once
 
 #include <functional>
+#include <new>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -44,9 +45,37 @@ inline int pass_first(const PlaneGeom &pg, int dir) { return kDirs[dir].sg > 0 ?
 inline int pass_count(const PlaneGeom &pg) { return pg.nplanes - 1; }
 
 // Error recording (thread-local message readable by fold3d_last_error).
-int set_error(int code, const std::string &msg);
+int set_error(int code, const char *msg);
+int set_errorf(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
 int cuda_error(cudaError_t e, const char *what);
 void clear_error();
+
+// Runs an entry point's body: a host exception (an allocation that failed,
+// a mutex that could not be locked) becomes a status code instead of
+// crossing the C boundary.  Recording the error allocates nothing.
+template <class Fn> int host_guard(Fn &&fn)
+{
+    try {
+        return fn();
+    } catch (const std::bad_alloc &) {
+        return set_error(FOLD3D_ERR_NOMEM, "out of host memory");
+    } catch (...) {
+        return set_error(FOLD3D_ERR_INVALID, "unexpected host error");
+    }
+}
+
+// Argument checks shared by the solve entry points (fold3d_api.cu): a grid
+// with sizes >= 2, finite spacings > 0 and a bounded size; a finite drift
+// medium with F > 0.  FOLD3D_OK, or FOLD3D_ERR_INVALID with the message set.
+int check_grid(const fold3d_grid *g);
+int check_medium(const fold3d_medium *m);
+
+// Pitch of the reference's host helpers InitNode and updateVoxel, which take
+// no size (the reference compiles HEIGHT in): the grid of
+// fold3d_compat_set_grid if set, else the grid of the last
+// ImplicitInitialiser call.  false (error message set) when neither is known.
+void compat_note_host_grid(int nx, int ny, int nz);
+bool compat_host_pitch(long long &sy, long long &sz);
 
 struct DirTable;  // fold3d_fast.cuh
 

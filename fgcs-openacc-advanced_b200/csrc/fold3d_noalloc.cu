@@ -17,12 +17,18 @@
 // the stream before its first plane; two calls whose work overlaps on the GPU
 // (different streams, or different host threads, on one device) race on it.
 //
-// Host code cannot use g_sweep_maxd's name as a device address.  The first
-// call on a device looks the address up with cudaGetSymbolAddress, with that
-// device current, and keeps it for later calls; that first call should
-// therefore come before any stream capture that involves this library.
+// Host code cannot use g_sweep_maxd's name as a device address.  Its address
+// is looked up with cudaGetSymbolAddress, with the caller's device and
+// context current, by the first call in each CUDA context, and kept for later
+// calls in that context.  The cache is keyed on the context's unique id
+// (cuCtxGetId), not on the device ordinal: after cudaDeviceReset, or when a
+// caller makes another context current on the same device (an OpenACC
+// runtime with its own context, say), the module is loaded again at another
+// address and the next call looks it up afresh.  That first call in a
+// context should come before any stream capture that involves this library.
 #include <chrono>
 #include <cstring>
+#include <cuda.h>
 #include <mutex>
 
 #include "fold3d_fast.cuh"
@@ -33,22 +39,73 @@ namespace fold3d {
 static __device__ __align__(256) unsigned long long g_sweep_maxd[FOLD3D_NOALLOC_MAX_SWEEPS];
 
 namespace {
-constexpr int kMaxDevices = 128;
 std::mutex g_noalloc_mu;
-unsigned long long *g_noalloc_ptr[kMaxDevices] = {};
 
-// Device address of g_sweep_maxd on the current device (set up once per device).
-int noalloc_scratch(int dev, unsigned long long **out)
+// Driver entry points, fetched through the runtime (the library does not
+// link libcuda itself).
+using CtxGetCurrentFn = CUresult(CUDAAPI *)(CUcontext *);
+using CtxGetIdFn = CUresult(CUDAAPI *)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+
+// Contexts seen so far and g_sweep_maxd's address in each; a fixed table
+// (no allocation), the oldest entry replaced when it is full.
+constexpr int kCacheSlots = 64;
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    unsigned long long *ptr;
+};
+ScratchEntry g_cache[kCacheSlots];
+int g_cache_used = 0, g_cache_next = 0;
+
+int driver_entry_points()
 {
-    if (dev < 0 || dev >= kMaxDevices) return set_error(FOLD3D_ERR_UNSUPPORTED, "device ordinal too large");
+    if (g_ctx_current && g_ctx_id) return FOLD3D_OK;
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDriverEntryPoint");
+    if (!f1 || !f2 || q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "fold3d_solve_noalloc: the driver lacks cuCtxGetId");
+    g_ctx_current = (CtxGetCurrentFn)f1;
+    g_ctx_id = (CtxGetIdFn)f2;
+    return FOLD3D_OK;
+}
+
+// Device address of g_sweep_maxd in the current context (looked up once per
+// context).
+int noalloc_scratch(unsigned long long **out)
+{
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_sweep_maxd);
-        if (e != cudaSuccess || !p) return cuda_error(e, "cudaGetSymbolAddress(g_sweep_maxd)");
-        g_noalloc_ptr[dev] = (unsigned long long *)p;
+    int rc = driver_entry_points();
+    if (rc) return rc;
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS)
+        return set_error(FOLD3D_ERR_CUDA, "fold3d_solve_noalloc: cuCtxGetCurrent failed");
+    unsigned long long id = 0;
+    void *p = nullptr;
+    cudaError_t e;
+    if (ctx) {
+        if (g_ctx_id(ctx, &id) != CUDA_SUCCESS)
+            return set_error(FOLD3D_ERR_CUDA, "fold3d_solve_noalloc: cuCtxGetId failed");
+        for (int i = 0; i < g_cache_used; ++i)
+            if (g_cache[i].ctx_id == id) {
+                *out = g_cache[i].ptr;
+                return FOLD3D_OK;
+            }
     }
-    *out = g_noalloc_ptr[dev];
+    // first call in this context (or no context bound yet: the lookup
+    // initialises the runtime's primary context of the current device)
+    if ((e = cudaGetSymbolAddress(&p, g_sweep_maxd)) != cudaSuccess || !p)
+        return cuda_error(e, "cudaGetSymbolAddress(g_sweep_maxd)");
+    if (!ctx) {
+        if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx || g_ctx_id(ctx, &id) != CUDA_SUCCESS)
+            return set_error(FOLD3D_ERR_CUDA, "fold3d_solve_noalloc: no current CUDA context");
+    }
+    const int slot = (g_cache_used < kCacheSlots) ? g_cache_used++ : g_cache_next++ % kCacheSlots;
+    g_cache[slot] = ScratchEntry{id, (unsigned long long *)p};
+    *out = (unsigned long long *)p;
     return FOLD3D_OK;
 }
 }  // namespace
@@ -57,14 +114,14 @@ int noalloc_scratch(int dev, unsigned long long **out)
 
 using namespace fold3d;
 
-extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T,
-                                    const fold3d_opts *o, void *stream, fold3d_report *rep)
+namespace {
+int solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T, const fold3d_opts *o, void *stream,
+                  fold3d_report *rep)
 {
-    clear_error();
-    if (!g || !m || !T || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    if (g->nx < 2 || g->ny < 2 || g->nz < 2 || !(g->dx > 0 && g->dy > 0 && g->dz > 0))
-        return set_error(FOLD3D_ERR_INVALID, "grid sizes must be >= 2 and spacings > 0");
-    if (!(m->F > 0)) return set_error(FOLD3D_ERR_INVALID, "medium must have F > 0");
+    if (!T || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    int rc = check_grid(g);
+    if (rc) return rc;
+    if ((rc = check_medium(m))) return rc;
     if (o->max_sweeps < 1) return set_error(FOLD3D_ERR_INVALID, "max_sweeps must be >= 1");
     if (o->max_sweeps > FOLD3D_NOALLOC_MAX_SWEEPS)
         return set_error(FOLD3D_ERR_INVALID,
@@ -73,12 +130,9 @@ extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m
     if (!o->fixed && !(o->tol >= 0.0)) return set_error(FOLD3D_ERR_INVALID, "tol must be >= 0");
     if (o->variant != kVariantFast && o->variant != kVariantLiteral && o->variant != kVariantCompact)
         return set_error(FOLD3D_ERR_INVALID, "unknown solver variant");
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
     unsigned long long *slots = nullptr;
-    int rc = noalloc_scratch(dev, &slots);
-    if (rc) return rc;
+    if ((rc = noalloc_scratch(&slots))) return rc;
+    cudaError_t e;
 
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t s = (cudaStream_t)stream;
@@ -121,4 +175,12 @@ extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m
         rep->engine = FOLD3D_ENGINE_PLANES;
     }
     return FOLD3D_OK;
+}
+}  // namespace
+
+extern "C" int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T,
+                                    const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    clear_error();
+    return host_guard([&] { return solve_noalloc(g, m, T, o, stream, rep); });
 }

@@ -40,7 +40,7 @@ EXPORTED = (
     "fold3d_write_raw", "fold3d_solve_ellip_f32", "fold3d_solve_ellip_record_f32", "fold3d_adjoint_ellip_f32",
     "fold3d_solve_batch_f32", "fold3d_adjoint_batch_f32",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
-    "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser",
+    "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser", "InitNode", "updateVoxel", "x", "y", "z",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
     "acc_malloc", "acc_free", "acc_memcpy_to_device", "acc_memcpy_from_device",
@@ -137,6 +137,11 @@ def lib() -> C.CDLL:
     L.ImpSurfF.argtypes = [d] * 3
     L.ImpSurfF.restype = d
     L.ImplicitInitialiser.argtypes = [vp, i, i, i, d, d, d]
+    L.InitNode.argtypes = [d, d, d, i, i, i, vp]
+    L.updateVoxel.argtypes = [vp, i, i, i, d, d, d, d, d, d]
+    for n in ("x", "y", "z"):
+        getattr(L, n).argtypes = [i, d]
+        getattr(L, n).restype = d
     for n in ("function_x_down", "function_x_up", "function_y_up", "function_y_down",
               "function_k_up", "function_k_down"):
         getattr(L, n).argtypes = [vp, i] + [d] * 10

@@ -324,10 +324,14 @@ double fold3d_exact_time(const fold3d_medium *m, double x, double y, double z);
  * the process exits; calls with max_sweeps above that limit are rejected with
  * FOLD3D_ERR_INVALID.  All calls share the array and it keeps the previous
  * call's values: each sweep clears its own slot first, and calls whose work
- * overlaps on the GPU race on it.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  Synchronous like
- * fold3d_solve; rep->elapsed_ms is the call's host wall time. */
+ * overlaps on the GPU race on it.  The first call in each CUDA context looks
+ * up the array's device address (cudaGetSymbolAddress) with the caller's
+ * device and context current, and later calls in that context reuse it; a
+ * new context on the same device (after cudaDeviceReset, or another
+ * runtime's context made current) gets its own lookup.  Make the first call
+ * in a context before any stream capture.  Arguments are checked as by
+ * fold3d_solve.  Synchronous like fold3d_solve; rep->elapsed_ms is the
+ * call's host wall time. */
 #define FOLD3D_NOALLOC_MAX_SWEEPS 4096
 int fold3d_solve_noalloc(const fold3d_grid *g, const fold3d_medium *m, double *T_dev,
                          const fold3d_opts *o, void *stream, fold3d_report *rep);
@@ -363,9 +367,27 @@ double InitFoldFromPoint(double F, double ax, double ay, double az, double x, do
                          double z);
 double ImpSurfF(double x, double y, double z);
 /* Fold3dPMM.h:81-85 / Fold3dPMM.c:129-389: medium = the reference constants
- * F = 1.1, a = (-0.35, 0.4, 0.7). */
+ * F = 1.1, a = (-0.35, 0.4, 0.7).  Also remembers (nx, ny, nz) as the grid of
+ * InitNode and updateVoxel. */
 void ImplicitInitialiser(double *T, int nx, int ny, int nz, double dxx, double dyy,
                          double dzz);
+/* Fold3dPMM.h:64 / Fold3dPMM.c:35-54: min-update of host node (i, j, k) with
+ * the reference medium's exact time from the point (x, y, z) relative to it,
+ * keeping the node's sign.  The reference indexes T with its compile-time
+ * HEIGHT; here the pitch is nx+2 (and ny+2) of the grid set by
+ * fold3d_compat_set_grid, else of the last ImplicitInitialiser call.  With
+ * neither, nothing is written and fold3d_last_error says why. */
+void InitNode(double x, double y, double z, int i, int j, int k, double *T);
+/* Fold3dPMM.h:67-70 / Fold3dPMM.c:56-112: the 44 InitNode calls of one
+ * seeding point at (xp, yp, zp) in voxel (i, j, k), in the reference's order
+ * (same pitch rule as InitNode). */
+void updateVoxel(double *T, int i, int j, int k, double xp, double yp, double zp, double dxx,
+                 double dyy, double dzz);
+/* Fold3dPMM.h:72-76 / Fold3dPMM.c:115-126: coordinate of node i, j or k
+ * ((i - 1) * spacing + 0, the reference's domain starting at 0). */
+double x(int i, double DX);
+double y(int j, double dy);
+double z(int k, double dz);
 
 /* AN_ISO_1_OpenACC.c:180, 334, 485, 636, 790, 944.  T is a DEVICE pointer
  * (the reference's deviceptr(T), :189).  The plane index and the permuted

@@ -43,7 +43,9 @@ import sys
 import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("FOLD3D_REFERENCE", "/root/reference")
+# The reference checkout: $FOLD3D_REFERENCE, else a directory named
+# "reference" beside this checkout.
+REF_ROOT = os.environ.get("FOLD3D_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 REF_DIR = os.path.join(REF_ROOT, "Stencil-OpenACC")
 REF_OUT = os.path.join(HERE, "_ref")
 

@@ -20,8 +20,24 @@ Outputs:
                     128^3 (an_iso_1_openacc.txt, written by its unmodified
                     main).
 
+  digests_large.json  sha256 digests at the benchmarked sizes, from the
+                    OpenMP transform of the reference (libref_omp.so, the same
+                    arithmetic in the same order per point; a plane's points
+                    are independent, so the result is the same bits, which
+                    tests/test_oracle.py checks against libref.so):
+                      n512_init, n512_s8      implicit surface, 8 sweeps
+                      n512_point_s8           point source at (i,j,k) =
+                                              (65, 257, 257), 8 sweeps
+                      n1280_init, n1280_s1 .. implicit surface after 1, 2,
+                                              ... sweeps, as far as --sweeps1280
+                    Written after every result, so an interrupted run keeps
+                    what it finished.
+
     python tests/golden/make_golden.py            # everything but 128^3 dump
     python tests/golden/make_golden.py --dump128  # also run the 128^3 program (~30 s)
+    python tests/golden/make_golden.py --large [--sweeps1280 K]
+        # only digests_large.json: 512^3 (~20 min on 8 cores) and 1280^3
+        # (34 GB of host memory; init ~10 min, ~20 min per sweep on 8 cores)
 """
 from __future__ import annotations
 
@@ -60,7 +76,48 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
+# point source of the 512^3 digest (1-based i, j, k; x fastest)
+POINT_512 = (65, 257, 257)
+
+
+def main_large(sweeps1280: int) -> None:
+    path = os.path.join(HERE, "digests_large.json")
+    dig = json.load(open(path)) if os.path.exists(path) else {}
+
+    def put(key, T):
+        dig[key] = sha(T)
+        with open(path, "w") as fh:
+            json.dump(dig, fh, indent=1, sort_keys=True)
+        print(key, dig[key], flush=True)
+
+    build.build_ref(512)
+    r = RefLib(512, omp=True)
+    if "n512_s8" not in dig:
+        T = r.init_implicit()
+        put("n512_init", T)
+        r.sweeps(T, 8)
+        put("n512_s8", T)
+        del T
+    if "n512_point_s8" not in dig:
+        P = point_field(512, POINT_512)
+        r.sweeps(P, 8)
+        put("n512_point_s8", P)
+        del P
+    if sweeps1280 > 0:
+        build.build_ref(1280)
+        r = RefLib(1280, omp=True)
+        T = r.init_implicit()
+        put("n1280_init", T)
+        for s in range(1, sweeps1280 + 1):
+            r.sweeps(T, 1)
+            put("n1280_s%d" % s, T)
+
+
 def main():
+    if "--large" in sys.argv:
+        k = sys.argv.index("--sweeps1280") + 1 if "--sweeps1280" in sys.argv else 0
+        main_large(int(sys.argv[k]) if k else 1)
+        return
     out = {}
     for n in (8, 16):
         build.build_ref(n)

@@ -201,29 +201,22 @@ def test_struct_layouts_match_header(f3d, tmp_path):
         assert got[cname] == py, "%s: C %s, ctypes %s" % (cname, got[cname], py)
 
 
-def test_integration_c_example_compiles_and_links(f3d, tmp_path):
-    """The C caller shown in INTEGRATION.md compiles against the header and
-    links against the library as written."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    sec = doc[doc.index("## A C caller"):]
-    code = sec[sec.index("```c") + 4:sec.index("```", sec.index("```c") + 4)]
-    src = tmp_path / "caller.c"
-    src.write_text(code)
+def test_c_caller_compiles_and_links(f3d, tmp_path):
+    """A C caller of the native API (tests/csrc/caller.c) compiles against
+    the header and links against the library."""
     libdir = os.path.dirname(f3d.LIB_PATH)
-    subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o",
-                    str(tmp_path / "caller"), "-L", libdir, "-lfold3dpmm", "-Wl,-rpath," + libdir], check=True)
+    subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "csrc", "caller.c"), "-o", str(tmp_path / "caller"), "-L", libdir,
+                    "-lfold3dpmm", "-Wl,-rpath," + libdir], check=True)
 
 
-def test_integration_adjoint_example_compiles(tmp_path):
-    """The elliptical/adjoint C example of INTEGRATION.md compiles as written."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    sec = doc[doc.index("## Elliptical medium, batches and the adjoint from C"):]
-    code = sec[sec.index("```c") + 4:sec.index("```", sec.index("```c") + 4)]
-    src = tmp_path / "gradient.c"
-    src.write_text(code)
+def test_c_adjoint_caller_compiles(tmp_path):
+    """The elliptical solve and its adjoint called from C
+    (tests/csrc/gradient.c) compile against the header."""
     cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
-    subprocess.run(["gcc", "-Wall", "-Werror", "-c", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src),
-                    "-o", str(tmp_path / "gradient.o")], check=True)
+    subprocess.run(["gcc", "-Wall", "-Werror", "-c", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                    os.path.join(ROOT, "tests", "csrc", "gradient.c"), "-o", str(tmp_path / "gradient.o")],
+                   check=True)
 
 
 def test_newer_entry_points_reject_null_context(f3d, tmp_path):
@@ -295,3 +288,42 @@ def test_host_solve_rejects_a_short_output(f3d):
     with pytest.raises(ValueError, match="field's shape"):
         f3d.Context.solve(ctx, T, 1.0, out=np.zeros((6, 7, 7)))
     ctx._h = C.c_void_p()  # keep __del__ from closing anything
+
+
+@pytest.mark.parametrize("entry", ["fold3d_solve_noalloc", "fold3d_plane"])
+@pytest.mark.parametrize("bad", ["inf_spacing", "inf_F", "inf_drift", "huge_grid"])
+def test_noalloc_checks_arguments_like_solve(f3d, entry, bad):
+    """The allocation-free solve rejects the grids and media fold3d_solve and
+    fold3d_plane reject (infinite spacing, infinite F or drift, a grid too
+    large for the item counters), with the same code, before any CUDA call."""
+    L = f3d.lib()
+    inf = float("inf")
+    g = f3d.grid(8, 8, 8, 1.0)
+    m = f3d.medium()
+    if bad == "inf_spacing":
+        g = f3d.Grid(8, 8, 8, 1.0, inf, 1.0)
+    elif bad == "inf_F":
+        m = f3d.Medium(inf, 0.0, 0.0, 0.0)
+    elif bad == "inf_drift":
+        m = f3d.Medium(1.1, 0.0, -inf, 0.0)
+    else:
+        g = f3d.Grid(70000, 70000, 70000, 1.0, 1.0, 1.0)
+    if entry == "fold3d_solve_noalloc":
+        rc = L.fold3d_solve_noalloc(C.byref(g), C.byref(m), C.c_void_p(16), C.byref(f3d.opts(max_sweeps=2)),
+                                    None, None)
+    else:
+        rc = L.fold3d_plane(C.byref(g), C.byref(m), C.c_void_p(16), 0, 1, None)
+    assert rc == f3d.ERR_INVALID, f3d.last_error()
+    assert ("spacing" in f3d.last_error()) if bad == "inf_spacing" else True
+    assert ("too large" in f3d.last_error()) if bad == "huge_grid" else True
+    assert ("finite" in f3d.last_error()) if bad in ("inf_F", "inf_drift") else True
+
+
+def test_compat_sweep_without_grid_size_is_rejected(f3d):
+    """A reference-style sweep call on a pointer that did not come from
+    acc_malloc, with no grid size set, records an error and launches
+    nothing."""
+    L = f3d.lib()
+    assert L.fold3d_compat_set_grid(0, 0, 0) == f3d.OK
+    L.function_x_down(C.c_void_p(4096), 1, *([0.1] * 6), 1.1, 0.4, -0.35, 0.7)
+    assert "grid size unknown" in f3d.last_error()

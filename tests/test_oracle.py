@@ -155,6 +155,87 @@ def test_product_scalar_helpers_match_reference(f3d):
     assert L.InitFoldFromPoint(1.1, *REF_A, 0.0, 0.0, 0.0) == MAXT
 
 
+def test_product_node_helpers_match_reference(f3d):
+    """InitNode and updateVoxel (Fold3dPMM.c:35-112) and the coordinate
+    helpers x, y, z (:115-126) against the reference's own build at 8^3,
+    bit for bit, on fields of both signs; the pitch comes from
+    fold3d_compat_set_grid, then from the last ImplicitInitialiser call."""
+    import ctypes as C
+
+    from oracle import RefLib
+
+    n = 8
+    r = RefLib(n)
+    L = f3d.lib()
+    rng = np.random.default_rng(11)
+    h = ref_spacing(n)
+    try:
+        for how in ("set_grid", "initialiser"):
+            if how == "set_grid":
+                assert L.fold3d_compat_set_grid(n, n, n) == 0
+            else:
+                assert L.fold3d_compat_set_grid(0, 0, 0) == 0
+                scratch = np.empty((n + 2,) * 3)
+                L.ImplicitInitialiser(scratch.ctypes.data_as(C.c_void_p), n, n, n, h, h, h)
+            A = np.where(rng.random((n + 2,) * 3) < 0.5, -MAXT, MAXT)
+            B = A.copy()
+            pa, pb = A.ctypes.data_as(C.c_void_p), B.ctypes.data_as(C.c_void_p)
+            for _ in range(40):
+                i, j, k = (int(v) for v in rng.integers(2, n - 1, 3))
+                xp, yp, zp = rng.uniform(-1.5, 1.5, 3) * h
+                L.InitNode(xp, yp, zp, i, j, k, pa)
+                r.L.InitNode.argtypes = L.InitNode.argtypes
+                r.L.InitNode(xp, yp, zp, i, j, k, pb)
+                hh = rng.uniform(0.5, 2.0, 3) * h
+                L.updateVoxel(pa, i, j, k, xp, yp, zp, *hh)
+                r.L.updateVoxel.argtypes = L.updateVoxel.argtypes
+                r.L.updateVoxel(pb, i, j, k, xp, yp, zp, *hh)
+            assert_bitwise(A, B, how)
+            assert np.abs(A).min() < MAXT
+    finally:
+        L.fold3d_compat_set_grid(0, 0, 0)
+    for name in ("x", "y", "z"):
+        fr = getattr(r.L, name)
+        fr.argtypes, fr.restype = [C.c_int, C.c_double], C.c_double
+        for q in range(-1, n + 3):
+            assert getattr(L, name)(q, 0.37) == fr(q, 0.37)
+
+
+def test_reference_header_program_links_to_library_alone(f3d, tmp_path):
+    """A C program written against the reference's own Fold3dPMM.h, calling
+    all of its host functions (tests/csrc/ref_helpers.c), links against
+    libfold3dpmm.so alone and prints the same bits as when it is linked
+    against the reference's own build."""
+    import subprocess
+
+    from oracle import build
+
+    if not build.reference_available():
+        pytest.skip("the reference's header is not available")
+    build.build_ref(8)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "tests", "csrc", "ref_helpers.c")
+    inc = ["-DREF_HEADER", "-I", build.REF_DIR]
+    libdir = os.path.dirname(f3d.LIB_PATH)
+    ours = tmp_path / "ours"
+    subprocess.run(["gcc", "-Wall", *inc, src, "-o", str(ours), "-L", libdir, "-lfold3dpmm",
+                    "-Wl,-rpath," + libdir], check=True, capture_output=True)
+    refdir = os.path.dirname(build.ref_lib_path(8))
+    theirs = tmp_path / "theirs"
+    subprocess.run(["gcc", "-Wall", *inc, src, "-o", str(theirs), "-L", refdir, "-lref",
+                    "-Wl,-rpath," + refdir, "-lm"], check=True, capture_output=True)
+    ldd = subprocess.run(["ldd", str(ours)], capture_output=True, text=True).stdout
+    assert "libfold3dpmm.so" in ldd and "libref" not in ldd
+    a = subprocess.run([str(ours)], capture_output=True, text=True, check=True).stdout
+    b = subprocess.run([str(theirs)], capture_output=True, text=True, check=True).stdout
+    assert len(a.splitlines()) == 7 and a == b
+    # and against this library's own header
+    own = tmp_path / "own"
+    subprocess.run(["gcc", "-Wall", "-Werror", "-I", os.path.join(root, "include"), src, "-o", str(own), "-L",
+                    libdir, "-lfold3dpmm", "-Wl,-rpath," + libdir], check=True, capture_output=True)
+    assert subprocess.run([str(own)], capture_output=True, text=True, check=True).stdout == a
+
+
 def test_product_point_init(f3d):
     T = f3d.init_point(5, 4, 3, (2, 3, 1))
     assert T[1, 3, 2] == 0.0
