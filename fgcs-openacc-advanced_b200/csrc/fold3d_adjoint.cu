@@ -369,7 +369,10 @@ __global__ void __launch_bounds__(kListThreads) adj_fill_kernel(const BatchAdjIn
 // dL/dM(x) = lambda(x) d(time(x))/dM(x), six arrays (component-major) in the
 // field layout, accumulated in the order of the CPU statement.  Every cell is
 // written (ghosts and cells without a winner get 0), or, with accumulate,
-// added to.
+// added to.  For a medium given by its parameters (kParamF64) the four
+// arrays written are the gradients with respect to s, eps, nx and ny instead
+// (the chain rule through M = a I + b n n^T, nz depending on nx and ny; where
+// nz = 0 the axis components get only their direct terms).
 template <class R>
 __global__ void __launch_bounds__(256) adj_grad_kernel(const R *__restrict__ T, const R *__restrict__ lam,
                                                        const unsigned char *__restrict__ W,
@@ -405,6 +408,44 @@ __global__ void __launch_bounds__(256) adj_grad_kernel(const R *__restrict__ T, 
             }
         }
         const R L = interior ? lam[x] : R(0);
+        if (med.kind == kParamF64) {
+            // chain to the parameters (s, eps, nx, ny) of M = a I + b n n^T
+            // (ell_metric_from_param), nz depending on nx and ny
+            R g[4] = {R(0), R(0), R(0), R(0)};
+            if (interior) {
+                const double *P[4] = {static_cast<const double *>(med.m[0]), static_cast<const double *>(med.m[1]),
+                                      static_cast<const double *>(med.m[2]), static_cast<const double *>(med.m[3])};
+                const double ps = P[0][x], eps = P[1][x], nx_ = P[2][x], ny_ = P[3][x];
+                const double s2 = ps * ps, den = 1.0 + 2.0 * eps;
+                const double a = s2 / den, b = s2 - a;
+                const double q = (1.0 - nx_ * nx_) - ny_ * ny_;
+                const double nz_ = sqrt(q > 0.0 ? q : 0.0);
+                double gm[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) gm[m] = (double)L * (double)dM[m];
+                const double ga = gm[0] + gm[3] + gm[5];
+                const double gb = gm[0] * nx_ * nx_ + gm[3] * ny_ * ny_ + gm[5] * nz_ * nz_ + gm[1] * nx_ * ny_ +
+                                  gm[2] * nx_ * nz_ + gm[4] * ny_ * nz_;
+                double gnx = 2.0 * b * nx_ * gm[0] + b * ny_ * gm[1] + b * nz_ * gm[2];
+                double gny = 2.0 * b * ny_ * gm[3] + b * nx_ * gm[1] + b * nz_ * gm[4];
+                const double gnz = 2.0 * b * nz_ * gm[5] + b * nx_ * gm[2] + b * ny_ * gm[4];
+                if (nz_ > 0.0) {
+                    gnx -= gnz * nx_ / nz_;
+                    gny -= gnz * ny_ / nz_;
+                }
+                const double da_ds = 2.0 * ps / den, da_de = -2.0 * s2 / (den * den);
+                g[0] = (R)(ga * da_ds + gb * (2.0 * ps - da_ds));
+                g[1] = (R)(ga * da_de - gb * da_de);
+                g[2] = (R)gnx;
+                g[3] = (R)gny;
+            }
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                R *o = dLdM + m * cells + x;
+                *o = accumulate ? *o + g[m] : g[m];
+            }
+            continue;
+        }
 #pragma unroll
         for (int m = 0; m < 6; ++m) {
             R *o = dLdM + m * cells + x;

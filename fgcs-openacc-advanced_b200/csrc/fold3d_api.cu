@@ -438,7 +438,7 @@ static int wave_scratch(fold3d_ctx *c, const fold3d_grid &g)
 }
 
 // Elliptical-medium constants of a sweep direction.
-static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int dir)
+static EllipParam ellip_param(const fold3d_grid &g, const EllipMedium &m, int dir)
 {
     const DirSpec &d = kDirs[dir];
     const double h[3] = {g.dx, g.dy, g.dz};
@@ -457,13 +457,12 @@ static EllipParam ellip_param(const fold3d_grid &g, const fold3d_ellip &m, int d
     p.dir.ixy = pair[d.xa][d.ya];
     p.dir.ixz = pair[d.xa][d.nrm];
     p.dir.iyz = pair[d.ya][d.nrm];
-    const float *arr[6] = {m.mxx, m.mxy, m.mxz, m.myy, m.myz, m.mzz};
-    for (int k = 0; k < 6; ++k) p.med.m[k] = arr[k];
+    p.med = m;
     return p;
 }
 
 // T: double, or float when f32 (elliptical medium only).
-static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const fold3d_ellip *em,
+static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium *fm, const EllipMedium *em,
                            void *T, bool f32, const fold3d_opts &o, cudaStream_t s, fold3d_report *rep,
                            unsigned char *winners = nullptr)
 {
@@ -650,15 +649,34 @@ static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
 }
 
 // Instances of the batched drivers: fields of doubles, or of floats (f32).
+// Internal medium of the elliptical solvers from the public structs.
+static EllipMedium medium_of(const fold3d_ellip &m)
+{
+    EllipMedium e;
+    const float *arr[6] = {m.mxx, m.mxy, m.mxz, m.myy, m.myz, m.mzz};
+    for (int k = 0; k < 6; ++k) e.m[k] = arr[k];
+    e.kind = kMetricF32;
+    return e;
+}
+static EllipMedium medium_of(const fold3d_tti &m)
+{
+    EllipMedium e;
+    const double *arr[4] = {m.s, m.eps, m.nx, m.ny};
+    for (int k = 0; k < 4; ++k) e.m[k] = arr[k];
+    e.m[4] = e.m[5] = nullptr;
+    e.kind = kParamF64;
+    return e;
+}
+
 struct SolveInst {
     fold3d_grid grid;
-    fold3d_ellip medium;
+    EllipMedium medium;
     void *T;
     unsigned char *winners;
 };
 struct AdjInst {
     fold3d_grid grid;
-    fold3d_ellip medium;
+    EllipMedium medium;
     const void *T;
     const unsigned char *winners;
     const void *dLdT;
@@ -1053,11 +1071,8 @@ static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
             geo.pg[d] = make_geom(in[i].grid, d);
             geo.d[d] = ellip_param(in[i].grid, in[i].medium, d).dir;
         }
-        EllipMedium med;
-        const float *arr[6] = {in[i].medium.mxx, in[i].medium.mxy, in[i].medium.mxz,
-                               in[i].medium.myy, in[i].medium.myz, in[i].medium.mzz};
-        for (int k = 0; k < 6; ++k) med.m[k] = arr[k];
-        if ((e = launch_adj_grad(in[i].T, in[i].lambda, in[i].winners, geo, med, in[i].grid, in[i].dLdM, accumulate,
+        if ((e = launch_adj_grad(in[i].T, in[i].lambda, in[i].winners, geo, in[i].medium, in[i].grid, in[i].dLdM,
+                                 accumulate,
                                  f32, s)) != cudaSuccess)
             return cuda_error(e, "gradient");
     }
@@ -1078,9 +1093,21 @@ static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
     return FOLD3D_OK;
 }
 
-static bool metric_ok(const fold3d_ellip *m)
+// Every array of the medium present; the FP64 parameter medium only with
+// float64 fields.
+static bool metric_ok(const EllipMedium &m)
 {
-    return m && m->mxx && m->mxy && m->mxz && m->myy && m->myz && m->mzz;
+    const int n = (m.kind == kParamF64) ? 4 : 6;
+    for (int k = 0; k < n; ++k)
+        if (!m.m[k]) return false;
+    return true;
+}
+static int medium_ok(const EllipMedium &m, bool f32)
+{
+    if (!metric_ok(m)) return set_error(FOLD3D_ERR_INVALID, "medium array is NULL");
+    if (f32 && m.kind == kParamF64)
+        return set_error(FOLD3D_ERR_UNSUPPORTED, "the FP64 parameter medium runs with float64 fields");
+    return FOLD3D_OK;
 }
 
 static int ellip_opts_ok(const fold3d_opts *o)
@@ -1093,15 +1120,16 @@ static int ellip_opts_ok(const fold3d_opts *o)
 }
 
 // fold3d_solve_ellip(_record)(_f32): W == NULL for no record.
-static int ellip_entry(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, void *T, bool f32,
+static int ellip_entry(fold3d_ctx *c, const fold3d_grid *g, const EllipMedium *m, void *T, bool f32,
                        unsigned char *W, bool record, const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
     clear_error();
     if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
     if (record && !W) return set_error(FOLD3D_ERR_INVALID, "winner array is NULL");
-    if (!T || !o) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    if (!metric_ok(m)) return set_error(FOLD3D_ERR_INVALID, "metric array is NULL");
-    int rc = check_grid(g);
+    if (!T || !o || !m) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    int rc = medium_ok(*m, f32);
+    if (rc) return rc;
+    rc = check_grid(g);
     if (rc || (rc = ellip_opts_ok(o))) return rc;
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
@@ -1123,8 +1151,9 @@ static int adjoint_entry(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
     for (int i = 0; i < n; ++i) {
         int rc = check_grid(&in[i].grid);
         if (rc) return rc;
-        if (!in[i].T || !in[i].winners || !in[i].dLdT || !in[i].lambda || !in[i].dLdM || !metric_ok(&in[i].medium))
+        if (!in[i].T || !in[i].winners || !in[i].dLdT || !in[i].lambda || !in[i].dLdM || !metric_ok(in[i].medium))
             return set_error(FOLD3D_ERR_INVALID, n == 1 ? "NULL argument" : "instance with a NULL array");
+        if ((rc = medium_ok(in[i].medium, f32))) return rc;
     }
     DeviceGuard dg(c->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
@@ -1140,7 +1169,8 @@ static int batch_entry(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cons
     for (int i = 0; i < n; ++i) {
         int rc = check_grid(&in[i].grid);
         if (rc) return rc;
-        if (!in[i].T || !metric_ok(&in[i].medium)) return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
+        if (!in[i].T || !metric_ok(in[i].medium)) return set_error(FOLD3D_ERR_INVALID, "instance with a NULL array");
+        if ((rc = medium_ok(in[i].medium, f32))) return rc;
     }
     int rc = ellip_opts_ok(o);
     if (rc) {
@@ -1166,7 +1196,7 @@ int fold3d_solve_batch(fold3d_ctx *c, int n, const fold3d_instance *in, const fo
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
     return host_guard([&] {
         std::vector<SolveInst> v(n);
-        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners};
         return batch_entry(c, n, v.data(), false, o, stream, reps);
     });
 }
@@ -1177,7 +1207,7 @@ int fold3d_solve_batch_f32(fold3d_ctx *c, int n, const fold3d_instance_f32 *in, 
     if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
     return host_guard([&] {
         std::vector<SolveInst> v(n);
-        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners};
+        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners};
         return batch_entry(c, n, v.data(), true, o, stream, reps);
     });
 }
@@ -1224,7 +1254,8 @@ int fold3d_adjoint_batch(fold3d_ctx *c, int n, const fold3d_adjoint_instance *in
     return host_guard([&] {
         std::vector<AdjInst> v(n);
         for (int i = 0; i < n; ++i)
-            v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+            v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners, in[i].dLdT, in[i].lambda,
+                    in[i].dLdM};
         return adjoint_entry(c, n, v.data(), false, max_sweeps, tol, accumulate, stream, reps);
     });
 }
@@ -1236,7 +1267,8 @@ int fold3d_adjoint_batch_f32(fold3d_ctx *c, int n, const fold3d_adjoint_instance
     return host_guard([&] {
         std::vector<AdjInst> v(n);
         for (int i = 0; i < n; ++i)
-            v[i] = {in[i].grid, in[i].medium, in[i].T, in[i].winners, in[i].dLdT, in[i].lambda, in[i].dLdM};
+            v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners, in[i].dLdT, in[i].lambda,
+                    in[i].dLdM};
         return adjoint_entry(c, n, v.data(), true, max_sweeps, tol, accumulate, stream, reps);
     });
 }
@@ -1347,25 +1379,33 @@ void fold3d_ellip_metric(double vz, double eps, double ax, double ay, double az,
 int fold3d_solve_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T, const fold3d_opts *o,
                        void *stream, fold3d_report *rep)
 {
-    return ellip_entry(c, g, m, T, false, nullptr, false, o, stream, rep);
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, false, nullptr, false, o, stream, rep);
 }
 
 int fold3d_solve_ellip_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, float *T,
                            const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
-    return ellip_entry(c, g, m, T, true, nullptr, false, o, stream, rep);
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, true, nullptr, false, o, stream, rep);
 }
 
 int fold3d_solve_ellip_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, double *T,
                               unsigned char *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
-    return ellip_entry(c, g, m, T, false, W, true, o, stream, rep);
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, false, W, true, o, stream, rep);
 }
 
 int fold3d_solve_ellip_record_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, float *T,
                                   unsigned char *W, const fold3d_opts *o, void *stream, fold3d_report *rep)
 {
-    return ellip_entry(c, g, m, T, true, W, true, o, stream, rep);
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, true, W, true, o, stream, rep);
 }
 
 int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip *m, const double *T,
@@ -1373,7 +1413,7 @@ int fold3d_adjoint_ellip(fold3d_ctx *c, const fold3d_grid *g, const fold3d_ellip
                          double tol, void *stream, fold3d_report *rep)
 {
     if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    const AdjInst one = {*g, *m, T, W, dLdT, lam, dLdM};
+    const AdjInst one = {*g, medium_of(*m), T, W, dLdT, lam, dLdM};
     return adjoint_entry(c, 1, &one, false, max_sweeps, tol, 0, stream, rep);
 }
 
@@ -1382,8 +1422,57 @@ int fold3d_adjoint_ellip_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_e
                              double tol, void *stream, fold3d_report *rep)
 {
     if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
-    const AdjInst one = {*g, *m, T, W, dLdT, lam, dLdM};
+    const AdjInst one = {*g, medium_of(*m), T, W, dLdT, lam, dLdM};
     return adjoint_entry(c, 1, &one, true, max_sweeps, tol, 0, stream, rep);
+}
+
+int fold3d_solve_tti(fold3d_ctx *c, const fold3d_grid *g, const fold3d_tti *m, double *T, const fold3d_opts *o,
+                     void *stream, fold3d_report *rep)
+{
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, false, nullptr, false, o, stream, rep);
+}
+
+int fold3d_solve_tti_record(fold3d_ctx *c, const fold3d_grid *g, const fold3d_tti *m, double *T, unsigned char *W,
+                            const fold3d_opts *o, void *stream, fold3d_report *rep)
+{
+    if (!m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const EllipMedium em = medium_of(*m);
+    return ellip_entry(c, g, &em, T, false, W, true, o, stream, rep);
+}
+
+int fold3d_adjoint_tti(fold3d_ctx *c, const fold3d_grid *g, const fold3d_tti *m, const double *T,
+                       const unsigned char *W, const double *dLdT, double *lam, double *dLdP, int max_sweeps,
+                       double tol, void *stream, fold3d_report *rep)
+{
+    if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    const AdjInst one = {*g, medium_of(*m), T, W, dLdT, lam, dLdP};
+    return adjoint_entry(c, 1, &one, false, max_sweeps, tol, 0, stream, rep);
+}
+
+int fold3d_solve_batch_tti(fold3d_ctx *c, int n, const fold3d_tti_instance *in, const fold3d_opts *o, void *stream,
+                           fold3d_report *reps)
+{
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    return host_guard([&] {
+        std::vector<SolveInst> v(n);
+        for (int i = 0; i < n; ++i) v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners};
+        return batch_entry(c, n, v.data(), false, o, stream, reps);
+    });
+}
+
+int fold3d_adjoint_batch_tti(fold3d_ctx *c, int n, const fold3d_tti_adjoint_instance *in, int max_sweeps, double tol,
+                             int accumulate, void *stream, fold3d_report *reps)
+{
+    if (!in || n < 1) return clear_error(), set_error(FOLD3D_ERR_INVALID, in ? "n must be >= 1" : "NULL argument");
+    return host_guard([&] {
+        std::vector<AdjInst> v(n);
+        for (int i = 0; i < n; ++i)
+            v[i] = {in[i].grid, medium_of(in[i].medium), in[i].T, in[i].winners, in[i].dLdT, in[i].lambda,
+                    in[i].dLdP};
+        return adjoint_entry(c, n, v.data(), false, max_sweeps, tol, accumulate, stream, reps);
+    });
 }
 
 int fold3d_solve_host(fold3d_ctx *c, const fold3d_grid *g, const fold3d_medium *m, const double *T_in,

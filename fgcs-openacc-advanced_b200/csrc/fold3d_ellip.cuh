@@ -45,9 +45,18 @@ struct EllipDir {
     int ixx, iyy, izz, ixy, ixz, iyz;  // which global metric array feeds each local entry
 };
 
-// The six metric arrays, field layout, ordered xx xy xz yy yz zz (axes i, j, k).
+// How the per-cell medium is stored (field layout, axes i, j, k):
+//  kMetricF32: six float32 arrays of the metric, ordered xx xy xz yy yz zz;
+//  kParamF64:  four float64 arrays of the tilted elliptical medium's
+//              parameters -- slowness s = 1/Vz, Thomsen epsilon, and the x
+//              and y components of the unit symmetry axis n (its z
+//              component sqrt(1 - nx^2 - ny^2) >= 0; n and -n are the same
+//              axis) -- from which the metric is formed per cell in FP64
+//              (ell_metric_from_param).
+enum { kMetricF32 = 0, kParamF64 = 1 };
 struct EllipMedium {
-    const float *m[6];
+    const void *m[6];
+    int kind;
 };
 
 struct EllipParam {
@@ -198,18 +207,70 @@ __host__ __device__ __forceinline__ int ell_ri(int r)
 }
 __host__ __device__ __forceinline__ int ell_rj(int r) { return (r >= 1 && r <= 3) ? 1 : (r >= 5) ? -1 : 0; }
 
+__host__ __device__ __forceinline__ double ell_ld(const double *p)
+{
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+// The metric M = a I + b n n^T of the tilted elliptical medium from its
+// parameters: a = s^2 / (1 + 2 eps), b = s^2 - a, n = (nx, ny, nz) with
+// nz = sqrt(max(0, (1 - nx nx) - ny ny)).  Entries xx xy xz yy yz zz, in this
+// operation order on every side (the oracle's orc_tti_metric states the
+// same), so host and device agree bit for bit.
+__host__ __device__ __forceinline__ void ell_metric_from_param(double s, double eps, double nx, double ny,
+                                                               double out[6])
+{
+    const double s2 = s * s;
+    const double a = s2 / (1.0 + 2.0 * eps);
+    const double b = s2 - a;
+    const double q = (1.0 - nx * nx) - ny * ny;
+    const double nz = sqrt(q > 0.0 ? q : 0.0);
+    const double bx = b * nx, by = b * ny, bz = b * nz;
+    out[0] = a + bx * nx;
+    out[1] = bx * ny;
+    out[2] = bx * nz;
+    out[3] = a + by * ny;
+    out[4] = by * nz;
+    out[5] = a + bz * nz;
+}
+
+// Metric entry k (xx xy xz yy yz zz) of cell t, stored as float32.
+__host__ __device__ __forceinline__ double ell_entry(const EllipMedium &M, int k, long long t)
+{
+    return (double)ell_ld(static_cast<const float *>(M.m[k]) + t);
+}
+
 // Scaled local metric of the target at field index t.
 template <class R>
 __host__ __device__ __forceinline__ EllipAT<R> ell_local(const EllipMedium &M, const EllipDir &D, long long t)
 {
     const R hx = (R)D.hx, hy = (R)D.hy, hz = (R)D.hz;
     EllipAT<R> A;
-    A.xx = (R)ell_ld(M.m[D.ixx] + t) * hx * hx;
-    A.yy = (R)ell_ld(M.m[D.iyy] + t) * hy * hy;
-    A.zz = (R)ell_ld(M.m[D.izz] + t) * hz * hz;
-    A.xy = (R)D.sxy * (R)ell_ld(M.m[D.ixy] + t) * hx * hy;
-    A.xz = (R)D.sxz * (R)ell_ld(M.m[D.ixz] + t) * hx * hz;
-    A.yz = (R)D.syz * (R)ell_ld(M.m[D.iyz] + t) * hy * hz;
+    if (M.kind == kParamF64) {
+        double m[6];
+        ell_metric_from_param(ell_ld(static_cast<const double *>(M.m[0]) + t),
+                              ell_ld(static_cast<const double *>(M.m[1]) + t),
+                              ell_ld(static_cast<const double *>(M.m[2]) + t),
+                              ell_ld(static_cast<const double *>(M.m[3]) + t), m);
+        A.xx = (R)m[D.ixx] * hx * hx;
+        A.yy = (R)m[D.iyy] * hy * hy;
+        A.zz = (R)m[D.izz] * hz * hz;
+        A.xy = (R)D.sxy * (R)m[D.ixy] * hx * hy;
+        A.xz = (R)D.sxz * (R)m[D.ixz] * hx * hz;
+        A.yz = (R)D.syz * (R)m[D.iyz] * hy * hz;
+        return A;
+    }
+    const float *const *f = reinterpret_cast<const float *const *>(M.m);
+    A.xx = (R)ell_ld(f[D.ixx] + t) * hx * hx;
+    A.yy = (R)ell_ld(f[D.iyy] + t) * hy * hy;
+    A.zz = (R)ell_ld(f[D.izz] + t) * hz * hz;
+    A.xy = (R)D.sxy * (R)ell_ld(f[D.ixy] + t) * hx * hy;
+    A.xz = (R)D.sxz * (R)ell_ld(f[D.ixz] + t) * hx * hz;
+    A.yz = (R)D.syz * (R)ell_ld(f[D.iyz] + t) * hy * hz;
     return A;
 }
 

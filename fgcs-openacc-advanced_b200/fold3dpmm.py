@@ -40,6 +40,8 @@ EXPORTED = (
     "fold3d_write_raw", "fold3d_solve_ellip_f32", "fold3d_solve_ellip_record_f32", "fold3d_adjoint_ellip_f32",
     "fold3d_solve_batch_f32", "fold3d_adjoint_batch_f32",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
+    "fold3d_solve_tti", "fold3d_solve_tti_record", "fold3d_adjoint_tti", "fold3d_solve_batch_tti",
+    "fold3d_adjoint_batch_tti",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser", "InitNode", "updateVoxel", "x", "y", "z",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -73,6 +75,21 @@ class Instance(C.Structure):
 class AdjInstance(C.Structure):
     _fields_ = [("grid", Grid), ("medium", Ellip), ("T", C.c_void_p), ("winners", C.c_void_p),
                 ("dLdT", C.c_void_p), ("lambda_", C.c_void_p), ("dLdM", C.c_void_p)]
+
+
+class Tti(C.Structure):
+    """fold3d_tti: the FP64 parameter arrays (s, eps, nx, ny) of a tilted
+    elliptical medium."""
+    _fields_ = [(n, C.c_void_p) for n in ("s", "eps", "nx", "ny")]
+
+
+class TtiInstance(C.Structure):
+    _fields_ = [("grid", Grid), ("medium", Tti), ("T", C.c_void_p), ("winners", C.c_void_p)]
+
+
+class TtiAdjInstance(C.Structure):
+    _fields_ = [("grid", Grid), ("medium", Tti), ("T", C.c_void_p), ("winners", C.c_void_p),
+                ("dLdT", C.c_void_p), ("lambda_", C.c_void_p), ("dLdP", C.c_void_p)]
 
 
 class Opts(C.Structure):
@@ -150,6 +167,11 @@ def lib() -> C.CDLL:
     L.acc_free.argtypes = [vp]
     L.acc_memcpy_to_device.argtypes = [vp, vp, C.c_size_t]
     L.acc_memcpy_from_device.argtypes = [vp, vp, C.c_size_t]
+    L.fold3d_solve_tti.argtypes = [vp, P(Grid), P(Tti), vp, P(Opts), vp, P(Report)]
+    L.fold3d_solve_tti_record.argtypes = [vp, P(Grid), P(Tti), vp, vp, P(Opts), vp, P(Report)]
+    L.fold3d_adjoint_tti.argtypes = [vp, P(Grid), P(Tti), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
+    L.fold3d_solve_batch_tti.argtypes = [vp, i, P(TtiInstance), P(Opts), vp, P(Report)]
+    L.fold3d_adjoint_batch_tti.argtypes = [vp, i, P(TtiAdjInstance), i, d, i, vp, P(Report)]
     # the float32 build takes the same arguments (float fields)
     L.fold3d_solve_ellip_f32.argtypes = list(L.fold3d_solve_ellip.argtypes)
     L.fold3d_solve_ellip_record_f32.argtypes = list(L.fold3d_solve_ellip_record.argtypes)
@@ -221,9 +243,12 @@ def _dev_ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
-def init_implicit(nx, ny, nz, h, med: Medium | None = None) -> np.ndarray:
-    """Host field initialised from the reference's implicit surface."""
-    T = np.empty((nz + 2, ny + 2, nx + 2), dtype=np.float64)
+def init_implicit(nx, ny, nz, h, med: Medium | None = None, out: np.ndarray | None = None) -> np.ndarray:
+    """Host field initialised from the reference's implicit surface (into
+    `out`, a float64 array of the field's shape, when given)."""
+    if out is not None and out.shape != (nz + 2, ny + 2, nx + 2):
+        raise ValueError("out must have the field's shape")
+    T = np.empty((nz + 2, ny + 2, nx + 2), dtype=np.float64) if out is None else out
     _check(lib().fold3d_init_implicit(_host_ptr(T), C.byref(grid(nx, ny, nz, h)),
                                       C.byref(med or medium())))
     return T
@@ -355,6 +380,42 @@ def ellip(M, like=None):
     return Ellip(*(C.c_void_p(m.data_ptr()) for m in M))
 
 
+def tti(P, like=None):
+    """fold3d_tti from four contiguous float64 CUDA tensors (slowness,
+    epsilon, axis x and y components), each shaped like the field `like`."""
+    import torch
+
+    if len(P) != 4:
+        raise ValueError("a parameter medium is four arrays (s, eps, nx, ny), got %d" % len(P))
+    for m in P:
+        if like is not None and (tuple(m.shape) != tuple(like.shape) or m.device != like.device):
+            raise ValueError("medium arrays must have the field's shape %s and device %s, got %s on %s"
+                             % (tuple(like.shape), like.device, tuple(m.shape), m.device))
+        if m.dtype != torch.float64 or not m.is_cuda or not m.is_contiguous():
+            raise ValueError("parameter arrays must be contiguous float64 CUDA tensors")
+    return Tti(*(C.c_void_p(m.data_ptr()) for m in P))
+
+
+def is_tti(M) -> bool:
+    """A medium given as four FP64 parameter arrays (else six float32 metric
+    arrays)."""
+    return len(M) == 4
+
+
+def _medium_arg(M, T):
+    """(struct, entry-point suffix, gradient arrays) of a medium: the six
+    float32 metric arrays (fold3d_*_ellip) or the four FP64 parameter arrays
+    (fold3d_*_tti, float64 fields only: the library cannot see a field's type
+    behind its pointer)."""
+    if is_tti(M):
+        import torch
+
+        if T.dtype != torch.float64:
+            raise ValueError("the FP64 parameter medium needs a float64 field")
+        return tti(M, T), "tti", 4
+    return ellip(M, T), "ellip", 6
+
+
 def _on_context(ctx, T, name="field"):
     """T must live on the context's device."""
     if getattr(T, "is_cuda", False) and T.device.index != ctx.device:
@@ -396,16 +457,17 @@ def _entry(name, f32):
 
 def solve_ellip(ctx: "Context", T, h, M, o: Opts | None = None, stream=None) -> Report:
     """Solve in place on a float64 (or float32: the float32 build) CUDA
-    tensor with an elliptical medium M (six float32 CUDA tensors in the field
-    layout)."""
+    tensor with an elliptical medium M: six float32 CUDA metric tensors in
+    the field layout (fold3d_solve_ellip), or four float64 parameter tensors
+    s, eps, nx, ny (fold3d_solve_tti, float64 fields only)."""
     nx, ny, nz = grid_of(T)
     rep = Report()
-    e = ellip(M, T)
+    e, kind, _ = _medium_arg(M, T)
     ptr, f32 = _field_ptr(T)
     _on_context(ctx, T)
-    _check(_entry("fold3d_solve_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr,
-                                             C.byref(o or opts()), C.c_void_p(stream) if stream else None,
-                                             C.byref(rep)))
+    fn = lib().fold3d_solve_tti if kind == "tti" else _entry("fold3d_solve_ellip", f32)
+    _check(fn(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr, C.byref(o or opts()),
+              C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 
@@ -429,31 +491,34 @@ def solve_ellip_record(ctx: "Context", T, h, M, W, o: Opts | None = None, stream
     rep = Report()
     ptr, f32 = _field_ptr(T)
     _on_context(ctx, T)
-    _check(_entry("fold3d_solve_ellip_record", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M, T)), ptr,
-                                           C.c_void_p(W.data_ptr()), C.byref(o or opts()),
-                                           C.c_void_p(stream) if stream else None, C.byref(rep)))
+    e, kind, _ = _medium_arg(M, T)
+    fn = lib().fold3d_solve_tti_record if kind == "tti" else _entry("fold3d_solve_ellip_record", f32)
+    _check(fn(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr, C.c_void_p(W.data_ptr()), C.byref(o or opts()),
+              C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 
 def adjoint_ellip(ctx: "Context", T, h, M, W, dLdT, lam, dLdM, max_sweeps=1000, tol=0.0, stream=None) -> Report:
     """fold3d_adjoint_ellip(_f32): lam <- dL/dT (total), dLdM (shape
     (6,)+T.shape) <- dL/dM, from the converged T, its winner record W and
-    dLdT (all of T's dtype).  Backward sweeps stop once one pushes at most
+    dLdT (all of T's dtype).  With a parameter medium (four arrays,
+    fold3d_adjoint_tti) dLdM has shape (4,)+T.shape and receives dL/ds,
+    dL/deps, dL/dnx and dL/dny.  Backward sweeps stop once one pushes at most
     tol times the first sweep's largest push (tol 0: once one pushes
     nothing)."""
     _check_like("W", W, T, 1)
     _check_like("dLdT", dLdT, T)
     _check_like("lam", lam, T)
-    _check_like("dLdM", dLdM, T, lead=(6,))
+    e, kind, ng = _medium_arg(M, T)
+    _check_like("dLdM", dLdM, T, lead=(ng,))
     nx, ny, nz = grid_of(T)
     rep = Report()
     ptr, f32 = _field_ptr(T)
     _on_context(ctx, T)
-    _check(_entry("fold3d_adjoint_ellip", f32)(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(ellip(M, T)), ptr,
-                                               C.c_void_p(W.data_ptr()), C.c_void_p(dLdT.data_ptr()),
-                                               C.c_void_p(lam.data_ptr()), C.c_void_p(dLdM.data_ptr()),
-                                               int(max_sweeps), float(tol), C.c_void_p(stream) if stream else None,
-                                               C.byref(rep)))
+    fn = lib().fold3d_adjoint_tti if kind == "tti" else _entry("fold3d_adjoint_ellip", f32)
+    _check(fn(ctx._h, C.byref(grid(nx, ny, nz, h)), C.byref(e), ptr, C.c_void_p(W.data_ptr()),
+              C.c_void_p(dLdT.data_ptr()), C.c_void_p(lam.data_ptr()), C.c_void_p(dLdM.data_ptr()), int(max_sweeps),
+              float(tol), C.c_void_p(stream) if stream else None, C.byref(rep)))
     return rep
 
 
@@ -464,12 +529,15 @@ def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream
     reports."""
     n = len(fields)
     _same_length(fields=fields, hs=hs, media=media, **({} if winners is None else {"winners": winners}))
-    arr = (Instance * n)()
+    tti_batch = n > 0 and is_tti(media[0])
+    if any(is_tti(M) != tti_batch for M in media):
+        raise ValueError("a batch's media are all metric arrays or all parameter arrays")
+    arr = ((TtiInstance if tti_batch else Instance) * n)()
     kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
-        arr[i].medium = ellip(M, T)
+        arr[i].medium = _medium_arg(M, T)[0]
         arr[i].T, f32 = _field_ptr(T)
         _on_context(ctx, T, "fields[%d]" % i)
         kinds.add(f32)
@@ -479,8 +547,8 @@ def solve_batch(ctx: "Context", fields, hs, media, o: Opts | None = None, stream
     if len(kinds) > 1:
         raise ValueError("a batch is all float64 or all float32")
     reps = (Report * n)()
-    _check(_entry("fold3d_solve_batch", kinds.pop())(ctx._h, n, arr, C.byref(o or opts()),
-                                                     C.c_void_p(stream) if stream else None, reps))
+    fn = lib().fold3d_solve_batch_tti if tti_batch else _entry("fold3d_solve_batch", kinds.pop())
+    _check(fn(ctx._h, n, arr, C.byref(o or opts()), C.c_void_p(stream) if stream else None, reps))
     return list(reps)
 
 
@@ -492,29 +560,35 @@ def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, m
     Returns the per-instance reports."""
     n = len(fields)
     _same_length(fields=fields, hs=hs, media=media, winners=winners, dLdT=dLdT, lam=lam, dLdM=dLdM)
-    arr = (AdjInstance * n)()
+    tti_batch = n > 0 and is_tti(media[0])
+    if any(is_tti(M) != tti_batch for M in media):
+        raise ValueError("a batch's media are all metric arrays or all parameter arrays")
+    arr = ((TtiAdjInstance if tti_batch else AdjInstance) * n)()
     kinds = set()
     for i, (T, h, M) in enumerate(zip(fields, hs, media)):
         _check_like("winners[%d]" % i, winners[i], T, 1)
         _check_like("dLdT[%d]" % i, dLdT[i], T)
         _check_like("lam[%d]" % i, lam[i], T)
-        _check_like("dLdM[%d]" % i, dLdM[i], T, lead=(6,))
+        _check_like("dLdM[%d]" % i, dLdM[i], T, lead=(4 if tti_batch else 6,))
         nx, ny, nz = grid_of(T)
         arr[i].grid = grid(nx, ny, nz, h)
-        arr[i].medium = ellip(M, T)
+        arr[i].medium = _medium_arg(M, T)[0]
         arr[i].T, f32 = _field_ptr(T)
         _on_context(ctx, T, "fields[%d]" % i)
         kinds.add(f32)
         arr[i].winners = winners[i].data_ptr()
         arr[i].dLdT = dLdT[i].data_ptr()
         arr[i].lambda_ = lam[i].data_ptr()
-        arr[i].dLdM = dLdM[i].data_ptr()
+        if tti_batch:
+            arr[i].dLdP = dLdM[i].data_ptr()
+        else:
+            arr[i].dLdM = dLdM[i].data_ptr()
     if len(kinds) > 1:
         raise ValueError("a batch is all float64 or all float32")
     reps = (Report * n)()
-    _check(_entry("fold3d_adjoint_batch", kinds.pop())(ctx._h, n, arr, int(max_sweeps), float(tol),
-                                                       int(bool(accumulate)), C.c_void_p(stream) if stream else None,
-                                                       reps))
+    fn = lib().fold3d_adjoint_batch_tti if tti_batch else _entry("fold3d_adjoint_batch", kinds.pop())
+    _check(fn(ctx._h, n, arr, int(max_sweeps), float(tol), int(bool(accumulate)),
+              C.c_void_p(stream) if stream else None, reps))
     return list(reps)
 
 

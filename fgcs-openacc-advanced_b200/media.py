@@ -6,7 +6,9 @@ here from a seed.  A medium is the per-cell metric M = a I + b n n^T of a
 tilted elliptical cell (a = 1/(Vz^2 (1 + 2 eps)), b = 1/Vz^2 - a, n the
 symmetry axis), returned as six float32 arrays (xx, xy, xz, yy, yz, zz in the
 i, j, k axes) in the field layout, shape (nz+2, ny+2, nx+2), ghost layer
-copied from the nearest interior cell.
+copied from the nearest interior cell; or as the FP64 parameter medium
+(slowness, eps and the axis's x and y components, four float64 arrays) from
+which the solver forms M per cell (params_from, heterogeneous_tti_params).
 
 heterogeneous_tti() follows the construction of the 512^3 configuration:
 Vz = 1500 + 0.8 * depth (m), times 1 + the sum of 16 Gaussian anomalies of
@@ -33,6 +35,41 @@ def metric_from(vz, eps, n_axis):
     b = 1.0 / (vz * vz) - a
     comps = (a + b * nx * nx, b * nx * ny, b * nx * nz, a + b * ny * ny, b * ny * nz, a + b * nz * nz)
     return [c.to(torch.float32) for c in comps]
+
+
+def params_from(vz, eps, n_axis):
+    """The FP64 parameter medium (fold3d_tti) of a tilted elliptical cell:
+    slowness s = 1/vz, eps, and the x, y components of the unit axis, the
+    axis flipped where needed so that its z component is >= 0 (n and -n are
+    the same axis).  Four float64 tensors."""
+    nx, ny, nz = (a.to(torch.float64) for a in n_axis)
+    nn = torch.sqrt(nx * nx + ny * ny + nz * nz)
+    sg = torch.where(nz < 0, -1.0, 1.0).to(torch.float64)
+    return [(1.0 / vz.to(torch.float64)).contiguous(), eps.to(torch.float64).contiguous(),
+            (sg * nx / nn).contiguous(), (sg * ny / nn).contiguous()]
+
+
+def homogeneous_tti(nx, ny, nz, vz, eps, tilt_deg, azimuth_deg, device="cpu"):
+    """homogeneous_ellip() as the FP64 parameter medium (four arrays)."""
+    th, ph = math.radians(tilt_deg), math.radians(azimuth_deg)
+    shape = (nz + 2, ny + 2, nx + 2)
+    f = lambda v: torch.full(shape, float(v), dtype=torch.float64, device=device)
+    return params_from(f(vz), f(eps), (f(math.sin(th) * math.cos(ph)), f(math.sin(th) * math.sin(ph)),
+                                       f(math.cos(th))))
+
+
+def heterogeneous_tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
+    """The seeded heterogeneous medium of heterogeneous_tti() as the FP64
+    parameter medium (four float64 arrays, field layout, ghosts copied).
+    The construction runs in float64; each parameter array is padded as soon
+    as it is formed."""
+    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=torch.float64)
+    out = []
+    P = params_from(vz, eps, axis)
+    del vz, eps, axis
+    while P:
+        out.append(_pad(P.pop(0)))
+    return out
 
 
 def _pad(t):

@@ -5,8 +5,10 @@ fold3d_adjoint_ellip).
 
 EllipSolve.apply(T0, h, max_sweeps, tol, adj_tol, *M) returns the converged
 field for the initial field T0 (a point source; float64, or float32 for the
-float32 build) and a metric M (six CUDA tensors, xx xy xz yy yz zz, field
-layout; the solver stores it as float32).  tol stops the forward sweeps (max |dT| <= tol), adj_tol the
+float32 build) and a medium M in the field layout: either six CUDA tensors of
+the metric, xx xy xz yy yz zz (the solver stores them as float32), or four
+float64 CUDA tensors of the FP64 parameter medium, slowness, eps and the
+axis's x and y components (fold3d_*_tti; gradients with respect to them).  tol stops the forward sweeps (max |dT| <= tol), adj_tol the
 backward ones (fold3d_adjoint_ellip's tol).
 Its backward pass returns dL/dM in float64, so torch carries the gradient on
 to whatever produced M (slowness, epsilon and axis through
@@ -45,10 +47,19 @@ def context(device=None) -> f3d.Context:
     return _ctx[dev]
 
 
+def _stored(M):
+    """The medium as the library reads it: four FP64 parameter arrays (s,
+    eps, nx, ny; fold3d_*_tti) as they are, or six metric arrays rounded to
+    float32 (fold3d_*_ellip)."""
+    if f3d.is_tti(M):
+        return [m.detach().to(torch.float64).contiguous() for m in M]
+    return [m.detach().to(torch.float32).contiguous() for m in M]
+
+
 class EllipSolve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, T0, h, max_sweeps, tol, adj_tol, *M):
-        M32 = [m.detach().to(torch.float32).contiguous() for m in M]
+        M32 = _stored(M)
         T = T0.detach().clone()
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         ctx.mdtypes = [m.dtype for m in M]
@@ -64,10 +75,11 @@ class EllipSolve(torch.autograd.Function):
     def backward(ctx, gT):
         T, W, *M32 = ctx.saved_tensors
         lam = torch.empty_like(T)
-        dLdM = torch.empty((6,) + tuple(T.shape), dtype=T.dtype, device=T.device)
+        ng = len(M32)
+        dLdM = torch.empty((ng,) + tuple(T.shape), dtype=T.dtype, device=T.device)
         _note("adjoint", f3d.adjoint_ellip(context(T.device.index), T, ctx.h, M32, W, gT.to(T.dtype).contiguous(),
                                            lam, dLdM, tol=ctx.adj_tol))
-        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(6))
+        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(ng))
 
 
 def solve(T0, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):
@@ -82,7 +94,7 @@ class EllipSolveBatch(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, T0s, h, max_sweeps, tol, adj_tol, *M):
-        M32 = [m.detach().to(torch.float32).contiguous() for m in M]
+        M32 = _stored(M)
         T = T0s.detach().clone().contiguous()
         W = torch.empty(T.shape, dtype=torch.uint8, device=T.device)
         S = T.shape[0]
@@ -103,13 +115,14 @@ class EllipSolveBatch(torch.autograd.Function):
         S = T.shape[0]
         gT = gT.to(T.dtype).contiguous()
         lam = torch.empty_like(T)
-        dLdM = torch.zeros((6,) + tuple(T.shape[1:]), dtype=T.dtype, device=T.device)
+        ng = len(M32)
+        dLdM = torch.zeros((ng,) + tuple(T.shape[1:]), dtype=T.dtype, device=T.device)
         reps = f3d.adjoint_batch(context(T.device.index), [T[s] for s in range(S)], [ctx.h] * S, [M32] * S,
                                  [W[s] for s in range(S)], [gT[s] for s in range(S)], [lam[s] for s in range(S)],
                                  [dLdM] * S, tol=ctx.adj_tol, accumulate=True)
         for r in reps:
             _note("adjoint_batch", r)
-        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(6))
+        return (None, None, None, None, None) + tuple(dLdM[m].to(ctx.mdtypes[m]) for m in range(ng))
 
 
 def solve_batch(T0s, h, M, max_sweeps=1000, tol=0.0, adj_tol=0.0):

@@ -275,6 +275,52 @@ int fold3d_solve_batch_f32(fold3d_ctx *ctx, int n, const fold3d_instance_f32 *in
 int fold3d_adjoint_batch_f32(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance_f32 *inst, int max_sweeps,
                              double tol, int accumulate, void *stream, fold3d_report *reps);
 
+/* The tilted elliptical medium given by its FP64 parameters (no counterpart
+ * in the reference).  Four double arrays in the field layout: slowness
+ * s = 1/Vz, Thomsen epsilon, and the x and y components of the unit symmetry
+ * axis n (its z component is sqrt(1 - nx^2 - ny^2) >= 0; n and -n are the
+ * same axis).  The kernels form M = a I + b n n^T with a = s^2/(1 + 2 eps),
+ * b = s^2 - a per cell in FP64, so nothing is rounded to float.  Fields are
+ * float64; the solver, winner records, batches and the adjoint are those of
+ * the six-array medium above.  32 bytes of medium per cell (1280^3: 67 GB). */
+typedef struct {
+    const double *s, *eps, *nx, *ny;
+} fold3d_tti;
+
+typedef struct {
+    fold3d_grid grid;
+    fold3d_tti medium;
+    double *T;
+    unsigned char *winners;  /* or NULL */
+} fold3d_tti_instance;
+
+typedef struct {
+    fold3d_grid grid;
+    fold3d_tti medium;
+    const double *T;
+    const unsigned char *winners;
+    const double *dLdT;
+    double *lambda;
+    double *dLdP;  /* 4 x cells: dL/ds, dL/deps, dL/dnx, dL/dny */
+} fold3d_tti_adjoint_instance;
+
+int fold3d_solve_tti(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_tti *m, double *T_dev,
+                     const fold3d_opts *o, void *stream, fold3d_report *rep);
+int fold3d_solve_tti_record(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_tti *m, double *T_dev,
+                            unsigned char *winners_dev, const fold3d_opts *o, void *stream,
+                            fold3d_report *rep);
+/* As fold3d_adjoint_ellip, but the gradient is with respect to the medium's
+ * parameters: dLdP holds four arrays (dL/ds, dL/deps, dL/dnx, dL/dny; the
+ * axis components at fixed unit length, nz following them; where nz = 0 only
+ * the direct terms). */
+int fold3d_adjoint_tti(fold3d_ctx *ctx, const fold3d_grid *g, const fold3d_tti *m, const double *T_dev,
+                       const unsigned char *winners_dev, const double *dLdT_dev, double *lambda_dev,
+                       double *dLdP_dev, int max_sweeps, double tol, void *stream, fold3d_report *rep);
+int fold3d_solve_batch_tti(fold3d_ctx *ctx, int n, const fold3d_tti_instance *inst, const fold3d_opts *o,
+                           void *stream, fold3d_report *reps);
+int fold3d_adjoint_batch_tti(fold3d_ctx *ctx, int n, const fold3d_tti_adjoint_instance *inst, int max_sweeps,
+                             double tol, int accumulate, void *stream, fold3d_report *reps);
+
 /* Implicit-surface source initialisation of a host field (the reference's
  * ImplicitInitialiser, Fold3dPMM.c:129-389, with run-time sizes and medium).
  * Uses all host cores. */

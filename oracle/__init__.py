@@ -91,6 +91,11 @@ class Oracle:
         L.orc_ell_adjoint_rec.argtypes = [_ptr, C.POINTER(C.c_void_p), _ptr, _int, _int, _int, _dbl, _dbl, _dbl, _ptr,
                                           _ptr, _ptr]
         L.orc_ell_adjoint_rec.restype = C.c_long
+        L.orc_tti_metric.argtypes = [_ptr, _ptr, _ptr, _ptr, C.c_int64, C.POINTER(C.c_void_p)]
+        L.orc_ell_solve_rec_d.argtypes = list(L.orc_ell_solve_rec.argtypes)
+        L.orc_ell_solve_rec_d.restype = _int
+        L.orc_ell_adjoint_rec_d.argtypes = list(L.orc_ell_adjoint_rec.argtypes)
+        L.orc_ell_adjoint_rec_d.restype = C.c_long
         self.L = L
 
     @staticmethod
@@ -174,11 +179,70 @@ class Oracle:
                                         r.ctypes.data_as(_ptr), lam.ctypes.data_as(_ptr), g.ctypes.data_as(_ptr))
         return lam, g, nc
 
+    def tti_metric(self, P):
+        """The six float64 metric arrays (xx xy xz yy yz zz) of the FP64
+        parameter medium P = (s, eps, nx, ny), formed as the GPU kernels do."""
+        P = [np.ascontiguousarray(a, dtype=np.float64) for a in P]
+        out = [np.empty_like(P[0]) for _ in range(6)]
+        ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in out))
+        self.L.orc_tti_metric(*(_p(a) for a in P), P[0].size, ptrs)
+        return out
+
+    def tti_solve_rec(self, T, P, h, nsweeps, tol=-1.0):
+        """The FP64 parameter medium P = (s, eps, nx, ny) (field layout), in
+        place: (sweeps, last change, winner record)."""
+        Md = self.tti_metric(P)
+        ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in Md))
+        W = np.full(T.shape, 0xFF, dtype=np.uint8)
+        d = _dbl(0.0)
+        s = self.L.orc_ell_solve_rec_d(_p(T), ptrs, W.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2],
+                                       nsweeps, tol, C.byref(d))
+        if s < 0:
+            raise MemoryError("orc_ell_solve_rec_d failed")
+        return s, d.value, W
+
+    def tti_adjoint(self, T, P, h, W, r):
+        """FP64 adjoint of the parameter medium: (lambda, dL/dP (4, ...) with
+        respect to s, eps, nx, ny, number of non-causal weights).  The chain
+        from the metric entries to the parameters is the one the GPU gradient
+        kernel applies."""
+        Md = self.tti_metric(P)
+        ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in Md))
+        lam = np.zeros_like(T)
+        g = np.zeros((6,) + T.shape)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        Wc = np.ascontiguousarray(W, dtype=np.uint8)
+        nc = self.L.orc_ell_adjoint_rec_d(_p(T), ptrs, Wc.ctypes.data_as(_ptr), *self._dims(T), h[0], h[1], h[2],
+                                          r.ctypes.data_as(_ptr), lam.ctypes.data_as(_ptr), g.ctypes.data_as(_ptr))
+        return lam, tti_param_gradient(P, g), nc
+
     def fold_from_point(self, F, ax, ay, az, x, y, z) -> float:
         return self.L.orc_fold_from_point(F, ax, ay, az, x, y, z)
 
     def overfull_voxels(self) -> int:
         return self.L.orc_last_overfull()
+
+
+def tti_param_gradient(P, gM):
+    """dL/d(s, eps, nx, ny) from dL/dM (six entries xx xy xz yy yz zz) for
+    M = a I + b n n^T, a = s^2/(1+2 eps), b = s^2 - a, nz = sqrt(1 - nx^2 -
+    ny^2) following nx and ny (where nz = 0 only the direct terms)."""
+    s, eps, nx, ny = (np.asarray(a, dtype=np.float64) for a in P)
+    s2, den = s * s, 1.0 + 2.0 * eps
+    a = s2 / den
+    b = s2 - a
+    nz = np.sqrt(np.maximum((1.0 - nx * nx) - ny * ny, 0.0))
+    g = gM
+    ga = g[0] + g[3] + g[5]
+    gb = g[0] * nx * nx + g[3] * ny * ny + g[5] * nz * nz + g[1] * nx * ny + g[2] * nx * nz + g[4] * ny * nz
+    gnx = 2.0 * b * nx * g[0] + b * ny * g[1] + b * nz * g[2]
+    gny = 2.0 * b * ny * g[3] + b * nx * g[1] + b * nz * g[4]
+    gnz = 2.0 * b * nz * g[5] + b * nx * g[2] + b * ny * g[4]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        gnx = np.where(nz > 0, gnx - gnz * nx / nz, gnx)
+        gny = np.where(nz > 0, gny - gnz * ny / nz, gny)
+    da_ds, da_de = 2.0 * s / den, -2.0 * s2 / (den * den)
+    return np.stack([ga * da_ds + gb * (2.0 * s - da_ds), ga * da_de - gb * da_de, gnx, gny])
 
 
 # The reference driver's sweep order and argument permutations

@@ -670,6 +670,45 @@ static double orc_ell_point(double told, double st, const double nb[8], const or
 #define ORC_NCAND 33
 #define ORC_NOWIN 0xffu
 
+/* The per-cell metric of the FP64 statement: six float arrays (the stored
+ * float32 medium) or six double arrays (formed from the FP64 parameter
+ * medium by orc_tti_metric); entries xx xy xz yy yz zz. */
+typedef struct {
+    const float *const *f;
+    const double *const *d;
+} orc_metric;
+
+static double orc_mget(const orc_metric *M, int k, int64_t t)
+{
+    return M->d ? M->d[k][t] : (double)M->f[k][t];
+}
+
+/* The metric M = a I + b n n^T of the tilted elliptical medium from its FP64
+ * parameters (slowness s, Thomsen eps, axis components nx, ny with
+ * nz = sqrt(max(0, (1 - nx nx) - ny ny))), cell by cell into six double
+ * arrays, in the operation order of the GPU kernels'
+ * ell_metric_from_param. */
+void orc_tti_metric(const double *S, const double *E, const double *NX, const double *NY, int64_t cells,
+                    double *const *out)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cells; ++c) {
+        const double s2 = S[c] * S[c];
+        const double a = s2 / (1.0 + 2.0 * E[c]);
+        const double b = s2 - a;
+        const double nx = NX[c], ny = NY[c];
+        const double q = (1.0 - nx * nx) - ny * ny;
+        const double nz = sqrt(q > 0.0 ? q : 0.0);
+        const double bx = b * nx, by = b * ny, bz = b * nz;
+        out[0][c] = a + bx * nx;
+        out[1][c] = bx * ny;
+        out[2][c] = bx * nz;
+        out[3][c] = a + by * ny;
+        out[4][c] = by * nz;
+        out[5][c] = a + bz * nz;
+    }
+}
+
 /* index of the global metric component (p,q), arrays ordered xx xy xz yy yz zz */
 static int orc_mi(int p, int q)
 {
@@ -680,8 +719,8 @@ static int orc_mi(int p, int q)
 
 /* One plane step of the elliptical medium.  M: six float arrays (xx, xy, xz,
  * yy, yz, zz of the metric in the i, j, k axes) in the field layout. */
-void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
-                       double dy, double dz, int dir, int src)
+static void orc_ell_plane_m(double *T, const orc_metric *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                            double dy, double dz, int dir, int src)
 {
     const orc_grid g = orc_make_grid(nx, ny, nz);
     const orc_dir d = ORC_DIRS[dir];
@@ -702,12 +741,12 @@ void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int n
             const int64_t t = s + d.sg * sn;
             /* local metric M'_pq = s_p s_q M[ax_p][ax_q], scaled by the spacings */
             orc_aq A;
-            A.xx = (double)M[orc_mi(ax[0], ax[0])][t] * hx * hx;
-            A.yy = (double)M[orc_mi(ax[1], ax[1])][t] * hy * hy;
-            A.zz = (double)M[orc_mi(ax[2], ax[2])][t] * hz * hz;
-            A.xy = (double)(sgn[0] * sgn[1]) * (double)M[orc_mi(ax[0], ax[1])][t] * hx * hy;
-            A.xz = (double)(sgn[0] * sgn[2]) * (double)M[orc_mi(ax[0], ax[2])][t] * hx * hz;
-            A.yz = (double)(sgn[1] * sgn[2]) * (double)M[orc_mi(ax[1], ax[2])][t] * hy * hz;
+            A.xx = orc_mget(M, orc_mi(ax[0], ax[0]), t) * hx * hx;
+            A.yy = orc_mget(M, orc_mi(ax[1], ax[1]), t) * hy * hy;
+            A.zz = orc_mget(M, orc_mi(ax[2], ax[2]), t) * hz * hz;
+            A.xy = (double)(sgn[0] * sgn[1]) * orc_mget(M, orc_mi(ax[0], ax[1]), t) * hx * hy;
+            A.xz = (double)(sgn[0] * sgn[2]) * orc_mget(M, orc_mi(ax[0], ax[2]), t) * hx * hz;
+            A.yz = (double)(sgn[1] * sgn[2]) * orc_mget(M, orc_mi(ax[1], ax[2]), t) * hy * hz;
             double nb[8];
             for (int r = 0; r < 8; ++r) nb[r] = fabs(T[s + ORC_RIM[r][0] * sx + ORC_RIM[r][1] * sy]);
             int win;
@@ -718,6 +757,13 @@ void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int n
         }
 }
 
+void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                       double dy, double dz, int dir, int src)
+{
+    const orc_metric m = {M, NULL};
+    orc_ell_plane_m(T, &m, W, nx, ny, nz, dx, dy, dz, dir, src);
+}
+
 void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
                    int dir, int src)
 {
@@ -726,8 +772,8 @@ void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, dou
 
 /* Sweeps of the elliptical medium in the reference's direction order;
  * semantics as orc_solve. */
-int orc_ell_solve_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
-                      double dy, double dz, int nsweeps, double tol, double *last_delta)
+static int orc_ell_solve_m(double *T, const orc_metric *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                           double dy, double dz, int nsweeps, double tol, double *last_delta)
 {
     const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
     const int n[3] = {nx, ny, nz};
@@ -741,9 +787,9 @@ int orc_ell_solve_rec(double *T, const float *const *M, unsigned char *W, int nx
             const orc_dir d = ORC_DIRS[dir];
             const int nn = n[d.nrm];
             if (d.sg > 0)
-                for (int p = 1; p < nn; ++p) orc_ell_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
+                for (int p = 1; p < nn; ++p) orc_ell_plane_m(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
             else
-                for (int p = nn; p > 1; --p) orc_ell_plane_rec(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
+                for (int p = nn; p > 1; --p) orc_ell_plane_m(T, M, W, nx, ny, nz, dx, dy, dz, dir, p);
         }
         ++s;
         delta = 0.0;
@@ -756,6 +802,21 @@ int orc_ell_solve_rec(double *T, const float *const *M, unsigned char *W, int nx
     free(prev);
     if (last_delta) *last_delta = delta;
     return s;
+}
+
+int orc_ell_solve_rec(double *T, const float *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                      double dy, double dz, int nsweeps, double tol, double *last_delta)
+{
+    const orc_metric m = {M, NULL};
+    return orc_ell_solve_m(T, &m, W, nx, ny, nz, dx, dy, dz, nsweeps, tol, last_delta);
+}
+
+/* The same with a double metric (the FP64 parameter medium, orc_tti_metric). */
+int orc_ell_solve_rec_d(double *T, const double *const *M, unsigned char *W, int nx, int ny, int nz, double dx,
+                        double dy, double dz, int nsweeps, double tol, double *last_delta)
+{
+    const orc_metric m = {NULL, M};
+    return orc_ell_solve_m(T, &m, W, nx, ny, nz, dx, dy, dz, nsweeps, tol, last_delta);
 }
 
 int orc_ell_solve(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
@@ -1027,22 +1088,22 @@ static double orc_ell_cand(const orc_aq *A, const double tv[9], int id, int pt[3
     }
 }
 
-static void orc_ell_local(const float *const *M, int64_t t, const orc_dir *d, const double h[3], orc_aq *A,
+static void orc_ell_local(const orc_metric *M, int64_t t, const orc_dir *d, const double h[3], orc_aq *A,
                           double *hx, double *hy, double *hz)
 {
     const int ax[3] = {d->xa, d->ya, d->nrm};
     const int sgn[3] = {d->xs, d->ys, d->sg};
     *hz = h[d->nrm]; *hx = h[d->xa]; *hy = h[d->ya];
-    A->xx = (double)M[orc_mi(ax[0], ax[0])][t] * *hx * *hx;
-    A->yy = (double)M[orc_mi(ax[1], ax[1])][t] * *hy * *hy;
-    A->zz = (double)M[orc_mi(ax[2], ax[2])][t] * *hz * *hz;
-    A->xy = (double)(sgn[0] * sgn[1]) * (double)M[orc_mi(ax[0], ax[1])][t] * *hx * *hy;
-    A->xz = (double)(sgn[0] * sgn[2]) * (double)M[orc_mi(ax[0], ax[2])][t] * *hx * *hz;
-    A->yz = (double)(sgn[1] * sgn[2]) * (double)M[orc_mi(ax[1], ax[2])][t] * *hy * *hz;
+    A->xx = orc_mget(M, orc_mi(ax[0], ax[0]), t) * *hx * *hx;
+    A->yy = orc_mget(M, orc_mi(ax[1], ax[1]), t) * *hy * *hy;
+    A->zz = orc_mget(M, orc_mi(ax[2], ax[2]), t) * *hz * *hz;
+    A->xy = (double)(sgn[0] * sgn[1]) * orc_mget(M, orc_mi(ax[0], ax[1]), t) * *hx * *hy;
+    A->xz = (double)(sgn[0] * sgn[2]) * orc_mget(M, orc_mi(ax[0], ax[2]), t) * *hx * *hz;
+    A->yz = (double)(sgn[1] * sgn[2]) * orc_mget(M, orc_mi(ax[1], ax[2]), t) * *hy * *hz;
 }
 
 /* Winner of interior cell (i,j,k) of a converged field. */
-static void orc_ell_winner_at(const double *T, const float *const *M, const orc_grid *g, const double h[3], int i,
+static void orc_ell_winner_at(const double *T, const orc_metric *M, const orc_grid *g, const double h[3], int i,
                               int j, int k, orc_winner *wn)
 {
     memset(wn, 0, sizeof *wn);
@@ -1119,7 +1180,7 @@ static void orc_ell_winner_at(const double *T, const float *const *M, const orc_
 
 /* Weights and metric derivative of the recorded winner (dir, id) of cell x,
  * evaluated with the final field. */
-static void orc_ell_weights(const double *T, const float *const *M, const orc_grid *g, const double h[3], int64_t x,
+static void orc_ell_weights(const double *T, const orc_metric *M, const orc_grid *g, const double h[3], int64_t x,
                             int dir, int id, orc_winner *wn)
 {
     memset(wn, 0, sizeof *wn);
@@ -1161,9 +1222,10 @@ static int orc_cmp_desc(const void *a, const void *b)
 }
 
 /* Winners of all interior cells: dir/id (-1 if none) and weights, for tests. */
-void orc_ell_winners(const double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
-                     int *dir_out, int *id_out, double *w_out /* 3 per cell */)
+void orc_ell_winners(const double *T, const float *const *Mf, int nx, int ny, int nz, double dx, double dy,
+                     double dz, int *dir_out, int *id_out, double *w_out /* 3 per cell */)
 {
+    const orc_metric mm = {Mf, NULL}, *M = &mm;
     const orc_grid g = orc_make_grid(nx, ny, nz);
     const double h[3] = {dx, dy, dz};
     const size_t cells = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
@@ -1186,8 +1248,8 @@ void orc_ell_winners(const double *T, const float *const *M, int nx, int ny, int
  * layout).  Cells are processed by decreasing time; the return value is the
  * number of winner weights that point to a source point whose time is not
  * smaller (0 for a causal field, for which the order is exact). */
-long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned char *rec, int nx, int ny, int nz,
-                         double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
+static long orc_ell_adjoint_m(const double *T, const orc_metric *M, const unsigned char *rec, int nx, int ny,
+                              int nz, double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
 {
     const orc_grid g = orc_make_grid(nx, ny, nz);
     const double h[3] = {dx, dy, dz};
@@ -1230,6 +1292,22 @@ long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned 
     free(W);
     free(order);
     return noncausal;
+}
+
+long orc_ell_adjoint_rec(const double *T, const float *const *M, const unsigned char *rec, int nx, int ny, int nz,
+                         double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
+{
+    const orc_metric m = {M, NULL};
+    return orc_ell_adjoint_m(T, &m, rec, nx, ny, nz, dx, dy, dz, r, lambda, dLdM);
+}
+
+/* The same with a double metric (the FP64 parameter medium, orc_tti_metric);
+ * dLdM is the gradient with respect to its six entries. */
+long orc_ell_adjoint_rec_d(const double *T, const double *const *M, const unsigned char *rec, int nx, int ny,
+                           int nz, double dx, double dy, double dz, const double *r, double *lambda, double *dLdM)
+{
+    const orc_metric m = {NULL, M};
+    return orc_ell_adjoint_m(T, &m, rec, nx, ny, nz, dx, dy, dz, r, lambda, dLdM);
 }
 
 /* Adjoint with winners found from the converged field (first candidate, in

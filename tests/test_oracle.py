@@ -454,3 +454,79 @@ def test_oracle_float_statement_close_to_double():
     inner = Wf[I]
     assert (inner == 0xFF).sum() == 1 and int(inner[inner != 0xFF].max()) < 6 * 33
     assert (Wf[I] != Wd[I]).mean() < 0.05  # winners differ only where candidates tie within float rounding
+
+
+def test_oracle_tti_metric_matches_float64_formula():
+    """orc_tti_metric (the FP64 parameter medium's metric, in the kernels'
+    operation order) against the same formula evaluated by numpy, and the
+    parameter form of a seeded medium against its six-array form."""
+    import torch
+
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    dims = (9, 7, 8)
+    vz, eps, axis = media.tti_params(*dims, 10.0, seed=6, pad=True)
+    P = [p.numpy() for p in media.params_from(vz, eps, axis)]
+    Md = o.tti_metric(P)
+    s, e, nx, ny = P
+    s2 = s * s
+    a = s2 / (1.0 + 2.0 * e)
+    b = s2 - a
+    nz = np.sqrt(np.maximum((1.0 - nx * nx) - ny * ny, 0.0))
+    want = [a + b * nx * nx, b * nx * ny, b * nx * nz, a + b * ny * ny, b * ny * nz, a + b * nz * nz]
+    for k in range(6):
+        np.testing.assert_allclose(Md[k], want[k], rtol=1e-15, atol=1e-15 * np.abs(want[k]).max())
+    M32 = media.metric_from(vz, eps, axis)
+    for k in range(6):
+        np.testing.assert_allclose(Md[k], M32[k].double().numpy(), rtol=2e-6,
+                                   atol=2e-6 * float(torch.max(torch.abs(M32[k]))))
+
+
+def test_oracle_tti_adjoint_matches_finite_differences():
+    """The FP64 CPU adjoint of the parameter medium, chained to (s, eps, nx,
+    ny), against central differences of the oracle's own solve (relative step
+    1e-6) on a small seeded case: the chain rule the GPU gradient kernel
+    applies, checked without a GPU."""
+    import media
+    from oracle import Oracle
+
+    o = Oracle()
+    dims, h = (11, 9, 10), (10.0,) * 3
+    vz, eps, axis = media.tti_params(*dims, 10.0, seed=8, pad=True)
+    P = [p.numpy().copy() for p in media.params_from(vz, eps, axis)]
+    T0 = o.init_point(*dims, (6, 5, 2))
+    rec = (slice(1, 2), slice(1, -1), slice(1, -1))
+
+    def solve(Px):
+        T = T0.copy()
+        s, d, W = o.tti_solve_rec(T, Px, h, 200, tol=0.0)
+        return T, W
+
+    T, W = solve(P)
+    tobs = T[rec] * 0.97
+    r = np.zeros_like(T)
+    r[rec] = T[rec] - tobs
+    lam, g, nc = o.tti_adjoint(T, P, h, W, r)
+    assert nc == 0
+
+    def loss(Px):
+        Tx, _ = solve(Px)
+        return 0.5 * float(((Tx[rec] - tobs) ** 2).sum())
+
+    rng = np.random.default_rng(2)
+    errs = []
+    for v in range(4):
+        cand = np.argwhere(np.abs(g[v]) >= 1e-3 * np.abs(g[v]).max())
+        for q in rng.choice(len(cand), 4, replace=False):
+            k, j, i = cand[q]
+            base = P[v][k, j, i]
+            step = 1e-6 * max(abs(base), 1e-3)
+            up = [p.copy() for p in P]
+            dn = [p.copy() for p in P]
+            up[v][k, j, i] = base + step
+            dn[v][k, j, i] = base - step
+            fd = (loss(up) - loss(dn)) / (up[v][k, j, i] - dn[v][k, j, i])
+            errs.append(abs(fd - g[v][k, j, i]) / max(abs(fd), abs(g[v][k, j, i])))
+    assert np.median(errs) < 1e-6 and max(errs) < 1e-4, (np.median(errs), max(errs))

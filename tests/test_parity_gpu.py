@@ -214,6 +214,45 @@ def test_compat_rejects_unknown_grid(f3d, cuda):
         L.fold3d_compat_set_grid(0, 0, 0)
 
 
+def test_compat_rejects_pointer_inside_acc_block(f3d, cuda):
+    """A sweep call given a pointer into the middle of an acc_malloc block
+    (no grid size set) is rejected: the grid cannot be inferred from the
+    block, and a field placed there would run past the block's end.  With a
+    grid set, the field must fit between the pointer and the block's end.
+    Nothing is launched in the rejected calls."""
+    L = f3d.lib()
+    nbytes = 10 * 10 * 10 * 8
+    d = L.acc_malloc(nbytes)
+    assert d
+    try:
+        L.function_x_down(C.c_void_p(d + 8 * 100), 1, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+        assert "not at its start" in f3d.last_error()
+        assert L.fold3d_compat_set_grid(8, 8, 8) == f3d.OK
+        L.function_x_down(C.c_void_p(d + 8 * 100), 1, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+        assert "does not fit" in f3d.last_error()
+        L.function_x_down(C.c_void_p(d), 1, *([1.0] * 6), 1.1, 0.4, 0.7, -0.35)
+        assert f3d.last_error() == ""
+    finally:
+        L.fold3d_compat_set_grid(0, 0, 0)
+        L.acc_free(C.c_void_p(d))
+
+
+@pytest.mark.parametrize("bad", ["inf_spacing", "inf_F"])
+def test_solve_rejects_infinite_grid_or_medium(f3d, ctx, cuda, bad):
+    """fold3d_solve and fold3d_solve_noalloc reject an infinite spacing or
+    medium constant with the same code."""
+    T = cuda.from_numpy(f3d.init_point(8, 8, 8, (4, 4, 4))).cuda()
+    L = f3d.lib()
+    inf = float("inf")
+    g = f3d.Grid(8, 8, 8, 1.0, inf, 1.0) if bad == "inf_spacing" else f3d.grid(8, 8, 8, 1.0)
+    m = f3d.Medium(inf, 0, 0, 0) if bad == "inf_F" else f3d.medium()
+    o = f3d.opts(max_sweeps=2, fixed=True)
+    assert L.fold3d_solve(ctx._h, C.byref(g), C.byref(m), C.c_void_p(T.data_ptr()), C.byref(o), None,
+                          None) == f3d.ERR_INVALID
+    assert L.fold3d_solve_noalloc(C.byref(g), C.byref(m), C.c_void_p(T.data_ptr()), C.byref(o), None,
+                                  None) == f3d.ERR_INVALID
+
+
 def test_full_size_planes_512(f3d, orc, ctx, cuda):
     """At the benchmark size (512^3, reference medium and source), the first
     planes of every direction match the oracle bit for bit."""
