@@ -558,9 +558,11 @@ def run_batch(args):
     seq_ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     ibits = lambda t: t.view(torch.int64 if t.element_size() == 8 else torch.int32)
     same = all(torch.equal(ibits(a), ibits(b)) for a, b in zip(batched, T))
+    tuned_rows, tuned_ctas = f3d.batch_get_config(ctx)
+    # one graph per batched solve: the prologue's table kernel, then per sweep six passes and the restage kernel
     nominal, evald, nsame, launches = over_ranks(
         [sum(r.nominal_updates for r in reps), sum(r.evaluated_updates for r in reps), int(same),
-         6 * max(r.sweeps for r in reps) * args.steps], dist, "sum")
+         (7 * max(r.sweeps for r in reps) + 1) * args.steps], dist, "sum")
     smin, = over_ranks([min(r.sweeps for r in reps)], dist, "min")
     smax, = over_ranks([max(r.sweeps for r in reps)], dist, "max")
     cells = sum((d[0] + 2) * (d[1] + 2) * (d[2] + 2) for d in dims)
@@ -590,7 +592,9 @@ def run_batch(args):
         "config": {"workload": "batch of %d solves, dims per axis U[%d,%d] (seed 1), h=10 m, each run to "
                                "max|dT|<=1e-10" % (args.batch, lo, hi), "cells": cells,
                    "sweeps_min_max": [int(smin), int(smax)],
-                   "engine": "wavefront batch", "skip": bool(args.skip),
+                   "engine": "wavefront batch, sweep loop on the device (one CUDA graph)", "skip": bool(args.skip),
+                   "autotuned": {"tile_rows": tuned_rows, "threads_per_cta": 32 * tuned_rows,
+                                 "ctas_per_sm": tuned_ctas},
                    "parallelism": "instances split over %d ranks by cells, no exchange" % world
                    if world > 1 else "single",
                    "instances_per_rank": [len(q) for q in parts]},

@@ -172,7 +172,14 @@ struct fold3d_ctx {
     unsigned *w_counters = nullptr;          // [0] work, [1] status
     unsigned long long *w_evaluated = nullptr;
     unsigned epoch = 0;                      // passes run so far on this context (never decreases)
-    int sms = 0, batch_bps = 0, batch_adj_bps = 0;
+    int sms = 0, batch_adj_bps = 0;
+    int batch_bps[2][9] = {};                // resident batched-pass CTAs per SM, [f32][tile height]
+    int btv = kWaveTV;                       // tile height the batch scratch is laid out for
+    int tune_tv = 0, tune_bps = 0;           // fold3d_batch_set_config (0: autotune)
+    int last_tv = 0, last_bps = 0;           // configuration of the last batched solve
+    std::map<std::vector<long long>, std::pair<int, int>> tuned;  // size mix -> (tile height, CTAs per SM)
+    double *tune_T = nullptr;                // autotuner: copies of a few instances' fields
+    size_t tune_cells = 0;
     int wave_bps[2][2][2] = {};              // [ellip][f32][large plane] resident CTAs per SM
     // batched solves: per-instance scratch and per-direction staging
     std::vector<int> bkey;                   // dims of the instances the scratch is sized for
@@ -195,6 +202,7 @@ struct fold3d_ctx {
     size_t adj_cnt_cap = 0;
     char *b_stage_d = nullptr, *b_stage_h = nullptr;
     size_t b_stage_bytes = 0;
+    char *b_ctl = nullptr;                   // device state of the batched sweep loop (BatchCtl)
 };
 
 namespace {
@@ -278,6 +286,8 @@ void fold3d_destroy(fold3d_ctx *c)
     if (c->adj_off) cudaFree(c->adj_off);
     if (c->b_stage_d) cudaFree(c->b_stage_d);
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
+    if (c->b_ctl) cudaFree(c->b_ctl);
+    if (c->tune_T) cudaFree(c->tune_T);
     if (c->d_maxd) cudaFree(c->d_maxd);
     if (c->h_maxd) cudaFreeHost(c->h_maxd);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -370,12 +380,12 @@ static int solve_planes(fold3d_ctx *c, const fold3d_grid &g, const fold3d_medium
 }
 
 // WAVEFRONT tiles (32 x kWaveTV) per plane of the orientation with normal axis b.
-static void orient_tiles(const fold3d_grid &g, int b, int &ntu, int &ntv)
+static void orient_tiles(const fold3d_grid &g, int b, int &ntu, int &ntv, int tv = kWaveTV)
 {
     const int n[3] = {g.nx, g.ny, g.nz};
     const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
     ntu = (n[ub] + 31) / 32;
-    ntv = (n[vb] + kWaveTV - 1) / kWaveTV;
+    ntv = (n[vb] + tv - 1) / tv;
 }
 
 // Pass numbers travel as (pass << 1) | changed in 32-bit flags.  Far before
@@ -562,7 +572,27 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 static constexpr size_t kStageInst = sizeof(BatchInst) > sizeof(BatchAdjInst) ? sizeof(BatchInst) : sizeof(BatchAdjInst);
 
-static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
+// Device state of the batched sweep loop: total[6], epoch_base, sweep[2],
+// then active[n], sweeps[n] and delta[n].
+static size_t batch_ctl_bytes(int n) { return 64 + align_up((size_t)n * 4, 256) * 2 + (size_t)n * 8; }
+struct BatchCtlMem {
+    unsigned *total, *epoch_base;
+    int *sweep, *active, *sweeps;
+    double *delta;
+};
+static BatchCtlMem batch_ctl_mem(char *base, int n)
+{
+    BatchCtlMem m;
+    m.total = reinterpret_cast<unsigned *>(base);
+    m.epoch_base = m.total + 6;
+    m.sweep = reinterpret_cast<int *>(base + 32);
+    m.active = reinterpret_cast<int *>(base + 64);
+    m.sweeps = reinterpret_cast<int *>(base + 64 + align_up((size_t)n * 4, 256));
+    m.delta = reinterpret_cast<double *>(base + 64 + 2 * align_up((size_t)n * 4, 256));
+    return m;
+}
+
+static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids, int tv = kWaveTV)
 {
     const int n = (int)grids.size();
     std::vector<int> key(3 * (size_t)n);
@@ -571,14 +601,16 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
         key[3 * i + 1] = grids[i].ny;
         key[3 * i + 2] = grids[i].nz;
     }
-    if (c->b_scratch && key == c->bkey) return FOLD3D_OK;
+    if (c->b_scratch && key == c->bkey && tv == c->btv) return FOLD3D_OK;
     if (c->b_scratch) cudaFree(c->b_scratch);
     if (c->b_slots) cudaFree(c->b_slots);
     if (c->b_stage_d) cudaFree(c->b_stage_d);
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
+    if (c->b_ctl) cudaFree(c->b_ctl);
     c->b_scratch = nullptr;
     c->b_slots = nullptr;
     c->b_stage_d = c->b_stage_h = nullptr;
+    c->b_ctl = nullptr;
     c->bkey.clear();
     size_t words = 0;
     int max_steps = 0;
@@ -590,7 +622,7 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
         size_t fw = 0;
         for (int b = 0; b < 3; ++b) {
             int ntu, ntv;
-            orient_tiles(g, b, ntu, ntv);
+            orient_tiles(g, b, ntu, ntv, tv);
             fw = std::max(fw, (size_t)(dims[b] - 1) * ntu * ntv);
             c->b_mod_off[b][i] = words;
             words += (size_t)(dims[b] + 2) * ntu * ntv;
@@ -606,21 +638,24 @@ static int batch_scratch(fold3d_ctx *c, const std::vector<fold3d_grid> &grids)
         return set_errorf(FOLD3D_ERR_NOMEM, "batch scratch: %s", cudaGetErrorString(e));
     if (!c->b_counters && (e = cudaMalloc(&c->b_counters, 2 * sizeof(unsigned))) != cudaSuccess)
         return set_errorf(FOLD3D_ERR_NOMEM, "batch scratch: %s", cudaGetErrorString(e));
-    // per direction: inst[n], step_off[max_steps+1], step_k[max_steps], tile_pre[n+1]
+    // per direction: inst[n], step_off[max_steps+1], step_k[max_steps], tile_pre[n+1], then the
+    // device loop's order[n], steps[n], tiles[n] and act[n]
     const size_t per = align_up((size_t)n * kStageInst, 256) + align_up((max_steps + 1) * 8, 256) +
-                       align_up((size_t)max_steps * 4, 256) + align_up(((size_t)n + 1) * 8, 256);
+                       align_up((size_t)max_steps * 4, 256) + align_up(((size_t)n + 1) * 8, 256) +
+                       2 * align_up((size_t)n * 4, 256) + align_up((size_t)n * 8, 256) + align_up((size_t)n * 4, 256);
     c->b_stage_bytes = per;
     if ((e = cudaMalloc(&c->b_stage_d, 6 * per)) != cudaSuccess ||
-        (e = cudaMallocHost(&c->b_stage_h, 6 * per)) != cudaSuccess)
+        (e = cudaMallocHost(&c->b_stage_h, 6 * per)) != cudaSuccess ||
+        (e = cudaMalloc(&c->b_ctl, batch_ctl_bytes(n))) != cudaSuccess)
         return set_errorf(FOLD3D_ERR_NOMEM, "batch staging: %s", cudaGetErrorString(e));
     if (!c->sms) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    if (!c->batch_bps) c->batch_bps = batch_blocks_per_sm(false);
     if (!c->batch_adj_bps) c->batch_adj_bps = batch_adj_blocks_per_sm(false);
     c->bkey = key;
+    c->btv = tv;
     return FOLD3D_OK;
 }
 
@@ -631,6 +666,9 @@ struct BatchStage {
     long long *step_off;
     int *step_k;
     long long *tile_pre;
+    int *order, *steps;
+    long long *tiles;
+    int *act;
 };
 static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
 {
@@ -645,6 +683,14 @@ static BatchStage batch_stage(fold3d_ctx *c, char *base, int dir, int n)
     s.step_k = reinterpret_cast<int *>(p);
     p += align_up((size_t)max_steps * 4, 256);
     s.tile_pre = reinterpret_cast<long long *>(p);
+    p += align_up(((size_t)n + 1) * 8, 256);
+    s.order = reinterpret_cast<int *>(p);
+    p += align_up((size_t)n * 4, 256);
+    s.steps = reinterpret_cast<int *>(p);
+    p += align_up((size_t)n * 4, 256);
+    s.tiles = reinterpret_cast<long long *>(p);
+    p += align_up((size_t)n * 8, 256);
+    s.act = reinterpret_cast<int *>(p);
     return s;
 }
 
@@ -684,139 +730,189 @@ struct AdjInst {
     void *dLdM;
 };
 
-static int solve_batch(fold3d_ctx *c, int n, const SolveInst *in, bool f32, const fold3d_opts &o, cudaStream_t s,
-                       fold3d_report *reps)
+// Batched solve: the whole sweep loop runs on the device as one CUDA graph.
+// Its prologue builds the item tables; a conditional while-node repeats the
+// body -- the six directions' batched passes, then the restage kernel, which
+// folds each instance's change into its state, drops converged instances,
+// rebuilds the tables and decides whether to loop again -- so the host
+// neither waits nor re-stages between sweeps.  The host only writes the
+// per-direction instance tables once (every instance, in the direction's
+// order) and reads the per-instance results at the end.  tv, bps: tile
+// height and resident CTAs per SM.
+static int solve_batch_cfg(fold3d_ctx *c, int n, const SolveInst *in, bool f32, const fold3d_opts &o, cudaStream_t s,
+                           fold3d_report *reps, int tv, int bps)
 {
     int rc = reserve_passes(c, 6u * (unsigned)std::min(o.max_sweeps, 1 << 20) + 12u);
     if (rc) return rc;
     std::vector<fold3d_grid> grids(n);
     for (int i = 0; i < n; ++i) grids[i] = in[i].grid;
-    if ((rc = batch_scratch(c, grids))) return rc;
+    if ((rc = batch_scratch(c, grids, tv))) return rc;
     cudaError_t e;
-    std::vector<char> active(n, 1);
-    std::vector<int> sweeps(n, 0);
-    std::vector<double> delta(n, 0.0);
-    std::vector<unsigned long long> slots(2 * (size_t)n);
-    if ((e = cudaMemsetAsync(c->b_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess ||
-        (e = cudaMemsetAsync(c->b_slots + n, 0, (size_t)n * 8, s)) != cudaSuccess)
-        return cuda_error(e, "cudaMemsetAsync");
     const unsigned e0 = c->epoch + 1;
     const unsigned skip_from = o.skip ? e0 + 6 : 0xffffffffu;
     int max_steps = 0;
     for (int v : c->bkey) max_steps = std::max(max_steps, v - 1);
+    const BatchCtlMem cm = batch_ctl_mem(c->b_ctl, n);
     BatchArgs args[6];
-    // (re)build the six directions' staging for the current active set
-    auto stage = [&]() -> int {
-        for (int dir = 0; dir < 6; ++dir) {
-            const DirSpec &d = kDirs[dir];
-            BatchStage h = batch_stage(c, c->b_stage_h, dir, n);
-            BatchStage dv = batch_stage(c, c->b_stage_d, dir, n);
-            std::vector<int> order;
-            for (int i = 0; i < n; ++i)
-                if (active[i]) order.push_back(i);
-            auto steps_of = [&](int i) {
-                const int dims[3] = {in[i].grid.nx, in[i].grid.ny, in[i].grid.nz};
-                return dims[d.nrm] - 1;
-            };
-            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return steps_of(x) > steps_of(y); });
-            const int k = (int)order.size();
-            h.tile_pre[0] = 0;
-            for (int q = 0; q < k; ++q) {
-                const int i = order[q];
-                const fold3d_grid &g = in[i].grid;
-                BatchInst &bi = static_cast<BatchInst *>(h.inst)[q];
-                memset(&bi, 0, sizeof bi);
-                WaveArgs &a = bi.a;
-                a.pg = make_geom(g, dir);
-                a.nrm = d.nrm;
-                a.ua = (d.nrm == 0) ? 1 : 0;
-                a.va = (d.nrm == 2) ? 1 : 2;
-                a.sg = d.sg;
-                orient_tiles(g, d.nrm, a.ntu, a.ntv);
-                a.steps = pass_count(a.pg);
-                a.first_src = pass_first(a.pg, dir);
-                a.timeout_ns = 4000000000ull;
-                a.flags = c->b_scratch + c->b_flag_off[i];
-                for (int b = 0; b < 3; ++b) {
-                    int ntu, ntv;
-                    orient_tiles(g, b, ntu, ntv);
-                    a.mod[b] = c->b_scratch + c->b_mod_off[b][i];
-                    a.mod_ntu[b] = ntu;
-                    a.mod_ntiles[b] = ntu * ntv;
-                }
-                a.work = c->b_counters;
-                a.status = c->b_counters + 1;
-                a.maxd = c->b_slots + i;
-                a.evaluated = c->b_slots + n + i;
-                a.dir = dir;
-                a.winners = in[i].winners;
-                bi.p = ellip_param(g, in[i].medium, dir);
-                bi.T = in[i].T;
-                h.tile_pre[q + 1] = h.tile_pre[q] + (long long)a.ntu * a.ntv;
+    BatchCtl ctl;
+    memset(&ctl, 0, sizeof ctl);
+    long long max_total = 0;
+    for (int dir = 0; dir < 6; ++dir) {
+        const DirSpec &d = kDirs[dir];
+        BatchStage h = batch_stage(c, c->b_stage_h, dir, n);
+        BatchStage dv = batch_stage(c, c->b_stage_d, dir, n);
+        std::vector<int> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        auto steps_of = [&](int i) {
+            const int dims[3] = {in[i].grid.nx, in[i].grid.ny, in[i].grid.nz};
+            return dims[d.nrm] - 1;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return steps_of(x) > steps_of(y); });
+        long long items = 0;
+        for (int q = 0; q < n; ++q) {
+            const int i = order[q];
+            const fold3d_grid &g = in[i].grid;
+            BatchInst &bi = static_cast<BatchInst *>(h.inst)[q];
+            memset(&bi, 0, sizeof bi);
+            WaveArgs &a = bi.a;
+            a.pg = make_geom(g, dir);
+            a.nrm = d.nrm;
+            a.ua = (d.nrm == 0) ? 1 : 0;
+            a.va = (d.nrm == 2) ? 1 : 2;
+            a.sg = d.sg;
+            orient_tiles(g, d.nrm, a.ntu, a.ntv, tv);
+            a.steps = pass_count(a.pg);
+            a.first_src = pass_first(a.pg, dir);
+            a.timeout_ns = 4000000000ull;
+            a.flags = c->b_scratch + c->b_flag_off[i];
+            for (int b = 0; b < 3; ++b) {
+                int ntu, ntv;
+                orient_tiles(g, b, ntu, ntv, tv);
+                a.mod[b] = c->b_scratch + c->b_mod_off[b][i];
+                a.mod_ntu[b] = ntu;
+                a.mod_ntiles[b] = ntu * ntv;
             }
-            h.step_off[0] = 0;
-            for (int p = 0; p < max_steps; ++p) {
-                int kk = 0;
-                while (kk < k && steps_of(order[kk]) > p) ++kk;
-                h.step_k[p] = kk;
-                h.step_off[p + 1] = h.step_off[p] + h.tile_pre[kk];
-            }
-            if (h.step_off[max_steps] >= (1ll << 31)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
-            args[dir].inst = static_cast<const BatchInst *>(dv.inst);
-            args[dir].step_off = dv.step_off;
-            args[dir].step_k = dv.step_k;
-            args[dir].tile_pre = dv.tile_pre;
-            args[dir].max_steps = max_steps;
-            args[dir].total = (unsigned)h.step_off[max_steps];
-            args[dir].work = c->b_counters;
-            args[dir].status = c->b_counters + 1;
-            args[dir].skip_from = skip_from;
+            a.work = c->b_counters;
+            a.status = c->b_counters + 1;
+            a.maxd = c->b_slots + i;
+            a.evaluated = c->b_slots + n + i;
+            a.dir = dir;
+            a.winners = in[i].winners;
+            bi.p = ellip_param(g, in[i].medium, dir);
+            bi.T = in[i].T;
+            h.order[q] = i;
+            h.steps[q] = a.steps;
+            h.tiles[q] = (long long)a.ntu * a.ntv;
+            items += h.tiles[q] * a.steps;
         }
-        cudaError_t ce = cudaMemcpyAsync(c->b_stage_d, c->b_stage_h, 6 * c->b_stage_bytes, cudaMemcpyHostToDevice, s);
-        return ce == cudaSuccess ? FOLD3D_OK : cuda_error(ce, "batch staging upload");
-    };
-    if ((rc = stage())) return rc;
-    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
-    int sweep = 0, left = n;
-    unsigned hstat[2] = {0, 0};
-    while (sweep < o.max_sweeps && left > 0) {
-        if ((e = cudaMemsetAsync(c->b_slots, 0, (size_t)n * 8, s)) != cudaSuccess) return cuda_error(e, "memset");
-        for (int dir = 0; dir < 6; ++dir) {
-            args[dir].epoch = ++c->epoch;
-            const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_bps);
-            if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
-                return cuda_error(e, "memset");
-            if (grid > 0 && (e = launch_batch_pass(args[dir], f32, grid, s)) != cudaSuccess)
-                return cuda_error(e, "batch pass");
-        }
-        ++sweep;
-        for (int i = 0; i < n; ++i)
-            if (active[i]) ++sweeps[i];
-        if (!o.fixed || sweep == o.max_sweeps) {
-            if ((e = cudaMemcpyAsync(slots.data(), c->b_slots, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) !=
-                    cudaSuccess ||
-                (e = cudaMemcpyAsync(hstat, c->b_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-                return cuda_error(e, "cudaMemcpyAsync");
-            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "sweep");
-            if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "batch: a dependency wait gave up");
-            bool changed = false;
-            for (int i = 0; i < n; ++i) {
-                if (!active[i]) continue;
-                memcpy(&delta[i], &slots[i], 8);
-                if (!o.fixed && delta[i] <= o.tol) {
-                    active[i] = 0;
-                    --left;
-                    changed = true;
-                }
-            }
-            if (changed && left > 0 && (rc = stage())) return rc;
-        }
+        if (items >= (1ll << 31)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
+        max_total = std::max(max_total, items);
+        BatchDirTables &t = ctl.dir[dir];
+        t.order = dv.order;
+        t.steps = dv.steps;
+        t.tiles = dv.tiles;
+        t.act = dv.act;
+        t.step_off = dv.step_off;
+        t.step_k = dv.step_k;
+        t.tile_pre = dv.tile_pre;
+        args[dir].inst = static_cast<const BatchInst *>(dv.inst);
+        args[dir].act = dv.act;
+        args[dir].step_off = dv.step_off;
+        args[dir].step_k = dv.step_k;
+        args[dir].tile_pre = dv.tile_pre;
+        args[dir].total = cm.total + dir;
+        args[dir].epoch_base = cm.epoch_base;
+        args[dir].max_steps = max_steps;
+        args[dir].dir = dir;
+        args[dir].work = c->b_counters;
+        args[dir].status = c->b_counters + 1;
+        args[dir].skip_from = skip_from;
     }
-    if ((e = cudaEventRecord(c->ev1, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
-    if ((e = cudaMemcpyAsync(slots.data() + n, c->b_slots + n, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) !=
+    ctl.n = n;
+    ctl.max_steps = max_steps;
+    ctl.fixed = o.fixed ? 1 : 0;
+    ctl.max_sweeps = o.max_sweeps;
+    ctl.tol = o.tol;
+    ctl.epoch0 = e0 - 1;
+    ctl.total = cm.total;
+    ctl.epoch_base = cm.epoch_base;
+    ctl.sweep = cm.sweep;
+    ctl.active = cm.active;
+    ctl.sweeps = cm.sweeps;
+    ctl.delta = cm.delta;
+    ctl.maxd = c->b_slots;
+    ctl.status = c->b_counters + 1;
+    // a grid as large as the biggest pass can use (instances drop out later)
+    const int grid = (int)std::min<long long>(max_total, (long long)c->sms * bps);
+
+    // the graph: prologue (tables), then while (more) { six passes; restage }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto fail = [&](cudaError_t err, const char *what) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_error(err, what);
+    };
+    if ((e = cudaMemcpyAsync(c->b_stage_d, c->b_stage_h, 6 * c->b_stage_bytes, cudaMemcpyHostToDevice, s)) !=
             cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_counters, 0, 2 * sizeof(unsigned), s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(c->b_slots + n, 0, (size_t)n * 8, s)) != cudaSuccess)
+        return cuda_error(e, "batch setup");
+    if ((e = cudaGraphCreate(&graph, 0)) != cudaSuccess) return cuda_error(e, "cudaGraphCreate");
+    cudaGraphConditionalHandle cond;
+    if ((e = cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+        return fail(e, "cudaGraphConditionalHandleCreate");
+    ctl.cond = (unsigned long long)cond;
+    cudaStream_t cs = c->stream;  // the context's own stream captures; the graph runs on s
+    cudaError_t le = cudaSuccess;
+    if ((e = cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return fail(e, "cudaStreamBeginCaptureToGraph");
+    le = launch_batch_restage(ctl, true, cs);
+    if ((e = cudaStreamEndCapture(cs, &graph)) != cudaSuccess || le != cudaSuccess)
+        return fail(le != cudaSuccess ? le : e, "capturing the batch prologue");
+    cudaGraphNode_t pro = nullptr;
+    size_t nn = 1;
+    if ((e = cudaGraphGetNodes(graph, &pro, &nn)) != cudaSuccess || nn != 1)
+        return fail(e != cudaSuccess ? e : cudaErrorUnknown, "batch prologue");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop = nullptr;
+    if ((e = cudaGraphAddNode(&loop, graph, &pro, 1, &cp)) != cudaSuccess) return fail(e, "conditional node");
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+        cudaSuccess)
+        return fail(e, "cudaStreamBeginCaptureToGraph");
+    for (int dir = 0; dir < 6 && le == cudaSuccess; ++dir) {
+        le = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), cs);
+        if (le == cudaSuccess && grid > 0) le = launch_batch_pass(args[dir], f32, tv, grid, cs);
+    }
+    if (le == cudaSuccess) le = launch_batch_restage(ctl, false, cs);
+    if ((e = cudaStreamEndCapture(cs, &body)) != cudaSuccess || le != cudaSuccess)
+        return fail(le != cudaSuccess ? le : e, "capturing the batch sweep");
+    if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return fail(e, "cudaGraphInstantiate");
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess || (e = cudaGraphLaunch(exec, s)) != cudaSuccess ||
+        (e = cudaEventRecord(c->ev1, s)) != cudaSuccess)
+        return fail(e, "batch graph");
+    std::vector<unsigned long long> evald(n);
+    std::vector<int> sweeps(n);
+    std::vector<double> delta(n);
+    int loop_state[2] = {0, 0};
+    unsigned hstat[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(evald.data(), c->b_slots + n, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(sweeps.data(), cm.sweeps, (size_t)n * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(delta.data(), cm.delta, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(loop_state, cm.sweep, sizeof loop_state, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hstat, c->b_counters, sizeof hstat, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaStreamSynchronize(s)) != cudaSuccess)
-        return cuda_error(e, "batch");
+        return fail(e, "batch");
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    c->epoch = e0 - 1 + 6u * (unsigned)loop_state[0];  // passes the loop numbered
+    if (hstat[1]) return set_error(FOLD3D_ERR_TIMEOUT, "batch: a dependency wait gave up");
     if (reps) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -825,11 +921,127 @@ static int solve_batch(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cons
             reps[i].max_delta = delta[i];
             reps[i].elapsed_ms = ms;
             reps[i].nominal_updates = nominal_per_sweep(in[i].grid) * (uint64_t)sweeps[i];
-            reps[i].evaluated_updates = slots[n + i];
+            reps[i].evaluated_updates = evald[i];
             reps[i].engine = FOLD3D_ENGINE_WAVEFRONT;
         }
     }
     return FOLD3D_OK;
+}
+
+// Resident batched-pass CTAs per SM at tile height tv (the occupancy limit).
+static int batch_occupancy_of(fold3d_ctx *c, bool f32, int tv)
+{
+    int &v = c->batch_bps[f32 ? 1 : 0][tv];
+    if (!v) v = batch_blocks_per_sm(f32, tv);
+    return v;
+}
+
+// The batch autotuner.  For a size mix it has not seen (number of instances,
+// total and largest extent, field type), it times one full sweep of each
+// candidate configuration -- tile heights of 2, 4 and 8 rows (64, 128 and 256
+// threads per CTA), each at its occupancy limit of resident CTAs per SM and
+// at three quarters of it -- on copies of up to four instances of median
+// size (the caller's fields are not touched), and keeps the fastest for the
+// size mix.  Every configuration gives the same results bit for bit; they
+// differ only in speed.
+static int batch_config(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cudaStream_t s, int &tv, int &bps)
+{
+    if (!c->sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    if (c->tune_tv > 0) {  // fixed by fold3d_batch_set_config
+        tv = c->tune_tv;
+        const int occ = batch_occupancy_of(c, f32, tv);
+        bps = c->tune_bps > 0 ? std::min(c->tune_bps, occ) : occ;
+        return FOLD3D_OK;
+    }
+    if (n < 8) {  // too few instances to be worth a tuning run
+        tv = kWaveTV;
+        bps = batch_occupancy_of(c, f32, tv);
+        return FOLD3D_OK;
+    }
+    long long total = 0, big = 0;
+    std::vector<std::pair<size_t, int>> by_size(n);
+    for (int i = 0; i < n; ++i) {
+        const fold3d_grid &g = in[i].grid;
+        total += (long long)g.nx * g.ny * g.nz;
+        big = std::max<long long>(big, std::max(g.nx, std::max(g.ny, g.nz)));
+        by_size[i] = {field_cells(g), i};
+    }
+    const std::vector<long long> key = {n, f32 ? 1 : 0, (long long)std::llround(4.0 * std::log2((double)total)),
+                                        (long long)std::llround(4.0 * std::log2((double)big))};
+    auto hit = c->tuned.find(key);
+    if (hit != c->tuned.end()) {
+        tv = hit->second.first;
+        bps = hit->second.second;
+        return FOLD3D_OK;
+    }
+    // up to four instances around the median size, on copies of their fields
+    std::sort(by_size.begin(), by_size.end());
+    const int k = std::min(4, n), first = std::max(0, n / 2 - k / 2);
+    size_t cells = 0;
+    for (int q = 0; q < k; ++q) cells += by_size[first + q].first;
+    const size_t esz = f32 ? sizeof(float) : sizeof(double);
+    cudaError_t e;
+    if (c->tune_cells * sizeof(double) < cells * esz) {
+        if (c->tune_T) cudaFree(c->tune_T);
+        c->tune_T = nullptr;
+        c->tune_cells = 0;
+        if ((e = cudaMalloc(&c->tune_T, cells * esz)) != cudaSuccess)
+            return set_error(FOLD3D_ERR_NOMEM, "batch autotuner scratch");
+        c->tune_cells = (cells * esz + sizeof(double) - 1) / sizeof(double);
+    }
+    std::vector<SolveInst> sub(k);
+    size_t off = 0;
+    for (int q = 0; q < k; ++q) {
+        const SolveInst &src = in[by_size[first + q].second];
+        sub[q] = src;
+        sub[q].T = reinterpret_cast<char *>(c->tune_T) + off * esz;
+        sub[q].winners = nullptr;
+        off += field_cells(src.grid);
+    }
+    fold3d_opts one;
+    fold3d_default_opts(&one);
+    one.max_sweeps = 1;
+    one.fixed = 1;
+    one.skip = 0;
+    std::vector<fold3d_report> r(k);
+    double best = 1e300;
+    tv = kWaveTV;
+    bps = batch_occupancy_of(c, f32, tv);
+    for (int ctv : {2, 4, 8}) {
+        const int occ = batch_occupancy_of(c, f32, ctv);
+        for (int cb : {occ, std::max(1, (3 * occ) / 4)}) {
+            for (int q = 0; q < k; ++q) {
+                const SolveInst &src = in[by_size[first + q].second];
+                const size_t bytes = field_cells(src.grid) * esz;
+                if ((e = cudaMemcpyAsync(sub[q].T, src.T, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                    return cuda_error(e, "batch autotuner");
+            }
+            int rc = solve_batch_cfg(c, k, sub.data(), f32, one, s, r.data(), ctv, cb);
+            if (rc) return rc;
+            if (r[0].elapsed_ms < best) {
+                best = r[0].elapsed_ms;
+                tv = ctv;
+                bps = cb;
+            }
+        }
+    }
+    c->tuned[key] = {tv, bps};
+    return FOLD3D_OK;
+}
+
+static int solve_batch(fold3d_ctx *c, int n, const SolveInst *in, bool f32, const fold3d_opts &o, cudaStream_t s,
+                       fold3d_report *reps)
+{
+    int tv = kWaveTV, bps = 1;
+    int rc = batch_config(c, n, in, f32, s, tv, bps);
+    if (rc) return rc;
+    c->last_tv = tv;
+    c->last_bps = bps;
+    return solve_batch_cfg(c, n, in, f32, o, s, reps, tv, bps);
 }
 
 // Adjoint scratch (lambda already pushed) for `cells` cells.
@@ -1424,6 +1636,27 @@ int fold3d_adjoint_ellip_f32(fold3d_ctx *c, const fold3d_grid *g, const fold3d_e
     if (!g || !m) return clear_error(), set_error(FOLD3D_ERR_INVALID, "NULL argument");
     const AdjInst one = {*g, medium_of(*m), T, W, dLdT, lam, dLdM};
     return adjoint_entry(c, 1, &one, true, max_sweeps, tol, 0, stream, rep);
+}
+
+int fold3d_batch_set_config(fold3d_ctx *c, int tile_rows, int ctas_per_sm)
+{
+    clear_error();
+    if (!c) return set_error(FOLD3D_ERR_INVALID, "ctx is NULL");
+    if (tile_rows != 0 && tile_rows != 2 && tile_rows != 4 && tile_rows != 8)
+        return set_error(FOLD3D_ERR_INVALID, "tile_rows must be 0 (autotune), 2, 4 or 8");
+    if (ctas_per_sm < 0) return set_error(FOLD3D_ERR_INVALID, "ctas_per_sm must be >= 0");
+    c->tune_tv = tile_rows;
+    c->tune_bps = tile_rows ? ctas_per_sm : 0;
+    return FOLD3D_OK;
+}
+
+int fold3d_batch_get_config(fold3d_ctx *c, int *tile_rows, int *ctas_per_sm)
+{
+    clear_error();
+    if (!c || !tile_rows || !ctas_per_sm) return set_error(FOLD3D_ERR_INVALID, "NULL argument");
+    *tile_rows = c->last_tv;
+    *ctas_per_sm = c->last_bps;
+    return FOLD3D_OK;
 }
 
 int fold3d_solve_tti(fold3d_ctx *c, const fold3d_grid *g, const fold3d_tti *m, double *T, const fold3d_opts *o,

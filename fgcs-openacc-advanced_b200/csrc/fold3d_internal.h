@@ -207,21 +207,64 @@ struct BatchInst {
 };
 static_assert(sizeof(BatchInst) % 4 == 0, "BatchInst is copied in words");
 
-// One batched pass: the active instances sorted by step count (descending),
-// the first global item of each step, the number of instances with a step p,
-// and the prefix sums of the instances' tiles per plane.
+// One batched pass of direction dir.  inst holds every instance of the batch
+// in this direction's order (step count descending); the active ones are
+// listed by act (their positions in inst, in that order), so that the
+// active instances of a step are a prefix of the list.  step_off: the first
+// global item of each step; step_k: the number of active instances with a
+// step p; tile_pre: prefix sums of the active instances' tiles per plane.
+// Those tables, the pass's item count and the sweep's pass numbers live in
+// device memory and are rewritten by the restage kernel after every sweep,
+// so a captured graph runs the whole sweep loop.
 struct BatchArgs {
     const BatchInst *inst;
-    const long long *step_off;  // [max_steps + 1]
-    const int *step_k;          // [max_steps]
-    const long long *tile_pre;  // [active + 1]
-    int max_steps;
-    unsigned total;
+    const int *act;               // [active]
+    const long long *step_off;    // [max_steps + 1]
+    const int *step_k;            // [max_steps]
+    const long long *tile_pre;    // [active + 1]
+    const unsigned *total;        // items of this pass
+    const unsigned *epoch_base;   // this sweep's first pass number minus 1; the pass is epoch_base + dir + 1
+    int max_steps, dir;
     unsigned *work, *status;
-    unsigned epoch, skip_from;  // pass number and first pass that may skip
+    unsigned skip_from;           // first pass that may skip
 };
-cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int grid, cudaStream_t s);
-int batch_blocks_per_sm(bool f32);
+// tv: tile height of the batch (2, 4 or 8 rows; 32 * tv threads per CTA).
+cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int tv, int grid, cudaStream_t s);
+int batch_blocks_per_sm(bool f32, int tv);
+
+// The sweep loop of a batched solve on the device (fold3d_wavefront.cu).
+// After each sweep the restage kernel folds every active instance's largest
+// change into its state (sweeps run, last change; converged instances drop
+// out), rebuilds each direction's active list and item tables, advances the
+// pass numbers, clears the per-sweep maxima, and sets the loop's condition:
+// another sweep while some instance is active, the sweep limit is not
+// reached and no dependency wait gave up.  With first set it only builds the
+// tables (before the first sweep).
+struct BatchDirTables {
+    const int *order;             // [n] instance at each position of this direction's order
+    const int *steps;             // [n] plane steps of the instance at each position
+    const long long *tiles;       // [n] tiles per plane of the instance at each position
+    int *act;                     // outputs, as in BatchArgs
+    long long *step_off;
+    int *step_k;
+    long long *tile_pre;
+};
+struct BatchCtl {
+    BatchDirTables dir[6];
+    int n, max_steps, fixed, max_sweeps;
+    double tol;
+    unsigned epoch0;              // first pass number minus 1 (first call)
+    unsigned *total;              // [6]
+    unsigned *epoch_base;
+    int *sweep;                   // [0] sweeps run, [1] instances still active
+    int *active;                  // [n]
+    int *sweeps;                  // [n]
+    double *delta;                // [n] largest change of the instance's last sweep
+    unsigned long long *maxd;     // [n] this sweep's largest change (IEEE bits), cleared here
+    const unsigned *status;
+    unsigned long long cond;      // cudaGraphConditionalHandle of the sweep loop
+};
+cudaError_t launch_batch_restage(const BatchCtl &ctl, bool first, cudaStream_t s);
 
 // Adjoint of the elliptical solver (fold3d_adjoint.cu).
 struct AdjGeom {

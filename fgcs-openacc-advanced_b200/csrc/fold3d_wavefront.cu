@@ -80,7 +80,7 @@ template <> struct WaveMedium<kMediumEllip> {
 // publish its flag.  Adds each changed point's |dT| into dmax and the
 // evaluated points into evaluated.  Returns false if a wait gave up (the
 // item is then left unpublished and the caller must leave).
-template <int MED, class R>
+template <int MED, class R, int TV = kWaveTV>
 __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
                                           const typename WaveMedium<MED>::type &tab, int item, double &dmax,
                                           unsigned long long &evaluated)
@@ -128,7 +128,7 @@ __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
     int changed = 0;
     if (!skip) {
         const int u = tu * 32 + lane + 1;
-        const int v = tv * kWaveTV + warp + 1;
+        const int v = tv * TV + warp + 1;
         if (u <= g.nu && v <= g.nv) {
             const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
             const long long d = s + g.sn;
@@ -165,7 +165,7 @@ __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
                     const int cb = (q == 0) ? u : v;
                     const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
                     const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
-                    const int tile = ((cv - 1) / kWaveTV) * a.mod_ntu[b] + ((cu - 1) >> 5);
+                    const int tile = ((cv - 1) / TV) * a.mod_ntu[b] + ((cu - 1) >> 5);
                     a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
                 }
             }
@@ -182,10 +182,11 @@ __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
 }
 
 // Block-wide maximum of d into *out (IEEE bits) and sum of e into *sum.
+template <int TV = kWaveTV>
 __device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsigned long long *out,
                                            unsigned long long *sum)
 {
-    __shared__ double wmax[kWaveTV];
+    __shared__ double wmax[TV];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
@@ -198,7 +199,7 @@ __device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsig
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = 0.0;
-        for (int w = 0; w < kWaveTV; ++w) m = fmax(m, wmax[w]);
+        for (int w = 0; w < TV; ++w) m = fmax(m, wmax[w]);
         if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
     }
     __syncthreads();
@@ -243,15 +244,21 @@ __global__ void __launch_bounds__(kWaveThreads, (wave_min_blocks<MED, R, LARGE>(
 // same instance) come earlier in that order, and the launch's claimed items
 // spread over many instances at once.
 // ---------------------------------------------------------------------------
-template <class R>
-__global__ void __launch_bounds__(kWaveThreads, FOLD3D_WAVE_MINB_BATCH) batch_pass_kernel(BatchArgs b)
+// Resident CTAs per SM the batched kernel is compiled for, by tile height:
+// the same register budget per thread (65536 / (128 * 8)) for every height.
+template <int TV> constexpr int batch_min_blocks() { return FOLD3D_WAVE_MINB_BATCH * kWaveTV / TV; }
+
+template <class R, int TV>
+__global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_kernel(BatchArgs b)
 {
     __shared__ int s_next;
     __shared__ int s_loc[2];
     __shared__ BatchInst s_inst;
+    const unsigned total = *b.total;
+    const unsigned epoch = *b.epoch_base + (unsigned)b.dir + 1u;
     if (threadIdx.x == 0) {
         const unsigned w = atomicAdd(b.work, 1u);
-        s_next = (w < b.total) ? (int)w : -1;
+        s_next = (w < total) ? (int)w : -1;
     }
     __syncthreads();
     for (;;) {
@@ -262,46 +269,136 @@ __global__ void __launch_bounds__(kWaveThreads, FOLD3D_WAVE_MINB_BATCH) batch_pa
             int it = -1;
             if (*(volatile unsigned *)b.status == 0) {
                 const unsigned w = atomicAdd(b.work, 1u);
-                if (w < b.total) it = (int)w;
+                if (w < total) it = (int)w;
             }
             s_next = it;
             batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, gitem, s_loc[0], s_loc[1]);
         }
         __syncthreads();
         {
-            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + s_loc[0]);
+            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + b.act[s_loc[0]]);
             unsigned *dst = reinterpret_cast<unsigned *>(&s_inst);
             for (int w = threadIdx.x; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = src[w];
         }
         __syncthreads();
         if (threadIdx.x == 0) {  // the pass number is per launch, not per staged instance
-            s_inst.a.epoch = b.epoch;
+            s_inst.a.epoch = epoch;
             s_inst.a.skip_from = b.skip_from;
         }
         __syncthreads();
         double dmax = 0.0;
         unsigned long long evaluated = 0;
-        if (!wave_item<kMediumEllip, R>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[1], dmax, evaluated))
+        if (!wave_item<kMediumEllip, R, TV>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[1], dmax,
+                                            evaluated))
             break;
-        wave_flush(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
+        wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
     }
 }
 
-cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int grid, cudaStream_t s)
+// The batch's state after a sweep and the next sweep's tables (BatchCtl).
+// One block: the instances are folded in parallel, then one thread per
+// direction rebuilds that direction's tables (a few thousand steps).
+__global__ void __launch_bounds__(256) batch_restage_kernel(BatchCtl c, int first)
 {
-    if (f32) batch_pass_kernel<float><<<grid, kWaveThreads, 0, s>>>(b);
-    else batch_pass_kernel<double><<<grid, kWaveThreads, 0, s>>>(b);
+    __shared__ int s_left;
+    if (threadIdx.x == 0) s_left = 0;
+    __syncthreads();
+    if (first) {
+        for (int i = threadIdx.x; i < c.n; i += blockDim.x) {
+            c.active[i] = 1;
+            c.sweeps[i] = 0;
+            c.delta[i] = 0.0;
+            c.maxd[i] = 0ull;
+        }
+        if (threadIdx.x == 0) {
+            *c.epoch_base = c.epoch0;
+            c.sweep[0] = 0;
+            c.sweep[1] = c.n;
+        }
+    } else {
+        int left = 0;
+        for (int i = threadIdx.x; i < c.n; i += blockDim.x) {
+            if (c.active[i]) {
+                c.sweeps[i] += 1;
+                const double d = __longlong_as_double((long long)c.maxd[i]);
+                c.delta[i] = d;
+                if (!c.fixed && d <= c.tol) c.active[i] = 0;
+                else ++left;
+            }
+            c.maxd[i] = 0ull;
+        }
+        atomicAdd(&s_left, left);
+    }
+    __syncthreads();
+    if (!first && threadIdx.x == 0) {
+        *c.epoch_base += 6u;
+        c.sweep[0] += 1;
+        c.sweep[1] = s_left;
+    }
+    if (threadIdx.x < 6) {
+        const BatchDirTables &t = c.dir[threadIdx.x];
+        int k = 0;
+        t.tile_pre[0] = 0;
+        for (int q = 0; q < c.n; ++q)
+            if (c.active[t.order[q]]) {
+                t.act[k] = q;
+                t.tile_pre[k + 1] = t.tile_pre[k] + t.tiles[q];
+                ++k;
+            }
+        // the active instances with a step p are a prefix of the list (steps
+        // descending): step_k[p] shrinks from k as p grows, dropping from the
+        // end the instances with at most p steps
+        int kk = k;
+        t.step_off[0] = 0;
+        for (int p = 0; p < c.max_steps; ++p) {
+            while (kk > 0 && t.steps[t.act[kk - 1]] <= p) --kk;
+            t.step_k[p] = kk;
+        }
+        for (int p = 0; p < c.max_steps; ++p) t.step_off[p + 1] = t.step_off[p] + t.tile_pre[t.step_k[p]];
+        c.total[threadIdx.x] = (unsigned)t.step_off[c.max_steps];
+    }
+    if (!first && threadIdx.x == 0) {
+        const int more = (*(volatile const unsigned *)c.status == 0) && c.sweep[0] < c.max_sweeps && s_left > 0;
+        cudaGraphSetConditional((cudaGraphConditionalHandle)c.cond, more ? 1u : 0u);
+    }
+}
+
+cudaError_t launch_batch_restage(const BatchCtl &ctl, bool first, cudaStream_t s)
+{
+    batch_restage_kernel<<<1, 256, 0, s>>>(ctl, first ? 1 : 0);
     return cudaGetLastError();
 }
 
-int batch_blocks_per_sm(bool f32)
+template <int TV> static cudaError_t launch_batch_tv(const BatchArgs &b, bool f32, int grid, cudaStream_t s)
+{
+    if (f32) batch_pass_kernel<float, TV><<<grid, 32 * TV, 0, s>>>(b);
+    else batch_pass_kernel<double, TV><<<grid, 32 * TV, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int tv, int grid, cudaStream_t s)
+{
+    switch (tv) {
+    case 2: return launch_batch_tv<2>(b, f32, grid, s);
+    case 4: return launch_batch_tv<4>(b, f32, grid, s);
+    case 8: return launch_batch_tv<8>(b, f32, grid, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int TV> static int batch_occupancy(bool f32)
 {
     int n = 0;
     const cudaError_t e =
-        f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<float>, kWaveThreads, 0)
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<double>, kWaveThreads, 0);
+        f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<float, TV>, 32 * TV, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<double, TV>, 32 * TV, 0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
+}
+
+int batch_blocks_per_sm(bool f32, int tv)
+{
+    return tv == 2 ? batch_occupancy<2>(f32) : tv == 8 ? batch_occupancy<8>(f32) : batch_occupancy<4>(f32);
 }
 
 cudaError_t launch_wave_pass(double *T, const WaveArgs &a, const DirTable &tab, int grid, cudaStream_t s, bool large)

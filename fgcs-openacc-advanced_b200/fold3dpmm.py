@@ -41,7 +41,7 @@ EXPORTED = (
     "fold3d_solve_batch_f32", "fold3d_adjoint_batch_f32",
     "fold3d_solve_ellip_record", "fold3d_adjoint_ellip",
     "fold3d_solve_tti", "fold3d_solve_tti_record", "fold3d_adjoint_tti", "fold3d_solve_batch_tti",
-    "fold3d_adjoint_batch_tti",
+    "fold3d_adjoint_batch_tti", "fold3d_batch_set_config", "fold3d_batch_get_config",
     "InitFoldFromPoint", "ImpSurfF", "ImplicitInitialiser", "InitNode", "updateVoxel", "x", "y", "z",
     "function_x_down", "function_x_up", "function_y_up", "function_y_down", "function_k_up",
     "function_k_down",
@@ -167,6 +167,8 @@ def lib() -> C.CDLL:
     L.acc_free.argtypes = [vp]
     L.acc_memcpy_to_device.argtypes = [vp, vp, C.c_size_t]
     L.acc_memcpy_from_device.argtypes = [vp, vp, C.c_size_t]
+    L.fold3d_batch_set_config.argtypes = [vp, i, i]
+    L.fold3d_batch_get_config.argtypes = [vp, P(i), P(i)]
     L.fold3d_solve_tti.argtypes = [vp, P(Grid), P(Tti), vp, P(Opts), vp, P(Report)]
     L.fold3d_solve_tti_record.argtypes = [vp, P(Grid), P(Tti), vp, vp, P(Opts), vp, P(Report)]
     L.fold3d_adjoint_tti.argtypes = [vp, P(Grid), P(Tti), vp, vp, vp, vp, vp, i, C.c_double, vp, P(Report)]
@@ -590,6 +592,19 @@ def adjoint_batch(ctx: "Context", fields, hs, media, winners, dLdT, lam, dLdM, m
     _check(fn(ctx._h, n, arr, int(max_sweeps), float(tol), int(bool(accumulate)),
               C.c_void_p(stream) if stream else None, reps))
     return list(reps)
+
+
+def batch_set_config(ctx: "Context", tile_rows=0, ctas_per_sm=0):
+    """fold3d_batch_set_config: fix the batched solves' tile height (2, 4 or
+    8 rows) and resident CTAs per SM, or 0 to let the autotuner choose."""
+    _check(lib().fold3d_batch_set_config(ctx._h, int(tile_rows), int(ctas_per_sm)))
+
+
+def batch_get_config(ctx: "Context"):
+    """(tile rows, CTAs per SM) of the last batched solve on ctx."""
+    a, b = C.c_int(), C.c_int()
+    _check(lib().fold3d_batch_get_config(ctx._h, C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def plane(T, h, dir_, src, med: Medium | None = None, stream=None):

@@ -275,6 +275,17 @@ int fold3d_solve_batch_f32(fold3d_ctx *ctx, int n, const fold3d_instance_f32 *in
 int fold3d_adjoint_batch_f32(fold3d_ctx *ctx, int n, const fold3d_adjoint_instance_f32 *inst, int max_sweeps,
                              double tol, int accumulate, void *stream, fold3d_report *reps);
 
+/* Configuration of the batched solves (no counterpart in the reference):
+ * tile height in rows of 32 points (2, 4 or 8; a CTA has 32 * rows threads)
+ * and resident CTAs per SM (0 or above the occupancy limit: the limit).
+ * tile_rows = 0 (the default) lets the context's autotuner choose: for each
+ * size mix it has not seen (8 or more instances), it times one sweep of each
+ * candidate on copies of a few median-size instances and keeps the fastest.
+ * Every configuration gives the same results bit for bit. */
+int fold3d_batch_set_config(fold3d_ctx *ctx, int tile_rows, int ctas_per_sm);
+/* The configuration the last batched solve on ctx ran with. */
+int fold3d_batch_get_config(fold3d_ctx *ctx, int *tile_rows, int *ctas_per_sm);
+
 /* The tilted elliptical medium given by its FP64 parameters (no counterpart
  * in the reference).  Four double arrays in the field layout: slowness
  * s = 1/Vz, Thomsen epsilon, and the x and y components of the unit symmetry

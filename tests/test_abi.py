@@ -327,3 +327,10 @@ def test_compat_sweep_without_grid_size_is_rejected(f3d):
     assert L.fold3d_compat_set_grid(0, 0, 0) == f3d.OK
     L.function_x_down(C.c_void_p(4096), 1, *([0.1] * 6), 1.1, 0.4, -0.35, 0.7)
     assert "grid size unknown" in f3d.last_error()
+
+
+def test_batch_config_rejects_bad_values(f3d):
+    L = f3d.lib()
+    assert L.fold3d_batch_set_config(None, 4, 0) == f3d.ERR_INVALID
+    a, b = C.c_int(), C.c_int()
+    assert L.fold3d_batch_get_config(None, C.byref(a), C.byref(b)) == f3d.ERR_INVALID

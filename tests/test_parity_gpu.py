@@ -557,6 +557,73 @@ def test_batch_equals_one_by_one(f3d, ctx, cuda, fixed):
         assert len(sweeps) > 1  # instances did stop at different sweeps
 
 
+def test_batch_c4_subset_equals_one_by_one(f3d, ctx, cuda):
+    """The batched configuration's size mix: 16 instances with dims drawn per
+    axis from [96, 320] (seed 1), each its own seeded heterogeneous medium
+    and source, converged to max|dT| <= 1e-10 in one batched call (the sweep
+    loop on the device, the configuration chosen by the autotuner).  Every
+    field, sweep count and last change equals the instance's own solve, bit
+    for bit."""
+    import media
+
+    rng = np.random.default_rng(1)
+    o = f3d.opts(max_sweeps=300, tol=1e-10)
+    fields, media_, alone = [], [], []
+    for i in range(16):
+        dims = tuple(int(v) for v in rng.integers(96, 321, 3))
+        src = tuple(int(rng.integers(1, d + 1)) for d in dims)
+        M = media.heterogeneous_tti(*dims, 10.0, seed=1000 + i, device="cuda")
+        T = torch_point_dims(cuda, dims, src)
+        t = T.clone()
+        alone.append((t, f3d.solve_ellip(ctx, t, 10.0, M, o)))
+        fields.append(T)
+        media_.append(M)
+    reps = f3d.solve_batch(ctx, fields, [10.0] * len(fields), media_, o)
+    for (t, r), f, rb in zip(alone, fields, reps):
+        assert rb.sweeps == r.sweeps and rb.max_delta == r.max_delta
+        assert cuda.equal(t.view(cuda.int64), f.view(cuda.int64))
+
+
+@pytest.mark.parametrize("rows,ctas", [(2, 0), (4, 0), (8, 0), (4, 3), (8, 1)])
+def test_batch_configurations_agree(f3d, ctx, cuda, rows, ctas):
+    """Every tile height and CTA count the autotuner may pick gives the
+    one-by-one results bit for bit (here forced with
+    fold3d_batch_set_config)."""
+    inst = _batch_instances(cuda, 9, 9, 45, seed=8)
+    o = f3d.opts(max_sweeps=300, tol=1e-10)
+    alone = []
+    for T, M in inst:
+        t = T.clone()
+        alone.append((t, f3d.solve_ellip(ctx, t, 10.0, M, o)))
+    fields = [T.clone() for T, _ in inst]
+    f3d.batch_set_config(ctx, rows, ctas)
+    try:
+        reps = f3d.solve_batch(ctx, fields, [10.0] * len(inst), [M for _, M in inst], o)
+        got_rows, got_ctas = f3d.batch_get_config(ctx)
+    finally:
+        f3d.batch_set_config(ctx, 0, 0)
+    assert got_rows == rows and got_ctas >= 1 and (ctas == 0 or got_ctas <= ctas)
+    for (t, r), f, rb in zip(alone, fields, reps):
+        assert rb.sweeps == r.sweeps and rb.max_delta == r.max_delta
+        assert cuda.equal(t.view(cuda.int64), f.view(cuda.int64))
+
+
+def test_batch_autotuner_picks_a_candidate(f3d, ctx, cuda):
+    """With 8 or more instances the autotuner runs once per size mix, on
+    copies (the caller's fields are solved once, with the chosen
+    configuration) and reports one of its candidates."""
+    inst = _batch_instances(cuda, 10, 20, 48, seed=12)
+    o = f3d.opts(max_sweeps=300, tol=1e-10)
+    fields = [T.clone() for T, _ in inst]
+    f3d.solve_batch(ctx, fields, [10.0] * len(inst), [M for _, M in inst], o)
+    rows, ctas = f3d.batch_get_config(ctx)
+    assert rows in (2, 4, 8) and ctas >= 1
+    for (T, M), f in zip(inst, fields):
+        t = T.clone()
+        f3d.solve_ellip(ctx, t, 10.0, M, o)
+        assert cuda.equal(t.view(cuda.int64), f.view(cuda.int64))
+
+
 def test_batch_rejects_bad_input(f3d, ctx, cuda):
     L = f3d.lib()
     assert L.fold3d_solve_batch(ctx._h, 0, None, C.byref(f3d.opts()), None, None) == f3d.ERR_INVALID
