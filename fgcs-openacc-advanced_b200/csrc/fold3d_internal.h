@@ -266,6 +266,34 @@ struct BatchCtl {
 };
 cudaError_t launch_batch_restage(const BatchCtl &ctl, bool first, cudaStream_t s);
 
+// One direction's item tables for the active instances (active[i] != 0 for
+// instance i): act, tile_pre, step_k and step_off; returns the pass's item
+// count.  The active instances with a step p are a prefix of the list (steps
+// descending), so step_k[p] shrinks from k as p grows, dropping from the end
+// the instances with at most p steps.  Host and device (the restage kernel).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline unsigned batch_tables(const BatchDirTables &t, const int *active, int n, int max_steps)
+{
+    int k = 0;
+    t.tile_pre[0] = 0;
+    for (int q = 0; q < n; ++q)
+        if (active[t.order[q]]) {
+            t.act[k] = q;
+            t.tile_pre[k + 1] = t.tile_pre[k] + t.tiles[q];
+            ++k;
+        }
+    int kk = k;
+    t.step_off[0] = 0;
+    for (int p = 0; p < max_steps; ++p) {
+        while (kk > 0 && t.steps[t.act[kk - 1]] <= p) --kk;
+        t.step_k[p] = kk;
+    }
+    for (int p = 0; p < max_steps; ++p) t.step_off[p + 1] = t.step_off[p] + t.tile_pre[t.step_k[p]];
+    return (unsigned)t.step_off[max_steps];
+}
+
 // Adjoint of the elliptical solver (fold3d_adjoint.cu).
 struct AdjGeom {
     PlaneGeom pg[6];

@@ -335,28 +335,7 @@ __global__ void __launch_bounds__(256) batch_restage_kernel(BatchCtl c, int firs
         c.sweep[0] += 1;
         c.sweep[1] = s_left;
     }
-    if (threadIdx.x < 6) {
-        const BatchDirTables &t = c.dir[threadIdx.x];
-        int k = 0;
-        t.tile_pre[0] = 0;
-        for (int q = 0; q < c.n; ++q)
-            if (c.active[t.order[q]]) {
-                t.act[k] = q;
-                t.tile_pre[k + 1] = t.tile_pre[k] + t.tiles[q];
-                ++k;
-            }
-        // the active instances with a step p are a prefix of the list (steps
-        // descending): step_k[p] shrinks from k as p grows, dropping from the
-        // end the instances with at most p steps
-        int kk = k;
-        t.step_off[0] = 0;
-        for (int p = 0; p < c.max_steps; ++p) {
-            while (kk > 0 && t.steps[t.act[kk - 1]] <= p) --kk;
-            t.step_k[p] = kk;
-        }
-        for (int p = 0; p < c.max_steps; ++p) t.step_off[p + 1] = t.step_off[p] + t.tile_pre[t.step_k[p]];
-        c.total[threadIdx.x] = (unsigned)t.step_off[c.max_steps];
-    }
+    if (threadIdx.x < 6) c.total[threadIdx.x] = batch_tables(c.dir[threadIdx.x], c.active, c.n, c.max_steps);
     if (!first && threadIdx.x == 0) {
         const int more = (*(volatile const unsigned *)c.status == 0) && c.sweep[0] < c.max_sweeps && s_left > 0;
         cudaGraphSetConditional((cudaGraphConditionalHandle)c.cond, more ? 1u : 0u);

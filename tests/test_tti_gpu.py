@@ -107,10 +107,11 @@ def test_tti_adjoint_matches_cpu_adjoint(f3d, orc, ctx, cuda):
         np.testing.assert_allclose(gg[m], gr[m], rtol=1e-9, atol=1e-12 * np.abs(gr[m]).max())
 
 
-def _fd_check(cuda, P, T0, h, rec, ncells, rng_seed):
+def _fd_check(cuda, P, T0, h, rec, ncells, rng_seed, floor=1e-3):
     """Relative errors of dL/ds and dL/deps from the adjoint against central
     differences with step 1e-6 of the parameter, at ncells cells (each
-    variable) among those whose gradient is at least 1e-3 of its largest."""
+    variable) among those whose gradient is at least `floor` of its
+    largest."""
     import tomo
 
     Pg = [p.clone().requires_grad_(True) for p in P]
@@ -127,7 +128,7 @@ def _fd_check(cuda, P, T0, h, rec, ncells, rng_seed):
     errs = {"s": [], "eps": []}
     for var, v in (("s", 0), ("eps", 1)):
         G = Pg[v].grad
-        cand = cuda.nonzero(G.abs() >= 1e-3 * G.abs().max()).cpu().numpy()
+        cand = cuda.nonzero(G.abs() >= floor * G.abs().max()).cpu().numpy()
         for q in rng.choice(len(cand), min(ncells, len(cand)), replace=False):
             k, j, i = (int(x) for x in cand[q])
             base = float(P[v][k, j, i])
@@ -160,23 +161,28 @@ def test_tti_gradient_finite_differences_256(cuda):
     """The tomography configuration's size: 256^3 seeded heterogeneous medium
     (seed 2) as FP64 parameters, one source 10 cells below the top face,
     4096 receivers on the top face; dL/ds and dL/deps against central
-    differences (1e-6 relative step) at 16 cells each.  Median relative error
-    at most 1e-6, every sample below 1e-5."""
+    differences (1e-6 relative step) at 16 cells each, among those whose
+    gradient is at least 1e-2 of the largest.  Median relative error at most
+    1e-6, every sample below 1e-5.  (Below that floor a cell moves the
+    receivers' times by so little that the difference quotient is dominated
+    by the solves' rounding, a few ulps of each time: about 1e-10 relative
+    divided by the cell's sensitivity.)"""
     n, h = 256, 10.0
     P = hetero((n, n, n), 2)
     T0 = cuda.full((n + 2,) * 3, MAXT, dtype=cuda.float64, device="cuda")
     T0[11, 100, 140] = 0.0
     ridx = cuda.arange(3, n + 1, 4, device="cuda")
     rec = (1, ridx.view(-1, 1), ridx.view(1, -1))
-    errs = _fd_check(cuda, P, T0, h, rec, 16, 11)
+    errs = _fd_check(cuda, P, T0, h, rec, 16, 11, floor=1e-2)
     for var, e in errs.items():
         assert np.median(e) <= 1e-6 and max(e) < 1e-5, (var, np.median(e), max(e))
 
 
 def test_tti_batch_equals_one_by_one(f3d, ctx, cuda):
     """A batch of parameter-medium instances (non-cubic grids, own media and
-    sources) gives each one its own solve's field, record and sweep count;
-    the batched adjoint equals the single adjoints."""
+    sources) gives each one its own solve's field, record and sweep count,
+    bit for bit; the batched adjoint equals the single adjoints to rounding
+    (relative 1e-12)."""
     rng = np.random.default_rng(9)
     inst = []
     for q in range(5):
@@ -204,7 +210,9 @@ def test_tti_batch_equals_one_by_one(f3d, ctx, cuda):
         l1 = cuda.empty_like(T)
         g1 = cuda.empty_like(gb)
         f3d.adjoint_ellip(ctx, T, 10.0, P, W, d, l1, g1)
-        assert cuda.equal(la, l1) and cuda.equal(gb, g1), dims
+        # lambda is pushed with atomic adds, whose order differs between launches: equal to rounding
+        assert cuda.allclose(la, l1, rtol=1e-12, atol=0), dims
+        assert cuda.allclose(gb, g1, rtol=1e-12, atol=1e-12 * float(g1.abs().max())), dims
 
 
 def test_tti_rejects_float32_fields(f3d, ctx, cuda):
