@@ -330,17 +330,25 @@ def oracle_adjoint_sample(T0, T, M, h, W, r, fwd_sweeps):
     parts: one recording forward sweep (six passes, OpenMP) from the initial
     field T0, and the whole FP64 adjoint (winner weights, cells by decreasing
     time, dL/dM) from the converged field T, its winner record W and
-    r = dL/dT.  Host arrays; M as six float32 metric arrays.  Returns
-    (seconds per source-gradient = sweep time x fwd_sweeps + adjoint time,
-    sweep seconds, adjoint seconds)."""
+    r = dL/dT.  Host arrays; M as six float32 metric arrays, or four FP64
+    parameter arrays (the FP64 statement with the metric formed from them,
+    and the chain rule to the parameters).  Returns (seconds per
+    source-gradient = sweep time x fwd_sweeps + adjoint time, sweep seconds,
+    adjoint seconds)."""
     from oracle import Oracle
 
     orc = Oracle()
     t1 = time.perf_counter()
-    orc.ell_solve_rec(T0.copy(), M, (h,) * 3, 1, tol=0.0)
+    if len(M) == 4:
+        orc.tti_solve_rec(T0.copy(), M, (h,) * 3, 1, tol=0.0)
+    else:
+        orc.ell_solve_rec(T0.copy(), M, (h,) * 3, 1, tol=0.0)
     sweep_s = time.perf_counter() - t1
     t1 = time.perf_counter()
-    orc.ell_adjoint(T, M, (h,) * 3, W, r)
+    if len(M) == 4:
+        orc.tti_adjoint(T, M, (h,) * 3, W, r)
+    else:
+        orc.ell_adjoint(T, M, (h,) * 3, W, r)
     adj_s = time.perf_counter() - t1
     return sweep_s * fwd_sweeps + adj_s, sweep_s, adj_s
 
@@ -348,8 +356,11 @@ def oracle_adjoint_sample(T0, T, M, h, W, r, fwd_sweeps):
 def run_tti(args):
     """--medium tti: the 512^3 heterogeneous tilted-elliptical configuration
     (seeded medium, point source at depth index 64 of the centre column), each
-    step a solve run to max|dT| <= 1e-10.  Bytes per update: 16 for the field
-    plus 24 for the six float32 metric words of the target."""
+    step a solve run to max|dT| <= 1e-10.  The medium is the FP64 parameter
+    form (slowness, eps, axis; fold3d_solve_tti) with float64 fields, or the
+    six float32 metric arrays (--tti-medium metric, and the float32 build).
+    Bytes per update: 16 for the field plus 32 for the four FP64 parameter
+    words of the target (24 for six float32 metric words)."""
     import numpy as np
     import torch
 
@@ -364,8 +375,12 @@ def run_tti(args):
     n, h = args.size, args.spacing
     # grids above 768^3 are built in float32 (float64 temporaries would not fit)
     gen_dtype = torch.float64 if n <= 768 else torch.float32
+    param = args.tti_medium == "param" and args.field_dtype == "f64"
     t0 = time.perf_counter()
-    M = media.heterogeneous_tti(n, n, n, h, seed=0, device="cuda", dtype=gen_dtype)
+    if param:
+        M = media.heterogeneous_tti_params(n, n, n, h, seed=0, device="cuda", dtype=gen_dtype)
+    else:
+        M = media.heterogeneous_tti(n, n, n, h, seed=0, device="cuda", dtype=gen_dtype)
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     gen_peak_gb = torch.cuda.max_memory_allocated() / 1e9
@@ -420,13 +435,14 @@ def run_tti(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        nb_in = hT0.numel() * hT0.element_size() + sum(m.numel() * 4 for m in hM)
+        nb_in = hT0.numel() * hT0.element_size() + sum(m.numel() * m.element_size() for m in hM)
         e2e = {"value": world * upd * args.steps / (ems / 1e3) / 1e9, "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": nb_in, "d2h_bytes_per_step": hT0.numel() * hT0.element_size(),
                "ms_per_step": ems / args.steps}
     peak, peak_kind = load_peaks()
     per_ms = solve_ms / args.steps
-    bpu = 40.0 if fdt == torch.float64 else 32.0  # field read + write, six float32 metric words
+    # field read + write, and the target's medium: four FP64 parameters or six float32 metric words
+    bpu = (16.0 if fdt == torch.float64 else 8.0) + (32.0 if param else 24.0)
     achieved = bpu * upd / (per_ms / 1e3) / 1e9
     launches = rep.sweeps * 6
     cpu = None
@@ -434,11 +450,19 @@ def run_tti(args):
         try:
             from oracle import Oracle
 
+            if param and n > 640:
+                raise RuntimeError("the CPU statement's double metric for %d^3 would need %.0f GB of host memory"
+                                   % (n, 6 * (n + 2) ** 3 * 8 / 1e9))
             orc = Oracle()
             Th = T0.cpu().numpy()
-            Mh = [m.cpu().numpy() for m in M]
-            arrs, ptrs = orc._metric(Mh)
             import ctypes as C
+
+            if param:  # the metric formed from the FP64 parameters, as the kernels form it
+                Md = orc.tti_metric([m.cpu().numpy() for m in M])
+                ptrs = (C.c_void_p * 6)(*(a.ctypes.data for a in Md))
+            else:
+                Mh = [m.cpu().numpy() for m in M]
+                arrs, ptrs = orc._metric(Mh)
 
             planes, upd_cpu = 0, 0
             t1 = time.perf_counter()
@@ -448,6 +472,9 @@ def run_tti(args):
                     if fdt == torch.float32:
                         orc.L.orc_ellf_plane_rec(Th.ctypes.data_as(C.c_void_p), ptrs, None, n, n, n, h, h, h, d,
                                                  first + step * planes)
+                    elif param:
+                        orc.L.orc_ell_plane_d(Th.ctypes.data_as(C.c_void_p), ptrs, n, n, n, h, h, h, d,
+                                              first + step * planes)
                     else:
                         orc.L.orc_ell_plane(Th.ctypes.data_as(C.c_void_p), ptrs, n, n, n, h, h, h, d,
                                             first + step * planes)
@@ -469,8 +496,10 @@ def run_tti(args):
         "config": {"workload": "TTI %d^3 h=%g m heterogeneous (seed 0), source (i,j,k)=%s, run to max|dT|<=1e-10"
                                % (n, h, src), "grid": n, "sweeps": rep.sweeps, "engine": "wavefront",
                    "medium_construction": str(gen_dtype).replace("torch.", ""),
-                   "skip": bool(args.skip), "medium": "6 float32 metric words per cell",
-                   "l2": "field + medium %.1f GB > 126 MB L2" % ((n + 2) ** 3 * 32 / 1e9),
+                   "skip": bool(args.skip),
+                   "medium": "4 FP64 parameter words per cell (slowness, eps, axis x, y); metric formed in the "
+                             "kernel" if param else "6 float32 metric words per cell",
+                   "l2": "field + medium %.1f GB > 126 MB L2" % ((n + 2) ** 3 * bpu / 2 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "kernel": "wave_pass_kernel<ellip>",
@@ -664,8 +693,13 @@ def run_adjoint(args):
     nsrc_side, nrec_side = 8, 64
     t0 = time.perf_counter()
     vz_t, eps_t, ax_t = media.tti_params(n, n, n, h, seed=2, device="cuda", pad=True)
-    M_true = [m.double() for m in media.metric_from(vz_t, eps_t, ax_t)]
+    # FP64 fields: the FP64 parameter medium (fold3d_*_tti), gradients straight to slowness and eps;
+    # the float32 build: six metric arrays and torch's chain rule from them
+    param = args.field_dtype == "f64" and args.tti_medium == "param"
+    M_true = media.params_from(vz_t, eps_t, ax_t) if param else \
+        [m.double() for m in media.metric_from(vz_t, eps_t, ax_t)]
     vz0, eps0, ax0 = media.smooth_params(vz_t, eps_t, ax_t, 16.0)
+    axis0 = media.params_from(vz0, eps0, ax0)[2:] if param else None
     del vz_t, eps_t, ax_t
     rng = np.random.default_rng(2)
     cell = n / nsrc_side
@@ -711,8 +745,12 @@ def run_adjoint(args):
     def step():
         s = (1.0 / vz0).requires_grad_(True)
         e = eps0.clone().requires_grad_(True)
-        Mg = [m.double() for m in media.metric_from(1.0 / s, e, ax0)]
-        Ml = [m.detach().requires_grad_(True) for m in Mg]
+        if param:
+            Mg = None
+            Ml = [s, e] + list(axis0)
+        else:
+            Mg = [m.double() for m in media.metric_from(1.0 / s, e, ax0)]
+            Ml = [m.detach().requires_grad_(True) for m in Mg]
         loss = torch.zeros((1,), dtype=torch.float64, device="cuda")
         if B > 1:  # B sources per batched forward solve and batched adjoint
             for c0 in range(0, len(srcs), B):
@@ -726,7 +764,8 @@ def run_adjoint(args):
                 Ls = 0.5 * ((T[rec].double() - to.double()) ** 2).sum()
                 Ls.backward()
                 loss += Ls.detach()
-        torch.autograd.backward(Mg, [m.grad for m in Ml])
+        if Mg is not None:
+            torch.autograd.backward(Mg, [m.grad for m in Ml])
         shard.sum_over_ranks_([loss, s.grad, e.grad], dist)  # the survey's loss and gradient on every rank
         return float(loss), s.grad, e.grad
 
@@ -757,8 +796,10 @@ def run_adjoint(args):
         per_batch = lambda rs: [rs[q:q + B] for q in range(0, len(rs), B)]
         fwd = sum(g[0].elapsed_ms for g in per_batch(fr)) / len(fr)
         adj = sum(g[0].elapsed_ms for g in per_batch(ar)) / len(ar)
-        # one launch per direction pass of the slowest instance, plus one gradient launch per source
-        launches = sum(6 * max(r.sweeps for r in g) for g in per_batch(fr)) + \
+        # forward: one graph per batch (its table kernel, then per sweep six passes and the restage
+        # kernel); adjoint: one launch per direction pass of the slowest instance, plus one gradient
+        # launch per source
+        launches = sum(7 * max(r.sweeps for r in g) + 1 for g in per_batch(fr)) + \
             sum(6 * max(r.sweeps for r in g) + len(g) for g in per_batch(ar))
     else:
         fr = [r for k, r in reps if k == "forward"]
@@ -777,7 +818,8 @@ def run_adjoint(args):
         try:
             import fold3dpmm as f3d
 
-            M32 = [m.double().float().contiguous() for m in media.metric_from(1.0 / (1.0 / vz0), eps0, ax0)]
+            M32 = [(1.0 / vz0).contiguous(), eps0.contiguous()] + list(axis0) if param else \
+                [m.double().float().contiguous() for m in media.metric_from(1.0 / (1.0 / vz0), eps0, ax0)]
             Tc = t0_of(srcs[0]).double()
             T0h = Tc.cpu().numpy()
             Wc = torch.empty(Tc.shape, dtype=torch.uint8, device="cuda")
@@ -806,6 +848,9 @@ def run_adjoint(args):
                                % (n, nsrc, nsrc_side, nsrc_side, nrec_side ** 2, nrec_side, nrec_side),
                    "grid": n, "sources": nsrc, "receivers": nrec_side ** 2,
                    "gradient": "slowness and eps (torch autograd over the C-ABI)", "adjoint_tol": args.adj_tol,
+                   "medium": "4 FP64 parameter words per cell (slowness, eps, axis x, y); gradients with respect "
+                             "to them from the library" if param else "6 float32 metric words per cell; torch's "
+                             "chain rule from dL/dM",
                    "sources_per_batch": B,
                    "parallelism": "sources split over %d ranks, gradient summed by all-reduce" % world
                    if world > 1 else "single",
@@ -861,6 +906,9 @@ def main():
     ap.add_argument("--adj-tol", type=float, default=1e-12,
                     help="--medium adjoint: backward sweeps stop once one pushes at most this fraction of the "
                          "first sweep's largest push (0: until nothing is pushed)")
+    ap.add_argument("--tti-medium", choices=["param", "metric"], default="param",
+                    help="--medium tti: the FP64 parameter medium (slowness, eps, axis; float64 fields) or six "
+                         "float32 metric arrays")
     ap.add_argument("--medium", choices=["fold", "tti", "batch", "adjoint"], default="fold",
                     help="fold: the reference's drift medium and source (default); tti: the "
                          "heterogeneous tilted-elliptical configuration")

@@ -58,12 +58,14 @@ def homogeneous_tti(nx, ny, nz, vz, eps, tilt_deg, azimuth_deg, device="cpu"):
                                        f(math.cos(th))))
 
 
-def heterogeneous_tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16):
+def heterogeneous_tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, dtype=torch.float64):
     """The seeded heterogeneous medium of heterogeneous_tti() as the FP64
     parameter medium (four float64 arrays, field layout, ghosts copied).
-    The construction runs in float64; each parameter array is padded as soon
-    as it is formed."""
-    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=torch.float64)
+    dtype: working precision of the construction (float64 by default;
+    float32 for grids too large for float64 temporaries, the parameters then
+    being float32 values held in float64).  Each parameter array is padded as
+    soon as it is formed."""
+    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=dtype)
     out = []
     P = params_from(vz, eps, axis)
     del vz, eps, axis

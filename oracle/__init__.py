@@ -92,6 +92,7 @@ class Oracle:
                                           _ptr, _ptr]
         L.orc_ell_adjoint_rec.restype = C.c_long
         L.orc_tti_metric.argtypes = [_ptr, _ptr, _ptr, _ptr, C.c_int64, C.POINTER(C.c_void_p)]
+        L.orc_ell_plane_d.argtypes = list(L.orc_ell_plane.argtypes)
         L.orc_ell_solve_rec_d.argtypes = list(L.orc_ell_solve_rec.argtypes)
         L.orc_ell_solve_rec_d.restype = _int
         L.orc_ell_adjoint_rec_d.argtypes = list(L.orc_ell_adjoint_rec.argtypes)

@@ -764,6 +764,15 @@ void orc_ell_plane_rec(double *T, const float *const *M, unsigned char *W, int n
     orc_ell_plane_m(T, &m, W, nx, ny, nz, dx, dy, dz, dir, src);
 }
 
+/* One plane step with a double metric (the FP64 parameter medium, formed by
+ * orc_tti_metric). */
+void orc_ell_plane_d(double *T, const double *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
+                     int dir, int src)
+{
+    const orc_metric m = {NULL, M};
+    orc_ell_plane_m(T, &m, NULL, nx, ny, nz, dx, dy, dz, dir, src);
+}
+
 void orc_ell_plane(double *T, const float *const *M, int nx, int ny, int nz, double dx, double dy, double dz,
                    int dir, int src)
 {
