@@ -1176,6 +1176,14 @@ static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
     std::vector<int> cnt((size_t)max_steps * n);
     std::vector<long long> offs((size_t)max_steps * n + 1);
     BatchAdjArgs args[6];
+    // The launches of each direction's backward pass: one over every active
+    // instance, except for the x-normal passes, whose planes have no
+    // contiguous axis: there every cell of an instance's plane sits in its
+    // own 32-byte sectors of the field, lambda, pushed amounts and winner
+    // record, which later plane steps reuse only while they stay in L2.  Those
+    // passes run over groups of instances whose sectors fit in kAdjXGroupBytes
+    // of L2 together, one launch per group.
+    std::vector<BatchAdjArgs> launches[6];
     int slots_k[6] = {0, 0, 0, 0, 0, 0};
     auto stage = [&]() -> int {
         for (int dir = 0; dir < 6; ++dir) {
@@ -1220,25 +1228,42 @@ static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
         }
         cudaError_t ce = cudaMemcpyAsync(c->b_stage_d, c->b_stage_h, 6 * c->b_stage_bytes, cudaMemcpyHostToDevice, s);
         if (ce != cudaSuccess) return cuda_error(ce, "batch staging upload");
-        // the six item lists: counts, exclusive scan (step-major, slot-minor), fill
+        // the item lists, one per launch: counts, exclusive scan (step-major, slot-minor), fill
         for (int dir = 0; dir < 6; ++dir) {
+            launches[dir].clear();
             const int k = slots_k[dir];
             if (k == 0) continue;
-            if ((ce = launch_adj_list(args[dir].inst, k, max_steps, c->adj_cnt, nullptr, nullptr, s)) != cudaSuccess ||
-                (ce = cudaMemcpyAsync(cnt.data(), c->adj_cnt, (size_t)max_steps * k * sizeof(int),
-                                      cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-                (ce = cudaStreamSynchronize(s)) != cudaSuccess)
-                return cuda_error(ce, "adjoint item counts");
-            offs[0] = 0;
-            for (size_t q = 0; q < (size_t)max_steps * k; ++q) offs[q + 1] = offs[q] + cnt[q];
-            if (offs[(size_t)max_steps * k] >= (1ll << 32)) return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
-            args[dir].total = (unsigned)offs[(size_t)max_steps * k];
-            if ((ce = cudaMemcpyAsync(c->adj_off, offs.data(), ((size_t)max_steps * k + 1) * sizeof(long long),
-                                      cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-                (ce = launch_adj_list(args[dir].inst, k, max_steps, nullptr, c->adj_off,
-                                      const_cast<unsigned long long *>(args[dir].items), s)) != cudaSuccess ||
-                (ce = cudaStreamSynchronize(s)) != cudaSuccess)  // offs is reused by the next direction
-                return cuda_error(ce, "adjoint item lists");
+            int group = k;
+            if (kDirs[dir].nrm == 0 && kAdjXGroupBytes > 0) {
+                size_t per = 0;  // the largest instance's plane: 4 sectors of 32 bytes per cell
+                for (int i = 0; i < n; ++i)
+                    if (active[i]) per = std::max(per, (size_t)(in[i].grid.ny + 2) * (in[i].grid.nz + 2) * 128);
+                group = (int)std::max<size_t>(1, std::min<size_t>(k, kAdjXGroupBytes / std::max<size_t>(per, 1)));
+            }
+            unsigned long long *items = const_cast<unsigned long long *>(args[dir].items);
+            for (int g0 = 0; g0 < k; g0 += group) {
+                const int kg = std::min(group, k - g0);
+                BatchAdjArgs ga = args[dir];
+                ga.inst = args[dir].inst + g0;
+                ga.items = items;
+                if ((ce = launch_adj_list(ga.inst, kg, max_steps, c->adj_cnt, nullptr, nullptr, s)) != cudaSuccess ||
+                    (ce = cudaMemcpyAsync(cnt.data(), c->adj_cnt, (size_t)max_steps * kg * sizeof(int),
+                                          cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                    (ce = cudaStreamSynchronize(s)) != cudaSuccess)
+                    return cuda_error(ce, "adjoint item counts");
+                offs[0] = 0;
+                for (size_t q = 0; q < (size_t)max_steps * kg; ++q) offs[q + 1] = offs[q] + cnt[q];
+                if (offs[(size_t)max_steps * kg] >= (1ll << 32))
+                    return set_error(FOLD3D_ERR_UNSUPPORTED, "batch too large");
+                ga.total = (unsigned)offs[(size_t)max_steps * kg];
+                if ((ce = cudaMemcpyAsync(c->adj_off, offs.data(), ((size_t)max_steps * kg + 1) * sizeof(long long),
+                                          cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+                    (ce = launch_adj_list(ga.inst, kg, max_steps, nullptr, c->adj_off, items, s)) != cudaSuccess ||
+                    (ce = cudaStreamSynchronize(s)) != cudaSuccess)  // offs is reused by the next list
+                    return cuda_error(ce, "adjoint item lists");
+                items += ga.total;
+                launches[dir].push_back(ga);
+            }
         }
         return FOLD3D_OK;
     };
@@ -1249,12 +1274,15 @@ static int adjoint_batch(fold3d_ctx *c, int n, const AdjInst *in, bool f32, int 
     while (sweep < max_sweeps && left > 0) {
         if ((e = cudaMemsetAsync(c->b_slots, 0, (size_t)n * 8, s)) != cudaSuccess) return cuda_error(e, "memset");
         for (int dir = 5; dir >= 0; --dir) {  // the forward order reversed
-            args[dir].epoch = ++c->epoch;
-            const int grid = (int)std::min<long long>(args[dir].total, (long long)c->sms * c->batch_adj_bps);
-            if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
-                return cuda_error(e, "memset");
-            if (grid > 0 && (e = launch_batch_adj_pass(args[dir], f32, grid, s)) != cudaSuccess)
-                return cuda_error(e, "batched adjoint pass");
+            const unsigned epoch = ++c->epoch;
+            for (BatchAdjArgs &ga : launches[dir]) {
+                ga.epoch = epoch;  // the groups of a pass share its number (their flags are their own)
+                const int grid = (int)std::min<long long>(ga.total, (long long)c->sms * c->batch_adj_bps);
+                if ((e = cudaMemsetAsync(c->b_counters, 0, sizeof(unsigned), s)) != cudaSuccess)
+                    return cuda_error(e, "memset");
+                if (grid > 0 && (e = launch_batch_adj_pass(ga, f32, grid, s)) != cudaSuccess)
+                    return cuda_error(e, "batched adjoint pass");
+            }
         }
         ++sweep;
         if ((e = cudaMemcpyAsync(slots.data(), c->b_slots, (size_t)n * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

@@ -336,6 +336,12 @@ struct BatchAdjArgs {
     unsigned epoch;
 };
 cudaError_t launch_batch_adj_pass(const BatchAdjArgs &b, bool f32, int grid, cudaStream_t s);
+// L2 bytes the instances of one launch of a batched x-normal backward pass
+// may occupy together (0: one launch over every instance); build option.
+#ifndef FOLD3D_ADJ_XGROUP_MB
+#define FOLD3D_ADJ_XGROUP_MB 48
+#endif
+constexpr size_t kAdjXGroupBytes = (size_t)FOLD3D_ADJ_XGROUP_MB << 20;
 // Item list of a backward pass over k instance slots: with off == NULL,
 // cnt[p * k + q] <- tiles with work at step p of slot q; else items[] <- the
 // list, off[p * k + q] being the exclusive prefix of cnt in that order.

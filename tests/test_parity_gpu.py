@@ -881,6 +881,41 @@ def test_batch_records_equal_single_records(f3d, ctx, cuda):
         assert cuda.equal(Wbat, W1)
 
 
+def test_batch_adjoint_grouped_x_passes_match_single_adjoints(f3d, ctx, cuda):
+    """Eight sources in one medium whose x-normal planes are large (300^2
+    cells): the batched adjoint runs its x-normal backward passes over groups
+    of instances (one launch per group, sized to share L2), and every
+    source's lambda and dL/dM still equal its own adjoint's to rounding."""
+    dims = (30, 300, 296)
+    rng = np.random.default_rng(4)
+    srcs = [(int(rng.integers(1, 31)), int(rng.integers(1, 301)), int(rng.integers(1, 297))) for _ in range(8)]
+    import media
+
+    M = media.heterogeneous_tti(*dims, 10.0, seed=23, device="cuda")  # built on the GPU (a flat grid)
+    nx, ny, nz = dims
+    T0 = cuda.full((len(srcs), nz + 2, ny + 2, nx + 2), MAXT, dtype=cuda.float64, device="cuda")
+    for q, (i, j, k) in enumerate(srcs):
+        T0[q, k, j, i] = 0.0
+    S = len(srcs)
+    T = T0.clone()
+    W = cuda.empty(T.shape, dtype=cuda.uint8, device="cuda")
+    f3d.solve_batch(ctx, [T[s] for s in range(S)], [10.0] * S, [M] * S, f3d.opts(max_sweeps=300, tol=0.0),
+                    winners=[W[s] for s in range(S)])
+    r = cuda.zeros_like(T)
+    r[:, 1, 1:-1:7, 1:-1:7] = T[:, 1, 1:-1:7, 1:-1:7] * 0.01
+    shape = tuple(T.shape[1:])
+    lamb = cuda.full_like(T, float("nan"))
+    gb = cuda.full((S, 6) + shape, float("nan"), dtype=cuda.float64, device="cuda")
+    f3d.adjoint_batch(ctx, [T[s] for s in range(S)], [10.0] * S, [M] * S, [W[s] for s in range(S)],
+                      [r[s] for s in range(S)], [lamb[s] for s in range(S)], [gb[s] for s in range(S)])
+    for s in range(S):
+        lam = cuda.empty(shape, dtype=cuda.float64, device="cuda")
+        g = cuda.empty((6,) + shape, dtype=cuda.float64, device="cuda")
+        f3d.adjoint_ellip(ctx, T[s], 10.0, M, W[s], r[s].contiguous(), lam, g)
+        assert cuda.allclose(lamb[s], lam, rtol=1e-12, atol=0), s
+        assert cuda.allclose(gb[s], g, rtol=1e-12, atol=1e-12 * float(g.abs().max())), s
+
+
 def test_batch_adjoint_matches_single_adjoints(f3d, ctx, cuda):
     """fold3d_adjoint_batch equals fold3d_adjoint_ellip per source (to the
     rounding of the atomic sums), and with accumulate its shared dL/dM is the
