@@ -419,11 +419,11 @@ def run_tti(args):
     upd = rep.nominal_updates
     value = world * upd * args.steps / (ms / 1e3) / 1e9
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and n <= 768:  # larger: the pinned copies of field and medium would not fit the host
         hT0 = T0.cpu().pin_memory()
         hM = [m.cpu().pin_memory() for m in M]
         hout = torch.empty_like(hT0).pin_memory()
-        dM = [torch.empty_like(m) for m in M]
+        dM = M  # the medium is uploaded into its own device arrays every step (the same values)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
@@ -560,6 +560,7 @@ def run_batch(args):
     gen_s = time.perf_counter() - t0
     T = [t.clone() for t in T0]
     ctx = f3d.Context(local)
+    f3d.batch_set_config(ctx, *args.batch_config)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     o = f3d.opts(max_sweeps=2000, fixed=False, tol=1e-10, skip=bool(args.skip))
@@ -893,6 +894,9 @@ def main():
                     help="local-solver form (identical results)")
     ap.add_argument("--batch", type=int, default=256, help="instances of --medium batch")
     ap.add_argument("--batch-dims", type=int, nargs=2, default=(96, 320), help="grid size range per axis")
+    ap.add_argument("--batch-config", type=int, nargs=2, default=(0, 0), metavar=("ROWS", "CTAS"),
+                    help="--medium batch: tile rows (2, 4, 8) and CTAs per SM of the batched kernel; 0 0: the "
+                         "library's autotuner (default)")
     ap.add_argument("--adj-size", type=int, default=256, help="grid of --medium adjoint")
     ap.add_argument("--spacing", type=float, default=10.0, help="--medium tti: grid spacing h (m)")
     ap.add_argument("--source", choices=["depth", "top"], default="depth",

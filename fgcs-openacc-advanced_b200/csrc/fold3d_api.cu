@@ -938,12 +938,14 @@ static int batch_occupancy_of(fold3d_ctx *c, bool f32, int tv)
 
 // The batch autotuner.  For a size mix it has not seen (number of instances,
 // total and largest extent, field type), it times one full sweep of each
-// candidate configuration -- tile heights of 2, 4 and 8 rows (64, 128 and 256
-// threads per CTA), each at its occupancy limit of resident CTAs per SM and
-// at three quarters of it -- on copies of up to four instances of median
-// size (the caller's fields are not touched), and keeps the fastest for the
-// size mix.  Every configuration gives the same results bit for bit; they
-// differ only in speed.
+// candidate tile height -- 2, 4 and 8 rows (64, 128 and 256 threads per CTA),
+// each at its occupancy limit of resident CTAs per SM -- on copies of
+// instances of median size, as many as it takes to give every resident CTA
+// work (at least kTuneCells cells; the caller's fields are not touched), and
+// keeps the fastest for the size mix.  Every configuration gives the same
+// results bit for bit; they differ only in speed.  (Fewer resident CTAs than
+// the limit were candidates too, but on a sample they won where the whole
+// batch then ran slower, and they never won on a whole batch.)
 static int batch_config(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cudaStream_t s, int &tv, int &bps)
 {
     if (!c->sms) {
@@ -978,11 +980,16 @@ static int batch_config(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cud
         bps = hit->second.second;
         return FOLD3D_OK;
     }
-    // up to four instances around the median size, on copies of their fields
+    // instances around the median size, enough to fill the GPU, on copies of their fields
     std::sort(by_size.begin(), by_size.end());
-    const int k = std::min(4, n), first = std::max(0, n / 2 - k / 2);
+    constexpr size_t kTuneCells = (size_t)64 << 20;
+    int lo = n / 2, hi = n / 2;  // the sample: sorted positions [lo, hi), grown around the median
     size_t cells = 0;
-    for (int q = 0; q < k; ++q) cells += by_size[first + q].first;
+    while (hi - lo < n && cells < kTuneCells) {
+        if (hi < n && ((hi - lo) % 2 == 0 || lo == 0)) cells += by_size[hi++].first;
+        else cells += by_size[--lo].first;
+    }
+    const int k = hi - lo, first = lo;
     const size_t esz = f32 ? sizeof(float) : sizeof(double);
     cudaError_t e;
     if (c->tune_cells * sizeof(double) < cells * esz) {
@@ -1012,21 +1019,19 @@ static int batch_config(fold3d_ctx *c, int n, const SolveInst *in, bool f32, cud
     tv = kWaveTV;
     bps = batch_occupancy_of(c, f32, tv);
     for (int ctv : {2, 4, 8}) {
-        const int occ = batch_occupancy_of(c, f32, ctv);
-        for (int cb : {occ, std::max(1, (3 * occ) / 4)}) {
-            for (int q = 0; q < k; ++q) {
-                const SolveInst &src = in[by_size[first + q].second];
-                const size_t bytes = field_cells(src.grid) * esz;
-                if ((e = cudaMemcpyAsync(sub[q].T, src.T, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
-                    return cuda_error(e, "batch autotuner");
-            }
-            int rc = solve_batch_cfg(c, k, sub.data(), f32, one, s, r.data(), ctv, cb);
-            if (rc) return rc;
-            if (r[0].elapsed_ms < best) {
-                best = r[0].elapsed_ms;
-                tv = ctv;
-                bps = cb;
-            }
+        const int cb = batch_occupancy_of(c, f32, ctv);
+        for (int q = 0; q < k; ++q) {
+            const SolveInst &src = in[by_size[first + q].second];
+            const size_t bytes = field_cells(src.grid) * esz;
+            if ((e = cudaMemcpyAsync(sub[q].T, src.T, bytes, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                return cuda_error(e, "batch autotuner");
+        }
+        int rc = solve_batch_cfg(c, k, sub.data(), f32, one, s, r.data(), ctv, cb);
+        if (rc) return rc;
+        if (r[0].elapsed_ms < best) {
+            best = r[0].elapsed_ms;
+            tv = ctv;
+            bps = cb;
         }
     }
     c->tuned[key] = {tv, bps};

@@ -100,6 +100,13 @@ enum Variant {
 #endif
 constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 
+// Single-solve dataflow passes over large planes: each warp owns whole items
+// (1), or the CTA's warps share each item's rows (0); build option.
+#ifndef FOLD3D_WAVE_WARP_ITEMS
+#define FOLD3D_WAVE_WARP_ITEMS 1
+#endif
+constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
+
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4
 #endif

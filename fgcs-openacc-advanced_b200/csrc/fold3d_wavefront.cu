@@ -181,6 +181,107 @@ __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
     return true;
 }
 
+// The same work item done by one warp alone: its 32 lanes take the tile's
+// rows one after the other, lanes 0..8 watch the nine neighbour flags, and
+// lane 0 publishes after a __syncwarp (which orders every lane's stores
+// before lane 0's release store).  The warps of a CTA each own their items,
+// so none waits at a CTA barrier for the slowest row of another's.
+template <int MED, class R, int TV = kWaveTV>
+__device__ __forceinline__ bool wave_item_warp(R *__restrict__ T, const WaveArgs &a,
+                                               const typename WaveMedium<MED>::type &tab, int item, double &dmax,
+                                               unsigned long long &evaluated)
+{
+    const int lane = threadIdx.x & 31;
+    const PlaneGeom &g = a.pg;
+    const int ntiles = a.ntu * a.ntv;
+    const unsigned want = a.epoch << 1;  // flags hold (pass << 1) | changed
+    const bool may_skip = a.epoch >= a.skip_from;
+    const int p = item / ntiles, t = item - p * ntiles;
+    const int tu = t % a.ntu, tv = t / a.ntu;
+    const int src = a.first_src + p * a.sg;
+    const int tgt = src + a.sg;
+
+    int timed_out = 0, recent = 0;
+    if (lane < 9) {
+        const int nu = tu + lane % 3 - 1, nv = tv + lane / 3 - 1;
+        if (nu >= 0 && nu < a.ntu && nv >= 0 && nv < a.ntv) {
+            const int nt = nv * a.ntu + nu;
+            if (may_skip) recent = (__ldcg(a.mod[a.nrm] + (long long)src * ntiles + nt) + 5u >= a.epoch);
+            if (p > 0) {
+                const unsigned *fl = a.flags + (long long)(p - 1) * ntiles + nt;
+                const unsigned long long t0 = global_ns();
+                unsigned spins = 0, f;
+                while ((f = ld_acquire(fl)) < want) {
+                    if (++spins > (1u << 26) || global_ns() - t0 > a.timeout_ns ||
+                        *(volatile unsigned *)a.status != 0) {
+                        atomicCAS(a.status, 0u, 1u);  // FOLD3D_ERR_TIMEOUT
+                        timed_out = 1;
+                        break;
+                    }
+                    if (kPollNs) __nanosleep(kPollNs);
+                }
+                if (!timed_out) recent |= (int)(f & 1u);
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, timed_out)) return false;
+    const bool skip = may_skip && !__any_sync(0xffffffffu, recent);
+
+    int changed = 0;
+    if (!skip) {
+        const int u = tu * 32 + lane + 1;
+        for (int r = 0; r < TV; ++r) {
+            const int v = tv * TV + r + 1;
+            if (u <= g.nu && v <= g.nv) {
+                const long long s = (long long)src * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
+                const long long d = s + g.sn;
+                const R st = fabs(ld_cg(T + s));
+                const R xt = fabs(ld_cg(T + s + g.sx));
+                const R yt = fabs(ld_cg(T + s + g.sy));
+                const R xnt = fabs(ld_cg(T + s - g.sx));
+                const R ynt = fabs(ld_cg(T + s - g.sy));
+                const R txm = fabs(ld_cg(T + s + g.sx - g.sy));
+                const R txy = fabs(ld_cg(T + s + g.sx + g.sy));
+                const R tym = fabs(ld_cg(T + s - g.sx + g.sy));
+                const R txnyn = fabs(ld_cg(T + s - g.sx - g.sy));
+                const R told = ld_cg(T + d);
+                R tnew;
+                if constexpr (MED == kMediumDrift) {
+                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                } else {
+                    const R nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
+                    int win;
+                    tnew = point_update_ellip(told, st, nb, ell_local<R>(tab.med, tab.dir, d), win);
+                    if (a.winners && bits_differ(tnew, told))
+                        a.winners[d] =
+                            (win < 0) ? (unsigned char)kNoWinner : (unsigned char)(a.dir * kEllipCands + win);
+                }
+                if (bits_differ(tnew, told)) {
+                    T[d] = tnew;
+                    changed = 1;
+                    dmax = fmax(dmax, (double)fabs(tnew - told));
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {  // the point's tile in the two other orientations
+                        const int b = (q == 0) ? a.ua : a.va;
+                        const int ub = (b == 0) ? 1 : 0, vb = (b == 2) ? 1 : 2;
+                        const int cb = (q == 0) ? u : v;
+                        const int cu = (ub == a.nrm) ? tgt : (ub == a.ua) ? u : v;
+                        const int cv = (vb == a.nrm) ? tgt : (vb == a.ua) ? u : v;
+                        const int tile = ((cv - 1) / TV) * a.mod_ntu[b] + ((cu - 1) >> 5);
+                        a.mod[b][(long long)cb * a.mod_ntiles[b] + tile] = a.epoch;
+                    }
+                }
+                ++evaluated;
+            }
+        }
+        changed = __any_sync(0xffffffffu, changed);
+        if (changed && lane == 0) a.mod[a.nrm][(long long)tgt * ntiles + t] = a.epoch;
+    }
+    __syncwarp();
+    if (lane == 0) st_release(a.flags + item, want | (unsigned)changed);
+    return true;
+}
+
 // Block-wide maximum of d into *out (IEEE bits) and sum of e into *sum.
 template <int TV = kWaveTV>
 __device__ __forceinline__ void wave_flush(double d, unsigned long long e, unsigned long long *out,
@@ -213,6 +314,32 @@ __global__ void __launch_bounds__(kWaveThreads, (wave_min_blocks<MED, R, LARGE>(
     const long long total = (long long)a.steps * a.ntu * a.ntv;
     double dmax = 0.0;
     unsigned long long evaluated = 0;
+    if constexpr (kWaveWarpItems && LARGE) {
+        // large planes: every warp claims and processes its own items
+        // (wave_item_warp).  A plane then has enough tiles to keep all warps
+        // busy, and no warp waits at a CTA barrier for another's row.  On
+        // smaller planes the plane-to-plane chain binds instead, and an item
+        // shared by the CTA's warps (each one row) finishes sooner.
+        const int lane = threadIdx.x & 31;
+        int item = -1;
+        if (lane == 0) {
+            const unsigned w = atomicAdd(a.work, 1u);
+            item = (w < total) ? (int)w : -1;
+        }
+        item = __shfl_sync(0xffffffffu, item, 0);
+        while (item >= 0) {
+            int next = -1;  // claimed now, processed after this one
+            if (lane == 0 && *(volatile unsigned *)a.status == 0) {
+                const unsigned w = atomicAdd(a.work, 1u);
+                if (w < total) next = (int)w;
+            }
+            next = __shfl_sync(0xffffffffu, next, 0);
+            if (!wave_item_warp<MED, R>(T, a, tab, item, dmax, evaluated)) break;
+            item = next;
+        }
+        wave_flush(dmax, evaluated, a.maxd, a.evaluated);
+        return;
+    }
     if (threadIdx.x == 0) {
         const unsigned w = atomicAdd(a.work, 1u);
         s_next = (w < total) ? (int)w : -1;
@@ -253,14 +380,21 @@ __global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_ke
 {
     __shared__ int s_next;
     __shared__ int s_loc[2];
+    __shared__ int s_cur;  // the active slot staged in s_inst, -1 for none
     __shared__ BatchInst s_inst;
     const unsigned total = *b.total;
     const unsigned epoch = *b.epoch_base + (unsigned)b.dir + 1u;
     if (threadIdx.x == 0) {
         const unsigned w = atomicAdd(b.work, 1u);
         s_next = (w < total) ? (int)w : -1;
+        s_cur = -1;
     }
     __syncthreads();
+    // Consecutive items mostly belong to one instance (its tiles of a step
+    // come together): the instance stays staged, and its largest change and
+    // evaluated points are flushed only when the CTA moves to another one.
+    double dmax = 0.0;
+    unsigned long long evaluated = 0;
     for (;;) {
         const int gitem = s_next;
         if (gitem < 0) break;
@@ -275,24 +409,28 @@ __global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_ke
             batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, gitem, s_loc[0], s_loc[1]);
         }
         __syncthreads();
-        {
+        if (s_loc[0] != s_cur) {  // the same for every thread
+            if (s_cur >= 0) {
+                wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
+                dmax = 0.0;
+                evaluated = 0;
+            }
             const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + b.act[s_loc[0]]);
             unsigned *dst = reinterpret_cast<unsigned *>(&s_inst);
             for (int w = threadIdx.x; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            if (threadIdx.x == 0) {  // the pass number is per launch, not per staged instance
+                s_inst.a.epoch = epoch;
+                s_inst.a.skip_from = b.skip_from;
+                s_cur = s_loc[0];
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {  // the pass number is per launch, not per staged instance
-            s_inst.a.epoch = epoch;
-            s_inst.a.skip_from = b.skip_from;
-        }
-        __syncthreads();
-        double dmax = 0.0;
-        unsigned long long evaluated = 0;
         if (!wave_item<kMediumEllip, R, TV>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[1], dmax,
                                             evaluated))
             break;
-        wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
     }
+    if (s_cur >= 0) wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
 }
 
 // The batch's state after a sweep and the next sweep's tables (BatchCtl).

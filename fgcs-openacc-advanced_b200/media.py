@@ -65,13 +65,27 @@ def heterogeneous_tti_params(nx, ny, nz, h, seed=0, device="cpu", anomalies=16, 
     float32 for grids too large for float64 temporaries, the parameters then
     being float32 values held in float64).  Each parameter array is padded as
     soon as it is formed."""
-    vz, eps, axis = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=dtype)
-    out = []
-    P = params_from(vz, eps, axis)
-    del vz, eps, axis
-    while P:
-        out.append(_pad(P.pop(0)))
-    return out
+    vz, eps, (ax, ay, az) = tti_params(nx, ny, nz, h, seed, device, anomalies, dtype=dtype)
+    # one parameter at a time, each padded as soon as it is formed and its
+    # inputs freed: the peak stays near the construction's own (params_from's
+    # arithmetic, in the working precision, then float64)
+    s = _pad((1.0 / vz).to(torch.float64))
+    del vz
+    e = _pad(eps.to(torch.float64))
+    del eps
+    nn = torch.sqrt(ax * ax + ay * ay + az * az)
+    sg = torch.where(az < 0, -1.0, 1.0).to(nn.dtype)
+    del az
+    nn.reciprocal_().mul_(sg)
+    del sg
+    ax.mul_(nn)
+    ay.mul_(nn)
+    del nn
+    nx_ = _pad(ax.to(torch.float64))
+    del ax
+    ny_ = _pad(ay.to(torch.float64))
+    del ay
+    return [s, e, nx_, ny_]
 
 
 def _pad(t):
