@@ -922,6 +922,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=4.0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--prof-nz", type=int, default=0,
+                    help="with --prof-sweep: planes along z (the grid is size x size x prof-nz), to profile the "
+                         "kernels of large z-normal planes on a small field")
     ap.add_argument("--prof-sweep", type=int, default=0,
                     help="profiling aid: run sweeps 1..S-1, then sweep S inside a CUDA profiler range "
                          "(for ncu --profile-from-start off), then exit")
@@ -958,8 +961,9 @@ def main():
     ctx = f3d.Context(local)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    shape = (n + 2,) * 3
-    large = load_large_digests()
+    nz = args.prof_nz if (args.prof_sweep > 0 and args.prof_nz > 0) else n
+    shape = (nz + 2, n + 2, n + 2)
+    large = load_large_digests() if nz == n else {}
     parity = {}
 
     # the initial field: the reference's ImplicitInitialiser built on the
@@ -976,7 +980,7 @@ def main():
     init_s = None
     if ("n%d_init" % n) in large:
         parity["init_reference_digest"] = "match" if sha256_of(T0_host) == large["n%d_init" % n] else "MISMATCH"
-    elif n <= 640:  # against the host initialiser (pinned to the reference by the tests)
+    elif n <= 640 and nz == n:  # against the host initialiser (pinned to the reference by the tests)
         t0 = time.perf_counter()
         Th = f3d.init_implicit(n, n, n, h)
         init_s = time.perf_counter() - t0

@@ -107,6 +107,13 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
 
+// Batched passes: each warp owns whole items (1), or the CTA's warps share
+// each item's rows (0); build option.
+#ifndef FOLD3D_BATCH_WARP_ITEMS
+#define FOLD3D_BATCH_WARP_ITEMS 0
+#endif
+constexpr bool kBatchWarpItems = FOLD3D_BATCH_WARP_ITEMS != 0;
+
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4
 #endif
