@@ -53,6 +53,10 @@ for _p in (ROOT, PKG):
 PUBLISHED_S = {512: 3.037851, 1280: 35.163471}  # plots/perfect-2-gpu.py:24 (V2, A100, 8 sweeps)
 REF_F, REF_A = 1.1, (-0.35, 0.4, 0.7)
 BYTES_PER_UPDATE = 16  # read old target + write new target, FP64; medium is constant (m = 0)
+# DRAM bytes (read + write) per update of wave_pass_kernel<drift>, from an ncu
+# capture of the x_down, x_up and k_up passes of one sweep at 512^3 without
+# tile skipping: 4.1662 GB over 3 x 511 x 512^2 updates
+WAVE_DRAM_BYTES_PER_UPDATE = 4166210304 / (3 * 511 * 512 * 512)
 
 
 def load_large_digests():
@@ -1080,17 +1084,31 @@ def main():
     alg_bytes = BYTES_PER_UPDATE * upd
     launches = launches_per_step * args.steps
     achieved = alg_bytes / (solve_ms / 1e3) / 1e9
-    # DRAM bytes (read + write) of one pass from an ncu capture of this workload
-    # (profiles/wave_pass_kernel_fold512_dram.md); other sizes: not measured
-    traffic = 1090855424 + 178331648 if (n == 512 and rep.engine == f3d.ENGINE_WAVEFRONT) else None
+    # DRAM bytes per launch: the bytes per update that ncu measured for this
+    # kernel (profiles/wave_pass_kernel_fold512_full.md) times this launch's
+    # updates, and the FP64 pipe's share of the active cycles from the capture
+    # of the same code path (512^2 planes: CTA items; 1280^2 planes: warp
+    # items, profiles/wave_pass_kernel_fold1280_planes.md)
+    wave = rep.engine == f3d.ENGINE_WAVEFRONT
+    upd_launch = upd / launches_per_step
+    traffic = WAVE_DRAM_BYTES_PER_UPDATE * upd_launch if wave else None
+    large_planes = n * n >= 8192 * 128
+    fp64 = None
+    if wave:
+        fp64 = ({"pct_of_active_cycles": 35.0, "issue_active_pct": 71.9,
+                 "capture": "k_up pass over 1280^2 planes (1280x1280x16 grid, sweep 2)"} if large_planes else
+                {"pct_of_active_cycles": 30.5, "issue_active_pct": 50.9,
+                 "capture": "x_down, x_up, k_up passes of sweep 3 at 512^3 (mean)"})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "plane_kernel" if rep.engine == f3d.ENGINE_PLANES else "wavefront_kernel",
+                "kernel": "plane_kernel" if rep.engine == f3d.ENGINE_PLANES else "wave_pass_kernel<drift>",
                 "alg_bytes_per_launch": alg_bytes / launches_per_step,
                 "avg_launch_us": solve_ms * 1e3 / launches_per_step,
-                "note": "FP64-ALU bound: ~100 FLOP per 16 B",
-                "traffic_note": "one pass's DRAM bytes from an ncu capture of the kernel before it skipped "
-                                "solver bodies; every point still loads the same ten values" if traffic else None}
+                "note": "FP64 latency bound, not HBM bound: ~100 dependent FP64 operations per 16 B",
+                "fp64_pipe": fp64,
+                "traffic_note": ("ncu's %.2f DRAM bytes per update (512^3, three passes of a sweep without tile "
+                                 "skipping) x %.4g updates per launch; each target is read once, the source "
+                                 "plane comes from L2" % (WAVE_DRAM_BYTES_PER_UPDATE, upd_launch)) if wave else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
