@@ -107,12 +107,14 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
 
-// Batched passes: each warp owns whole items (1), or the CTA's warps share
-// each item's rows (0); build option.
-#ifndef FOLD3D_BATCH_WARP_ITEMS
-#define FOLD3D_BATCH_WARP_ITEMS 0
+// Warp-owned items of the drift medium: mark the call sites that could still
+// lower the time first and run only those (1), or test every site in turn
+// (0); build option.  Without CTA barriers, a warp's uneven work costs no
+// other warp a wait.
+#ifndef FOLD3D_WARP_SITE_MASK
+#define FOLD3D_WARP_SITE_MASK 0
 #endif
-constexpr bool kBatchWarpItems = FOLD3D_BATCH_WARP_ITEMS != 0;
+constexpr bool kWarpSiteMask = FOLD3D_WARP_SITE_MASK != 0;
 
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4

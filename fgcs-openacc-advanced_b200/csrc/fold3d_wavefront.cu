@@ -247,7 +247,7 @@ __device__ __forceinline__ bool wave_item_warp(R *__restrict__ T, const WaveArgs
                 const R told = ld_cg(T + d);
                 R tnew;
                 if constexpr (MED == kMediumDrift) {
-                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                    tnew = point_update_fast<kWarpSiteMask>(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
                 } else {
                     const R nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
                     int win;
@@ -435,79 +435,6 @@ __global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_ke
     if (s_cur >= 0) wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
 }
 
-// The batched pass with each warp owning its items (FOLD3D_BATCH_WARP_ITEMS):
-// every warp claims, locates and processes its own items (wave_item_warp),
-// with its own staged instance, so no warp waits at a CTA barrier for
-// another's item.
-template <class R, int TV>
-__global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_warp_kernel(BatchArgs b)
-{
-    __shared__ BatchInst s_inst[TV];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    BatchInst &wi = s_inst[warp];
-    const unsigned total = *b.total;
-    const unsigned epoch = *b.epoch_base + (unsigned)b.dir + 1u;
-    int cur = -1;  // the active slot staged in wi
-    double dmax = 0.0;
-    unsigned long long evaluated = 0;
-    int item = -1;
-    if (lane == 0) {
-        const unsigned w = atomicAdd(b.work, 1u);
-        item = (w < total) ? (int)w : -1;
-    }
-    item = __shfl_sync(0xffffffffu, item, 0);
-    while (item >= 0) {
-        int next = -1, slot = 0, local = 0;
-        if (lane == 0) {
-            if (*(volatile unsigned *)b.status == 0) {
-                const unsigned w = atomicAdd(b.work, 1u);
-                if (w < total) next = (int)w;
-            }
-            batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, item, slot, local);
-        }
-        next = __shfl_sync(0xffffffffu, next, 0);
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        local = __shfl_sync(0xffffffffu, local, 0);
-        if (slot != cur) {
-            if (cur >= 0) {  // this warp's share of the previous instance's maximum and count
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-                if (lane == 0) {
-                    if (evaluated) atomicAdd(wi.a.evaluated, evaluated);
-                    if (dmax > 0.0) atomicMax(wi.a.maxd, (unsigned long long)__double_as_longlong(dmax));
-                }
-                dmax = 0.0;
-                evaluated = 0;
-            }
-            __syncwarp();
-            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + b.act[slot]);
-            unsigned *dst = reinterpret_cast<unsigned *>(&wi);
-            for (int w = lane; w < (int)(sizeof(BatchInst) / 4); w += 32) dst[w] = src[w];
-            __syncwarp();
-            if (lane == 0) {  // the pass number is per launch, not per staged instance
-                wi.a.epoch = epoch;
-                wi.a.skip_from = b.skip_from;
-            }
-            __syncwarp();
-            cur = slot;
-        }
-        if (!wave_item_warp<kMediumEllip, R, TV>(static_cast<R *>(wi.T), wi.a, wi.p, local, dmax, evaluated)) break;
-        item = next;
-    }
-    if (cur >= 0) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-        if (lane == 0) {
-            if (evaluated) atomicAdd(wi.a.evaluated, evaluated);
-            if (dmax > 0.0) atomicMax(wi.a.maxd, (unsigned long long)__double_as_longlong(dmax));
-        }
-    }
-}
-
 // The batch's state after a sweep and the next sweep's tables (BatchCtl).
 // One block: the instances are folded in parallel, then one thread per
 // direction rebuilds that direction's tables (a few thousand steps).
@@ -563,13 +490,8 @@ cudaError_t launch_batch_restage(const BatchCtl &ctl, bool first, cudaStream_t s
 
 template <int TV> static cudaError_t launch_batch_tv(const BatchArgs &b, bool f32, int grid, cudaStream_t s)
 {
-    if constexpr (kBatchWarpItems) {
-        if (f32) batch_pass_warp_kernel<float, TV><<<grid, 32 * TV, 0, s>>>(b);
-        else batch_pass_warp_kernel<double, TV><<<grid, 32 * TV, 0, s>>>(b);
-    } else {
-        if (f32) batch_pass_kernel<float, TV><<<grid, 32 * TV, 0, s>>>(b);
-        else batch_pass_kernel<double, TV><<<grid, 32 * TV, 0, s>>>(b);
-    }
+    if (f32) batch_pass_kernel<float, TV><<<grid, 32 * TV, 0, s>>>(b);
+    else batch_pass_kernel<double, TV><<<grid, 32 * TV, 0, s>>>(b);
     return cudaGetLastError();
 }
 
@@ -586,13 +508,9 @@ cudaError_t launch_batch_pass(const BatchArgs &b, bool f32, int tv, int grid, cu
 template <int TV> static int batch_occupancy(bool f32)
 {
     int n = 0;
-    cudaError_t e;
-    if constexpr (kBatchWarpItems)
-        e = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_warp_kernel<float, TV>, 32 * TV, 0)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_warp_kernel<double, TV>, 32 * TV, 0);
-    else
-        e = f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<float, TV>, 32 * TV, 0)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<double, TV>, 32 * TV, 0);
+    const cudaError_t e =
+        f32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<float, TV>, 32 * TV, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_pass_kernel<double, TV>, 32 * TV, 0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
