@@ -195,21 +195,23 @@ def over_ranks(vals, dist, op, device="cuda"):
     return t.tolist()
 
 
-def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None):
-    """Time the reference's own sweep functions (oracle/_ref, OpenMP
-    transform on `threads` cores) on the first planes of each of the six
-    passes of sweep 1, starting from T0.  Returns (updates/s, info)."""
+def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None, omp=True):
+    """Time the reference's own sweep functions (oracle/_ref: the OpenMP
+    transform on `threads` cores, or with omp=False the unmodified build,
+    whose OpenACC regions run on one host thread) on the first planes of each
+    of the six passes of sweep 1, starting from T0.  Returns (updates/s,
+    info)."""
     import numpy as np
 
     from oracle import RefLib, build
 
-    if threads:
+    if threads and omp:
         os.environ["OMP_NUM_THREADS"] = str(threads)
-    path = build.ref_lib_path(n, omp=True)
+    path = build.ref_lib_path(n, omp=omp)
     kind = "reference"
     if not os.path.exists(path):
         raise RuntimeError("reference host build missing: %s" % path)
-    r = RefLib(n, omp=True)
+    r = RefLib(n, omp=omp)
     if planes is None:  # calibrate: one plane of x_down
         T = np.array(T0, copy=True)
         t = time.perf_counter()
@@ -225,11 +227,22 @@ def reference_cpu_sample(T0, n, seconds=None, planes=None, threads=None):
             r.plane(T, d, first + step * p)
     dt = time.perf_counter() - t
     upd = 6 * planes * n * n
-    info = {"kind": kind, "cores": int(os.environ.get("OMP_NUM_THREADS", host_threads())),
+    info = {"kind": kind, "cores": int(os.environ.get("OMP_NUM_THREADS", host_threads())) if omp else 1,
             "sample": "%d planes of each of the 6 passes of sweep 1 at %d^3 (%d updates), reference "
-                      "AN_ISO_1_OpenACC.c host build, OpenMP transform" % (planes, n, upd),
+                      "AN_ISO_1_OpenACC.c host build, %s" % (
+                          planes, n, upd, "OpenMP transform" if omp else "unmodified (one thread)"),
             "seconds": dt, "planes": planes}
     return upd / dt, info
+
+
+def single_thread_reference(T0, n, seconds=3.0):
+    """The unmodified reference build's rate on one host thread, over a short
+    sample, for the line's cpu_baseline ({} if unavailable)."""
+    try:
+        rate, info = reference_cpu_sample(T0, n, seconds=seconds, omp=False)
+        return {"single_thread_value": rate / 1e9, "single_thread_sample": info["sample"]}
+    except Exception as e:
+        return {"single_thread_value": None, "single_thread_sample": "unavailable: %s" % str(e).splitlines()[0]}
 
 
 def run_reference(args):
@@ -284,7 +297,7 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic: reference implicit-surface source",
         "config": workload_config(args),
         "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": info["cores"], "kind": "reference",
-                         "sample": info["sample"] + "; " + setup},
+                         "sample": info["sample"] + "; " + setup} | single_thread_reference(T0, n),
         "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -1115,7 +1128,7 @@ def main():
         try:
             rate, info = reference_cpu_sample(T0_pin.numpy(), n, seconds=args.cpu_seconds, threads=host_threads())
             cpu = {"value": rate / 1e9, "unit": "Gcell-updates/s", "cores": info["cores"], "kind": info["kind"],
-                   "sample": info["sample"]}
+                   "sample": info["sample"]} | single_thread_reference(T0_pin.numpy(), n)
         except Exception as e:
             cpu = {"value": None, "unit": "Gcell-updates/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % str(e).splitlines()[0]}

@@ -272,10 +272,19 @@ __host__ __device__ __forceinline__ double point_update_fast(double told, double
     if (st < tn && t.d1_ok) tn = kmin(tn, st + t.K1);
     if (!(tn < st && tn < kmin(xt, yt) && tn < kmin(txy, txm) && tn < kmin(txnyn, tym))) {
         if constexpr (MASK) {
-            unsigned todo = live_sites(tn, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, t);
+            const unsigned mine = live_sites(tn, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, t);
+#ifdef __CUDA_ARCH__
+            // the converged lanes of a warp walk the union of their sites
+            // together, each lane running only its own, so that the lanes
+            // stay on one site at a time
+            unsigned todo = __reduce_or_sync(__activemask(), mine);
+#else
+            unsigned todo = mine;
+#endif
             while (todo) {
                 const int k = low_bit(todo);
                 todo &= todo - 1;
+                if (!((mine >> k) & 1u)) continue;
                 if (k < 8) {
                     const double s1 = (k < 2) ? xt : (k < 4) ? xnt : (k < 6) ? ynt : yt;
                     const int m = k & 3;

@@ -56,6 +56,28 @@ def test_reference_arm_runs_on_rank_0_only():
     assert p.stdout.strip() == ""
 
 
+def test_reference_arm_line_on_a_small_grid():
+    """The reference arm's JSON line at 64^3: the OpenMP transform's rate as
+    the value, the unmodified one-thread build's rate beside it."""
+    import json
+
+    env = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        env.pop(k, None)
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--size", "64",
+                        "--steps", "1", "--warmup", "0", "--ref-seconds", "0.5"], env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    line = json.loads(p.stdout.strip().splitlines()[-1])
+    if "unavailable" in line:
+        pytest.skip(line["unavailable"])
+    assert line["impl"] == "reference" and line["value"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == line["value"]
+    assert cb["single_thread_value"] > 0 and "unmodified" in cb["single_thread_sample"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
 def test_oracle_sample_times_the_elliptical_statement():
     """bench.py's CPU sample of the elliptical statement: runs the first
     sweep of small instances (float64 and float32) and counts their updates."""
