@@ -201,68 +201,8 @@ __host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1
     if (tn > kmin(s1, s2) && !(k.nblock && s1 > s2)) edge_k(tn, s1, s2, k.nest, t.F);
 }
 
-// Lowest set bit of a non-zero mask.
-__host__ __device__ __forceinline__ int low_bit(unsigned m)
-{
-#ifdef __CUDA_ARCH__
-    return __ffs(m) - 1;
-#else
-    return __builtin_ctz(m);
-#endif
-}
-
-// The sixteen call sites that could still lower a time bounded by tb (5.
-// below), bit k for FoldSurf3Points call k, bit 8 + k for FoldEdge2Points
-// call k.
-__host__ __device__ __forceinline__ unsigned live_sites(double tb, double st, double xt, double yt, double xnt,
-                                                        double ynt, double txy, double txm, double tym,
-                                                        double txnyn, const SideTable &t)
-{
-    unsigned todo = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double s1 = (k < 2) ? xt : (k < 4) ? xnt : (k < 6) ? ynt : yt;
-        const int m = k & 3;
-        const double s2 = (m == 0) ? ((k < 4) ? txy : txnyn)
-                        : (m == 1) ? txm
-                        : (m == 2) ? ((k < 4) ? txnyn : txy)
-                                   : tym;
-        const SurfK &K = t.surf[k];
-        const double mn = kmin(st, kmin(s1, s2));
-        const bool entry = !(tb < mn || (K.e1 && s1 > st) || (K.e2 && s2 > s1));
-        const bool body = !(tb <= mn + K.B);
-        const double mn2 = kmin(s2, s1);  // the nested FoldEdge2Points on (s1, s2)
-        const bool nest = tb > mn2 && !(K.nblock && s1 > s2) && !(K.nest.early && s2 > s1) &&
-                          (!(tb <= mn2 + K.nest.B) || (K.nest.fb_ok && s2 + K.nest.K < tb));
-        if (entry && (body || nest)) todo |= 1u << k;
-    }
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double s1 = (k == 0) ? xt : (k == 1) ? txy : (k == 2) ? yt : (k == 3) ? tym
-                        : (k == 4) ? xnt : (k == 5) ? txnyn : (k == 6) ? ynt : txm;
-        const EdgeK &E = t.edge[k];
-        const double mn = kmin(s1, st);
-        const bool entry = !(tb < mn || (E.early && s1 > st));
-        if (entry && (!(tb <= mn + E.B) || (E.fb_ok && s1 + E.K < tb))) todo |= 1u << (8 + k);
-    }
-    return todo;
-}
-
 // New signed value of a target whose stored value is `told`, from the nine
 // previous-plane magnitudes (named as in the reference, :195-204).
-//
-// 5. With MASK, one straight-line pass over all sixteen call sites
-//    (constants at fixed table offsets, no dependence between sites) first
-//    marks the sites that could still change the time, judged with the time
-//    after the 1-D candidate, which bounds the running time at every site
-//    from above: a site is left out when its entry test returns (:71, :132),
-//    its body is gated off (3. and 4. above) and neither its nested edge
-//    (:170) nor its fall-back (:99-113) could go below that bound.  Each of
-//    those tests only gets truer as the time falls, so a site left out would
-//    have changed nothing; the marked sites then run in the reference's
-//    order, with every test applied to the running time.  Fewer instructions
-//    per point, but a point's work depends more on its data.
-template <bool MASK = false>
 __host__ __device__ __forceinline__ double point_update_fast(double told, double st, double xt, double yt,
                                                              double xnt, double ynt, double txy, double txm,
                                                              double tym, double txnyn, const DirTable *tab)
@@ -271,37 +211,6 @@ __host__ __device__ __forceinline__ double point_update_fast(double told, double
     const SideTable &t = tab->side[told < 0 ? 1 : 0];
     if (st < tn && t.d1_ok) tn = kmin(tn, st + t.K1);
     if (!(tn < st && tn < kmin(xt, yt) && tn < kmin(txy, txm) && tn < kmin(txnyn, tym))) {
-        if constexpr (MASK) {
-            const unsigned mine = live_sites(tn, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, t);
-#ifdef __CUDA_ARCH__
-            // the converged lanes of a warp walk the union of their sites
-            // together, each lane running only its own, so that the lanes
-            // stay on one site at a time
-            unsigned todo = __reduce_or_sync(__activemask(), mine);
-#else
-            unsigned todo = mine;
-#endif
-            while (todo) {
-                const int k = low_bit(todo);
-                todo &= todo - 1;
-                if (!((mine >> k) & 1u)) continue;
-                if (k < 8) {
-                    const double s1 = (k < 2) ? xt : (k < 4) ? xnt : (k < 6) ? ynt : yt;
-                    const int m = k & 3;
-                    const double s2 = (m == 0) ? ((k < 4) ? txy : txnyn)
-                                    : (m == 1) ? txm
-                                    : (m == 2) ? ((k < 4) ? txnyn : txy)
-                                               : tym;
-                    surf_k(tn, st, s1, s2, t.surf[k], t);
-                } else {
-                    const int e = k - 8;
-                    const double s1 = (e == 0) ? xt : (e == 1) ? txy : (e == 2) ? yt : (e == 3) ? tym
-                                    : (e == 4) ? xnt : (e == 5) ? txnyn : (e == 6) ? ynt : txm;
-                    edge_k(tn, st, s1, t.edge[e], t.F);
-                }
-            }
-            return ((told > 0) ? 1.0 : -1.0) * tn;
-        }
 #pragma unroll 1
         for (int k = 0; k < 8; ++k) {
             // (xt,txy) (xt,txm) (xnt,txnyn) (xnt,tym) (ynt,txnyn) (ynt,txm) (yt,txy) (yt,tym)
@@ -320,6 +229,98 @@ __host__ __device__ __forceinline__ double point_update_fast(double told, double
                             : (k == 4) ? xnt : (k == 5) ? txnyn : (k == 6) ? ynt : txm;
             edge_k(tn, st, s1, t.edge[k], t.F);
         }
+    }
+    return ((told > 0) ? 1.0 : -1.0) * tn;
+}
+
+// 5. The same update with the sixteen call sites unrolled: every entry test
+//    and skip gate reads its operands and constants at fixed positions (no
+//    operand selection, no slot loop), and the solver bodies, which the
+//    gates of 3. and 4. leave to a minority of the calls, are shared
+//    out-of-line functions.  Same calls, same order, same arithmetic as
+//    surf_k and edge_k.
+static __host__ __device__ __noinline__ double edge_body(double tn, double s0, double s1, double mn, const EdgeK &k,
+                                                  double F)
+{
+    const double d = div_by_const(s1 - s0, k.hx, k.rhx);
+    double c = (1.0 - d * k.ax);
+    double q = k.g * (c * c - d * d * k.ga);
+    if (0.0 < q) {
+        c = div_by_const(-k.az * c + sqrt(q), k.ga, k.rga);
+        q = s0 + k.hz * c;
+        if (q < tn && q > mn) {
+            const double g = sqrt(div_by_const((d * d + c * c) * F * F, k.g, k.rg));
+            const double xe = -k.hz * (d + k.ax * g) / (c + k.az * g);
+            if (0.0 < xe && xe < k.hx) tn = q;
+        }
+    }
+    return tn;
+}
+
+static __host__ __device__ __noinline__ double surf_body(double tn, double s0, double s1, double s2, double mn,
+                                                  const SurfK &k, const SideTable &t)
+{
+    const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
+    const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
+    double dd = dx * dx + dy * dy;
+    double al = 1.0 - k.ax * dx - k.ay * dy;
+    double q = al * al - dd * t.g;
+    if (q > 0.0) {
+        al = div_by_const(-t.az * al + t.F * sqrt(q), t.g, t.rg);
+        const double g = s0 + t.hz * al;
+        if (g < tn && g > mn) {
+            q = sqrt(dd + al * al);
+            dd = -t.hz / (t.F * al + t.az * q);
+            const double xe = dd * (t.F * dx + k.ax * q);
+            const double ye = dd * (t.F * dy + k.ay * q);
+            if (0.0 <= kmin(xe, ye) && ye * k.hx <= xe * k.hy && xe <= k.hx) tn = g;
+        }
+    }
+    return tn;
+}
+
+__host__ __device__ __forceinline__ void edge_site(double &tn, double s0, double s1, const EdgeK &k, double F)
+{
+    const double mn = kmin(s1, s0);
+    if (tn < mn || (k.early && s1 > s0)) return;
+    if (!(tn <= mn + k.B)) tn = edge_body(tn, s0, s1, mn, k, F);
+    if (tn > s1 && k.fb_ok) tn = kmin(tn, s1 + k.K);
+}
+
+template <int K>
+__host__ __device__ __forceinline__ void surf_site(double &tn, double s0, double s1, double s2, const SideTable &t)
+{
+    const SurfK &k = t.surf[K];
+    const double mn = kmin(s0, kmin(s1, s2));
+    if (tn < mn || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
+    if (!(tn <= mn + k.B)) tn = surf_body(tn, s0, s1, s2, mn, k, t);
+    if (tn > kmin(s1, s2) && !(k.nblock && s1 > s2)) edge_site(tn, s1, s2, k.nest, t.F);
+}
+
+__host__ __device__ __forceinline__ double point_update_unrolled(double told, double st, double xt, double yt,
+                                                                 double xnt, double ynt, double txy, double txm,
+                                                                 double tym, double txnyn, const DirTable *tab)
+{
+    double tn = fabs(told);
+    const SideTable &t = tab->side[told < 0 ? 1 : 0];
+    if (st < tn && t.d1_ok) tn = kmin(tn, st + t.K1);
+    if (!(tn < st && tn < kmin(xt, yt) && tn < kmin(txy, txm) && tn < kmin(txnyn, tym))) {
+        surf_site<0>(tn, st, xt, txy, t);
+        surf_site<1>(tn, st, xt, txm, t);
+        surf_site<2>(tn, st, xnt, txnyn, t);
+        surf_site<3>(tn, st, xnt, tym, t);
+        surf_site<4>(tn, st, ynt, txnyn, t);
+        surf_site<5>(tn, st, ynt, txm, t);
+        surf_site<6>(tn, st, yt, txy, t);
+        surf_site<7>(tn, st, yt, tym, t);
+        edge_site(tn, st, xt, t.edge[0], t.F);
+        edge_site(tn, st, txy, t.edge[1], t.F);
+        edge_site(tn, st, yt, t.edge[2], t.F);
+        edge_site(tn, st, tym, t.edge[3], t.F);
+        edge_site(tn, st, xnt, t.edge[4], t.F);
+        edge_site(tn, st, txnyn, t.edge[5], t.F);
+        edge_site(tn, st, ynt, t.edge[6], t.F);
+        edge_site(tn, st, txm, t.edge[7], t.F);
     }
     return ((told > 0) ? 1.0 : -1.0) * tn;
 }

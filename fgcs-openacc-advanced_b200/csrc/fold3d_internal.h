@@ -107,14 +107,13 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
 
-// Warp-owned items of the drift medium: mark the call sites that could still
-// lower the time first and run only those (1), or test every site in turn
-// (0); build option.  Without CTA barriers, a warp's uneven work costs no
-// other warp a wait.
-#ifndef FOLD3D_WARP_SITE_MASK
-#define FOLD3D_WARP_SITE_MASK 0
+// Drift-medium dataflow passes: the point update with its sixteen call sites
+// unrolled and the solver bodies out of line (1), or the slot loops (0);
+// build option.
+#ifndef FOLD3D_SITE_UNROLL
+#define FOLD3D_SITE_UNROLL 0
 #endif
-constexpr bool kWarpSiteMask = FOLD3D_WARP_SITE_MASK != 0;
+constexpr bool kSiteUnroll = FOLD3D_SITE_UNROLL != 0;
 
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4

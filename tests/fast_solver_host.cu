@@ -59,14 +59,14 @@ void clear_bounds(SideTable &t)
 // Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  skip:
 // 1 the tables as solves build them (searched bounds), 2 the closed-form
 // bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all; plus
-// 4: the update marks its live call sites first (point_update_fast<true>).
+// 4: the update with its call sites unrolled (point_update_unrolled).
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
                                 double a0, double a1, double a2, int sweeps, int skip)
 {
     const int n[3] = {nx, ny, nz};
     const int64_t stride[3] = {1, (int64_t)nx + 2, ((int64_t)nx + 2) * (ny + 2)};
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
-    const bool mask = (skip & 4) != 0;
+    const bool unrolled = (skip & 4) != 0;
     skip &= 3;
     DirTable tabs[6];
     for (int dir = 0; dir < 6; ++dir) {
@@ -92,10 +92,10 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
                         const double v[9] = {std::fabs(p[0]),       std::fabs(p[sx]),      std::fabs(p[sy]),
                                              std::fabs(p[-sx]),      std::fabs(p[-sy]),     std::fabs(p[sx + sy]),
                                              std::fabs(p[sx - sy]),  std::fabs(p[-sx + sy]), std::fabs(p[-sx - sy])};
-                        T[ti] = mask ? point_update_fast<true>(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6],
-                                                               v[7], v[8], &tabs[dir])
-                                     : point_update_fast<false>(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6],
-                                                                v[7], v[8], &tabs[dir]);
+                        T[ti] = unrolled ? point_update_unrolled(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6],
+                                                                 v[7], v[8], &tabs[dir])
+                                         : point_update_fast(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7],
+                                                             v[8], &tabs[dir]);
                     }
             }
         }

@@ -75,7 +75,7 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
     ref = T0.copy()
     orc.solve(ref, h, 8, F=F, a=a)
     # searched bounds, closed-form bounds (the no-alloc solve's), none; and
-    # the searched bounds with the live-site mark first (warp-owned items)
+    # the searched bounds through the unrolled form of the update
     for skip in (1, 2, 0, 5):
         T = T0.copy()
         _host_sweeps(host, T, h, F, a, 8, skip)
@@ -97,7 +97,7 @@ def test_host_build_matches_reference_off_centre_sources(orc, host, digests, n, 
 @pytest.mark.parametrize("skip", [1, 5])
 def test_host_build_matches_reference_digest_99(host, digests, skip):
     """The reference's own 8-sweep result at 99^3 (partial tiles on every
-    axis), through the host build (skip 5: the live-site mark first)."""
+    axis), through the host build (skip 5: the unrolled form of the update)."""
     from oracle import Oracle
 
     n = 99
