@@ -233,98 +233,6 @@ __host__ __device__ __forceinline__ double point_update_fast(double told, double
     return ((told > 0) ? 1.0 : -1.0) * tn;
 }
 
-// 5. The same update with the sixteen call sites unrolled: every entry test
-//    and skip gate reads its operands and constants at fixed positions (no
-//    operand selection, no slot loop), and the solver bodies, which the
-//    gates of 3. and 4. leave to a minority of the calls, are shared
-//    out-of-line functions.  Same calls, same order, same arithmetic as
-//    surf_k and edge_k.
-static __host__ __device__ __noinline__ double edge_body(double tn, double s0, double s1, double mn, const EdgeK &k,
-                                                  double F)
-{
-    const double d = div_by_const(s1 - s0, k.hx, k.rhx);
-    double c = (1.0 - d * k.ax);
-    double q = k.g * (c * c - d * d * k.ga);
-    if (0.0 < q) {
-        c = div_by_const(-k.az * c + sqrt(q), k.ga, k.rga);
-        q = s0 + k.hz * c;
-        if (q < tn && q > mn) {
-            const double g = sqrt(div_by_const((d * d + c * c) * F * F, k.g, k.rg));
-            const double xe = -k.hz * (d + k.ax * g) / (c + k.az * g);
-            if (0.0 < xe && xe < k.hx) tn = q;
-        }
-    }
-    return tn;
-}
-
-static __host__ __device__ __noinline__ double surf_body(double tn, double s0, double s1, double s2, double mn,
-                                                  const SurfK &k, const SideTable &t)
-{
-    const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
-    const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
-    double dd = dx * dx + dy * dy;
-    double al = 1.0 - k.ax * dx - k.ay * dy;
-    double q = al * al - dd * t.g;
-    if (q > 0.0) {
-        al = div_by_const(-t.az * al + t.F * sqrt(q), t.g, t.rg);
-        const double g = s0 + t.hz * al;
-        if (g < tn && g > mn) {
-            q = sqrt(dd + al * al);
-            dd = -t.hz / (t.F * al + t.az * q);
-            const double xe = dd * (t.F * dx + k.ax * q);
-            const double ye = dd * (t.F * dy + k.ay * q);
-            if (0.0 <= kmin(xe, ye) && ye * k.hx <= xe * k.hy && xe <= k.hx) tn = g;
-        }
-    }
-    return tn;
-}
-
-__host__ __device__ __forceinline__ void edge_site(double &tn, double s0, double s1, const EdgeK &k, double F)
-{
-    const double mn = kmin(s1, s0);
-    if (tn < mn || (k.early && s1 > s0)) return;
-    if (!(tn <= mn + k.B)) tn = edge_body(tn, s0, s1, mn, k, F);
-    if (tn > s1 && k.fb_ok) tn = kmin(tn, s1 + k.K);
-}
-
-template <int K>
-__host__ __device__ __forceinline__ void surf_site(double &tn, double s0, double s1, double s2, const SideTable &t)
-{
-    const SurfK &k = t.surf[K];
-    const double mn = kmin(s0, kmin(s1, s2));
-    if (tn < mn || (k.e1 && s1 > s0) || (k.e2 && s2 > s1)) return;
-    if (!(tn <= mn + k.B)) tn = surf_body(tn, s0, s1, s2, mn, k, t);
-    if (tn > kmin(s1, s2) && !(k.nblock && s1 > s2)) edge_site(tn, s1, s2, k.nest, t.F);
-}
-
-__host__ __device__ __forceinline__ double point_update_unrolled(double told, double st, double xt, double yt,
-                                                                 double xnt, double ynt, double txy, double txm,
-                                                                 double tym, double txnyn, const DirTable *tab)
-{
-    double tn = fabs(told);
-    const SideTable &t = tab->side[told < 0 ? 1 : 0];
-    if (st < tn && t.d1_ok) tn = kmin(tn, st + t.K1);
-    if (!(tn < st && tn < kmin(xt, yt) && tn < kmin(txy, txm) && tn < kmin(txnyn, tym))) {
-        surf_site<0>(tn, st, xt, txy, t);
-        surf_site<1>(tn, st, xt, txm, t);
-        surf_site<2>(tn, st, xnt, txnyn, t);
-        surf_site<3>(tn, st, xnt, tym, t);
-        surf_site<4>(tn, st, ynt, txnyn, t);
-        surf_site<5>(tn, st, ynt, txm, t);
-        surf_site<6>(tn, st, yt, txy, t);
-        surf_site<7>(tn, st, yt, tym, t);
-        edge_site(tn, st, xt, t.edge[0], t.F);
-        edge_site(tn, st, txy, t.edge[1], t.F);
-        edge_site(tn, st, yt, t.edge[2], t.F);
-        edge_site(tn, st, tym, t.edge[3], t.F);
-        edge_site(tn, st, xnt, t.edge[4], t.F);
-        edge_site(tn, st, txnyn, t.edge[5], t.F);
-        edge_site(tn, st, ynt, t.edge[6], t.F);
-        edge_site(tn, st, txm, t.edge[7], t.F);
-    }
-    return ((told > 0) ? 1.0 : -1.0) * tn;
-}
-
 // ---------------------------------------------------------------------------
 // Candidate values for the compacted kernel.  Each function returns the
 // smallest candidate its reference call would accept when entered with the

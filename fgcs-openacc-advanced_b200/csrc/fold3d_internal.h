@@ -107,14 +107,6 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
 
-// Drift-medium dataflow passes: the point update with its sixteen call sites
-// unrolled and the solver bodies out of line (1), or the slot loops (0);
-// build option.
-#ifndef FOLD3D_SITE_UNROLL
-#define FOLD3D_SITE_UNROLL 0
-#endif
-constexpr bool kSiteUnroll = FOLD3D_SITE_UNROLL != 0;
-
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4
 #endif

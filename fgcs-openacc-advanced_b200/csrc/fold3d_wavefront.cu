@@ -145,10 +145,7 @@ __device__ __forceinline__ bool wave_item(R *__restrict__ T, const WaveArgs &a,
             R tnew;
             if constexpr (MED == kMediumDrift) {
                 static_assert(sizeof(R) == 8, "the drift medium is solved in double");
-                if constexpr (kSiteUnroll)
-                    tnew = point_update_unrolled(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
-                else
-                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
             } else {
                 const R nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
                 int win;
@@ -250,10 +247,7 @@ __device__ __forceinline__ bool wave_item_warp(R *__restrict__ T, const WaveArgs
                 const R told = ld_cg(T + d);
                 R tnew;
                 if constexpr (MED == kMediumDrift) {
-                    if constexpr (kSiteUnroll)
-                        tnew = point_update_unrolled(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
-                    else
-                        tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
+                    tnew = point_update_fast(told, st, xt, yt, xnt, ynt, txy, txm, tym, txnyn, &tab);
                 } else {
                     const R nb[8] = {xt, txy, yt, tym, xnt, txnyn, ynt, txm};
                     int win;

@@ -58,16 +58,13 @@ void clear_bounds(SideTable &t)
 
 // Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  skip:
 // 1 the tables as solves build them (searched bounds), 2 the closed-form
-// bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all; plus
-// 4: the update with its call sites unrolled (point_update_unrolled).
+// bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all.
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
                                 double a0, double a1, double a2, int sweeps, int skip)
 {
     const int n[3] = {nx, ny, nz};
     const int64_t stride[3] = {1, (int64_t)nx + 2, ((int64_t)nx + 2) * (ny + 2)};
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
-    const bool unrolled = (skip & 4) != 0;
-    skip &= 3;
     DirTable tabs[6];
     for (int dir = 0; dir < 6; ++dir) {
         build_dir_table(host_frame(dir, h, F, a), tabs[dir], skip != 2);
@@ -89,13 +86,10 @@ extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, do
                         const int64_t si = (int64_t)src * sn + c * stride[u] + b * stride[v];
                         const int64_t ti = si + d.sg * sn;
                         const double *p = T + si;
-                        const double v[9] = {std::fabs(p[0]),       std::fabs(p[sx]),      std::fabs(p[sy]),
-                                             std::fabs(p[-sx]),      std::fabs(p[-sy]),     std::fabs(p[sx + sy]),
-                                             std::fabs(p[sx - sy]),  std::fabs(p[-sx + sy]), std::fabs(p[-sx - sy])};
-                        T[ti] = unrolled ? point_update_unrolled(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6],
-                                                                 v[7], v[8], &tabs[dir])
-                                         : point_update_fast(T[ti], v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7],
-                                                             v[8], &tabs[dir]);
+                        T[ti] = point_update_fast(T[ti], std::fabs(p[0]), std::fabs(p[sx]), std::fabs(p[sy]),
+                                                  std::fabs(p[-sx]), std::fabs(p[-sy]), std::fabs(p[sx + sy]),
+                                                  std::fabs(p[sx - sy]), std::fabs(p[-sx + sy]),
+                                                  std::fabs(p[-sx - sy]), &tabs[dir]);
                     }
             }
         }
