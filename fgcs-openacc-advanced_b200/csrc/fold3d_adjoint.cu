@@ -151,11 +151,33 @@ __device__ __forceinline__ long long fan_index(long long x, const PlaneGeom &g, 
 
 constexpr int kAdjThreads = 32 * kWaveTV;
 
+// The source points and weights of target x's winner `w` (a cell of the
+// pass's direction): np = 0 when the candidate is not finite.
+template <class R>
+__device__ __forceinline__ void adj_weights(const R *T, const EllipParam &ep, const PlaneGeom &g, long long x,
+                                            unsigned w, long long src[3], R wt[3], int &np)
+{
+    R tv9[9], c[3], n;
+    int pt[3];
+    fan_times(T, x, g, tv9);
+    if (!(ell_cand(ell_local<R>(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) < r_inf<R>()))
+        np = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
+}
+
 // One item (step p, tile t) of a backward pass, for all threads of the CTA:
 // prepare the pushes, wait for those of the 3 x 3 tiles of step p-1 that
 // have work, push, publish.
 // Adds the largest pushed |amount| into dmax.  Returns false if a wait gave
 // up (the item is then left unpublished and the caller must leave).
+//
+// A cell pushes only when its lambda moved since its last push.  Its winner's
+// weights (fan times, local metric, one candidate) are worked out while the
+// items it waits for still run when lambda has already moved before the
+// wait, which is every cell of the first backward sweeps; a cell whose
+// lambda only moves during the wait works them out after it, and a cell
+// whose lambda did not move, the most of them in the later sweeps, never.
 template <class R>
 __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam &ep, int item, double &dmax)
 {
@@ -170,28 +192,23 @@ __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam 
     const int p = item / ntiles, t = item - p * ntiles;
     const int tu = t % a.ntu, tv = t / a.ntu;
     const int tgt = a.first_src - p * a.sg;
-    // Everything but lambda is fixed during the adjoint: find this thread's
-    // cell, its winner's source points and weights, and what it pushed
-    // before, while the items it waits for are still running.
     const int u = tu * 32 + lane + 1;
     const int v = tv * kWaveTV + warp + 1;
     long long x = -1, src[3] = {0, 0, 0};
     R wt[3] = {R(0), R(0), R(0)}, P = R(0);
     int np = 0;
+    unsigned win = 0;
+    bool ready = false;
     if (u <= g.nu && v <= g.nv) {
         const long long xc = (long long)tgt * g.s_nrm + (long long)u * g.su + (long long)v * g.sv;
-        const unsigned w = b.W[xc];
-        if (w != kNoWinner && (int)(w / kEllipCands) == a.dir) {
+        win = b.W[xc];
+        if (win != kNoWinner && (int)(win / kEllipCands) == a.dir) {
             x = xc;
             P = pushed[x];
-            R tv9[9], c[3], n;
-            int pt[3];
-            fan_times(T, x, g, tv9);
-            if (!(ell_cand(ell_local<R>(ep.med, ep.dir, x), tv9, (int)(w % kEllipCands), pt, wt, np, c, n) <
-                  r_inf<R>()))
-                np = 0;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) src[q] = (q < np) ? fan_index(x, g, pt[q]) : 0;
+            if (__ldcg(lam + x) != P) {
+                adj_weights<R>(T, ep, g, x, win, src, wt, np);
+                ready = true;
+            }
         }
     }
     int timed_out = 0;
@@ -219,6 +236,7 @@ __device__ __forceinline__ bool adj_item(const AdjWaveArgs &b, const EllipParam 
         const R L = __ldcg(lam + x);
         const R D = L - P;
         if (D != R(0)) {
+            if (!ready) adj_weights<R>(T, ep, g, x, win, src, wt, np);
             pushed[x] = L;
 #pragma unroll
             for (int q = 0; q < 3; ++q)
