@@ -107,6 +107,13 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
 
+// Items a batched pass's CTA claims at a time (1..32); build option.
+#ifndef FOLD3D_BATCH_CHUNK
+#define FOLD3D_BATCH_CHUNK 4
+#endif
+constexpr int kBatchChunk = FOLD3D_BATCH_CHUNK;
+static_assert(kBatchChunk >= 1 && kBatchChunk <= 32, "batch chunk");
+
 #ifndef FOLD3D_WAVE_TV
 #define FOLD3D_WAVE_TV 4
 #endif

@@ -380,55 +380,72 @@ template <int TV> constexpr int batch_min_blocks() { return FOLD3D_WAVE_MINB_BAT
 template <class R, int TV>
 __global__ void __launch_bounds__(32 * TV, batch_min_blocks<TV>()) batch_pass_kernel(BatchArgs b)
 {
-    __shared__ int s_next;
-    __shared__ int s_loc[2];
-    __shared__ int s_cur;  // the active slot staged in s_inst, -1 for none
+    // A CTA claims kBatchChunk consecutive items at a time, and the first
+    // lanes of warp 0 locate them in parallel (two binary searches each over
+    // the launch's tables): consecutive items mostly belong to one instance
+    // (its tiles of a step come together), so the instance is staged once for
+    // several items, and the searches' dependent loads are paid once per
+    // chunk.  Claims stay in increasing order and a chunk's items run in
+    // order, so the lowest unfinished item always runs and every wait ends.
+    __shared__ int s_next;  // first item of the CTA's next chunk, -1 for none
+    __shared__ int s_loc[kBatchChunk][2];
+    __shared__ int s_n;     // items of the current chunk
+    __shared__ int s_cur;   // the active slot staged in s_inst, -1 for none
     __shared__ BatchInst s_inst;
     const unsigned total = *b.total;
-    const unsigned epoch = *b.epoch_base + (unsigned)b.dir + 1u;
     if (threadIdx.x == 0) {
-        const unsigned w = atomicAdd(b.work, 1u);
+        const unsigned w = atomicAdd(b.work, (unsigned)kBatchChunk);
         s_next = (w < total) ? (int)w : -1;
+        s_n = 0;
         s_cur = -1;
     }
     __syncthreads();
-    // Consecutive items mostly belong to one instance (its tiles of a step
-    // come together): the instance stays staged, and its largest change and
-    // evaluated points are flushed only when the CTA moves to another one.
+    // The instance stays staged, and its largest change and evaluated points
+    // are flushed only when the CTA moves to another one.
     double dmax = 0.0;
     unsigned long long evaluated = 0;
-    for (;;) {
-        const int gitem = s_next;
-        if (gitem < 0) break;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int it = -1;
-            if (*(volatile unsigned *)b.status == 0) {
-                const unsigned w = atomicAdd(b.work, 1u);
-                if (w < total) it = (int)w;
+    for (int q = 0;; ++q) {
+        if (q == s_n) {  // the same for every thread
+            const int c0 = s_next;
+            if (c0 < 0) break;
+            __syncthreads();  // every thread has read s_n and s_next
+            if (threadIdx.x < 32) {
+                const int n = (int)min((unsigned)kBatchChunk, total - (unsigned)c0);
+                if ((int)threadIdx.x < n)
+                    batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, c0 + (int)threadIdx.x,
+                                 s_loc[threadIdx.x][0], s_loc[threadIdx.x][1]);
+                if (threadIdx.x == 0) {
+                    int it = -1;
+                    if (*(volatile unsigned *)b.status == 0) {
+                        const unsigned w = atomicAdd(b.work, (unsigned)kBatchChunk);
+                        if (w < total) it = (int)w;
+                    }
+                    s_next = it;
+                    s_n = n;
+                }
             }
-            s_next = it;
-            batch_locate(b.step_off, b.step_k, b.tile_pre, b.max_steps, gitem, s_loc[0], s_loc[1]);
+            __syncthreads();
+            q = 0;
         }
-        __syncthreads();
-        if (s_loc[0] != s_cur) {  // the same for every thread
+        const int slot = s_loc[q][0];
+        if (slot != s_cur) {  // the same for every thread
             if (s_cur >= 0) {
                 wave_flush<TV>(dmax, evaluated, s_inst.a.maxd, s_inst.a.evaluated);
                 dmax = 0.0;
                 evaluated = 0;
             }
-            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + b.act[s_loc[0]]);
+            const unsigned *src = reinterpret_cast<const unsigned *>(b.inst + b.act[slot]);
             unsigned *dst = reinterpret_cast<unsigned *>(&s_inst);
             for (int w = threadIdx.x; w < (int)(sizeof(BatchInst) / 4); w += blockDim.x) dst[w] = src[w];
             __syncthreads();
             if (threadIdx.x == 0) {  // the pass number is per launch, not per staged instance
-                s_inst.a.epoch = epoch;
+                s_inst.a.epoch = *b.epoch_base + (unsigned)b.dir + 1u;
                 s_inst.a.skip_from = b.skip_from;
-                s_cur = s_loc[0];
+                s_cur = slot;
             }
             __syncthreads();
         }
-        if (!wave_item<kMediumEllip, R, TV>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[1], dmax,
+        if (!wave_item<kMediumEllip, R, TV>(static_cast<R *>(s_inst.T), s_inst.a, s_inst.p, s_loc[q][1], dmax,
                                             evaluated))
             break;
     }
