@@ -1109,7 +1109,8 @@ def main():
     fp64 = None
     if wave:
         fp64 = ({"pct_of_active_cycles": 35.0, "issue_active_pct": 71.9,
-                 "capture": "k_up pass over 1280^2 planes (1280x1280x16 grid, sweep 2)"} if large_planes else
+                 "capture": "k_up pass over 1280^2 planes (1280x1280x16 grid, sweep 2) of the kernel built for 8 CTAs "
+                            "per SM (64 registers); the kernel timed here is built for 7 (72 registers)"} if large_planes else
                 {"pct_of_active_cycles": 30.5, "issue_active_pct": 50.9,
                  "capture": "x_down, x_up, k_up passes of sweep 3 at 512^3 (mean)"})
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

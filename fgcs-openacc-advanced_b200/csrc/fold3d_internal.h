@@ -138,7 +138,13 @@ constexpr int kWaveTV = FOLD3D_WAVE_TV;
 #define FOLD3D_WAVE_MINB_BATCH 8
 #endif
 #ifndef FOLD3D_WAVE_MINB_LARGE
-#define FOLD3D_WAVE_MINB_LARGE 8
+#define FOLD3D_WAVE_MINB_LARGE 8  // large planes, float32 elliptical medium
+#endif
+#ifndef FOLD3D_WAVE_MINB_LARGE_DRIFT
+#define FOLD3D_WAVE_MINB_LARGE_DRIFT 7
+#endif
+#ifndef FOLD3D_WAVE_MINB_LARGE_ELLIP
+#define FOLD3D_WAVE_MINB_LARGE_ELLIP 7
 #endif
 #ifndef FOLD3D_WAVE_LARGE_TILES
 #define FOLD3D_WAVE_LARGE_TILES 8192

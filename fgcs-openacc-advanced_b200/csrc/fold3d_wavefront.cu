@@ -60,7 +60,9 @@ constexpr int kWaveThreads = 32 * kWaveTV;
 
 template <int MED, class R, bool LARGE> constexpr int wave_min_blocks()
 {
-    return LARGE ? FOLD3D_WAVE_MINB_LARGE
+    return LARGE ? (MED == kMediumDrift   ? FOLD3D_WAVE_MINB_LARGE_DRIFT
+                    : sizeof(R) == 8      ? FOLD3D_WAVE_MINB_LARGE_ELLIP
+                                          : FOLD3D_WAVE_MINB_LARGE)
                  : MED == kMediumDrift ? FOLD3D_WAVE_MINB_DRIFT
                                        : (sizeof(R) == 8 ? FOLD3D_WAVE_MINB_ELLIP : FOLD3D_WAVE_MINB_ELLIP_F32);
 }
