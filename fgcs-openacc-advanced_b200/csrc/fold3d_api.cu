@@ -198,12 +198,6 @@ struct fold3d_ctx {
     double *i_stage[2] = {nullptr, nullptr}; // ... and two pinned slabs of it on the host
     size_t i_stage_bytes = 0;
     int *adj_cnt = nullptr;                  // per (step, slot) counts, then offsets
-    // the drift medium's gradient bins (fold3d_fast.cuh, 5.) of the last
-    // WAVEFRONT solve's six frames: built on the host, copied to the device
-    DirBins *g_bins_h = nullptr;
-    DirBins *g_bins_d = nullptr;
-    LocalFrameH g_bins_key[6] = {};
-    bool g_bins_ok = false;
     long long *adj_off = nullptr;
     size_t adj_cnt_cap = 0;
     char *b_stage_d = nullptr, *b_stage_h = nullptr;
@@ -294,8 +288,6 @@ void fold3d_destroy(fold3d_ctx *c)
     if (c->b_stage_h) cudaFreeHost(c->b_stage_h);
     if (c->b_ctl) cudaFree(c->b_ctl);
     if (c->tune_T) cudaFree(c->tune_T);
-    if (c->g_bins_d) cudaFree(c->g_bins_d);
-    delete[] c->g_bins_h;
     if (c->d_maxd) cudaFree(c->d_maxd);
     if (c->h_maxd) cudaFreeHost(c->h_maxd);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -508,38 +500,11 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
     a.timeout_ns = 4000000000ull;
     const unsigned e0 = c->epoch + 1;
     a.skip_from = o.skip ? e0 + 6 : 0xffffffffu;
+    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
     int sweeps = 0;
     double delta = 0.0;
     unsigned hstat[2] = {0, 0};
-    DirTable tabs[6];
-    if (!em) {  // the drift medium's six direction tables, with their gradient bins
-        DirBins *hb = nullptr;
-        if (kGradBins) {
-            if (!c->g_bins_h) c->g_bins_h = new (std::nothrow) DirBins[6];
-            if (c->g_bins_h && !c->g_bins_d && cudaMalloc(&c->g_bins_d, 6 * sizeof(DirBins)) != cudaSuccess) {
-                cudaGetLastError();
-                c->g_bins_d = nullptr;  // no bins: the tables' own bounds still hold
-            }
-            if (c->g_bins_h && c->g_bins_d) hb = c->g_bins_h;
-        }
-        LocalFrameH fr[6];
-        for (int dir = 0; dir < 6; ++dir) {
-            fr[dir] = make_frame(g, *fm, dir);
-            build_dir_table(fr[dir], tabs[dir], true, hb ? hb + dir : nullptr);
-        }
-        if (hb) {
-            if (!c->g_bins_ok || memcmp(c->g_bins_key, fr, sizeof fr) != 0) {
-                c->g_bins_ok = false;
-                if ((e = cudaMemcpyAsync(c->g_bins_d, hb, 6 * sizeof(DirBins), cudaMemcpyHostToDevice, s)) !=
-                    cudaSuccess)
-                    return cuda_error(e, "gradient bins");
-                memcpy(c->g_bins_key, fr, sizeof fr);
-                c->g_bins_ok = true;
-            }
-            for (int dir = 0; dir < 6; ++dir) attach_dir_bins(tabs[dir], c->g_bins_d + dir);
-        }
-    }
-    if ((e = cudaEventRecord(c->ev0, s)) != cudaSuccess) return cuda_error(e, "cudaEventRecord");
+    DirTable tab;
     while (sweeps < o.max_sweeps) {
         if ((e = cudaMemsetAsync(c->d_maxd, 0, sizeof(unsigned long long), s)) != cudaSuccess)
             return cuda_error(e, "cudaMemsetAsync");
@@ -566,7 +531,8 @@ static int solve_wavefront(fold3d_ctx *c, const fold3d_grid &g, const fold3d_med
             if (em) {
                 e = launch_wave_pass_ellip(T, f32, a, ellip_param(g, *em, dir), grid, s, large);
             } else {
-                e = launch_wave_pass(static_cast<double *>(T), a, tabs[dir], grid, s, large);
+                build_dir_table(make_frame(g, *fm, dir), tab);
+                e = launch_wave_pass(static_cast<double *>(T), a, tab, grid, s, large);
             }
             if (e != cudaSuccess) return cuda_error(e, "wavefront pass");
         }

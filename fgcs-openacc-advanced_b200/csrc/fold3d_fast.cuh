@@ -68,30 +68,11 @@
 //    the body's single gradient d (fold3d_tables.cpp), less the same
 //    relative 1e-3 margin.  The fall-back candidate from s1 alone is not
 //    gated.
-//
-// 5. Gradient bins sharpen both gates.  A FoldEdge2Points body's increment
-//    over min(s0, s1) depends only on its gradient d = (s1 - s0)/dxx (the
-//    value the body computes first), a FoldSurf3Points body's only on
-//    (dx, dy).  The host splits the gradient range where a candidate can
-//    exist (the edge: between the roots of its q; the triangle: the square
-//    around the disc where its q > 0) into bins and proves a lower bound of
-//    the accepted increment per bin by the same interval search, over each
-//    bin widened by a millionth of its width (so a gradient that rounding
-//    puts in a bin lies inside it), less the same relative 1e-3.  The body
-//    then also returns when the time is at most min + the bound of its
-//    gradient's bin, or when the gradient lies outside every bin (no
-//    candidate there).  Bounds are stored as float rounded down.
 #pragma once
 #include <cstdint>
 #include <cstring>
 
 namespace fold3d {
-
-// Gradient bins (5. above): a FoldEdge2Points body's gradient range split
-// into kEdgeBins bins, a FoldSurf3Points body's gradient square into
-// kSurfBins x kSurfBins.
-constexpr int kEdgeBins = 64;
-constexpr int kSurfBins = 24;
 
 // Constants of one FoldEdge2Points call site (AN_ISO_1_OpenACC.c:59-114).
 struct EdgeK {
@@ -104,8 +85,6 @@ struct EdgeK {
     double B;           // body skipped when the time is <= min(s0, s1) + B (4. above)
     int early;          // ax > 0: return when s1 > s0 (:71)
     int fb_ok;          // fall-back defined: its q > 0 and c > 0
-    double blo, binv;   // gradient bins: bin of d is (d - blo) * binv (5. above)
-    const float *bins;  // kEdgeBins lower bounds of the increment, or null
 };
 
 // Constants of one FoldSurf3Points call site (:119-175).
@@ -117,8 +96,6 @@ struct SurfK {
     int nblock;         // ax*dzz + az*dxx > 0: nested edge skipped when s1 > s2 (:170)
     int pad_;
     double B;           // body skipped when the time is <= min(s0, s1, s2) + B (3. above)
-    double blo, binv;   // gradient bins: bin of dx is (dx - blo) * binv, of dy the same (5. above)
-    const float *bins;  // kSurfBins^2 lower bounds of the increment, [bin of dx][bin of dy], or null
     EdgeK nest;         // the nested FoldEdge2Points call (:172-173)
 };
 
@@ -138,18 +115,6 @@ struct SideTable {
 
 struct DirTable {
     SideTable side[2];  // [0]: target >= 0 (or 0), [1]: target < 0 (drift negated)
-};
-
-// Gradient bins of one direction's call sites (5. above): per side,
-// kEdgeBins bounds per FoldEdge2Points site and per nested one, kSurfBins^2
-// per FoldSurf3Points site ([bin of dx][bin of dy]).
-struct SideBins {
-    float edge[8][kEdgeBins];
-    float nest[8][kEdgeBins];
-    float surf[8][kSurfBins * kSurfBins];
-};
-struct DirBins {
-    SideBins side[2];
 };
 
 // Safe operand range of div_by_const: |x| and |c| in [2^-400, 2^401), which
@@ -189,35 +154,12 @@ __host__ __device__ __forceinline__ double div_by_const(double x, double c, doub
 
 __host__ __device__ __forceinline__ double kmin(double a, double b) { return (a < b) ? a : b; }
 
-// A gradient bin's bound (5. above), read through the read-only cache.
-__host__ __device__ __forceinline__ double bin_bound(const float *p)
-{
-#ifdef __CUDA_ARCH__
-    return (double)__ldg(p);
-#else
-    return (double)*p;
-#endif
-}
-
-// Bin of a gradient: x = (d - lo) * inv in [0, n], the top edge in the last
-// bin; -1 outside (rounding of x is far inside the bins' widening).
-__host__ __device__ __forceinline__ int grad_bin(double x, int n)
-{
-    if (!(x >= 0.0 && x <= (double)n)) return -1;
-    const int i = (int)x;
-    return i < n ? i : n - 1;
-}
-
 __host__ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1, const EdgeK &k, double F)
 {
     const double mn = kmin(s1, s0);
     if (tn < mn || (k.early && s1 > s0)) return;
     if (!(tn <= mn + k.B)) {  // 4. above
         const double d = div_by_const(s1 - s0, k.hx, k.rhx);
-        if (k.bins) {  // 5. above
-            const int i = grad_bin((d - k.blo) * k.binv, kEdgeBins);
-            if (i < 0 || tn <= mn + bin_bound(k.bins + i)) goto fall_back;
-        }
         double c = (1.0 - d * k.ax);
         double q = k.g * (c * c - d * d * k.ga);
         if (0.0 < q) {
@@ -230,7 +172,6 @@ __host__ __device__ __forceinline__ void edge_k(double &tn, double s0, double s1
             }
         }
     }
-fall_back:
     if (tn > s1 && k.fb_ok) tn = kmin(tn, s1 + k.K);
 }
 
@@ -242,10 +183,6 @@ __host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1
     if (!(tn <= mn + k.B)) {  // 3. above
         const double dx = div_by_const(s1 - s0, k.hx, k.rhx);
         const double dy = div_by_const(s2 - s1, k.hy, k.rhy);
-        if (k.bins) {  // 5. above
-            const int i = grad_bin((dx - k.blo) * k.binv, kSurfBins), j = grad_bin((dy - k.blo) * k.binv, kSurfBins);
-            if (i < 0 || j < 0 || tn <= mn + bin_bound(k.bins + i * kSurfBins + j)) goto nested;
-        }
         double dd = dx * dx + dy * dy;
         double al = 1.0 - k.ax * dx - k.ay * dy;
         double q = al * al - dd * t.g;
@@ -261,7 +198,6 @@ __host__ __device__ __forceinline__ void surf_k(double &tn, double s0, double s1
             }
         }
     }
-nested:
     if (tn > kmin(s1, s2) && !(k.nblock && s1 > s2)) edge_k(tn, s1, s2, k.nest, t.F);
 }
 

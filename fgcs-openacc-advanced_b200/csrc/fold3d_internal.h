@@ -79,18 +79,11 @@ bool compat_host_pitch(long long &sy, long long &sz);
 
 struct DirTable;  // fold3d_fast.cuh
 
-struct DirBins;   // fold3d_fast.cuh
-
 // Per-direction solver constants, evaluated on the host (fold3d_tables.cpp).
 // The direction table of a frame.  search: prove the tight skip bounds (a
 // host search, memoised per thread); false: closed-form bounds only, with
-// no memory allocated (fold3d_solve_noalloc).  With `bins`, also the
-// gradient bins (search only); the table then holds their ranges, and
-// attach_dir_bins points its call sites at a copy of them (host or device
-// memory) -- until then the table's bin pointers are null, which turns the
-// bins off.
-void build_dir_table(const LocalFrameH &L, DirTable &out, bool search = true, DirBins *bins = nullptr);
-void attach_dir_bins(DirTable &t, const DirBins *b);
+// no memory allocated (fold3d_solve_noalloc).
+void build_dir_table(const LocalFrameH &L, DirTable &out, bool search = true);
 
 // Solver variants of the plane kernel.
 enum Variant {
@@ -113,13 +106,6 @@ constexpr unsigned kPollNs = FOLD3D_POLL_NS;
 #define FOLD3D_WAVE_WARP_ITEMS 1
 #endif
 constexpr bool kWaveWarpItems = FOLD3D_WAVE_WARP_ITEMS != 0;
-
-// Drift-medium WAVEFRONT solves: gate the solver bodies with the gradient
-// bins' bounds too (fold3d_fast.cuh, 5.); build option.
-#ifndef FOLD3D_GRAD_BINS
-#define FOLD3D_GRAD_BINS 0
-#endif
-constexpr bool kGradBins = FOLD3D_GRAD_BINS != 0;
 
 // Items a batched pass's CTA claims at a time (1..32); build option.
 #ifndef FOLD3D_BATCH_CHUNK

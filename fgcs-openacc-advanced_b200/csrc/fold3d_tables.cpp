@@ -134,10 +134,16 @@ double edge_point(const EdgeK &k, double F, double d)
     return (0.0 < xe && xe < k.hx) ? D : HUGE_VAL;
 }
 
-// The lower end of the increments the body can accept for d in [lo, hi]
-// (HUGE_VAL when it can accept none there), after at most `iters` splits.
-double edge_bb_range(const EdgeK &k, double F, double lo, double hi, int iters)
+// The proved lower bound (0 when the search does not apply).
+double edge_bb_search(const EdgeK &k, double F)
 {
+    if (!(k.g > 0.0 && k.ga > 0.0 && k.hx > 0.0 && k.hz > 0.0 && F > 0.0)) return 0.0;
+    const double sga = std::sqrt(k.ga);
+    if (!(std::fabs(k.ax) < 0.99 * sga)) return 0.0;
+    // Q > 0 between the roots 1/(ax - sqrt ga) < 0 < 1/(ax + sqrt ga), widened
+    double lo = 1.0 / (k.ax - sga) * (1.0 + 1e-9), hi = 1.0 / (k.ax + sga) * (1.0 + 1e-9);
+    if (k.early) hi = 0.0;  // ax > 0: the body returns when s1 > s0, i.e. d > 0 (:71)
+    if (!(lo < hi) || !std::isfinite(lo) || !std::isfinite(hi)) return 0.0;
     using Item = std::pair<double, Iv>;
     auto cmp = [](const Item &a, const Item &b) { return a.first > b.first; };
     std::priority_queue<Item, std::vector<Item>, decltype(cmp)> heap(cmp);
@@ -146,7 +152,7 @@ double edge_bb_range(const EdgeK &k, double F, double lo, double hi, int iters)
     const double min_width = (hi - lo) * 1e-12;
     double frozen = HUGE_VAL;  // sub-intervals too narrow to split
     double seen = HUGE_VAL;    // smallest increment accepted at a sampled point
-    for (int it = 0; it < iters && !heap.empty(); ++it) {
+    for (int it = 0; it < 2000 && !heap.empty(); ++it) {
         const Item top = heap.top();
         if (top.first >= 0.99 * seen) break;  // within 1%: the bound is tight enough
         heap.pop();
@@ -163,29 +169,6 @@ double edge_bb_range(const EdgeK &k, double F, double lo, double hi, int iters)
     }
     double b = frozen;
     if (!heap.empty()) b = std::min(b, heap.top().first);
-    return b;
-}
-
-// The range of d where the body can accept (Q > 0 between the roots
-// 1/(ax - sqrt ga) < 0 < 1/(ax + sqrt ga), widened; d <= 0 for an early
-// call site); false when the search does not apply.
-bool edge_d_range(const EdgeK &k, double F, double &lo, double &hi)
-{
-    if (!(k.g > 0.0 && k.ga > 0.0 && k.hx > 0.0 && k.hz > 0.0 && F > 0.0)) return false;
-    const double sga = std::sqrt(k.ga);
-    if (!(std::fabs(k.ax) < 0.99 * sga)) return false;
-    lo = 1.0 / (k.ax - sga) * (1.0 + 1e-9);
-    hi = 1.0 / (k.ax + sga) * (1.0 + 1e-9);
-    if (k.early) hi = 0.0;  // ax > 0: the body returns when s1 > s0, i.e. d > 0 (:71)
-    return lo < hi && std::isfinite(lo) && std::isfinite(hi);
-}
-
-// The proved lower bound (0 when the search does not apply).
-double edge_bb_search(const EdgeK &k, double F)
-{
-    double lo, hi;
-    if (!edge_d_range(k, F, lo, hi)) return 0.0;
-    const double b = edge_bb_range(k, F, lo, hi, 2000);
     if (b == HUGE_VAL) return 0.0;  // nothing can be accepted; 0 keeps the plain gates
     return std::max(b, 0.0);
 }
@@ -245,13 +228,14 @@ double surf_point(double F, double az, double hz, double g, double ax, double ay
     return (0.0 <= std::min(xe, ye) && ye * hx <= xe * hy && xe <= hx) ? D : HUGE_VAL;
 }
 
-// The lower end of the increments the body can accept for (dx, dy) in the
-// box `root` (HUGE_VAL when it can accept none there), after at most
-// `iters` splits; R scales the narrowest box split.
-double surf_bb_box(double F, double az, double hz, double ax, double ay, double hx, double hy, const Box &root,
-                   double R, int iters)
+double surf_bb_search(double F, double az, double hz, double ax, double ay, double hx, double hy)
 {
     const double g = F * F - az * az;
+    if (!(g > 0.0 && hx > 0.0 && hy > 0.0 && hz > 0.0 && F > 0.0)) return 0.0;
+    const double ain = std::sqrt(ax * ax + ay * ay), sg = std::sqrt(g);
+    if (!(ain < 0.99 * sg)) return 0.0;
+    const double R = 1.0 / (sg - ain) * (1.0 + 1e-9);
+    Box root{{-R, ax > 0.0 ? 0.0 : R}, {-R, ay > 0.0 ? 0.0 : R}};
     using Item = std::pair<double, Box>;
     auto cmp = [](const Item &a, const Item &b) { return a.first > b.first; };
     std::priority_queue<Item, std::vector<Item>, decltype(cmp)> heap(cmp);
@@ -260,7 +244,7 @@ double surf_bb_box(double F, double az, double hz, double ax, double ay, double 
     const double min_width = R * 1e-12;
     double frozen = HUGE_VAL;
     double seen = HUGE_VAL;
-    for (int it = 0; it < iters && !heap.empty(); ++it) {
+    for (int it = 0; it < 6000 && !heap.empty(); ++it) {
         const Item top = heap.top();
         if (top.first >= 0.99 * seen) break;
         heap.pop();
@@ -286,27 +270,6 @@ double surf_bb_box(double F, double az, double hz, double ax, double ay, double 
     }
     double bound = frozen;
     if (!heap.empty()) bound = std::min(bound, heap.top().first);
-    return bound;
-}
-
-// The half-width R of the square of gradients where the body can accept (the
-// disc where q > 0, widened); false when the search does not apply.
-bool surf_grad_radius(double F, double az, double hz, double ax, double ay, double hx, double hy, double &R)
-{
-    const double g = F * F - az * az;
-    if (!(g > 0.0 && hx > 0.0 && hy > 0.0 && hz > 0.0 && F > 0.0)) return false;
-    const double ain = std::sqrt(ax * ax + ay * ay), sg = std::sqrt(g);
-    if (!(ain < 0.99 * sg)) return false;
-    R = 1.0 / (sg - ain) * (1.0 + 1e-9);
-    return std::isfinite(R);
-}
-
-double surf_bb_search(double F, double az, double hz, double ax, double ay, double hx, double hy)
-{
-    double R;
-    if (!surf_grad_radius(F, az, hz, ax, ay, hx, hy, R)) return 0.0;
-    const Box root{{-R, ax > 0.0 ? 0.0 : R}, {-R, ay > 0.0 ? 0.0 : R}};
-    const double bound = surf_bb_box(F, az, hz, ax, ay, hx, hy, root, R, 6000);
     if (bound == HUGE_VAL) return 0.0;
     return std::max(bound, 0.0);
 }
@@ -328,83 +291,6 @@ double surf_bb_bound(double F, double az, double hz, double ax, double ay, doubl
         return surf_bb_search(F, az, hz, ax, ay, hx, hy);
     } catch (...) {
         return 0.0;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Gradient bins (fold3d_fast.cuh, 5.): per call site, the increment's lower
-// bound over each bin of the gradient range, each bin widened by a
-// millionth of its width on both sides, by the searches above with a
-// smaller budget; never below the site's own bound B.  A bin where the body
-// can accept nothing gets +inf.
-// ---------------------------------------------------------------------------
-constexpr double kBinWiden = 1e-6;
-constexpr int kBinIters = 96;
-
-// b as a float no larger than b.
-float float_down(double b)
-{
-    if (!(b > 0.0)) return 0.0f;
-    float f = (float)b;
-    if ((double)f > b) f = std::nextafter(f, -HUGE_VALF);
-    return f;
-}
-
-// The bin bound from a search result r (HUGE_VAL: nothing accepted).
-float bin_value(double r, double B)
-{
-    const double b = (r == HUGE_VAL) ? HUGE_VAL : std::max(r * (1.0 - 1e-3), 0.0);
-    return float_down(std::max(b, B));
-}
-
-// Bins of a FoldEdge2Points call site (drift arguments in k); leaves
-// k.binv = 0 (no bins) when the search does not apply.
-void edge_site_bins(EdgeK &k, double F, float *out)
-{
-    k.blo = 0.0;
-    k.binv = 0.0;
-    if (!(F * F >= 1.1 * (k.ax * k.ax + k.ay * k.ay + k.az * k.az))) return;
-    double lo, hi;
-    if (!edge_d_range(k, F, lo, hi)) return;
-    const double w = (hi - lo) / kEdgeBins;
-    for (int i = 0; i < kEdgeBins; ++i) {
-        const double a = lo + (i - kBinWiden) * w, b = lo + (i + 1 + kBinWiden) * w;
-        out[i] = bin_value(edge_bb_range(k, F, a, b, kBinIters), k.B);
-    }
-    k.blo = lo;
-    k.binv = kEdgeBins / (hi - lo);
-}
-
-// Bins of a FoldSurf3Points call site (the side's F, az, dzz); the same.
-void surf_site_bins(SurfK &k, double F, double az, double hz, float *out)
-{
-    k.blo = 0.0;
-    k.binv = 0.0;
-    if (!(F * F >= 1.1 * (k.ax * k.ax + k.ay * k.ay + az * az))) return;
-    double R;
-    if (!surf_grad_radius(F, az, hz, k.ax, k.ay, k.hx, k.hy, R)) return;
-    const double w = 2.0 * R / kSurfBins;
-    for (int i = 0; i < kSurfBins; ++i)
-        for (int j = 0; j < kSurfBins; ++j) {
-            Box b{{-R + (i - kBinWiden) * w, -R + (i + 1 + kBinWiden) * w},
-                  {-R + (j - kBinWiden) * w, -R + (j + 1 + kBinWiden) * w}};
-            // the early returns (:132) keep dx <= 0 when ax > 0, dy <= 0 when ay > 0
-            if (k.e1) b.x.hi = std::min(b.x.hi, 0.0);
-            if (k.e2) b.y.hi = std::min(b.y.hi, 0.0);
-            const bool empty = !(b.x.lo <= b.x.hi && b.y.lo <= b.y.hi);
-            out[i * kSurfBins + j] =
-                empty ? HUGE_VALF : bin_value(surf_bb_box(F, az, hz, k.ax, k.ay, k.hx, k.hy, b, R, kBinIters), k.B);
-        }
-    k.blo = -R;
-    k.binv = kSurfBins / (2.0 * R);
-}
-
-void side_bins(SideTable &t, SideBins &b)
-{
-    for (int k = 0; k < 8; ++k) {
-        surf_site_bins(t.surf[k], t.F, t.az, t.hz, b.surf[k]);
-        edge_site_bins(t.surf[k].nest, t.F, b.nest[k]);
-        edge_site_bins(t.edge[k], t.F, b.edge[k]);
     }
 }
 
@@ -531,7 +417,7 @@ void side_table(const LocalFrameH &L, bool negative, bool search, SideTable &t)
 
 }  // namespace
 
-void build_dir_table(const LocalFrameH &L, DirTable &out, bool search, DirBins *bins)
+void build_dir_table(const LocalFrameH &L, DirTable &out, bool search)
 {
     if (!search) {  // closed-form bounds only: nothing allocated
         side_table(L, false, false, out.side[0]);
@@ -539,64 +425,30 @@ void build_dir_table(const LocalFrameH &L, DirTable &out, bool search, DirBins *
         return;
     }
     // The skip bounds take a search per call site; a solve asks for the same
-    // six frames every sweep, so each thread keeps its last twelve tables
-    // (and their gradient bins, once asked for).
+    // six frames every sweep, so each thread keeps its last twelve tables.
     struct Entry {
         LocalFrameH key;
         DirTable tab;
-        DirBins bins;
-        bool used, has_bins;
+        bool used;
     };
     constexpr int kEntries = 12;
     thread_local std::unique_ptr<Entry[]> memo;
     thread_local int next = 0;
     if (!memo) memo.reset(new (std::nothrow) Entry[kEntries]());  // stays empty if that fails
-    Entry *hit = nullptr;
     if (memo)
         for (int i = 0; i < kEntries; ++i)
             if (memo[i].used && std::memcmp(&memo[i].key, &L, sizeof L) == 0) {
-                hit = &memo[i];
-                break;
+                out = memo[i].tab;
+                return;
             }
-    if (!hit) {
-        side_table(L, false, true, out.side[0]);
-        side_table(L, true, true, out.side[1]);
-        if (memo) {
-            hit = &memo[next];
-            next = (next + 1) % kEntries;
-            hit->key = L;
-            hit->tab = out;
-            hit->used = true;
-            hit->has_bins = false;
-        }
-    }
-    if (bins) {
-        if (hit && hit->has_bins) {
-            *bins = hit->bins;
-        } else {
-            DirTable &t = hit ? hit->tab : out;
-            side_bins(t.side[0], bins->side[0]);
-            side_bins(t.side[1], bins->side[1]);
-            if (hit) {
-                hit->bins = *bins;
-                hit->has_bins = true;
-            }
-        }
-    }
-    if (hit) out = hit->tab;
-}
-
-void attach_dir_bins(DirTable &t, const DirBins *b)
-{
-    for (int sd = 0; sd < 2; ++sd) {
-        SideTable &s = t.side[sd];
-        const SideBins &sb = b->side[sd];  // address arithmetic only: b may be a device address
-        for (int k = 0; k < 8; ++k) {
-            s.surf[k].bins = s.surf[k].binv > 0.0 ? sb.surf[k] : nullptr;
-            s.surf[k].nest.bins = s.surf[k].nest.binv > 0.0 ? sb.nest[k] : nullptr;
-            s.edge[k].bins = s.edge[k].binv > 0.0 ? sb.edge[k] : nullptr;
-        }
-    }
+    side_table(L, false, true, out.side[0]);
+    side_table(L, true, true, out.side[1]);
+    if (!memo) return;
+    Entry &e = memo[next];
+    next = (next + 1) % kEntries;
+    e.key = L;
+    e.tab = out;
+    e.used = true;
 }
 
 }  // namespace fold3d

@@ -5,7 +5,6 @@
 // with no contraction on either side, so the host build computes the bits the
 // kernels compute; tests/test_solver_host.py runs it against the oracle.
 // Test code only: the library has no host solver.
-#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -59,21 +58,16 @@ void clear_bounds(SideTable &t)
 
 // Runs `sweeps` sweeps on T ((nz+2)(ny+2)(nx+2) doubles, x fastest).  skip:
 // 1 the tables as solves build them (searched bounds), 2 the closed-form
-// bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all; plus
-// 4: with the gradient bins of the searched bounds (as WAVEFRONT solves).
+// bounds only (the tables of fold3d_solve_noalloc), 0 no bounds at all.
 extern "C" int fast_host_sweeps(double *T, int nx, int ny, int nz, double dx, double dy, double dz, double F,
                                 double a0, double a1, double a2, int sweeps, int skip)
 {
     const int n[3] = {nx, ny, nz};
     const int64_t stride[3] = {1, (int64_t)nx + 2, ((int64_t)nx + 2) * (ny + 2)};
     const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
-    const bool bins = (skip & 4) != 0;
-    skip &= 3;
     DirTable tabs[6];
-    static DirBins dbins[6];
     for (int dir = 0; dir < 6; ++dir) {
-        build_dir_table(host_frame(dir, h, F, a), tabs[dir], skip != 2, bins ? &dbins[dir] : nullptr);
-        if (bins) attach_dir_bins(tabs[dir], &dbins[dir]);
+        build_dir_table(host_frame(dir, h, F, a), tabs[dir], skip != 2);
         if (!skip) {
             clear_bounds(tabs[dir].side[0]);
             clear_bounds(tabs[dir].side[1]);
@@ -121,72 +115,4 @@ extern "C" void fast_host_bounds(double dx, double dy, double dz, double F, doub
             }
         }
     }
-}
-
-// The gradient bins' bounds against the increments the bodies accept at
-// sampled gradients inside each bin (fold3d_fast.cuh, 5.): returns how many
-// samples were accepted below their bin's bound (0 when every bound holds),
-// and the number of accepted samples in *checked.
-extern "C" long long fast_host_check_bins(double dx, double dy, double dz, double F, double a0, double a1, double a2,
-                                          long long *checked)
-{
-    const double h[3] = {dx, dy, dz}, a[3] = {a0, a1, a2};
-    long long bad = 0, n = 0;
-    auto edge_incr = [](const EdgeK &k, double Fs, double d) {
-        const double c0 = 1.0 - d * k.ax, Q = k.g * (c0 * c0 - d * d * k.ga);
-        if (!(Q > 0.0)) return HUGE_VAL;
-        const double c = (-k.az * c0 + std::sqrt(Q)) / k.ga, D = k.hz * c - std::min(0.0, d * k.hx);
-        if (!(D > 0.0)) return HUGE_VAL;
-        const double G = std::sqrt((d * d + c * c) * Fs * Fs / k.g), xe = -k.hz * (d + k.ax * G) / (c + k.az * G);
-        return (0.0 < xe && xe < k.hx) ? D : HUGE_VAL;
-    };
-    auto check_edge = [&](const EdgeK &k, double Fs) {
-        if (!k.bins) return;
-        const double lo = k.blo, w = 1.0 / k.binv;
-        for (int i = 0; i < kEdgeBins; ++i)
-            for (int j = 0; j <= 64; ++j) {
-                const double d = lo + (i + j / 64.0) * w;
-                if (k.early && d > 0.0) continue;
-                const double D = edge_incr(k, Fs, d);
-                if (D == HUGE_VAL) continue;
-                ++n;
-                if (D < (double)k.bins[i]) ++bad;
-            }
-    };
-    for (int dir = 0; dir < 6; ++dir) {
-        DirTable t;
-        static DirBins b;
-        build_dir_table(host_frame(dir, h, F, a), t, true, &b);
-        attach_dir_bins(t, &b);
-        for (int sd = 0; sd < 2; ++sd) {
-            const SideTable &s = t.side[sd];
-            for (int k = 0; k < 8; ++k) {
-                check_edge(s.edge[k], s.F);
-                check_edge(s.surf[k].nest, s.F);
-                const SurfK &K = s.surf[k];
-                if (!K.bins) continue;
-                const double lo = K.blo, w = 1.0 / K.binv;
-                for (int i = 0; i < kSurfBins; ++i)
-                    for (int j = 0; j < kSurfBins; ++j)
-                        for (int p = 0; p <= 8; ++p)
-                            for (int q = 0; q <= 8; ++q) {
-                                const double gx = lo + (i + p / 8.0) * w, gy = lo + (j + q / 8.0) * w;
-                                if ((K.e1 && gx > 0.0) || (K.e2 && gy > 0.0)) continue;
-                                const double dd = gx * gx + gy * gy, al = 1.0 - K.ax * gx - K.ay * gy;
-                                const double qq = al * al - dd * s.g;
-                                if (!(qq > 0.0)) continue;
-                                const double al2 = (-s.az * al + s.F * std::sqrt(qq)) / s.g;
-                                const double D = s.hz * al2 - std::min(0.0, std::min(gx * K.hx, gx * K.hx + gy * K.hy));
-                                if (!(D > 0.0)) continue;
-                                const double r = std::sqrt(dd + al2 * al2), m = -s.hz / (s.F * al2 + s.az * r);
-                                const double xe = m * (s.F * gx + K.ax * r), ye = m * (s.F * gy + K.ay * r);
-                                if (!(0.0 <= std::min(xe, ye) && ye * K.hx <= xe * K.hy && xe <= K.hx)) continue;
-                                ++n;
-                                if (D < (double)K.bins[i * kSurfBins + j]) ++bad;
-                            }
-            }
-        }
-    }
-    *checked = n;
-    return bad;
 }

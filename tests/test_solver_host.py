@@ -39,8 +39,6 @@ def host(tmp_path_factory):
     L.fast_host_sweeps.restype = _int
     L.fast_host_bounds.argtypes = [_dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _ptr]
     L.fast_host_bounds.restype = None
-    L.fast_host_check_bins.argtypes = [_dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, _ptr]
-    L.fast_host_check_bins.restype = C.c_longlong
     return L
 
 
@@ -76,9 +74,7 @@ def test_host_build_of_the_point_update_matches_oracle(orc, host, case):
         T0 = orc.init_point(nx, ny, nz, (nx // 3 + 1, ny // 2 + 1, nz - 2))
     ref = T0.copy()
     orc.solve(ref, h, 8, F=F, a=a)
-    # searched bounds, closed-form bounds (the no-alloc solve's), none, and
-    # the searched bounds with the gradient bins
-    for skip in (1, 2, 0, 5):
+    for skip in (1, 2, 0):  # searched bounds, closed-form bounds (the no-alloc solve's), none
         T = T0.copy()
         _host_sweeps(host, T, h, F, a, 8, skip)
         assert_bitwise(T, ref, "host build of the point update, skip mode %d" % skip)
@@ -96,16 +92,15 @@ def test_host_build_matches_reference_off_centre_sources(orc, host, digests, n, 
     assert hashlib.sha256(np.ascontiguousarray(P).tobytes()).hexdigest() == digests["n%d_%s_s8" % (n, name)]
 
 
-@pytest.mark.parametrize("skip", [1, 5])
-def test_host_build_matches_reference_digest_99(host, digests, skip):
+def test_host_build_matches_reference_digest_99(host, digests):
     """The reference's own 8-sweep result at 99^3 (partial tiles on every
-    axis), through the host build (skip 5: with the gradient bins)."""
+    axis), through the host build."""
     from oracle import Oracle
 
     n = 99
     h = (ref_spacing(n),) * 3
     T = Oracle().init_implicit(n, n, n, h)
-    _host_sweeps(host, T, h, REF_F, REF_A, 8, skip)
+    _host_sweeps(host, T, h, REF_F, REF_A, 8)
     assert hashlib.sha256(np.ascontiguousarray(T).tobytes()).hexdigest() == digests["n99_s8"]
 
 
@@ -353,18 +348,3 @@ def test_tables_are_the_same_from_concurrent_threads(host):
     for t in range(4):
         for q in range(len(media_)):
             assert np.array_equal(got[t][q], want[q])
-
-
-@pytest.mark.parametrize("case", CASES, ids=lambda c: "x".join(map(str, c[0])) + c[4])
-def test_gradient_bin_bounds_hold_at_sampled_gradients(host, case):
-    """fold3d_fast.cuh 5.: every gradient bin's bound lies at or below the
-    increment its body accepts at 65 gradients per edge bin and 81 per
-    triangle bin, in every direction and side of the medium."""
-    dims, h, F, a, _ = case
-    if h is None:
-        h = (ref_spacing(dims[0]),) * 3
-    n = C.c_longlong(0)
-    bad = host.fast_host_check_bins(*h, F, *a, C.byref(n))
-    assert bad == 0, (bad, n.value)
-    if F * F >= 1.1 * sum(x * x for x in a):
-        assert n.value > 1000  # the bins exist and the samples reach them
