@@ -120,11 +120,11 @@ static_assert(kBatchChunk >= 1 && kBatchChunk <= 32, "batch chunk");
 constexpr int kWaveTV = FOLD3D_WAVE_TV;
 
 // Resident CTAs per SM the forward dataflow kernels are compiled for (their
-// register budget is 65536 / (32 * kWaveTV * this)); build options.  Passes
-// over planes of fewer than kLargePlaneTiles tiles run best with fewer,
-// register-rich CTAs (no spills); passes over larger planes and batched
-// solves (many small instances) with more of them.  Measured with 32 x 4
-// tiles at 512^3 and 1280^3.
+// register budget is 65536 / (32 * kWaveTV * this)); build options, each the
+// count that measured fastest with 32 x 4 tiles: drift 7 (512^3) and 7 on
+// planes of kLargePlaneTiles tiles or more (1280^3, warp-owned items; 8:
+// 2% slower, 6: 4% slower); the FP64 elliptical medium 6, and 7 on large
+// planes; the float32 one 8; batched solves (many small instances) 8.
 #ifndef FOLD3D_WAVE_MINB_DRIFT
 #define FOLD3D_WAVE_MINB_DRIFT 7
 #endif
