@@ -372,3 +372,32 @@ def test_host_build_matches_oracle_in_random_media(orc, host):
         T = T0.copy()
         _host_sweeps(host, T, h, F, a, 8)
         assert_bitwise(T, ref, "random medium %d (F=%g, a=%s, h=%s)" % (it, F, a, h))
+
+
+@pytest.mark.parametrize("f32", [False, True], ids=["f64", "f32"])
+def test_host_build_of_the_elliptical_update_in_random_media(orc, ellip_host, f32):
+    """16 seeded random tilted ellipses (Vz 1000-4000, eps 0-0.4, any axis;
+    6-20 points per axis, spacings 3-15, a random point source): fields and
+    winner records after 6 sweeps equal the oracle's bit for bit."""
+    import media
+
+    rng = np.random.default_rng(1204 + int(f32))
+    dt = np.float32 if f32 else np.float64
+    for it in range(16):
+        nx, ny, nz = (int(x) for x in rng.integers(6, 21, size=3))
+        h = tuple(float(x) for x in rng.uniform(3.0, 15.0, size=3))
+        M = media.homogeneous_ellip(nx, ny, nz, float(rng.uniform(1000.0, 4000.0)), float(rng.uniform(0.0, 0.4)),
+                                    float(rng.uniform(0.0, 90.0)), float(rng.uniform(0.0, 360.0)))
+        M = [np.ascontiguousarray(m.numpy(), dtype=np.float32) for m in M]
+        src = tuple(int(rng.integers(1, m + 1)) for m in (nx, ny, nz))
+        T0 = np.full((nz + 2, ny + 2, nx + 2), 1e16, dtype=dt)
+        T0[src[2], src[1], src[0]] = 0.0
+        ref = T0.copy()
+        _, _, Wref = (orc.ellf_solve_rec if f32 else orc.ell_solve_rec)(ref, M, h, 6, tol=-1.0)
+        T = T0.copy()
+        W = np.full(T.shape, 0xFF, dtype=np.uint8)
+        ptrs = (C.c_void_p * 6)(*(m.ctypes.data for m in M))
+        ellip_host.ellip_host_sweeps(T.ctypes.data, W.ctypes.data, ptrs, nx, ny, nz, *h, 6, int(f32))
+        bits = np.uint32 if f32 else np.uint64
+        assert np.array_equal(T.view(bits), ref.view(bits)), (it, nx, ny, nz, h, src)
+        assert np.array_equal(W, Wref), it
